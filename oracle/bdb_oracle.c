@@ -1,0 +1,894 @@
+/* CPU restatement of BD_BOX's per-step hot path -- TEST ORACLE ONLY.
+ * See bdb_oracle.h for the contract; every function cites the reference
+ * code it restates. Compile without FMA contraction (plain x86-64 gcc -O2
+ * has no FMA) so the operation order below gives the reference's doubles. */
+#include "bdb_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* constants of data.h:207-211 (double build) and the float literal pi */
+#define KB 0.001986248532617
+#define KB_1_8PI 0.00007903031804378703
+#define KB_1_6PI 0.00010537375739171604
+#define SQRTPI 1.77245385090551602729
+#define M1_SQRTPI 0.5641895835
+#define M_PIF 3.14159265358979323846f
+
+void orc_prefactors(const orc_system* s, double* preDii, double* preDij)
+{
+    *preDii = KB_1_6PI * s->T / (s->visc * s->vfactor);
+    *preDij = KB_1_8PI * s->T / (s->visc * s->vfactor);
+}
+
+/* trans_dist_vec (trans.c:111-121): v = v2 - v1, minimum image when periodic */
+static void dist_vec(const orc_system* s, const double* v1, const double* v2, double* v)
+{
+    int k;
+    for (k = 0; k < 3; ++k) v[k] = v2[k] - v1[k];
+    if (s->bc != 1) return;
+    for (k = 0; k < 3; ++k) v[k] -= s->box[k] * floor(v[k] * s->inv_L[k] + 0.5f);
+}
+
+/* diff_tensor_calc_pos(a, b) (diff_tensor.c:45-92) */
+static void tile_free(const orc_system* s, double preDii, double preDij, int a, int b, double* tD)
+{
+    const double* c = s->coord;
+    double sigma_i = c[4 * b + 3], sigma_j = c[4 * a + 3];
+    double e[3], r_sq, r_norm, inv;
+    int i, j;
+    e[0] = c[4 * a] - c[4 * b];
+    e[1] = c[4 * a + 1] - c[4 * b + 1];
+    e[2] = c[4 * a + 2] - c[4 * b + 2];
+    r_sq = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+    r_norm = sqrt(r_sq);
+    inv = 1 / r_norm;
+    e[0] *= inv;
+    e[1] *= inv;
+    e[2] *= inv;
+    if (r_norm < sigma_i + sigma_j) {
+        double sigma = (sigma_i + sigma_j) / 2;
+        double pre = preDii / sigma;
+        double part1 = (1 - (9 * r_norm / (32 * sigma)));
+        tD[0] = tD[4] = tD[8] = part1;
+        for (i = 0; i < 3; ++i) {
+            tD[i + 3 * i] += 3 * e[i] * e[i] * r_norm / (32 * sigma);
+            tD[i + 3 * i] *= pre;
+            for (j = 0; j < i; ++j) {
+                tD[j + 3 * i] = pre * 3 * e[i] * e[j] * r_norm / (32 * sigma);
+                tD[i + 3 * j] = tD[j + 3 * i];
+            }
+        }
+    } else {
+        double pre = preDij / r_norm;
+        double sigm_r = (sigma_i * sigma_i + sigma_j * sigma_j) / r_sq;
+        tD[0] = tD[4] = tD[8] = 1 + sigm_r / 3;
+        for (i = 0; i < 3; ++i) {
+            tD[i + 3 * i] += e[i] * e[i] * (1 - sigm_r);
+            tD[i + 3 * i] *= pre;
+            for (j = 0; j < i; ++j) {
+                tD[j + 3 * i] = pre * e[i] * e[j] * (1 - sigm_r);
+                tD[i + 3 * j] = tD[j + 3 * i];
+            }
+        }
+    }
+}
+
+/* get_ev2_norms (math_help.c:85-101) */
+static void ev2(double x, double y, double z, double* e, double* r_norm, double* r_sq)
+{
+    double inv;
+    e[0] = x;
+    e[1] = y;
+    e[2] = z;
+    *r_sq = x * x + y * y + z * z;
+    *r_norm = sqrt(*r_sq);
+    inv = 1 / *r_norm;
+    e[0] *= inv;
+    e[1] *= inv;
+    e[2] *= inv;
+}
+
+/* diff_tensor_calc_ewald_beenakker(i, j) (diff_tensor.c:265-401) with the
+ * constants of init_tensor (diff_tensor.c:546-559) */
+static void tile_beenakker(const orc_system* s, double preDii, double preDij, int i, int j, double* _tD)
+{
+    const double* coord = s->coord;
+    double sigma_i = coord[4 * j + 3], sigma_j = coord[4 * i + 3];
+    double v[3], r[3];
+    const double sigma_sq = 0.5 * (sigma_i * sigma_i + sigma_j * sigma_j);
+    int k, l, f, g, h;
+    double Op[9] = {0}, Qp[9] = {0};
+    const double preQ = s->inv_L[0] * s->inv_L[0] * s->inv_L[0];
+    const double ewald_alpha = SQRTPI * s->inv_L[0];
+    const double alpha2 = ewald_alpha * ewald_alpha;
+    const double alpha3 = ewald_alpha * alpha2;
+    const double inv_alpha2 = 1.0f / alpha2;
+    const int ewald_rr = s->ewald_real;
+    const int rr_sq = s->ewald_real * s->ewald_real;
+    const double L = s->box[0];
+    r[0] = coord[4 * j] - coord[4 * i];
+    r[1] = coord[4 * j + 1] - coord[4 * i + 1];
+    r[2] = coord[4 * j + 2] - coord[4 * i + 2];
+
+    if ((r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) < (sigma_i + sigma_j) * (sigma_i + sigma_j) && i != j) {
+        double r_norm, r_sq, e[3];
+        int a, b;
+        ev2(r[0], r[1], r[2], e, &r_norm, &r_sq);
+        {
+            double sigma = (sigma_i + sigma_j) / 2;
+            double pre = preDii / sigma;
+            double part1 = (1 - (9 * r_norm / (32 * sigma)));
+            for (a = 0; a < 3; ++a) {
+                _tD[a + 3 * a] += pre * (part1 + 3 * e[a] * e[a] * r_norm / (32 * sigma));
+                for (b = 0; b < a; ++b) {
+                    double vval = pre * 3 * e[a] * e[b] * r_norm / (32 * sigma);
+                    _tD[b + 3 * a] += vval;
+                    _tD[a + 3 * b] += vval;
+                }
+            }
+        }
+        {
+            double pre = preDij / r_norm;
+            double sigm_r = (sigma_i * sigma_i + sigma_j * sigma_j) / r_sq;
+            double part1 = 1 + sigm_r / 3;
+            for (a = 0; a < 3; ++a) {
+                _tD[a + 3 * a] -= pre * (part1 + e[a] * e[a] * (1 - sigm_r));
+                for (b = 0; b < a; ++b) {
+                    double vval = pre * e[a] * e[b] * (1 - sigm_r);
+                    _tD[b + 3 * a] -= vval;
+                    _tD[a + 3 * b] -= vval;
+                }
+            }
+        }
+    }
+    v[0] = r[0] * s->inv_L[0];
+    v[1] = r[1] * s->inv_L[1];
+    v[2] = r[2] * s->inv_L[2];
+    for (h = -ewald_rr; h <= ewald_rr; ++h) {
+        int next_f = (int)sqrt(rr_sq - h * h);
+        for (f = -next_f; f <= next_f; ++f) {
+            int next_g = (int)sqrt(rr_sq - h * h - f * f);
+            for (g = -next_g; g <= next_g; ++g) {
+                double r_norm, r_sq, e[3], inv_r, inv_r2, inv_r3, sc, sc2;
+                ev2(r[0] + L * h, r[1] + L * f, r[2] + L * g, e, &r_norm, &r_sq);
+                if (r_norm != 0.0f) {
+                    inv_r = 1 / r_norm;
+                    inv_r2 = 1 / r_sq;
+                    inv_r3 = inv_r * inv_r2;
+                    sc = ewald_alpha * sigma_sq * inv_r2;
+                    sc += 14 * alpha3 * sigma_sq;
+                    sc += -4.5f * ewald_alpha;
+                    sc += -20 * alpha2 * alpha3 * sigma_sq * r_sq;
+                    sc += 3 * alpha3 * r_sq;
+                    sc += 4 * alpha3 * alpha2 * alpha2 * sigma_sq * r_sq * r_sq;
+                    sc *= exp(-alpha2 * r_sq);
+                    sc /= SQRTPI;
+                    sc += erfc(r_norm * ewald_alpha) * (0.75f * inv_r + 0.5f * sigma_sq * inv_r3);
+
+                    sc2 = -3 * ewald_alpha * sigma_sq * inv_r2;
+                    sc2 += -2 * alpha3 * sigma_sq;
+                    sc2 += 1.5f * ewald_alpha;
+                    sc2 += 16 * alpha2 * alpha3 * sigma_sq * r_sq;
+                    sc2 += -3 * alpha3 * r_sq;
+                    sc2 += -4 * alpha3 * alpha2 * alpha2 * sigma_sq * r_sq * r_sq;
+                    sc2 *= exp(-alpha2 * r_sq);
+                    sc2 /= SQRTPI;
+                    sc2 += erfc(r_norm * ewald_alpha) * (0.75f * inv_r - 1.5f * sigma_sq * inv_r3);
+                    for (k = 0; k < 3; ++k) {
+                        double sc_ek = e[k] * sc2;
+                        Op[k * 4] += sc + sc_ek * e[k];
+                        for (l = 0; l < k; ++l) Op[k + l * 3] += e[l] * sc_ek;
+                    }
+                }
+                ev2(h, f, g, e, &r_norm, &r_sq);
+                if (r_norm != 0.0f) {
+                    r_norm *= 2 * M_PIF;
+                    r_sq *= 4 * M_PIF * M_PIF;
+                    sc = 1 - sigma_sq * r_sq / 3;
+                    sc *= 1 + (inv_alpha2 * r_sq / 4) * (1 + inv_alpha2 * r_sq / 2);
+                    sc *= 6 * M_PIF * exp(-inv_alpha2 * r_sq / 4) / r_sq;
+                    sc *= cos(2 * M_PIF * (v[0] * h + v[1] * f + v[2] * g));
+                    for (k = 0; k < 3; ++k) {
+                        double sc_ek = sc * e[k];
+                        Qp[k * 4] += sc - sc_ek * e[k];
+                        for (l = 0; l < k; ++l) Qp[k + l * 3] -= e[l] * sc_ek;
+                    }
+                }
+            }
+        }
+    }
+    for (k = 0; k < 3; ++k) {
+        _tD[k * 4] += preDii * (Op[k * 4] + preQ * Qp[k * 4]);
+        for (l = 0; l < k; ++l) {
+            _tD[k + l * 3] += preDii * (Op[k + l * 3] + preQ * Qp[k + l * 3]);
+            _tD[l + k * 3] += preDii * (Op[k + l * 3] + preQ * Qp[k + l * 3]);
+        }
+    }
+}
+
+void orc_tile(const orc_system* s, int i, int j, double tD[9])
+{
+    double preDii, preDij;
+    int k;
+    orc_prefactors(s, &preDii, &preDij);
+    for (k = 0; k < 9; ++k) tD[k] = 0.0;
+    if (i == j) {
+        if (!s->ewald) {
+            tD[0] = tD[4] = tD[8] = preDii / s->coord[4 * i + 3];
+        } else {
+            /* diff_tensor_calc_ewald_beenakker_diag (diff_tensor.c:404-422) */
+            double aw = s->coord[4 * i + 3];
+            double ewald_alpha = SQRTPI * s->inv_L[0];
+            double alpha3 = ewald_alpha * ewald_alpha * ewald_alpha;
+            double sc3;
+            int l;
+            tile_beenakker(s, preDii, preDij, i, i, tD);
+            sc3 = -6 * ewald_alpha / SQRTPI + 40 * alpha3 * aw * aw / (3 * SQRTPI);
+            sc3 *= preDii;
+            for (k = 0; k < 3; ++k) {
+                tD[k * 4] = preDii / aw + sc3 + tD[k * 4];
+                for (l = 0; l < k; ++l) tD[l + 3 * k] = tD[k + 3 * l] = 0;
+            }
+        }
+    } else if (!s->ewald) {
+        tile_free(s, preDii, preDij, i, j, tD);
+    } else {
+        tile_beenakker(s, preDii, preDij, i, j, tD);
+    }
+}
+
+void orc_D(const orc_system* s, double* D)
+{
+    int n3 = 3 * s->n;
+    int i;
+    memset(D, 0, sizeof(double) * (size_t)n3 * n3);
+#pragma omp parallel for schedule(dynamic)
+    for (i = 0; i < s->n; ++i) {
+        int j, k, l;
+        double tD[9];
+        for (j = 0; j <= i; ++j) {
+            orc_tile(s, i, j, tD);
+            /* insert9 (diff_tensor.c:425-435): tile (i, j) goes to rows 3j+k,
+             * columns 3i+l of the upper triangle; mirror it below */
+            for (k = 0; k < 3; ++k)
+                for (l = 0; l < 3; ++l) {
+                    D[(size_t)(3 * j + k) * n3 + 3 * i + l] = tD[k + 3 * l];
+                    D[(size_t)(3 * i + l) * n3 + 3 * j + k] = tD[k + 3 * l];
+                }
+        }
+    }
+}
+
+int orc_cholesky(int n, double* A, int lda)
+{
+    /* right-looking unblocked Cholesky in the column order of the NR choldc
+     * that myblas.c:63-89 restates (L stored below the diagonal) */
+    int i, j, k;
+    for (j = 0; j < n; ++j) {
+        double d = A[(size_t)j * lda + j];
+        for (k = 0; k < j; ++k) d -= A[(size_t)j * lda + k] * A[(size_t)j * lda + k];
+        if (d <= 0.0) return j + 1;
+        d = sqrt(d);
+        A[(size_t)j * lda + j] = d;
+#pragma omp parallel for if (n - j > 256)
+        for (i = j + 1; i < n; ++i) {
+            double sum = A[(size_t)i * lda + j];
+            int kk;
+            for (kk = 0; kk < j; ++kk) sum -= A[(size_t)i * lda + kk] * A[(size_t)j * lda + kk];
+            A[(size_t)i * lda + j] = sum / d;
+        }
+    }
+    return 0;
+}
+
+void orc_trmv_lower(int n, const double* L, int lda, const double* x, double* y)
+{
+    int i;
+#pragma omp parallel for if (n > 512)
+    for (i = 0; i < n; ++i) {
+        double sum = 0.0;
+        int j;
+        for (j = 0; j <= i; ++j) sum += L[(size_t)i * lda + j] * x[j];
+        y[i] = sum;
+    }
+}
+
+void orc_symv_upper(int n, const double* A, int lda, const double* x, double* y)
+{
+    int i;
+#pragma omp parallel for if (n > 512)
+    for (i = 0; i < n; ++i) {
+        double sum = 0.0;
+        int j;
+        for (j = 0; j < n; ++j)
+            sum += (i <= j ? A[(size_t)i * lda + j] : A[(size_t)j * lda + i]) * x[j];
+        y[i] = sum;
+    }
+}
+
+void orc_df(const orc_system* s, const double* D, const double* F, double dt, double* Rf)
+{
+    int n3 = 3 * s->n, i;
+    double pre = dt / (KB * s->T);
+    double preDii, preDij;
+    orc_prefactors(s, &preDii, &preDij);
+    if (!s->hydro) {
+        /* diff_equation.c:138-146 */
+        for (i = 0; i < n3; ++i) Rf[i] = pre * (preDii / s->coord[4 * (i / 3) + 3]) * F[i];
+        return;
+    }
+    if (D) {
+        orc_symv_upper(n3, D, n3, F, Rf);
+    } else {
+        /* compute_Rf_geyer_in_fly (diff_equation.c:55-117) */
+        memset(Rf, 0, sizeof(double) * n3);
+        for (i = 0; i < s->n; ++i) {
+            int k, j, l;
+            double tD[9];
+            for (k = 0; k < i; ++k) {
+                orc_tile(s, i, k, tD);
+                for (j = 0; j < 3; ++j)
+                    for (l = 0; l < 3; ++l) {
+                        Rf[i * 3 + j] += F[k * 3 + l] * tD[j * 3 + l];
+                        Rf[k * 3 + l] += F[i * 3 + j] * tD[j * 3 + l];
+                    }
+            }
+            orc_tile(s, i, i, tD);
+            Rf[i * 3] += F[i * 3] * tD[0];
+            Rf[i * 3 + 1] += F[i * 3 + 1] * tD[4];
+            Rf[i * 3 + 2] += F[i * 3 + 2] * tD[8];
+        }
+    }
+    for (i = 0; i < n3; ++i) Rf[i] *= pre;
+}
+
+void orc_tea(const orc_system* s, const double* D, const double* gauss, double dt,
+             double* Rs, double* eps_out, double* beta_out)
+{
+    int n3 = 3 * s->n, i;
+    double preDii, preDij, eps = 0.0, a, beta;
+    double* X = (double*)malloc(sizeof(double) * n3);
+    double* C = (double*)calloc(n3, sizeof(double));
+    double* Feff = (double*)calloc(n3, sizeof(double));
+    double* diag = (double*)malloc(sizeof(double) * n3);
+    double* inv_diag = (double*)malloc(sizeof(double) * n3);
+    orc_prefactors(s, &preDii, &preDij);
+    /* diag_D / inv_diag_D (diff_decl.c:94-99): free-space self mobility */
+    for (i = 0; i < n3; ++i) {
+        diag[i] = preDii / s->coord[4 * (i / 3) + 3];
+        inv_diag[i] = 1 / diag[i];
+    }
+    for (i = 0; i < n3; ++i) X[i] = gauss[i] * sqrt(2 * dt * inv_diag[i]);
+    if (!D) {
+        for (i = 0; i < s->n; ++i) {
+            int k, j, l;
+            double tD[9];
+            for (k = 0; k < i; ++k) {
+                orc_tile(s, i, k, tD);
+                for (j = 0; j < 3; ++j)
+                    for (l = 0; l < 3; ++l) {
+                        C[i * 3 + j] += tD[j * 3 + l] * tD[j * 3 + l] * inv_diag[k * 3 + l];
+                        C[k * 3 + l] += tD[j * 3 + l] * tD[j * 3 + l] * inv_diag[i * 3 + j];
+                        Feff[i * 3 + j] += X[k * 3 + l] * tD[j * 3 + l];
+                        Feff[k * 3 + l] += X[i * 3 + j] * tD[j * 3 + l];
+                        eps += tD[j * 3 + l];
+                    }
+            }
+        }
+    } else {
+        for (i = 0; i < n3; ++i) {
+            int k;
+            for (k = 0; k < i; ++k) {
+                double d = D[(size_t)k * n3 + i];
+                C[i] += d * d * inv_diag[k];
+                C[k] += d * d * inv_diag[i];
+                Feff[i] += X[k] * d;
+                Feff[k] += X[i] * d;
+                eps += d;
+            }
+        }
+    }
+    /* diff_rand.c:197-228 */
+    eps /= n3;
+    eps /= (n3 - 1);
+    eps *= 2;
+    if (eps > 1.0) eps = 1.0;
+    a = (3 * s->n - 1) * eps * eps - (3 * s->n - 2) * eps;
+    if ((a < 0.0 ? -a : a) < 0.0000001f)
+        beta = 0.5;
+    else
+        beta = (1 - sqrt(1 - a)) / a;
+    for (i = 0; i < n3; ++i) {
+        double c = C[i] * (beta * beta * inv_diag[i]);
+        c = 1 / (1 + c);
+        c = sqrt(c);
+        Rs[i] = c * (beta * Feff[i] + diag[i] * X[i]);
+    }
+    if (eps_out) *eps_out = eps;
+    if (beta_out) *beta_out = beta;
+    free(X);
+    free(C);
+    free(Feff);
+    free(diag);
+    free(inv_diag);
+}
+
+/* ------------------------------------------------------------------ forces */
+
+static int bad(double v) { return isnan(v) || isinf(v); }
+
+static void v2_norms(const orc_system* s, int p1, int p2, double* e, double* r_norm, double* r_sq)
+{
+    double inv;
+    dist_vec(s, s->coord + 4 * p1, s->coord + 4 * p2, e);
+    *r_sq = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+    *r_norm = sqrt(*r_sq);
+    inv = 1 / *r_norm;
+    e[0] *= inv;
+    e[1] *= inv;
+    e[2] *= inv;
+}
+
+static int bonded_pair(const orc_system* s, int i, int j)
+{
+    /* are_conn (bond.c:87-92) is live only when a 1-2 scale differs from 1
+     * (alloc_connections, bond.c:113-130) */
+    int k;
+    if (!(s->n_bond && ((s->elec && s->bond_c_scale != 1) || (s->alpha_lj != 0.0 && s->bond_lj_scale != 1))))
+        return 0;
+    for (k = 0; k < s->n_bond; ++k) {
+        int a = s->bond_pairs[2 * k], b = s->bond_pairs[2 * k + 1];
+        if ((a == i && b == j) || (a == j && b == i)) return 1;
+    }
+    return 0;
+}
+
+static int lj_force(const orc_system* s, double r_norm, const double* e, double* F1, double* F2,
+                    const double* lj1, const double* lj2, double scale, double* E)
+{
+    /* LJ_force / LJ_force_scale (LJ.c:37-93) */
+    double sigma_ij = lj1[0] + lj2[0];
+    double epsilon_ij = sqrt(lj1[1] * lj2[1]);
+    double s6 = sigma_ij / r_norm;
+    double Fm, en = 0;
+    s6 *= s6;
+    s6 *= s6 * s6;
+    if (scale == 1.0) {
+        en = s->alpha_lj * epsilon_ij * (s6 * (s6 - s->lj_6_term));
+        Fm = s->alpha_lj * epsilon_ij * 6 * (s6 * (2 * s6 - s->lj_6_term)) / r_norm;
+    } else {
+        en = scale * s->alpha_lj * epsilon_ij * (s6 * (s6 - s->lj_6_term));
+        Fm = scale;
+        Fm *= s->alpha_lj * epsilon_ij * 6 * (s6 * (2 * s6 - s->lj_6_term)) / r_norm;
+    }
+    if (E) E[ORC_E_LJ] += en;
+    F1[0] -= e[0] * Fm;
+    F1[1] -= e[1] * Fm;
+    F1[2] -= e[2] * Fm;
+    F2[0] += e[0] * Fm;
+    F2[1] += e[1] * Fm;
+    F2[2] += e[2] * Fm;
+    return (sigma_ij > r_norm) || bad(Fm) || bad(e[0]) || bad(e[1]) || bad(e[2]) || (E ? bad(E[ORC_E_LJ]) : 0);
+}
+
+static int electro_force(const orc_system* s, double r_norm, double r_sq, const double* e, double* F1,
+                         double* F2, double Q1, double Q2, double scale, double* E)
+{
+    /* electro_force / electro_force_scale (electro.c:36-78) */
+    double Fm = (s->gamma_c / s->epsilon_c) * Q1 * Q2 * (1 + s->kappa_c * r_norm);
+    Fm *= exp(-s->kappa_c * r_norm) / r_sq;
+    if (scale != 1.0) Fm *= scale;
+    if (E) {
+        if (scale != 1.0)
+            E[ORC_E_COULOMB] += scale * (s->gamma_c / s->epsilon_c) * Q1 * Q2 * exp(-s->kappa_c * r_norm) / r_norm;
+        else
+            E[ORC_E_COULOMB] += (s->gamma_c / s->epsilon_c) * Q1 * Q2 * exp(-s->kappa_c * r_norm) / r_norm;
+    }
+    F1[0] -= e[0] * Fm;
+    F1[1] -= e[1] * Fm;
+    F1[2] -= e[2] * Fm;
+    F2[0] += e[0] * Fm;
+    F2[1] += e[1] * Fm;
+    F2[2] += e[2] * Fm;
+    return bad(Fm) || bad(e[0]) || bad(e[1]) || bad(e[2]) || (E ? bad(E[ORC_E_COULOMB]) : 0);
+}
+
+static double lj_range(const orc_system* s, int i, int j)
+{
+    return s->cutoff_lj > 0.0 ? s->cutoff_lj : 1.122462f * (s->LJ[2 * i] + s->LJ[2 * j]);
+}
+
+/* force_single (calc_func.c:370-409) */
+static int force_single(const orc_system* s, int i, int j, double* F, double* E, long long* counts)
+{
+    double r_norm, r_sq, e[3];
+    int rep = 0, conn;
+    const double* LJ = s->LJ;
+    v2_norms(s, i, j, e, &r_norm, &r_sq);
+    conn = bonded_pair(s, i, j);
+    if (s->elec && r_norm <= s->cutoff_c) {
+        if (counts) counts[0]++;
+        if (!conn)
+            electro_force(s, r_norm, r_sq, e, F + 3 * i, F + 3 * j, s->Q[i], s->Q[j], 1.0, E);
+        else if (s->bond_c_scale != 0.0)
+            electro_force(s, r_norm, r_sq, e, F + 3 * i, F + 3 * j, s->Q[i], s->Q[j], s->bond_c_scale, E);
+    }
+    if (s->alpha_lj != 0.0 && r_norm <= lj_range(s, i, j)) {
+        if (counts) counts[1]++;
+        if (!conn)
+            rep = lj_force(s, r_norm, e, F + 3 * i, F + 3 * j, LJ + 2 * i, LJ + 2 * j, 1.0, E);
+        else if (s->bond_lj_scale != 0.0)
+            rep = lj_force(s, r_norm, e, F + 3 * i, F + 3 * j, LJ + 2 * i, LJ + 2 * j, s->bond_lj_scale, E);
+        else
+            rep = (LJ[2 * i] + LJ[2 * j]) * (LJ[2 * i] + LJ[2 * j]) > r_sq;
+    } else {
+        rep = (LJ[2 * i] + LJ[2 * j]) * (LJ[2 * i] + LJ[2 * j]) > r_sq;
+    }
+    return s->check_overlap && rep;
+}
+
+static void v3_norms(const orc_system* s, int p1, int p2, int p3, double* e1, double* e2)
+{
+    /* get_v3_norms (math_help.c:103-123) */
+    double nrm1, nrm2;
+    dist_vec(s, s->coord + 4 * p1, s->coord + 4 * p2, e1);
+    dist_vec(s, s->coord + 4 * p3, s->coord + 4 * p2, e2);
+    nrm1 = 1.0f / sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    nrm2 = 1.0f / sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+    e1[0] *= nrm1;
+    e1[1] *= nrm1;
+    e1[2] *= nrm1;
+    e2[0] *= nrm2;
+    e2[1] *= nrm2;
+    e2[2] *= nrm2;
+}
+
+static double cos_vs(const double* a, const double* b)
+{
+    double c = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    if (c <= -1.0) c = -1.0;
+    if (c >= 1.0) c = 1.0;
+    return c;
+}
+
+static int bond_calc(const orc_system* s, int pos, double* F, double* E)
+{
+    /* bond.c:43-85 (an over-stretched bond is fatal there; here it is
+     * reported through the return value 2) */
+    double r_norm, r_sq, e[3];
+    double r_0 = s->bond_parms[3 * pos], r_max = s->bond_parms[3 * pos + 1], H = s->bond_parms[3 * pos + 2];
+    double Ff = 0, dist_rmax;
+    int a = s->bond_pairs[2 * pos], b = s->bond_pairs[2 * pos + 1];
+    double *F1 = F + 3 * a, *F2 = F + 3 * b;
+    v2_norms(s, a, b, e, &r_norm, &r_sq);
+    if (!(r_norm < r_max)) return 2;
+    if (E)
+        E[ORC_E_BOND] += -0.5 * H * (r_max * r_max * log((r_max * r_max - r_sq) / (r_max * r_max - r_0 * r_0)) +
+                                      r_0 * r_max * log((r_max + r_norm) * (r_max - r_0) / ((r_max - r_norm) * (r_max + r_0))));
+    dist_rmax = 1 - r_sq / (r_max * r_max);
+    Ff = H * (r_0 - r_norm) / dist_rmax;
+    F1[0] -= Ff * e[0];
+    F1[1] -= Ff * e[1];
+    F1[2] -= Ff * e[2];
+    F2[0] += Ff * e[0];
+    F2[1] += Ff * e[1];
+    F2[2] += Ff * e[2];
+    return bad(Ff) || bad(e[0]) || bad(e[1]) || bad(e[2]) || (E ? bad(E[ORC_E_BOND]) : 0);
+}
+
+static int angle_calc(const orc_system* s, int pos, double* F, double* E)
+{
+    /* angle.c:38-86 */
+    double phi_0 = s->angle_parms[2 * pos], k_phi = s->angle_parms[2 * pos + 1];
+    int p1 = s->angle_pairs[3 * pos], p2 = s->angle_pairs[3 * pos + 1], p3 = s->angle_pairs[3 * pos + 2];
+    double Fi[3], Fk[3], e1[3], e2[3], cos_phi, phi;
+    int k;
+    v3_norms(s, p1, p2, p3, e1, e2);
+    cos_phi = cos_vs(e1, e2);
+    if (cos_phi >= 1 - 0.000001 || cos_phi <= -1 + 0.000001) return 0;
+    phi = acos(cos_phi);
+    k_phi *= (phi - phi_0);
+    if (E) E[ORC_E_ANGLE] += 0.5f * k_phi * (phi - phi_0);
+    k_phi /= sqrt(1 - cos_phi * cos_phi);
+    for (k = 0; k < 3; ++k) {
+        Fi[k] = -k_phi * (e2[k] - e1[k] * cos_phi);
+        Fk[k] = -k_phi * (e1[k] - e2[k] * cos_phi);
+    }
+    for (k = 0; k < 3; ++k) {
+        F[3 * p1 + k] += Fi[k];
+        F[3 * p2 + k] += -Fi[k] - Fk[k];
+        F[3 * p3 + k] += Fk[k];
+    }
+    return bad(Fk[0]) || bad(Fk[1]) || bad(Fk[2]) || bad(Fi[0]) || bad(Fi[1]) || bad(Fi[2]) ||
+           (E ? bad(E[ORC_E_ANGLE]) : 0);
+}
+
+static int angle_cos_calc(const orc_system* s, int pos, double* F, double* E)
+{
+    /* angle_cos.c:36-81 */
+    double phi_0 = s->angle_cos_parms[2 * pos], k_phi = s->angle_cos_parms[2 * pos + 1];
+    int p1 = s->angle_cos_pairs[3 * pos], p2 = s->angle_cos_pairs[3 * pos + 1], p3 = s->angle_cos_pairs[3 * pos + 2];
+    double Fi[3], Fk[3], e1[3], e2[3], cos_phi;
+    int k;
+    v3_norms(s, p1, p2, p3, e1, e2);
+    cos_phi = cos_vs(e1, e2);
+    k_phi *= (cos_phi - phi_0);
+    if (E) E[ORC_E_ANGLE_COS] += 0.5f * k_phi * (cos_phi - phi_0);
+    for (k = 0; k < 3; ++k) {
+        Fi[k] = k_phi * (e2[k] - e1[k] * cos_phi);
+        Fk[k] = k_phi * (e1[k] - e2[k] * cos_phi);
+    }
+    for (k = 0; k < 3; ++k) {
+        F[3 * p1 + k] += Fi[k];
+        F[3 * p2 + k] += -Fi[k] - Fk[k];
+        F[3 * p3 + k] += Fk[k];
+    }
+    return bad(Fk[0]) || bad(Fk[1]) || bad(Fk[2]) || bad(Fi[0]) || bad(Fi[1]) || bad(Fi[2]) ||
+           (E ? bad(E[ORC_E_ANGLE_COS]) : 0);
+}
+
+static double delta_cos(int m, double c)
+{
+    /* get_delta_cos (dihe.c:146-159) */
+    switch (m) {
+    case 1: return 1;
+    case 2: return 4 * c;
+    case 3: return 12 * c * c - 3;
+    case 4: return c * (32 * c * c - 16);
+    case 5: return c * c * (80 * c * c - 60) + 5;
+    case 6: return c * (192 * c * c * (c * c - 1) + 36);
+    default: return 0;
+    }
+}
+
+static double m_cos(int m, double c)
+{
+    /* get_m_cos (dihe.c:161-174) */
+    switch (m) {
+    case 1: return c;
+    case 2: return 2 * c * c - 1;
+    case 3: return 4 * c * c * c - 3 * c;
+    case 4: return 8 * c * c * (c * c - 1) + 1;
+    case 5: return c * (c * c * (16 * c * c - 20) + 5);
+    case 6: return c * c * (c * c * (32 * c * c - 48) + 18) - 1;
+    default: return 1;
+    }
+}
+
+static int dihe_calc(const orc_system* s, int pos, double* F, double* E)
+{
+    /* dihe.c:42-144 */
+    const int* q = s->dihe_pairs + 4 * pos;
+    const double *ri = s->coord + 4 * q[0], *rj = s->coord + 4 * q[1], *rk = s->coord + 4 * q[2], *rl = s->coord + 4 * q[3];
+    double rim[3], rln[3], rkj[3], rij[3], rkl[3], Fi[3], Fj[3], Fk[3], Fl[3];
+    double inv_nrim, inv_nrln, sijkj, sklkj, nkjsq, cos_theta, dc, tmp;
+    double mkcd = s->dihe_parms[2 * pos];
+    int m = (int)s->dihe_parms[2 * pos + 1], k;
+    dist_vec(s, rk, rj, rkj);
+    nkjsq = rkj[0] * rkj[0] + rkj[1] * rkj[1] + rkj[2] * rkj[2];
+    dist_vec(s, ri, rj, rij);
+    dist_vec(s, rk, rl, rkl);
+    sijkj = (rij[0] * rkj[0] + rij[1] * rkj[1] + rij[2] * rkj[2]) / nkjsq;
+    sklkj = (rkl[0] * rkj[0] + rkl[1] * rkj[1] + rkl[2] * rkj[2]) / nkjsq;
+    for (k = 0; k < 3; ++k) rim[k] = -rij[k] + sijkj * rkj[k];
+    tmp = sqrt(rim[0] * rim[0] + rim[1] * rim[1] + rim[2] * rim[2]);
+    if ((tmp < 0 ? -tmp : tmp) < 0.000001) return 0;
+    inv_nrim = 1.0f / tmp;
+    for (k = 0; k < 3; ++k) rln[k] = rkl[k] - sklkj * rkj[k];
+    tmp = sqrt(rln[0] * rln[0] + rln[1] * rln[1] + rln[2] * rln[2]);
+    if ((tmp < 0 ? -tmp : tmp) < 0.000001) return 0;
+    inv_nrln = 1.0f / tmp;
+    cos_theta = (rim[0] * rln[0] + rim[1] * rln[1] + rim[2] * rln[2]) * inv_nrln * inv_nrim;
+    if (cos_theta < -1) cos_theta = -1;
+    if (cos_theta > 1) cos_theta = 1;
+    if (E) {
+        double am = mkcd < 0 ? -mkcd : mkcd;
+        E[ORC_E_DIHE] += am * (1 + am * m_cos(m, cos_theta));
+    }
+    dc = delta_cos(m, cos_theta);
+    tmp = mkcd * dc * inv_nrim;
+    for (k = 0; k < 3; ++k) Fi[k] = tmp * (rln[k] * inv_nrln - rim[k] * inv_nrim * cos_theta);
+    tmp = mkcd * dc * inv_nrln;
+    for (k = 0; k < 3; ++k) Fl[k] = tmp * (rim[k] * inv_nrim - rln[k] * inv_nrln * cos_theta);
+    for (k = 0; k < 3; ++k) Fj[k] = (sijkj - 1) * Fi[k] - sklkj * Fl[k];
+    for (k = 0; k < 3; ++k) Fk[k] = -Fi[k] - Fj[k] - Fl[k];
+    for (k = 0; k < 3; ++k) {
+        F[3 * q[0] + k] += Fi[k];
+        F[3 * q[1] + k] += Fj[k];
+        F[3 * q[2] + k] += Fk[k];
+        F[3 * q[3] + k] += Fl[k];
+    }
+    for (k = 0; k < 3; ++k)
+        if (bad(Fi[k]) || bad(Fj[k]) || bad(Fk[k]) || bad(Fl[k])) return 1;
+    return E ? bad(E[ORC_E_DIHE]) : 0;
+}
+
+static void cross(const double* a, const double* b, double* o)
+{
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+static void grad_dihedral(const double* p1, const double* p2, const double* p3, const double* p4,
+                          double* out_phi, double* g)
+{
+    /* measureAndCalcGradDihedral (dihe_angle.c:95-255) */
+    double K1 = 1, r12[3], r23[3], r34[3], A[3], B[3], C[3], rAinv, rBinv, rCinv;
+    double cos_phi, sin_phi, f1[3], f2[3], f3[3];
+    int k;
+    for (k = 0; k < 3; ++k) {
+        r12[k] = p2[k] - p1[k];
+        r23[k] = p3[k] - p2[k];
+        r34[k] = p4[k] - p3[k];
+    }
+    cross(r12, r23, A);
+    cross(r23, r34, B);
+    cross(r23, A, C);
+    rAinv = 1.0f / sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+    rBinv = 1.0f / sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    rCinv = 1.0f / sqrt(C[0] * C[0] + C[1] * C[1] + C[2] * C[2]);
+    cos_phi = (A[0] * B[0] + A[1] * B[1] + A[2] * B[2]) * (rAinv * rBinv);
+    sin_phi = (C[0] * B[0] + C[1] * B[1] + C[2] * B[2]) * (rCinv * rBinv);
+    if (cos_phi < -1) cos_phi = -1;
+    if (cos_phi > 1) cos_phi = 1;
+    if (sin_phi < -1) sin_phi = -1;
+    if (sin_phi > 1) sin_phi = 1;
+    *out_phi = -atan2(sin_phi, cos_phi);
+    for (k = 0; k < 3; ++k) B[k] *= rBinv;
+    if ((sin_phi < 0 ? -sin_phi : sin_phi) > 0.1f) {
+        double dcosdA[3], dcosdB[3];
+        for (k = 0; k < 3; ++k) A[k] *= rAinv;
+        for (k = 0; k < 3; ++k) {
+            dcosdA[k] = rAinv * (cos_phi * A[k] - B[k]);
+            dcosdB[k] = rBinv * (cos_phi * B[k] - A[k]);
+        }
+        K1 = K1 / sin_phi;
+        f1[0] = K1 * (r23[1] * dcosdA[2] - r23[2] * dcosdA[1]);
+        f1[1] = K1 * (r23[2] * dcosdA[0] - r23[0] * dcosdA[2]);
+        f1[2] = K1 * (r23[0] * dcosdA[1] - r23[1] * dcosdA[0]);
+        f3[0] = K1 * (r23[2] * dcosdB[1] - r23[1] * dcosdB[2]);
+        f3[1] = K1 * (r23[0] * dcosdB[2] - r23[2] * dcosdB[0]);
+        f3[2] = K1 * (r23[1] * dcosdB[0] - r23[0] * dcosdB[1]);
+        f2[0] = K1 * (r12[2] * dcosdA[1] - r12[1] * dcosdA[2] + r34[1] * dcosdB[2] - r34[2] * dcosdB[1]);
+        f2[1] = K1 * (r12[0] * dcosdA[2] - r12[2] * dcosdA[0] + r34[2] * dcosdB[0] - r34[0] * dcosdB[2]);
+        f2[2] = K1 * (r12[1] * dcosdA[0] - r12[0] * dcosdA[1] + r34[0] * dcosdB[1] - r34[1] * dcosdB[0]);
+    } else {
+        double dsindC[3], dsindB[3];
+        for (k = 0; k < 3; ++k) C[k] *= rCinv;
+        for (k = 0; k < 3; ++k) {
+            dsindC[k] = rCinv * (sin_phi * C[k] - B[k]);
+            dsindB[k] = rBinv * (sin_phi * B[k] - C[k]);
+        }
+        K1 = -K1 / cos_phi;
+        f1[0] = K1 * ((r23[1] * r23[1] + r23[2] * r23[2]) * dsindC[0] - r23[0] * r23[1] * dsindC[1] - r23[0] * r23[2] * dsindC[2]);
+        f1[1] = K1 * ((r23[2] * r23[2] + r23[0] * r23[0]) * dsindC[1] - r23[1] * r23[2] * dsindC[2] - r23[1] * r23[0] * dsindC[0]);
+        f1[2] = K1 * ((r23[0] * r23[0] + r23[1] * r23[1]) * dsindC[2] - r23[2] * r23[0] * dsindC[0] - r23[2] * r23[1] * dsindC[1]);
+        cross(dsindB, r23, f3);
+        for (k = 0; k < 3; ++k) f3[k] *= K1;
+        f2[0] = K1 * (-(r23[1] * r12[1] + r23[2] * r12[2]) * dsindC[0] + (2.0f * r23[0] * r12[1] - r12[0] * r23[1]) * dsindC[1] +
+                      (2.0f * r23[0] * r12[2] - r12[0] * r23[2]) * dsindC[2] + dsindB[2] * r34[1] - dsindB[1] * r34[2]);
+        f2[1] = K1 * (-(r23[2] * r12[2] + r23[0] * r12[0]) * dsindC[1] + (2.0f * r23[1] * r12[2] - r12[1] * r23[2]) * dsindC[2] +
+                      (2.0f * r23[1] * r12[0] - r12[1] * r23[0]) * dsindC[0] + dsindB[0] * r34[2] - dsindB[2] * r34[0]);
+        f2[2] = K1 * (-(r23[0] * r12[0] + r23[1] * r12[1]) * dsindC[2] + (2.0f * r23[2] * r12[0] - r12[2] * r23[0]) * dsindC[0] +
+                      (2.0f * r23[2] * r12[1] - r12[2] * r23[1]) * dsindC[1] + dsindB[1] * r34[0] - dsindB[0] * r34[1]);
+    }
+    for (k = 0; k < 3; ++k) {
+        g[k] = f1[k];
+        g[3 + k] = f2[k] - f1[k];
+        g[6 + k] = f3[k] - f2[k];
+        g[9 + k] = -f3[k];
+    }
+}
+
+static int dihe_angle_calc(const orc_system* s, int pos, double* F, double* E)
+{
+    /* dihe_angle.c:43-93 */
+    const int* q = s->dihe_angle_pairs + 4 * pos;
+    double oD[12], theta = 0, tmp;
+    double k_theta = s->dihe_angle_parms[2 * pos], theta_0 = s->dihe_angle_parms[2 * pos + 1];
+    int k, r = 0;
+    grad_dihedral(s->coord + 4 * q[0], s->coord + 4 * q[1], s->coord + 4 * q[2], s->coord + 4 * q[3], &theta, oD);
+    tmp = theta - theta_0;
+    if (tmp < -M_PIF) tmp += 2 * M_PIF;
+    if (tmp > M_PIF) tmp -= 2 * M_PIF;
+    k_theta *= -tmp;
+    if (E) E[ORC_E_DIHE_ANGLE] -= 0.5f * k_theta * tmp;
+    for (k = 0; k < 4; ++k) {
+        F[3 * q[k]] += k_theta * oD[3 * k];
+        F[3 * q[k] + 1] += k_theta * oD[3 * k + 1];
+        F[3 * q[k] + 2] += k_theta * oD[3 * k + 2];
+    }
+    for (k = 0; k < 12; ++k) r |= bad(oD[k]);
+    return r || bad(k_theta) || (E ? bad(E[ORC_E_DIHE_ANGLE]) : 0);
+}
+
+int orc_forces(const orc_system* s, double* F, double* E, long long counts[2])
+{
+    int i, j, rep = 0, r;
+    memset(F, 0, sizeof(double) * 3 * s->n);
+    if (E) memset(E, 0, sizeof(double) * ORC_E_LAST + sizeof(double));
+    if (counts) counts[0] = counts[1] = 0;
+    /* bonded_inter order (pre_func.c:97-159) */
+    for (i = 0; i < s->n_angle_cos; ++i) rep |= angle_cos_calc(s, i, F, E);
+    for (i = 0; i < s->n_angle; ++i) rep |= angle_calc(s, i, F, E);
+    for (i = 0; i < s->n_bond; ++i) {
+        r = bond_calc(s, i, F, E);
+        if (r == 2) return 2;
+        rep |= r;
+    }
+    for (i = 0; i < s->n_dihe; ++i) rep |= dihe_calc(s, i, F, E);
+    for (i = 0; i < s->n_dihe_angle; ++i) rep |= dihe_angle_calc(s, i, F, E);
+    /* brute_force_val (calc_func.c:188-228) */
+    if (s->elec || s->alpha_lj != 0.0) {
+        for (i = 0; i < s->n; ++i)
+            for (j = i + 1; j < s->n; ++j) rep |= force_single(s, i, j, F, E, counts);
+    } else if (s->check_overlap) {
+        for (i = 0; i < s->n; ++i)
+            for (j = i + 1; j < s->n; ++j) {
+                double e[3], rr, r_sq;
+                v2_norms(s, i, j, e, &rr, &r_sq);
+                rep |= (s->LJ[2 * i] + s->LJ[2 * j]) * (s->LJ[2 * i] + s->LJ[2 * j]) > r_sq;
+            }
+    }
+    return rep ? 1 : 0;
+}
+
+int orc_run_steps(orc_system* s, double* coord, double* F, double dt, int K, const double* gauss,
+                  int refresh, double* traj)
+{
+    int n3 = 3 * s->n, step, i, rep = 0;
+    double* D = NULL;
+    double* L = NULL;
+    double* Rf = (double*)malloc(sizeof(double) * n3);
+    double* Rs = (double*)malloc(sizeof(double) * n3);
+    double* X = (double*)malloc(sizeof(double) * n3);
+    double preDii, preDij;
+    s->coord = coord;
+    orc_prefactors(s, &preDii, &preDij);
+    if (s->hydro == 1) {
+        D = (double*)malloc(sizeof(double) * (size_t)n3 * n3);
+        L = (double*)malloc(sizeof(double) * (size_t)n3 * n3);
+    }
+    if (refresh < 1) refresh = 1;
+    for (step = 0; step < K; ++step) {
+        const double* xi = gauss + (size_t)step * n3;
+        if (s->hydro == 1) {
+            if (step % refresh == 0) {
+                orc_D(s, D);
+                memcpy(L, D, sizeof(double) * (size_t)n3 * n3);
+                if (orc_cholesky(n3, L, n3)) {
+                    rep = -1;
+                    break;
+                }
+            }
+            orc_df(s, D, F, dt, Rf);
+            for (i = 0; i < n3; ++i) X[i] = xi[i] * sqrt(2 * dt);
+            orc_trmv_lower(n3, L, n3, X, Rs);
+        } else if (s->hydro == 2) {
+            orc_df(s, NULL, F, dt, Rf);
+            orc_tea(s, NULL, xi, dt, Rs, NULL, NULL);
+        } else {
+            orc_df(s, NULL, F, dt, Rf);
+            for (i = 0; i < n3; ++i) Rs[i] = xi[i] * sqrt(preDii / coord[4 * (i / 3) + 3] * 2 * dt);
+        }
+        /* diff_equation.c:254-264 */
+        for (i = 0; i < s->n; ++i) {
+            int k;
+            for (k = 0; k < 3; ++k) coord[4 * i + k] = Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
+            if (s->bc == 1)
+                for (k = 0; k < 3; ++k)
+                    coord[4 * i + k] -= s->box[k] * floor(coord[4 * i + k] * s->inv_L[k] + 0.5f);
+        }
+        rep |= orc_forces(s, F, NULL, NULL);
+        if (traj) memcpy(traj + (size_t)step * 4 * s->n, coord, sizeof(double) * 4 * s->n);
+    }
+    free(D);
+    free(L);
+    free(Rf);
+    free(Rs);
+    free(X);
+    return rep;
+}
