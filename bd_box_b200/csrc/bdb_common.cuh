@@ -1,0 +1,177 @@
+// Shared definitions of the bdb200 engine: the system object, error
+// plumbing, physical constants and the exact-arithmetic helpers used where
+// a decision (cutoff, overlap, periodic image) must match BD_BOX's double
+// arithmetic bit for bit.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/bdb200.h"
+
+// data.h:207-211 (double build)
+#define BDB_KB 0.001986248532617
+#define BDB_KB_1_8PI 0.00007903031804378703
+#define BDB_KB_1_6PI 0.00010537375739171604
+#define BDB_SQRTPI 1.77245385090551602729
+#define BDB_M1_SQRTPI 0.5641895835
+#define BDB_M_PIF 3.14159265358979323846f
+
+namespace bdb {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define BDB_CUDA(call)                                              \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return ::bdb::cuda_fail(e_, #call);  \
+    } while (0)
+
+// Device status word bits, written by kernels, read by the host after a step.
+enum : unsigned {
+    ST_OVERLAP = 1u,      // overlap / NaN of a force term (retry contract)
+    ST_BOND = 2u,         // over-stretched FENE bond (fatal in the reference)
+    ST_NOT_SPD = 4u,      // non-positive Cholesky pivot
+    ST_TIMEOUT = 8u,      // a bounded wait gave up
+};
+
+// A bead segment: one independent system inside a batch.
+struct Segment {
+    int begin;     // first bead
+    int count;     // beads
+    int pbegin;    // first padded matrix row (stored-D systems)
+};
+
+// A TEA / D.F work item: bead tiles (I, J), I >= J, of one segment.
+struct TileJob {
+    int seg;
+    int I, J;
+};
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    int alloc(size_t count);
+    void release();
+    ~DevBuf() { release(); }
+};
+
+}  // namespace bdb
+
+struct bdb_system {
+    bdb_params p;
+    int n = 0;       // beads
+    int n3 = 0;      // 3n
+    int npad = 0;    // stored-matrix dimension (3n rounded up to the tile)
+    cudaStream_t stream = nullptr;
+    double inv_L[3] = {0, 0, 0};
+    double preDii = 0, preDij = 0;
+
+    std::vector<bdb::Segment> segs;
+    bdb::DevBuf<bdb::Segment> d_segs;
+    bdb::DevBuf<int> d_bead_seg;
+
+    // state
+    bdb::DevBuf<double4> pos, pos_save;
+    bdb::DevBuf<double> F, F_save, Q;
+    bdb::DevBuf<double2> LJ;
+    bool have_forces = false;
+
+    // bonded terms (CSR gather)
+    int n_bond = 0, n_angle = 0, n_angle_cos = 0, n_dihe = 0, n_dihe_angle = 0;
+    bdb::DevBuf<int> bond_pairs, angle_pairs, angle_cos_pairs, dihe_pairs, dihe_angle_pairs;
+    bdb::DevBuf<double> bond_parms, angle_parms, angle_cos_parms, dihe_parms, dihe_angle_parms;
+    bdb::DevBuf<int> slot_ptr, slot_list;      // bead -> contribution slots
+    bdb::DevBuf<double> contrib;               // 3 doubles per slot
+    bdb::DevBuf<double> term_energy;           // one per bonded term
+    int n_slots = 0, n_terms = 0;
+    bdb::DevBuf<int> conn_ptr, conn_list;      // 1-2 bonded neighbours (are_conn)
+    bool conn_live = false;
+
+    // cell list
+    bdb::DevBuf<unsigned long long> sorted_keys;   // (cell << 24 | local) per bead, per segment sorted
+    bdb::DevBuf<int> sorted_idx;
+    bdb::DevBuf<double4> grid;                 // per segment: origin xyz, cell size
+    bdb::DevBuf<int4> grid_dims;               // per segment: nx, ny, nz, brute flag
+    double cell_size = 0;
+
+    // force outputs
+    bdb::DevBuf<double> e_part;                // energy partials
+    bdb::DevBuf<unsigned> status;              // status word
+    bdb::DevBuf<unsigned long long> counts;    // pair counts
+
+    // hydrodynamics
+    bdb::DevBuf<double> Rf, Rs, X, dD, work;   // 3n vectors, diag, scratch
+    bdb::DevBuf<double> part;                  // TEA / symv partial sums
+    bdb::DevBuf<double> eps_part;
+    bdb::DevBuf<double> scal;                  // device scalars (eps, beta, ...)
+    bdb::DevBuf<bdb::TileJob> jobs;
+    bdb::DevBuf<unsigned char> tea_meta;       // TEA segment table + job offsets
+    int n_jobs = 0;
+    int tea_tile = 32;
+    bdb::DevBuf<double> M64;                   // stored D (upper) + L (lower), FP64
+    bdb::DevBuf<float> M32;                    // same, FP32 (mixed path)
+    bdb::DevBuf<double> panel64;               // Cholesky workspace
+    bool factor_valid = false;
+    int steps_since_refresh = 0;
+
+    // noise
+    uint64_t philox_counter = 0;
+
+    // timing
+    cudaEvent_t ev[8];
+    bool events = false;
+    double phase_ms[8] = {0};
+};
+
+namespace bdb {
+
+// ---- exact double arithmetic (no FMA contraction) -------------------------
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+// trans_dist_vec (trans.c:111-121): v = v2 - v1, minimum image if periodic,
+// evaluated exactly as the reference evaluates it.
+__device__ __forceinline__ void dist_vec(const double4& v1, const double4& v2, int periodic,
+                                         const double* box, const double* inv_L, double* v)
+{
+    v[0] = sub(v2.x, v1.x);
+    v[1] = sub(v2.y, v1.y);
+    v[2] = sub(v2.z, v1.z);
+    if (periodic) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            v[k] = sub(v[k], mul(box[k], floor(add(mul(v[k], inv_L[k]), 0.5))));
+    }
+}
+
+// sq3v (math_help.c:30-33)
+__device__ __forceinline__ double sq3(const double* v)
+{
+    return add(add(mul(v[0], v[0]), mul(v[1], v[1])), mul(v[2], v[2]));
+}
+
+}  // namespace bdb
+
+// kernel entry points used across translation units
+namespace bdb {
+int forces_setup(bdb_system* s);
+int forces_run(bdb_system* s, bool want_energy, bool want_counts);
+int bonded_setup(bdb_system* s);
+int tensor_build(bdb_system* s);       // stored D into M64/M32 + dD
+int tensor_tile_host(bdb_system* s, int i, int j, double* tD);
+int factor_run(bdb_system* s);         // Cholesky of the stored D in place
+int stored_matvec(bdb_system* s, bool want_rs);   // Rf = D.F (upper), Rs = L.X (lower)
+int tea_run(bdb_system* s, bool want_rs);         // matrix-free D.F (+ TEA noise)
+int noise_fill(bdb_system* s, const double* host_gauss);   // X = unit Gaussians
+int update_positions(bdb_system* s);  // pos += Rf + Rs, periodic wrap
+int diag_noise(bdb_system* s);        // hydro none: Rs = X sqrt(2 dt D_ii)
+int factor_error(bdb_system* s, double* rel);
+}  // namespace bdb

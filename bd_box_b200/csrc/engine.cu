@@ -1,0 +1,470 @@
+// The bdb_* C ABI (include/bdb200.h): system lifetime, host <-> device
+// copies and the step driver that sequences the kernels of one
+// Ermak-McCammon step exactly as compute_hydro_ermak (diff_equation.c:
+// 216-286) orders the work: D.F from the forces at the start of the step,
+// the random displacement, r += Rf + Rs with the periodic wrap, then the
+// forces at the new positions (comp_step_ermak, diff_comp.c:152-179).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bdb_common.cuh"
+
+namespace bdb {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+
+int fail(int code, const std::string& msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? BDB_ERR_NOMEM : BDB_ERR_CUDA;
+}
+
+template <typename T>
+int DevBuf<T>::alloc(size_t count)
+{
+    release();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e != cudaSuccess) {
+        p = nullptr;
+        n = 0;
+        cuda_fail(e, "cudaMalloc");
+        return 1;
+    }
+    n = count;
+    return 0;
+}
+
+template <typename T>
+void DevBuf<T>::release()
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+}
+
+template struct DevBuf<double>;
+template struct DevBuf<float>;
+template struct DevBuf<int>;
+template struct DevBuf<unsigned>;
+template struct DevBuf<unsigned long long>;
+template struct DevBuf<unsigned char>;
+template struct DevBuf<double2>;
+template struct DevBuf<double4>;
+template struct DevBuf<int4>;
+template struct DevBuf<Segment>;
+template struct DevBuf<TileJob>;
+
+static int check_status(bdb_system* s, bool* overlap)
+{
+    unsigned st = 0;
+    BDB_CUDA(cudaMemcpyAsync(&st, s->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+    BDB_CUDA(cudaStreamSynchronize(s->stream));
+    if (st & ST_BOND) return fail(BDB_ERR_BOND, "Overstretched bond (bond.c:73-78)");
+    if (st & ST_NOT_SPD) return fail(BDB_ERR_NOT_SPD, "Cholesky decomposition error: non-positive pivot");
+    if (st & ST_TIMEOUT) return fail(BDB_ERR_TIMEOUT, "device wait timed out");
+    if (overlap) *overlap = (st & ST_OVERLAP) != 0;
+    return BDB_OK;
+}
+
+static int ensure_matrix(bdb_system* s)
+{
+    const size_t nn = (size_t)s->npad * s->npad;
+    if (s->p.precision == BDB_PREC_FP64) {
+        if (s->M64.p) return BDB_OK;
+        if (s->M64.alloc(nn)) return BDB_ERR_NOMEM;
+        BDB_CUDA(cudaMemset(s->M64.p, 0, nn * sizeof(double)));
+        std::vector<double> one(1, 1.0);
+        for (int r = s->n3; r < s->npad; ++r)
+            BDB_CUDA(cudaMemcpy(s->M64.p + (size_t)r * s->npad + r, one.data(), sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        if (s->M32.p) return BDB_OK;
+        if (s->M32.alloc(nn)) return BDB_ERR_NOMEM;
+        BDB_CUDA(cudaMemset(s->M32.p, 0, nn * sizeof(float)));
+        float one = 1.0f;
+        for (int r = s->n3; r < s->npad; ++r)
+            BDB_CUDA(cudaMemcpy(s->M32.p + (size_t)r * s->npad + r, &one, sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return BDB_OK;
+}
+
+// D (and its factor) at the current positions
+static int refresh_factor(bdb_system* s)
+{
+    int rc = ensure_matrix(s);
+    if (rc) return rc;
+    rc = tensor_build(s);
+    if (rc) return rc;
+    rc = factor_run(s);
+    if (rc) return rc;
+    s->factor_valid = true;
+    s->steps_since_refresh = 0;
+    return BDB_OK;
+}
+
+static int one_step(bdb_system* s, const double* dev_gauss)
+{
+    int rc;
+    if (!s->have_forces) {
+        rc = forces_run(s, false, false);
+        if (rc) return rc;
+    }
+    if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
+        if (!s->factor_valid || s->steps_since_refresh >= std::max(1, s->p.refresh)) {
+            rc = refresh_factor(s);
+            if (rc) return rc;
+        }
+        rc = noise_fill(s, dev_gauss);
+        if (rc) return rc;
+        rc = stored_matvec(s, true);
+        if (rc) return rc;
+        s->steps_since_refresh++;
+    } else {
+        rc = noise_fill(s, dev_gauss);
+        if (rc) return rc;
+        rc = tea_run(s, true);
+        if (rc) return rc;
+    }
+    rc = update_positions(s);
+    if (rc) return rc;
+    return forces_run(s, false, false);
+}
+
+}  // namespace bdb
+
+using namespace bdb;
+
+extern "C" {
+
+const char* bdb_version(void) { return "bdb200 1.0 (sm_100a)"; }
+
+const char* bdb_last_error(void) { return g_err.c_str(); }
+
+int bdb_create(bdb_system** out, const bdb_params* p, const double* coord, const double* Q, const double* LJ)
+{
+    if (!out || !p || !coord || !Q || !LJ) return fail(BDB_ERR_ARG, "null argument");
+    if (p->n <= 1) return fail(BDB_ERR_ARG, "need at least two beads");
+    if (p->hydro < 0 || p->hydro > 2) return fail(BDB_ERR_ARG, "hydro must be none, cholesky or geyer");
+    if (p->bc == 1 && (p->box[0] <= 0 || p->box[1] <= 0 || p->box[2] <= 0))
+        return fail(BDB_ERR_ARG, "Wrong box size");
+    if (p->ewald && (p->ewald_real < 0 || p->ewald_real > 5)) return fail(BDB_ERR_ARG, "ewald_real wrong value, only 0..5");
+    if (p->ewald && !(p->box[0] == p->box[1] && p->box[1] == p->box[2]))
+        return fail(BDB_ERR_ARG, "In Ewald box must be cube");
+    if (p->visc == 0.0 || p->vfactor == 0.0) return fail(BDB_ERR_ARG, "Wrong value for visc/vfactor");
+    for (int i = 0; i < p->n; ++i)
+        if (!(coord[4 * i + 3] > 0.0)) return fail(BDB_ERR_ARG, "Wrong atom radii");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(BDB_ERR_CUDA, "no CUDA device");
+    bdb_system* s = new bdb_system();
+    s->p = *p;
+    if (s->p.refresh < 1) s->p.refresh = 1;
+    s->n = p->n;
+    s->n3 = 3 * p->n;
+    s->npad = (s->n3 + 127) / 128 * 128;
+    for (int k = 0; k < 3; ++k) s->inv_L[k] = p->bc == 1 ? 1 / p->box[k] : 0.0;
+    s->preDii = BDB_KB_1_6PI * p->T / (p->visc * p->vfactor);
+    s->preDij = BDB_KB_1_8PI * p->T / (p->visc * p->vfactor);
+    int rc = BDB_OK;
+#define TRY(x)                       \
+    do {                             \
+        if ((rc = (x)) != BDB_OK) {  \
+            bdb_destroy(s);          \
+            return rc;               \
+        }                            \
+    } while (0)
+#define TRYA(b, cnt)                             \
+    do {                                         \
+        if ((b).alloc(cnt)) {                    \
+            bdb_destroy(s);                      \
+            return BDB_ERR_NOMEM;                \
+        }                                        \
+    } while (0)
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete s;
+        return fail(BDB_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    s->segs.push_back(Segment{0, s->n, 0});
+    TRYA(s->d_segs, 1);
+    TRYA(s->d_bead_seg, s->n);
+    TRYA(s->pos, s->n);
+    TRYA(s->pos_save, s->n);
+    TRYA(s->Q, s->n);
+    TRYA(s->LJ, s->n);
+    TRYA(s->Rf, s->n3);
+    TRYA(s->Rs, s->n3);
+    TRYA(s->X, s->n3);
+    TRYA(s->dD, s->npad);
+    TRYA(s->scal, 64 + 4 * 1 + 64);
+    BDB_CUDA(cudaMemcpy(s->d_segs.p, s->segs.data(), sizeof(Segment), cudaMemcpyHostToDevice));
+    BDB_CUDA(cudaMemset(s->d_bead_seg.p, 0, sizeof(int) * s->n));
+    BDB_CUDA(cudaMemcpy(s->pos.p, coord, sizeof(double) * 4 * s->n, cudaMemcpyHostToDevice));
+    BDB_CUDA(cudaMemcpy(s->Q.p, Q, sizeof(double) * s->n, cudaMemcpyHostToDevice));
+    BDB_CUDA(cudaMemcpy(s->LJ.p, LJ, sizeof(double) * 2 * s->n, cudaMemcpyHostToDevice));
+    BDB_CUDA(cudaMemset(s->scal.p, 0, sizeof(double) * s->scal.n));
+    BDB_CUDA(cudaMemset(s->Rf.p, 0, sizeof(double) * s->n3));
+    BDB_CUDA(cudaMemset(s->Rs.p, 0, sizeof(double) * s->n3));
+    BDB_CUDA(cudaMemset(s->X.p, 0, sizeof(double) * s->n3));
+    {
+        std::vector<double> dd(s->npad, 1.0);
+        BDB_CUDA(cudaMemcpy(s->dD.p, dd.data(), sizeof(double) * s->npad, cudaMemcpyHostToDevice));
+    }
+    TRY(forces_setup(s));
+    TRY(bonded_setup(s));
+    BDB_CUDA(cudaMemset(s->status.p, 0, sizeof(unsigned) * 4));
+    for (int k = 0; k < 8; ++k) cudaEventCreate(&s->ev[k]);
+    s->events = true;
+#undef TRY
+#undef TRYA
+    *out = s;
+    return BDB_OK;
+}
+
+int bdb_destroy(bdb_system* s)
+{
+    if (!s) return BDB_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->events)
+        for (int k = 0; k < 8; ++k) cudaEventDestroy(s->ev[k]);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return BDB_OK;
+}
+
+int bdb_set_bonded(bdb_system* s, int n_bond, const int* bond_pairs, const double* bond_parms, int n_angle,
+                   const int* angle_pairs, const double* angle_parms, int n_angle_cos, const int* angle_cos_pairs,
+                   const double* angle_cos_parms, int n_dihe, const int* dihe_pairs, const double* dihe_parms,
+                   int n_dihe_angle, const int* dihe_angle_pairs, const double* dihe_angle_parms)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    struct T {
+        int cnt, members, npar;
+        const int* idx;
+        const double* par;
+        DevBuf<int>* di;
+        DevBuf<double>* dp;
+        int* store;
+    } terms[5] = {
+        {n_bond, 2, 3, bond_pairs, bond_parms, &s->bond_pairs, &s->bond_parms, &s->n_bond},
+        {n_angle, 3, 2, angle_pairs, angle_parms, &s->angle_pairs, &s->angle_parms, &s->n_angle},
+        {n_angle_cos, 3, 2, angle_cos_pairs, angle_cos_parms, &s->angle_cos_pairs, &s->angle_cos_parms, &s->n_angle_cos},
+        {n_dihe, 4, 2, dihe_pairs, dihe_parms, &s->dihe_pairs, &s->dihe_parms, &s->n_dihe},
+        {n_dihe_angle, 4, 2, dihe_angle_pairs, dihe_angle_parms, &s->dihe_angle_pairs, &s->dihe_angle_parms,
+         &s->n_dihe_angle},
+    };
+    for (auto& t : terms) {
+        if (t.cnt < 0 || (t.cnt && (!t.idx || !t.par))) return fail(BDB_ERR_ARG, "bonded term arrays");
+        for (int k = 0; k < t.cnt * t.members; ++k)
+            if (t.idx[k] < 0 || t.idx[k] >= s->n) return fail(BDB_ERR_ARG, "bonded term references a missing bead");
+    }
+    for (auto& t : terms) {
+        *t.store = t.cnt;
+        if (t.di->alloc(std::max(1, t.cnt * t.members)) || t.dp->alloc(std::max(1, t.cnt * t.npar)))
+            return BDB_ERR_NOMEM;
+        if (t.cnt) {
+            BDB_CUDA(cudaMemcpy(t.di->p, t.idx, sizeof(int) * t.cnt * t.members, cudaMemcpyHostToDevice));
+            BDB_CUDA(cudaMemcpy(t.dp->p, t.par, sizeof(double) * t.cnt * t.npar, cudaMemcpyHostToDevice));
+        }
+    }
+    s->have_forces = false;
+    return bonded_setup(s);
+}
+
+int bdb_set_coord(bdb_system* s, const double* coord)
+{
+    if (!s || !coord) return fail(BDB_ERR_ARG, "null argument");
+    BDB_CUDA(cudaMemcpyAsync(s->pos.p, coord, sizeof(double) * 4 * s->n, cudaMemcpyHostToDevice, s->stream));
+    s->have_forces = false;
+    s->factor_valid = false;
+    return BDB_OK;
+}
+
+int bdb_get_coord(bdb_system* s, double* coord)
+{
+    if (!s || !coord) return fail(BDB_ERR_ARG, "null argument");
+    BDB_CUDA(cudaMemcpyAsync(coord, s->pos.p, sizeof(double) * 4 * s->n, cudaMemcpyDeviceToHost, s->stream));
+    BDB_CUDA(cudaStreamSynchronize(s->stream));
+    return BDB_OK;
+}
+
+int bdb_save_state(bdb_system* s)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    BDB_CUDA(cudaMemcpyAsync(s->pos_save.p, s->pos.p, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+    BDB_CUDA(cudaMemcpyAsync(s->F_save.p, s->F.p, sizeof(double) * s->n3, cudaMemcpyDeviceToDevice, s->stream));
+    return BDB_OK;
+}
+
+int bdb_load_state(bdb_system* s)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    BDB_CUDA(cudaMemcpyAsync(s->pos.p, s->pos_save.p, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+    BDB_CUDA(cudaMemcpyAsync(s->F.p, s->F_save.p, sizeof(double) * s->n3, cudaMemcpyDeviceToDevice, s->stream));
+    s->have_forces = true;
+    return BDB_OK;
+}
+
+int bdb_compute_forces(bdb_system* s, double* F, double* E, long long* counts)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
+    int rc = forces_run(s, E != nullptr, counts != nullptr);
+    if (rc) return rc;
+    if (F) BDB_CUDA(cudaMemcpyAsync(F, s->F.p, sizeof(double) * s->n3, cudaMemcpyDeviceToHost, s->stream));
+    if (E) BDB_CUDA(cudaMemcpyAsync(E, s->scal.p + 16, sizeof(double) * (BDB_E_LAST + 1), cudaMemcpyDeviceToHost,
+                                    s->stream));
+    unsigned long long c[2] = {0, 0};
+    if (counts) BDB_CUDA(cudaMemcpyAsync(c, s->counts.p, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+    bool ov = false;
+    rc = check_status(s, &ov);
+    if (rc) return rc;
+    if (counts) {
+        counts[0] = (long long)c[0];
+        counts[1] = (long long)c[1];
+    }
+    return ov ? 1 : 0;
+}
+
+int bdb_compute_D(bdb_system* s, double* D)
+{
+    if (!s || !D) return fail(BDB_ERR_ARG, "null argument");
+    const int n3 = s->n3;
+    if (s->p.hydro == BDB_HYDRO_NONE) {
+        // compute_D does nothing without hydrodynamics; the tensor is diag_D
+        // (diff_tensor.c:477, main_loop.c:161-175)
+        std::vector<double4> pos(s->n);
+        BDB_CUDA(cudaMemcpy(pos.data(), s->pos.p, sizeof(double4) * s->n, cudaMemcpyDeviceToHost));
+        memset(D, 0, sizeof(double) * (size_t)n3 * n3);
+        for (int r = 0; r < n3; ++r) D[(size_t)r * n3 + r] = s->preDii / pos[r / 3].w;
+        return BDB_OK;
+    }
+    int rc = ensure_matrix(s);
+    if (rc) return rc;
+    rc = tensor_build(s);
+    if (rc) return rc;
+    s->factor_valid = false;
+    if (s->p.precision == BDB_PREC_FP64) {
+        BDB_CUDA(cudaMemcpy2DAsync(D, sizeof(double) * n3, s->M64.p, sizeof(double) * s->npad, sizeof(double) * n3, n3,
+                                   cudaMemcpyDeviceToHost, s->stream));
+        BDB_CUDA(cudaStreamSynchronize(s->stream));
+    } else {
+        std::vector<float> tmp((size_t)n3 * n3);
+        BDB_CUDA(cudaMemcpy2DAsync(tmp.data(), sizeof(float) * n3, s->M32.p, sizeof(float) * s->npad, sizeof(float) * n3,
+                                   n3, cudaMemcpyDeviceToHost, s->stream));
+        BDB_CUDA(cudaStreamSynchronize(s->stream));
+        for (size_t k = 0; k < tmp.size(); ++k) D[k] = tmp[k];
+    }
+    // the diagonal of D lives in dD (the matrix diagonal is shared with L)
+    std::vector<double> dd(n3);
+    BDB_CUDA(cudaMemcpy(dd.data(), s->dD.p, sizeof(double) * n3, cudaMemcpyDeviceToHost));
+    for (int r = 0; r < n3; ++r) D[(size_t)r * n3 + r] = dd[r];
+    return BDB_OK;
+}
+
+int bdb_compute_Dij(bdb_system* s, int i, int j, double* tD)
+{
+    if (!s || !tD || i < 0 || j < 0 || i >= s->n || j >= s->n) return fail(BDB_ERR_ARG, "bad tile index");
+    return tensor_tile_host(s, i, j, tD);
+}
+
+int bdb_compute_Rf(bdb_system* s, double* Rf)
+{
+    if (!s || !Rf) return fail(BDB_ERR_ARG, "null argument");
+    int rc;
+    if (!s->have_forces && (rc = forces_run(s, false, false))) return rc;
+    if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
+        if (!s->factor_valid && (rc = refresh_factor(s))) return rc;
+        rc = stored_matvec(s, false);
+    } else {
+        rc = tea_run(s, false);
+    }
+    if (rc) return rc;
+    BDB_CUDA(cudaMemcpyAsync(Rf, s->Rf.p, sizeof(double) * s->n3, cudaMemcpyDeviceToHost, s->stream));
+    return check_status(s, nullptr);
+}
+
+int bdb_compute_r(bdb_system* s, const double* gauss, double* Rs)
+{
+    if (!s || !Rs) return fail(BDB_ERR_ARG, "null argument");
+    int rc;
+    BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
+    if (!s->have_forces && (rc = forces_run(s, false, false))) return rc;
+    double* dg = nullptr;
+    if (gauss) {
+        dg = s->work.p;
+        BDB_CUDA(cudaMemcpyAsync(dg, gauss, sizeof(double) * s->n3, cudaMemcpyHostToDevice, s->stream));
+    }
+    if ((rc = noise_fill(s, dg))) return rc;
+    if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
+        if (!s->factor_valid && (rc = refresh_factor(s))) return rc;
+        rc = stored_matvec(s, true);
+    } else {
+        rc = tea_run(s, true);
+    }
+    if (rc) return rc;
+    BDB_CUDA(cudaMemcpyAsync(Rs, s->Rs.p, sizeof(double) * s->n3, cudaMemcpyDeviceToHost, s->stream));
+    return check_status(s, nullptr);
+}
+
+int bdb_step(bdb_system* s, int K, const double* gauss)
+{
+    if (!s || K < 0) return fail(BDB_ERR_ARG, "bad arguments");
+    if (s->p.noise == BDB_NOISE_HOST && !gauss) return fail(BDB_ERR_ARG, "host noise mode needs Gaussians");
+    DevBuf<double> g;
+    if (gauss) {
+        if (g.alloc((size_t)K * s->n3)) return BDB_ERR_NOMEM;
+        BDB_CUDA(cudaMemcpyAsync(g.p, gauss, sizeof(double) * K * s->n3, cudaMemcpyHostToDevice, s->stream));
+    }
+    BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
+    BDB_CUDA(cudaEventRecord(s->ev[0], s->stream));
+    for (int k = 0; k < K; ++k) {
+        int rc = one_step(s, gauss ? g.p + (size_t)k * s->n3 : nullptr);
+        if (rc) return rc;
+    }
+    BDB_CUDA(cudaEventRecord(s->ev[1], s->stream));
+    bool ov = false;
+    int rc = check_status(s, &ov);
+    if (rc) return rc;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
+    s->phase_ms[0] = ms;
+    return ov ? 1 : 0;
+}
+
+int bdb_factor_error(bdb_system* s, double* rel_err)
+{
+    if (!s || !rel_err) return fail(BDB_ERR_ARG, "null argument");
+    if (s->p.hydro != BDB_HYDRO_CHOLESKY) return fail(BDB_ERR_STATE, "no stored factor (hydro is not cholesky)");
+    int rc;
+    BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
+    if ((rc = refresh_factor(s))) return rc;
+    if ((rc = check_status(s, nullptr))) return rc;
+    return factor_error(s, rel_err);
+}
+
+int bdb_phase_ms(bdb_system* s, const char* phase, double* ms)
+{
+    if (!s || !phase || !ms) return fail(BDB_ERR_ARG, "null argument");
+    if (!strcmp(phase, "step")) {
+        *ms = s->phase_ms[0];
+        return BDB_OK;
+    }
+    return fail(BDB_ERR_ARG, "unknown phase");
+}
+
+void* bdb_stream(bdb_system* s) { return s ? (void*)s->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,204 @@
+// One pass over the stored matrix M (upper triangle: D, lower triangle
+// including the diagonal: its Cholesky factor L) computes both per-step
+// products of the Cholesky path:
+//   Rf = D F   (dsymv "U", diff_alg/diff_equation.c:152-159)
+//   Rs = L X   (my_dtrmv, myblas.c:94-118)
+// HBM-bound: every element of M is read once per step.
+//
+// Work item = one warp on (strip of 32 rows) x (column segment). A lane
+// owns 4 consecutive columns of every 128-column tile (one 16-byte load of
+// FP32 or two of FP64 per row). For each tile the 32 per-row lane partials
+// are combined by a 31-shuffle reduce-scatter, after which lane q holds
+// row q's sum. The transposed part of D F (left of the diagonal)
+// accumulates per column over the strip's 32 rows and is written as one
+// partial per (strip, column); k_mv_finish adds all partials in a fixed
+// order and applies the position update, so results are deterministic.
+// Products are accumulated in FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "bdb_common.cuh"
+
+namespace bdb {
+
+static constexpr int STRIP = 32;
+static constexpr int WARPS = 4;
+
+__device__ __forceinline__ void load4(const float* p, double* o)
+{
+    const float4 v = __ldcs(reinterpret_cast<const float4*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+}
+
+__device__ __forceinline__ void load4(const double* p, double* o)
+{
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b.x;
+    o[3] = b.y;
+}
+
+// v[q] per lane -> returns sum over lanes of v[lane]
+__device__ __forceinline__ double reduce_scatter32(double* v, int lane)
+{
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) {
+        const bool hi = (lane & w) != 0;
+#pragma unroll
+        for (int k = 0; k < w; ++k) {
+            const double send = hi ? v[k] : v[k + w];
+            const double keep = hi ? v[k + w] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, w);
+        }
+    }
+    return v[0];
+}
+
+// rowp: [nseg][n3][2] row partials (Rs, Rf right part); colp: [nstrip][n3]
+template <typename T>
+__global__ void __launch_bounds__(32 * WARPS)
+k_strip_mv(const T* __restrict__ M, int n3, int npad, int nseg, int seg_cols,
+           const double* __restrict__ F, const double* __restrict__ X, double* __restrict__ rowp,
+           double* __restrict__ colp)
+{
+    __shared__ double sF[WARPS][STRIP];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * WARPS + warp;
+    const int nstrip = (n3 + STRIP - 1) / STRIP;
+    if (item >= nstrip * nseg) return;
+    const int strip = item / nseg, seg = item % nseg;
+    const int r0 = strip * STRIP;
+    const int nrow = min(STRIP, n3 - r0);
+    const int c_beg = seg * seg_cols, c_end = min(n3, c_beg + seg_cols);
+    sF[warp][lane] = lane < nrow ? F[r0 + lane] : 0.0;
+    __syncwarp();
+    double rs_acc = 0, rf_acc = 0;
+    for (int c0 = c_beg; c0 < c_end; c0 += 128) {
+        const int c = c0 + 4 * lane;
+        double x[4], f[4], pc[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const bool ok = c + v < c_end;
+            x[v] = ok ? X[c + v] : 0.0;
+            f[v] = ok ? F[c + v] : 0.0;
+        }
+        const bool full = c + 3 < c_end;
+        const bool lower = c0 + 127 < r0;
+        const bool upper = c0 > r0 + STRIP - 1;
+        double pr[STRIP];
+        if (lower || upper) {
+            const double* w = lower ? x : f;
+#pragma unroll 8
+            for (int q = 0; q < STRIP; ++q) {
+                double m[4] = {0, 0, 0, 0};
+                if (q < nrow) {
+                    const T* rp = M + (size_t)(r0 + q) * npad + c;
+                    if (full) load4(rp, m);
+                    else
+                        for (int v = 0; v < 4; ++v)
+                            if (c + v < c_end) m[v] = (double)rp[v];
+                }
+                pr[q] = m[0] * w[0] + m[1] * w[1] + m[2] * w[2] + m[3] * w[3];
+                if (upper) {
+                    const double fq = sF[warp][q];
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) pc[v] += m[v] * fq;
+                }
+            }
+            const double red = reduce_scatter32(pr, lane);
+            if (lower) rs_acc += red; else rf_acc += red;
+        } else {
+            // tile crossing the diagonal: per element
+            double ps[STRIP];
+#pragma unroll 4
+            for (int q = 0; q < STRIP; ++q) {
+                const int r = r0 + q;
+                double m[4] = {0, 0, 0, 0};
+                if (q < nrow)
+                    for (int v = 0; v < 4; ++v)
+                        if (c + v < c_end) m[v] = (double)M[(size_t)r * npad + c + v];
+                double s = 0, t = 0;
+                const double fq = sF[warp][q];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    if (c + v <= r) s += m[v] * x[v];
+                    else {
+                        t += m[v] * f[v];
+                        pc[v] += m[v] * fq;
+                    }
+                }
+                ps[q] = s;
+                pr[q] = t;
+            }
+            rs_acc += reduce_scatter32(ps, lane);
+            rf_acc += reduce_scatter32(pr, lane);
+        }
+        if (!lower) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                if (c + v < c_end && c + v > r0) colp[(size_t)strip * n3 + c + v] = pc[v];
+        }
+    }
+    if (lane < nrow) {
+        rowp[((size_t)seg * n3 + r0 + lane) * 2] = rs_acc;
+        rowp[((size_t)seg * n3 + r0 + lane) * 2 + 1] = rf_acc;
+    }
+}
+
+// Rs = sum of row partials; Rf = pre * (row partials + dD F + column partials
+// of the strips above).
+__global__ void k_mv_finish(int n3, int nseg, const double* __restrict__ rowp, const double* __restrict__ colp,
+                            const double* __restrict__ dD, const double* __restrict__ F, double pre,
+                            double* __restrict__ Rf, double* __restrict__ Rs, int want_rs)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n3) return;
+    double s = 0, f = 0;
+    for (int g = 0; g < nseg; ++g) {
+        s += rowp[((size_t)g * n3 + r) * 2];
+        f += rowp[((size_t)g * n3 + r) * 2 + 1];
+    }
+    f += dD[r] * F[r];
+    for (int st = 0; st * STRIP < r; ++st) f += colp[(size_t)st * n3 + r];
+    Rf[r] = f * pre;
+    if (want_rs) Rs[r] = s;
+}
+
+int stored_matvec(bdb_system* s, bool want_rs)
+{
+    const int n3 = s->n3;
+    const int nstrip = (n3 + STRIP - 1) / STRIP;
+    // enough warps for the machine: aim at >= 16 warps per SM
+    int nseg = std::max(1, (148 * 16 + nstrip - 1) / nstrip);
+    int seg_cols = ((n3 + nseg - 1) / nseg + 127) / 128 * 128;
+    nseg = (n3 + seg_cols - 1) / seg_cols;
+    const size_t need_row = (size_t)nseg * n3 * 2, need_col = (size_t)nstrip * n3;
+    if (s->part.n < need_row + need_col) {
+        if (s->part.alloc(need_row + need_col)) return BDB_ERR_NOMEM;
+    }
+    double* rowp = s->part.p;
+    double* colp = s->part.p + need_row;
+    const int items = nstrip * nseg;
+    const int blocks = (items + WARPS - 1) / WARPS;
+    const double* X = want_rs ? s->X.p : s->F.p;   // any valid vector when Rs is not wanted
+    if (s->p.precision == BDB_PREC_FP64)
+        k_strip_mv<double><<<blocks, 32 * WARPS, 0, s->stream>>>(s->M64.p, n3, s->npad, nseg, seg_cols, s->F.p, X,
+                                                                 rowp, colp);
+    else
+        k_strip_mv<float><<<blocks, 32 * WARPS, 0, s->stream>>>(s->M32.p, n3, s->npad, nseg, seg_cols, s->F.p, X,
+                                                                rowp, colp);
+    BDB_CUDA(cudaGetLastError());
+    const double pre = s->p.dt / (BDB_KB * s->p.T);
+    k_mv_finish<<<(n3 + 255) / 256, 256, 0, s->stream>>>(n3, nseg, rowp, colp, s->dD.p, s->F.p, pre, s->Rf.p, s->Rs.p,
+                                                         want_rs);
+    BDB_CUDA(cudaGetLastError());
+    return BDB_OK;
+}
+
+}  // namespace bdb

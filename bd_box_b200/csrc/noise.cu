@@ -1,0 +1,123 @@
+// Gaussian noise and the position update.
+//
+// rand_move.c:132-168 draws unit Gaussians on the host (Marsaglia polar on
+// drand48_r) and the reference GPU build copies them to the device every
+// step (diff_alg/cuda/diff_rand.cu:143-180). Here they are either generated
+// on the device -- Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) keyed
+// by the seed, counter = (step, pair index), two 53-bit uniforms per call
+// and the Box-Muller transform -- or copied from a caller array (parity
+// runs that replay the reference's exact stream).
+//
+// The same kernel applies the per-method scaling of compute_r
+// (diff_rand.c:47-236): sqrt(2 dt) for Cholesky, sqrt(2 dt / D_ii) for TEA,
+// sqrt(2 dt D_ii) for hydro none.
+#include <cuda_runtime.h>
+
+#include "bdb_common.cuh"
+
+namespace bdb {
+
+__device__ __forceinline__ void philox_round(uint32_t* c, const uint32_t* k)
+{
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
+    const uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
+    const uint32_t n0 = hi1 ^ c[1] ^ k[0];
+    const uint32_t n2 = hi0 ^ c[3] ^ k[1];
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+}
+
+__device__ __forceinline__ void philox4x32_10(uint32_t* c, uint32_t k0, uint32_t k1)
+{
+    uint32_t k[2] = {k0, k1};
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        philox_round(c, k);
+        k[0] += 0x9E3779B9u;
+        k[1] += 0xBB67AE85u;
+    }
+}
+
+// two unit Gaussians for (stream, index)
+__device__ __forceinline__ void gauss2(uint64_t seed, uint64_t stream, uint32_t idx, double& z0, double& z1)
+{
+    uint32_t c[4] = {idx, (uint32_t)stream, (uint32_t)(stream >> 32), 0x42444242u};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double two53 = 9007199254740992.0;
+    const double u0 = ((double)(c[0] >> 5) * 67108864.0 + (double)(c[1] >> 6) + 0.5) / two53;   // (0,1)
+    const double u1 = ((double)(c[2] >> 5) * 67108864.0 + (double)(c[3] >> 6)) / two53;         // [0,1)
+    const double r = sqrt(-2.0 * log(u0));
+    double sn, cs;
+    sincospi(2.0 * u1, &sn, &cs);
+    z0 = r * cs;
+    z1 = r * sn;
+}
+
+// mode: 1 cholesky sqrt(2 dt); 2 TEA sqrt(2 dt / D_ii); 0 none sqrt(D_ii 2 dt)
+__global__ void k_noise(int n3, int mode, double dt, double preDii, const double4* __restrict__ pos,
+                        const double* __restrict__ host_g, uint64_t seed, uint64_t stream, double* __restrict__ X)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = 2 * t;
+    if (i0 >= n3) return;
+    double g[2];
+    if (host_g) {
+        g[0] = host_g[i0];
+        g[1] = i0 + 1 < n3 ? host_g[i0 + 1] : 0.0;
+    } else {
+        gauss2(seed, stream, (uint32_t)t, g[0], g[1]);
+    }
+    for (int q = 0; q < 2; ++q) {
+        const int i = i0 + q;
+        if (i >= n3) break;
+        const double d = preDii / pos[i / 3].w;   // diag_D (diff_decl.c:94-99)
+        double sc;
+        if (mode == 1) sc = sqrt(2 * dt);
+        else if (mode == 2) sc = sqrt(2 * dt * (1 / d));
+        else sc = sqrt(d * 2 * dt);
+        X[i] = g[q] * sc;
+    }
+}
+
+int noise_fill(bdb_system* s, const double* dev_gauss)
+{
+    const int n3 = s->n3;
+    const int threads = (n3 + 1) / 2;
+    k_noise<<<(threads + 255) / 256, 256, 0, s->stream>>>(n3, s->p.hydro, s->p.dt, s->preDii, s->pos.p, dev_gauss,
+                                                          s->p.seed, s->philox_counter, s->X.p);
+    BDB_CUDA(cudaGetLastError());
+    s->philox_counter++;
+    return BDB_OK;
+}
+
+// coord_out = Rf + Rs + coord; trans_to_box (diff_equation.c:254-264)
+__global__ void k_update(int n, int periodic, double3 box, double3 inv_L, const double* __restrict__ Rf,
+                         const double* __restrict__ Rs, double4* __restrict__ pos)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = pos[i];
+    p.x = add(add(Rf[3 * i], Rs[3 * i]), p.x);
+    p.y = add(add(Rf[3 * i + 1], Rs[3 * i + 1]), p.y);
+    p.z = add(add(Rf[3 * i + 2], Rs[3 * i + 2]), p.z);
+    if (periodic) {
+        p.x = sub(p.x, mul(box.x, floor(add(mul(p.x, inv_L.x), 0.5))));
+        p.y = sub(p.y, mul(box.y, floor(add(mul(p.y, inv_L.y), 0.5))));
+        p.z = sub(p.z, mul(box.z, floor(add(mul(p.z, inv_L.z), 0.5))));
+    }
+    pos[i] = p;
+}
+
+int update_positions(bdb_system* s)
+{
+    k_update<<<(s->n + 127) / 128, 128, 0, s->stream>>>(
+        s->n, s->p.bc == 1, make_double3(s->p.box[0], s->p.box[1], s->p.box[2]),
+        make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]), s->Rf.p, s->Rs.p, s->pos.p);
+    BDB_CUDA(cudaGetLastError());
+    return BDB_OK;
+}
+
+}  // namespace bdb

@@ -1,0 +1,177 @@
+// RPY diffusion-tensor tiles, shared by the stored-D build and the
+// matrix-free D.F / TEA kernels.
+//
+// A tile is the symmetric 3x3 block D_ij, kept as 6 values
+// {xx, yy, zz, xy, xz, yz}.
+//  * rpy_free: diff_tensor_calc_pos (diff_alg/diff_tensor.c:45-92), the
+//    free-space Rotne-Prager-Yamakawa tensor with the overlap form for
+//    r < a_i + a_j.
+//  * rpy_beenakker: diff_tensor_calc_ewald_beenakker (diff_tensor.c:265-401)
+//    with its self term (:404-422): real-space images r + L m and
+//    reciprocal vectors over the same sphere |m|^2 <= R^2, overlap
+//    correction on the raw (not minimum-image) separation, alpha = sqrt(pi)/L
+//    (init_tensor, :546-559). Constants that the reference forms from the
+//    float literal M_PIF are formed the same way on the host.
+#pragma once
+
+#include "bdb_common.cuh"
+
+namespace bdb {
+
+struct EwaldConst {
+    double L, inv_L, alpha, alpha2, alpha3, inv_alpha2, preQ;
+    double two_pif;      // 2*M_PIF evaluated in float
+    double four_pif2;    // 4*M_PIF*M_PIF evaluated in float
+    double six_pif;      // 6*M_PIF evaluated in float
+    int R, rr_sq;
+};
+
+inline EwaldConst make_ewald(double L, double inv_L, int R)
+{
+    EwaldConst e;
+    e.L = L;
+    e.inv_L = inv_L;
+    e.alpha = BDB_SQRTPI * inv_L;
+    e.alpha2 = e.alpha * e.alpha;
+    e.alpha3 = e.alpha * e.alpha2;
+    e.inv_alpha2 = 1.0f / e.alpha2;
+    e.preQ = inv_L * inv_L * inv_L;
+    volatile float pif = BDB_M_PIF;
+    volatile float two = 2 * pif;
+    volatile float four = 4 * pif;
+    volatile float four2 = four * pif;
+    volatile float six = 6 * pif;
+    e.two_pif = two;
+    e.four_pif2 = four2;
+    e.six_pif = six;
+    e.R = R;
+    e.rr_sq = R * R;
+    return e;
+}
+
+// diff_tensor_calc_pos(i, j): sigma_i is bead j's radius, sigma_j bead i's,
+// e = (r_i - r_j)/|r_i - r_j|.
+template <typename T>
+__device__ __forceinline__ void rpy_free(const double4& pi, const double4& pj, T preDii, T preDij, T* t)
+{
+    const T si = (T)pj.w, sj = (T)pi.w;
+    T e0 = (T)(pi.x - pj.x), e1 = (T)(pi.y - pj.y), e2 = (T)(pi.z - pj.z);
+    const T r_sq = e0 * e0 + e1 * e1 + e2 * e2;
+    const T r = sqrt(r_sq);
+    const T inv = (T)1 / r;
+    e0 *= inv;
+    e1 *= inv;
+    e2 *= inv;
+    if (r < si + sj) {
+        const T sigma = (si + sj) / 2;
+        const T pre = preDii / sigma;
+        const T q = r / (32 * sigma);
+        const T part1 = 1 - 9 * q;
+        const T q3 = 3 * q;
+        t[0] = (part1 + q3 * e0 * e0) * pre;
+        t[1] = (part1 + q3 * e1 * e1) * pre;
+        t[2] = (part1 + q3 * e2 * e2) * pre;
+        t[3] = pre * q3 * e0 * e1;
+        t[4] = pre * q3 * e0 * e2;
+        t[5] = pre * q3 * e1 * e2;
+    } else {
+        const T pre = preDij / r;
+        const T sigm_r = (si * si + sj * sj) / r_sq;
+        const T a = 1 + sigm_r / 3;
+        const T b = 1 - sigm_r;
+        t[0] = (a + e0 * e0 * b) * pre;
+        t[1] = (a + e1 * e1 * b) * pre;
+        t[2] = (a + e2 * e2 * b) * pre;
+        t[3] = pre * e0 * e1 * b;
+        t[4] = pre * e0 * e2 * b;
+        t[5] = pre * e1 * e2 * b;
+    }
+}
+
+// diff_tensor_calc_ewald_beenakker(i, j) (+ _diag for i == j), FP64.
+__device__ __forceinline__ void rpy_beenakker(const double4& pi, const double4& pj, bool self,
+                                              double preDii, double preDij, const EwaldConst& ec,
+                                              double* t)
+{
+    const double sigma_i = pj.w, sigma_j = pi.w;
+    const double r0 = pj.x - pi.x, r1 = pj.y - pi.y, r2 = pj.z - pi.z;
+    const double sigma_sq = 0.5 * (sigma_i * sigma_i + sigma_j * sigma_j);
+    double O[6] = {0, 0, 0, 0, 0, 0}, Qr[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 6; ++k) t[k] = 0;
+    const double rr = r0 * r0 + r1 * r1 + r2 * r2;
+    if (!self && rr < (sigma_i + sigma_j) * (sigma_i + sigma_j)) {
+        const double r = sqrt(rr), inv = 1 / r;
+        const double e[3] = {r0 * inv, r1 * inv, r2 * inv};
+        const double sigma = (sigma_i + sigma_j) / 2;
+        const double pre = preDii / sigma;
+        const double part1 = 1 - (9 * r / (32 * sigma));
+        const double pre2 = preDij / r;
+        const double sigm_r = (sigma_i * sigma_i + sigma_j * sigma_j) / rr;
+        const double p1 = 1 + sigm_r / 3;
+        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+        for (int k = 0; k < 3; ++k)
+            t[k] += pre * (part1 + 3 * e[k] * e[k] * r / (32 * sigma)) - pre2 * (p1 + e[k] * e[k] * (1 - sigm_r));
+        for (int k = 3; k < 6; ++k)
+            t[k] += pre * 3 * e[ia[k]] * e[ib[k]] * r / (32 * sigma) - pre2 * e[ia[k]] * e[ib[k]] * (1 - sigm_r);
+    }
+    const double v0 = r0 * ec.inv_L, v1 = r1 * ec.inv_L, v2 = r2 * ec.inv_L;
+    const double a = ec.alpha, a2 = ec.alpha2, a3 = ec.alpha3;
+    for (int h = -ec.R; h <= ec.R; ++h) {
+        const int nf = (int)sqrt((double)(ec.rr_sq - h * h));
+        for (int f = -nf; f <= nf; ++f) {
+            const int ng = (int)sqrt((double)(ec.rr_sq - h * h - f * f));
+            for (int g = -ng; g <= ng; ++g) {
+                // real space
+                const double x = r0 + ec.L * h, y = r1 + ec.L * f, z = r2 + ec.L * g;
+                const double r_sq = x * x + y * y + z * z;
+                if (r_sq != 0.0) {
+                    const double r = sqrt(r_sq);
+                    const double inv_r = 1 / r, inv_r2 = 1 / r_sq, inv_r3 = inv_r * inv_r2;
+                    const double e[3] = {x * inv_r, y * inv_r, z * inv_r};
+                    const double ex = exp(-a2 * r_sq);
+                    const double ec_ = erfc(r * a);
+                    double sc = a * sigma_sq * inv_r2 + 14 * a3 * sigma_sq - 4.5 * a -
+                                20 * a2 * a3 * sigma_sq * r_sq + 3 * a3 * r_sq +
+                                4 * a3 * a2 * a2 * sigma_sq * r_sq * r_sq;
+                    sc = sc * ex / BDB_SQRTPI + ec_ * (0.75 * inv_r + 0.5 * sigma_sq * inv_r3);
+                    double sc2 = -3 * a * sigma_sq * inv_r2 - 2 * a3 * sigma_sq + 1.5 * a +
+                                 16 * a2 * a3 * sigma_sq * r_sq - 3 * a3 * r_sq -
+                                 4 * a3 * a2 * a2 * sigma_sq * r_sq * r_sq;
+                    sc2 = sc2 * ex / BDB_SQRTPI + ec_ * (0.75 * inv_r - 1.5 * sigma_sq * inv_r3);
+                    O[0] += sc + sc2 * e[0] * e[0];
+                    O[1] += sc + sc2 * e[1] * e[1];
+                    O[2] += sc + sc2 * e[2] * e[2];
+                    O[3] += sc2 * e[0] * e[1];
+                    O[4] += sc2 * e[0] * e[2];
+                    O[5] += sc2 * e[1] * e[2];
+                }
+                // reciprocal space
+                const double k_sq = (double)(h * h + f * f + g * g);
+                if (k_sq != 0.0) {
+                    const double kn = sqrt(k_sq), ik = 1 / kn;
+                    const double e[3] = {h * ik, f * ik, g * ik};
+                    const double k2 = k_sq * ec.four_pif2;
+                    double sc = 1 - sigma_sq * k2 / 3;
+                    sc *= 1 + (ec.inv_alpha2 * k2 / 4) * (1 + ec.inv_alpha2 * k2 / 2);
+                    sc *= ec.six_pif * exp(-ec.inv_alpha2 * k2 / 4) / k2;
+                    sc *= cos(ec.two_pif * (v0 * h + v1 * f + v2 * g));
+                    Qr[0] += sc - sc * e[0] * e[0];
+                    Qr[1] += sc - sc * e[1] * e[1];
+                    Qr[2] += sc - sc * e[2] * e[2];
+                    Qr[3] -= sc * e[0] * e[1];
+                    Qr[4] -= sc * e[0] * e[2];
+                    Qr[5] -= sc * e[1] * e[2];
+                }
+            }
+        }
+    }
+    for (int k = 0; k < 6; ++k) t[k] += preDii * (O[k] + ec.preQ * Qr[k]);
+    if (self) {
+        const double aw = pi.w;
+        const double sc3 = (-6 * a / BDB_SQRTPI + 40 * a3 * aw * aw / (3 * BDB_SQRTPI)) * preDii;
+        for (int k = 0; k < 3; ++k) t[k] = preDii / aw + sc3 + t[k];
+        t[3] = t[4] = t[5] = 0;
+    }
+}
+
+}  // namespace bdb

@@ -1,0 +1,444 @@
+// Diffusion tensor on the device.
+//
+// 1. k_build: the stored 3N x 3N tensor of compute_D (diff_tensor.c:472-544)
+//    for the Cholesky path. One CTA per 32x32-bead tile (I >= J) evaluates
+//    the 1024 RPY tiles into shared memory and writes the 96x96 block twice
+//    with coalesced rows: as rows of block (I, J) below the diagonal and,
+//    transposed through shared memory, as rows of block (J, I) above it.
+//    The factorisation later overwrites the lower triangle with L; the upper
+//    triangle keeps D (the reference keeps Ds and S separately,
+//    diff_rand.c:76-82). The diagonal of D goes to dD.
+// 2. k_tea: matrix-free D.F (compute_Rf_geyer_in_fly, diff_equation.c:55-117)
+//    and the Geyer-Winter sums C_i, Feff_i, eps (compute_r DIFF_GEYER,
+//    diff_rand.c:86-196) in one pass over tile pairs (I >= J): every bead
+//    pair is evaluated once, staged in shared memory, and summed by rows
+//    (into bead i) and by columns (into bead j). Per (tile, bead) partials
+//    go to a scratch buffer that k_tea_finish reduces in a fixed order, so
+//    the result does not depend on scheduling.
+// 3. k_eps_beta + k_tea_finish: eps -> beta (diff_rand.c:197-217), the TEA
+//    displacement (:219-228) and the position update with the periodic wrap
+//    (compute_hydro_ermak, diff_equation.c:254-264), fused.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bdb_common.cuh"
+#include "rpy_tile.cuh"
+
+namespace bdb {
+
+static constexpr int TB = 32;   // beads per tile
+
+struct TensorArgs {
+    int n, npad;
+    double preDii, preDij;
+    int ewald;
+    EwaldConst ec;
+};
+
+static TensorArgs targs(const bdb_system* s)
+{
+    TensorArgs a;
+    a.n = s->n;
+    a.npad = s->npad;
+    a.preDii = s->preDii;
+    a.preDij = s->preDij;
+    a.ewald = s->p.ewald;
+    a.ec = make_ewald(s->p.box[0], s->inv_L[0], s->p.ewald_real);
+    return a;
+}
+
+template <typename T>
+__device__ __forceinline__ void tile_of(const TensorArgs& A, const double4* pos, int i, int j, T* t)
+{
+    const double4 pi = pos[i], pj = pos[j];
+    if (A.ewald) {
+        double d[6];
+        rpy_beenakker(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
+        for (int k = 0; k < 6; ++k) t[k] = (T)d[k];
+    } else if (i == j) {
+        const T d = (T)(A.preDii / pi.w);
+        t[0] = t[1] = t[2] = d;
+        t[3] = t[4] = t[5] = 0;
+    } else if (i > j) {
+        rpy_free<T>(pi, pj, (T)A.preDii, (T)A.preDij, t);
+    } else {
+        rpy_free<T>(pj, pi, (T)A.preDii, (T)A.preDij, t);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_build(TensorArgs A, const double4* __restrict__ pos, T* __restrict__ M,
+                                               double* __restrict__ dD)
+{
+    extern __shared__ __align__(16) unsigned char build_smem[];
+    T(*tile)[3 * TB + 1] = reinterpret_cast<T(*)[3 * TB + 1]>(build_smem);
+    const int I = blockIdx.y, J = blockIdx.x;
+    if (J > I) return;
+    const int tid = threadIdx.x;
+    const int n3 = 3 * A.n;
+    for (int p = tid; p < TB * TB; p += blockDim.x) {
+        const int li = p / TB, lj = p % TB;
+        const int i = I * TB + li, j = J * TB + lj;
+        T t[6] = {0, 0, 0, 0, 0, 0};
+        if (i < A.n && j < A.n) tile_of<T>(A, pos, i, j, t);
+        const int r = 3 * li, c = 3 * lj;
+        tile[r][c] = t[0];
+        tile[r + 1][c + 1] = t[1];
+        tile[r + 2][c + 2] = t[2];
+        tile[r][c + 1] = tile[r + 1][c] = t[3];
+        tile[r][c + 2] = tile[r + 2][c] = t[4];
+        tile[r + 1][c + 2] = tile[r + 2][c + 1] = t[5];
+    }
+    __syncthreads();
+    const int r0 = 3 * TB * I, c0 = 3 * TB * J;
+    for (int idx = tid; idx < 9 * TB * TB; idx += blockDim.x) {
+        const int r = idx / (3 * TB), c = idx % (3 * TB);
+        if (r0 + r < n3 && c0 + c < n3) M[(size_t)(r0 + r) * A.npad + c0 + c] = tile[r][c];
+    }
+    if (I != J) {
+        for (int idx = tid; idx < 9 * TB * TB; idx += blockDim.x) {
+            const int c = idx / (3 * TB), r = idx % (3 * TB);
+            if (r0 + r < n3 && c0 + c < n3) M[(size_t)(c0 + c) * A.npad + r0 + r] = tile[r][c];
+        }
+    } else {
+        for (int r = tid; r < 3 * TB; r += blockDim.x)
+            if (r0 + r < n3) dD[r0 + r] = (double)tile[r][r];
+    }
+}
+
+template <typename T>
+static size_t build_smem_bytes()
+{
+    return sizeof(T) * 3 * TB * (3 * TB + 1);
+}
+
+template <typename T>
+static size_t tea_smem_bytes()
+{
+    return sizeof(T) * TB * (TB + 1) * 6;
+}
+
+static int tensor_attrs();
+
+int tensor_build(bdb_system* s)
+{
+    int rc = tensor_attrs();
+    if (rc) return rc;
+    const TensorArgs A = targs(s);
+    const int nt = (s->n + TB - 1) / TB;
+    dim3 grid(nt, nt);
+    if (s->p.precision == BDB_PREC_FP64) {
+        k_build<double><<<grid, 256, build_smem_bytes<double>(), s->stream>>>(A, s->pos.p, s->M64.p, s->dD.p);
+    } else {
+        k_build<float><<<grid, 256, build_smem_bytes<float>(), s->stream>>>(A, s->pos.p, s->M32.p, s->dD.p);
+    }
+    BDB_CUDA(cudaGetLastError());
+    return BDB_OK;
+}
+
+__global__ void k_one_tile(TensorArgs A, const double4* pos, int i, int j, double* out)
+{
+    double t[6];
+    tile_of<double>(A, pos, i, j, t);
+    out[0] = t[0];
+    out[4] = t[1];
+    out[8] = t[2];
+    out[1] = out[3] = t[3];
+    out[2] = out[6] = t[4];
+    out[5] = out[7] = t[5];
+}
+
+int tensor_tile_host(bdb_system* s, int i, int j, double* tD)
+{
+    const TensorArgs A = targs(s);
+    double* d = s->work.p;
+    k_one_tile<<<1, 1, 0, s->stream>>>(A, s->pos.p, i, j, d);
+    BDB_CUDA(cudaGetLastError());
+    BDB_CUDA(cudaMemcpyAsync(tD, d, 9 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    BDB_CUDA(cudaStreamSynchronize(s->stream));
+    return BDB_OK;
+}
+
+// ------------------------------------------------------------------ TEA
+
+// part layout: record (9 doubles: Rf[3], C[3], Feff[3]) for (tile_other T,
+// bead b) of segment g at index  g.part_begin + T * g.count + (b - g.begin).
+struct TeaSeg {
+    int begin, count, ntile, part_begin;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__ segs,
+      const double4* __restrict__ pos, const double* __restrict__ F, const double* __restrict__ X,
+      double* __restrict__ part, double* __restrict__ eps_part, int want_rs)
+{
+    extern __shared__ __align__(16) unsigned char tea_smem[];
+    T(*tD)[TB + 1][6] = reinterpret_cast<T(*)[TB + 1][6]>(tea_smem);
+    __shared__ double sF[2][TB][3], sX[2][TB][3], sInv[2][TB];
+    __shared__ double sAcc[TB][9];
+    __shared__ double sEps[8];
+    const TileJob jb = jobs[blockIdx.x];
+    const TeaSeg g = segs[jb.seg];
+    const int tid = threadIdx.x;
+    const int bi0 = g.begin + jb.I * TB, bj0 = g.begin + jb.J * TB;
+    const int ni = min(TB, g.count - jb.I * TB), nj = min(TB, g.count - jb.J * TB);
+    const bool diag = jb.I == jb.J;
+    if (tid < TB) {
+        for (int side = 0; side < 2; ++side) {
+            const int b = (side ? bj0 : bi0) + tid;
+            const bool ok = tid < (side ? nj : ni);
+            for (int k = 0; k < 3; ++k) {
+                sF[side][tid][k] = ok ? F[3 * b + k] : 0.0;
+                sX[side][tid][k] = ok && want_rs ? X[3 * b + k] : 0.0;
+            }
+            sInv[side][tid] = ok ? pos[b].w / A.preDii : 0.0;   // 1/diag_D (diff_decl.c:94-99)
+        }
+    }
+    // phase 1: tiles
+    for (int p = tid; p < TB * TB; p += blockDim.x) {
+        const int li = p / TB, lj = p % TB;
+        T t[6] = {0, 0, 0, 0, 0, 0};
+        if (li < ni && lj < nj && (!diag || lj < li)) tile_of<T>(A, pos, bi0 + li, bj0 + lj, t);
+        for (int k = 0; k < 6; ++k) tD[li][lj][k] = t[k];
+    }
+    __syncthreads();
+    // phase 2: rows (into bead i of tile I), 8 lanes per row
+    const int row = tid >> 3, lane = tid & 7;
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double eps = 0;
+    for (int lj = lane; lj < TB; lj += 8) {
+        const T* t = tD[row][lj];
+        const double xx = t[0], yy = t[1], zz = t[2], xy = t[3], xz = t[4], yz = t[5];
+        const double* f = sF[1][lj];
+        const double* x = sX[1][lj];
+        const double inv = sInv[1][lj];
+        acc[0] += xx * f[0] + xy * f[1] + xz * f[2];
+        acc[1] += xy * f[0] + yy * f[1] + yz * f[2];
+        acc[2] += xz * f[0] + yz * f[1] + zz * f[2];
+        acc[3] += (xx * xx + xy * xy + xz * xz) * inv;
+        acc[4] += (xy * xy + yy * yy + yz * yz) * inv;
+        acc[5] += (xz * xz + yz * yz + zz * zz) * inv;
+        acc[6] += xx * x[0] + xy * x[1] + xz * x[2];
+        acc[7] += xy * x[0] + yy * x[1] + yz * x[2];
+        acc[8] += xz * x[0] + yz * x[1] + zz * x[2];
+        eps += xx + yy + zz + 2 * (xy + xz + yz);
+    }
+    for (int o = 1; o < 8; o <<= 1) {
+        for (int k = 0; k < 9; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+        eps += __shfl_xor_sync(0xffffffffu, eps, o);
+    }
+    if (lane == 0)
+        for (int k = 0; k < 9; ++k) sAcc[row][k] = acc[k];
+    // eps: one value per warp (rows 4w..4w+3), then fixed-order sum
+    {
+        double e = lane == 0 ? eps : 0.0;
+        for (int o = 8; o < 32; o <<= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        if ((tid & 31) == 0) sEps[tid >> 5] = e;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double e = 0;
+        for (int w = 0; w < 8; ++w) e += sEps[w];
+        eps_part[blockIdx.x] = e;
+    }
+    // write rows: record (T = J, bead in I); on the diagonal tile add the
+    // column sums below first
+    if (!diag) {
+        if (lane == 0 && row < ni) {
+            double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.J * g.count + jb.I * TB + row);
+            for (int k = 0; k < 9; ++k) dst[k] = sAcc[row][k];
+        }
+    }
+    // phase 3: columns (into bead j of tile J)
+    const int col = tid >> 3;
+    for (int k = 0; k < 9; ++k) acc[k] = 0;
+    for (int li = lane; li < TB; li += 8) {
+        const T* t = tD[li][col];
+        const double xx = t[0], yy = t[1], zz = t[2], xy = t[3], xz = t[4], yz = t[5];
+        const double* f = sF[0][li];
+        const double* x = sX[0][li];
+        const double inv = sInv[0][li];
+        acc[0] += xx * f[0] + xy * f[1] + xz * f[2];
+        acc[1] += xy * f[0] + yy * f[1] + yz * f[2];
+        acc[2] += xz * f[0] + yz * f[1] + zz * f[2];
+        acc[3] += (xx * xx + xy * xy + xz * xz) * inv;
+        acc[4] += (xy * xy + yy * yy + yz * yz) * inv;
+        acc[5] += (xz * xz + yz * yz + zz * zz) * inv;
+        acc[6] += xx * x[0] + xy * x[1] + xz * x[2];
+        acc[7] += xy * x[0] + yy * x[1] + yz * x[2];
+        acc[8] += xz * x[0] + yz * x[1] + zz * x[2];
+    }
+    for (int o = 1; o < 8; o <<= 1)
+        for (int k = 0; k < 9; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (lane == 0 && col < nj) {
+        double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.I * g.count + jb.J * TB + col);
+        if (diag) {
+            for (int k = 0; k < 9; ++k) dst[k] = acc[k] + sAcc[col][k];
+        } else {
+            for (int k = 0; k < 9; ++k) dst[k] = acc[k];
+        }
+    }
+}
+
+// eps -> beta per segment (diff_rand.c:197-217); scal[4g+0] = eps, [4g+1] = beta
+__global__ void k_eps_beta(const TeaSeg* __restrict__ segs, const int* __restrict__ job_begin,
+                           const double* __restrict__ eps_part, double* __restrict__ scal, unsigned* status)
+{
+    __shared__ double sh[256];
+    const TeaSeg g = segs[blockIdx.x];
+    const int b = job_begin[blockIdx.x], e = job_begin[blockIdx.x + 1];
+    double a = 0;
+    for (int k = b + threadIdx.x; k < e; k += blockDim.x) a += eps_part[k];
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const int n3 = 3 * g.count;
+        double eps = sh[0];
+        eps /= n3;
+        eps /= (n3 - 1);
+        eps *= 2;
+        if (eps > 1.0) eps = 1.0;
+        const double aa = (3 * g.count - 1) * eps * eps - (3 * g.count - 2) * eps;
+        double beta;
+        if (fabs(aa) < (double)0.0000001f) beta = 0.5;
+        else beta = (1 - sqrt(1 - aa)) / aa;
+        scal[4 * blockIdx.x] = eps;
+        scal[4 * blockIdx.x + 1] = beta;
+    }
+}
+
+__global__ void k_tea_finish(TensorArgs A, int n, const TeaSeg* __restrict__ segs, const int* __restrict__ bead_seg,
+                             const double* __restrict__ part, const double* __restrict__ scal,
+                             const double4* __restrict__ pos_in, const double* __restrict__ F,
+                             const double* __restrict__ X, double pre_f, int want_rs, int hydro,
+                             double* __restrict__ Rf, double* __restrict__ Rs)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int gi = bead_seg[i];
+    const TeaSeg g = segs[gi];
+    const int local = i - g.begin;
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (hydro) {
+        for (int T = 0; T < g.ntile; ++T) {
+            const double* src = part + 9 * ((size_t)g.part_begin + (size_t)T * g.count + local);
+            for (int k = 0; k < 9; ++k) acc[k] += src[k];
+        }
+    }
+    // self tile: D.F uses only its diagonal (diff_equation.c:96-102)
+    double self[6];
+    tile_of<double>(A, pos_in, i, i, self);
+    const double d = A.preDii / pos_in[i].w;   // diag_D (diff_decl.c:94-99)
+    const double inv_d = 1 / d;
+    for (int k = 0; k < 3; ++k) {
+        double rf = hydro ? acc[k] + F[3 * i + k] * self[k] : d * F[3 * i + k];
+        Rf[3 * i + k] = hydro ? rf * pre_f : pre_f * d * F[3 * i + k];
+    }
+    if (want_rs && !hydro) {
+        // DIFF_NONE (diff_rand.c:55-63): X already carries sqrt(2 dt D_ii)
+        for (int k = 0; k < 3; ++k) Rs[3 * i + k] = X[3 * i + k];
+    } else if (want_rs) {
+        const double beta = scal[4 * gi + 1];
+        for (int k = 0; k < 3; ++k) {
+            double c = acc[3 + k] * (beta * beta * inv_d);
+            c = 1 / (1 + c);
+            c = sqrt(c);
+            Rs[3 * i + k] = c * (beta * acc[6 + k] + d * X[3 * i + k]);
+        }
+    }
+}
+
+int tea_setup(bdb_system* s);
+
+int tea_run(bdb_system* s, bool want_rs)
+{
+    if (!s->tea_meta.p) {
+        int rc = tea_setup(s);
+        if (rc) return rc;
+    }
+    int rc0 = tensor_attrs();
+    if (rc0) return rc0;
+    const TensorArgs A = targs(s);
+    TeaSeg* tsegs = reinterpret_cast<TeaSeg*>(s->tea_meta.p);
+    if (s->p.hydro && s->n_jobs) {
+        if (s->p.precision == BDB_PREC_FP64 || s->p.ewald)
+            k_tea<double><<<s->n_jobs, 256, tea_smem_bytes<double>(), s->stream>>>(A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p,
+                                                           s->part.p, s->eps_part.p, want_rs);
+        else
+            k_tea<float><<<s->n_jobs, 256, tea_smem_bytes<float>(), s->stream>>>(A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p,
+                                                          s->part.p, s->eps_part.p, want_rs);
+        BDB_CUDA(cudaGetLastError());
+        if (want_rs) {
+            const int* job_begin = reinterpret_cast<const int*>(tsegs + s->segs.size());
+            k_eps_beta<<<(int)s->segs.size(), 256, 0, s->stream>>>(tsegs, job_begin, s->eps_part.p, s->scal.p + 64,
+                                                                   s->status.p);
+            BDB_CUDA(cudaGetLastError());
+        }
+    }
+    const double pre_f = s->p.dt / (BDB_KB * s->p.T);
+    k_tea_finish<<<(s->n + 127) / 128, 128, 0, s->stream>>>(A, s->n, tsegs, s->d_bead_seg.p, s->part.p, s->scal.p + 64,
+                                                            s->pos.p, s->F.p, s->X.p, pre_f, want_rs,
+                                                            s->p.hydro, s->Rf.p, s->Rs.p);
+    BDB_CUDA(cudaGetLastError());
+    return BDB_OK;
+}
+
+// Work list and scratch layout for k_tea: the TeaSeg table followed by the
+// per-segment job offsets, in tea_meta.
+int tea_setup(bdb_system* s)
+{
+    std::vector<TileJob> jobs;
+    std::vector<TeaSeg> ts;
+    std::vector<int> job_begin;
+    size_t part_records = 0;
+    for (size_t g = 0; g < s->segs.size(); ++g) {
+        const Segment& sg = s->segs[g];
+        TeaSeg t;
+        t.begin = sg.begin;
+        t.count = sg.count;
+        t.ntile = (sg.count + TB - 1) / TB;
+        t.part_begin = (int)part_records;
+        part_records += (size_t)t.ntile * sg.count;
+        ts.push_back(t);
+        job_begin.push_back((int)jobs.size());
+        for (int I = 0; I < t.ntile; ++I)
+            for (int J = 0; J <= I; ++J) jobs.push_back(TileJob{(int)g, I, J});
+    }
+    job_begin.push_back((int)jobs.size());
+    s->n_jobs = (int)jobs.size();
+    if (s->jobs.alloc(std::max<size_t>(1, jobs.size()))) return BDB_ERR_NOMEM;
+    if (s->eps_part.alloc(std::max<size_t>(1, jobs.size()))) return BDB_ERR_NOMEM;
+    if (s->part.alloc(std::max<size_t>(9, 9 * part_records))) return BDB_ERR_NOMEM;
+    const size_t head = sizeof(TeaSeg) * ts.size() + sizeof(int) * job_begin.size();
+    if (s->tea_meta.alloc(head)) return BDB_ERR_NOMEM;
+    BDB_CUDA(cudaMemcpy(s->jobs.p, jobs.data(), sizeof(TileJob) * jobs.size(), cudaMemcpyHostToDevice));
+    BDB_CUDA(cudaMemcpy(s->tea_meta.p, ts.data(), sizeof(TeaSeg) * ts.size(), cudaMemcpyHostToDevice));
+    BDB_CUDA(cudaMemcpy(s->tea_meta.p + sizeof(TeaSeg) * ts.size(), job_begin.data(),
+                        sizeof(int) * job_begin.size(), cudaMemcpyHostToDevice));
+    return BDB_OK;
+}
+
+static int tensor_attrs()
+{
+    static bool done = false;
+    if (done) return BDB_OK;
+    BDB_CUDA(cudaFuncSetAttribute(k_build<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)build_smem_bytes<double>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_build<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)build_smem_bytes<float>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_tea<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tea_smem_bytes<double>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_tea<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tea_smem_bytes<float>()));
+    done = true;
+    return BDB_OK;
+}
+
+}  // namespace bdb

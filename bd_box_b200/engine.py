@@ -1,0 +1,261 @@
+"""ctypes binding of libbdb200.so and a host mirror of BD_BOX's hot-path API.
+
+``System`` wraps one ``bdb_system`` (include/bdb200.h) built from a BD_BOX
+deck. Its methods carry the names and meaning of the reference functions
+they stand for:
+
+=====================  ==========================================================
+method                 reference
+=====================  ==========================================================
+``compute_forces``     compute_forces (potentials/calc_func.c:106-186)
+``compute_D``          compute_D / compute_single_D (diff_alg/diff_tensor.c:472-544)
+``compute_Dij``        compute_Dij (diff_tensor.c:437-470)
+``compute_Rf``         compute_Rf (diff_alg/diff_equation.c:119-214)
+``compute_r``          compute_r (diff_alg/diff_rand.c:47-236)
+``step``               comp_step_ermak + compute_hydro_ermak, no retries
+``compute_hydro``      comp_step_ermak with the overlap retry loop (diff_comp.c:152-179)
+``save_curr_coord``    save_curr_coord + save_curr_forces (diff_decl.c:219-227)
+``load_coord``         load_coord + load_forces (diff_decl.c:229-237)
+=====================  ==========================================================
+
+Errors raise ``BDBError`` instead of exiting (the reference's UNERR,
+err.c:48-90). The CUDA library is required: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import decks as _decks
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbdb200.so")
+
+PREC_FP64, PREC_MIXED = 0, 1
+NOISE_PHILOX, NOISE_HOST = 0, 1
+
+EXPORTS = [
+    "bdb_version", "bdb_last_error", "bdb_create", "bdb_destroy", "bdb_set_bonded",
+    "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
+    "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
+    "bdb_compute_r", "bdb_step", "bdb_factor_error", "bdb_phase_ms", "bdb_stream",
+]
+
+
+class BDBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"bdb error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("bc", C.c_int), ("box", C.c_double * 3),
+        ("hydro", C.c_int), ("ewald", C.c_int), ("ewald_real", C.c_int),
+        ("T", C.c_double), ("visc", C.c_double), ("vfactor", C.c_double), ("dt", C.c_double),
+        ("elec", C.c_int), ("epsilon_c", C.c_double), ("kappa_c", C.c_double),
+        ("gamma_c", C.c_double), ("cutoff_c", C.c_double),
+        ("alpha_lj", C.c_double), ("cutoff_lj", C.c_double), ("lj_6_term", C.c_int),
+        ("bond_lj_scale", C.c_double), ("bond_c_scale", C.c_double),
+        ("check_overlap", C.c_int), ("nb_list", C.c_int), ("max_force_cutoff", C.c_double),
+        ("precision", C.c_int), ("refresh", C.c_int), ("noise", C.c_int), ("seed", C.c_uint64),
+    ]
+
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libbdb200.so; raise if it is missing (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m bd_box_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(path)
+    lib.bdb_version.restype = C.c_char_p
+    lib.bdb_last_error.restype = C.c_char_p
+    lib.bdb_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Params), _dp, _dp, _dp]
+    lib.bdb_destroy.argtypes = [C.c_void_p]
+    lib.bdb_set_bonded.argtypes = [C.c_void_p] + [C.c_int, _ip, _dp] * 5
+    for name in ("bdb_set_coord", "bdb_get_coord"):
+        getattr(lib, name).argtypes = [C.c_void_p, _dp]
+    lib.bdb_save_state.argtypes = [C.c_void_p]
+    lib.bdb_load_state.argtypes = [C.c_void_p]
+    lib.bdb_compute_forces.argtypes = [C.c_void_p, _dp, _dp, C.POINTER(C.c_longlong)]
+    lib.bdb_compute_D.argtypes = [C.c_void_p, _dp]
+    lib.bdb_compute_Dij.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+    lib.bdb_compute_Rf.argtypes = [C.c_void_p, _dp]
+    lib.bdb_compute_r.argtypes = [C.c_void_p, _dp, _dp]
+    lib.bdb_step.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.bdb_factor_error.argtypes = [C.c_void_p, _dp]
+    lib.bdb_phase_ms.argtypes = [C.c_void_p, C.c_char_p, _dp]
+    lib.bdb_stream.argtypes = [C.c_void_p]
+    lib.bdb_stream.restype = C.c_void_p
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _ip_(a):
+    return None if a is None or a.size == 0 else a.ctypes.data_as(_ip)
+
+
+def params_from_deck(deck, precision=PREC_FP64, refresh=1, noise=NOISE_PHILOX, seed=None) -> Params:
+    p = deck.prm
+    P = Params()
+    P.n = deck.n
+    P.bc = 1 if p["bc"] == 1 else 0
+    for k in range(3):
+        P.box[k] = deck.box[k]
+    P.hydro = p["hydro"]
+    P.ewald = deck.ewald
+    P.ewald_real = p["ewald_real"]
+    P.T, P.visc, P.vfactor, P.dt = p["T"], p["visc"], p["vfactor"], p["dt"]
+    P.elec = p["elec"]
+    P.epsilon_c, P.kappa_c, P.gamma_c, P.cutoff_c = p["epsilon_c"], p["kappa_c"], p["gamma_c"], p["cutoff_c"]
+    P.alpha_lj, P.cutoff_lj, P.lj_6_term = p["alpha_lj"], p["cutoff_lj"], p["lj_6_term"]
+    P.bond_lj_scale, P.bond_c_scale = p["bond_lj_scale"], p["bond_c_scale"]
+    P.check_overlap = p["check_overlap"]
+    P.nb_list = p["nb_list"]
+    P.max_force_cutoff = deck.max_force_cutoff
+    P.precision = precision
+    P.refresh = refresh
+    P.noise = noise
+    P.seed = p["rand_seed"] if seed is None else seed
+    return P
+
+
+class System:
+    """One bead system resident on the current CUDA device."""
+
+    def __init__(self, deck, precision=PREC_FP64, refresh=1, noise=NOISE_PHILOX, seed=None):
+        self.lib = load_library()
+        self.deck = deck
+        self.n = deck.n
+        self.params = params_from_deck(deck, precision, refresh, noise, seed)
+        h = C.c_void_p()
+        coord = np.ascontiguousarray(deck.coord, dtype=np.float64)
+        rc = self.lib.bdb_create(C.byref(h), C.byref(self.params), _p(coord),
+                                 _p(np.ascontiguousarray(deck.Q, dtype=np.float64)),
+                                 _p(np.ascontiguousarray(deck.LJ, dtype=np.float64)))
+        self._check(rc)
+        self.h = h
+        self._bonded = [np.ascontiguousarray(a, dtype=t) for a, t in (
+            (deck.bond_pairs, np.int32), (deck.bond_parms, np.float64),
+            (deck.angle_pairs, np.int32), (deck.angle_parms, np.float64),
+            (deck.angle_cos_pairs, np.int32), (deck.angle_cos_parms, np.float64),
+            (deck.dihe_pairs, np.int32), (deck.dihe_parms, np.float64),
+            (deck.dihe_angle_pairs, np.int32), (deck.dihe_angle_parms, np.float64))]
+        b = self._bonded
+        args = []
+        for k in range(5):
+            args += [len(b[2 * k]), _ip_(b[2 * k]), _p(b[2 * k + 1]) if b[2 * k + 1].size else None]
+        self._check(self.lib.bdb_set_bonded(self.h, *args))
+
+    def _check(self, rc):
+        if rc < 0:
+            raise BDBError(rc, self.lib.bdb_last_error().decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bdb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n3(self):
+        return 3 * self.n
+
+    # -- state --------------------------------------------------------------
+    def get_coord(self) -> np.ndarray:
+        out = np.zeros((self.n, 4))
+        self._check(self.lib.bdb_get_coord(self.h, _p(out)))
+        return out
+
+    def set_coord(self, coord):
+        c = np.ascontiguousarray(coord, dtype=np.float64).reshape(self.n, 4)
+        self._check(self.lib.bdb_set_coord(self.h, _p(c)))
+
+    def save_curr_coord(self):
+        self._check(self.lib.bdb_save_state(self.h))
+
+    def load_coord(self):
+        self._check(self.lib.bdb_load_state(self.h))
+
+    # -- reference entry points --------------------------------------------
+    def compute_forces(self, energies: bool = True):
+        F = np.zeros(self.n3)
+        E = np.zeros(9) if energies else None
+        counts = (C.c_longlong * 2)()
+        rep = self._check(self.lib.bdb_compute_forces(self.h, _p(F), _p(E), counts))
+        return F, E, rep, (int(counts[0]), int(counts[1]))
+
+    def compute_D(self) -> np.ndarray:
+        D = np.zeros((self.n3, self.n3))
+        self._check(self.lib.bdb_compute_D(self.h, _p(D)))
+        return D
+
+    def compute_Dij(self, i, j) -> np.ndarray:
+        out = np.zeros(9)
+        self._check(self.lib.bdb_compute_Dij(self.h, i, j, _p(out)))
+        return out.reshape(3, 3)
+
+    def compute_Rf(self) -> np.ndarray:
+        out = np.zeros(self.n3)
+        self._check(self.lib.bdb_compute_Rf(self.h, _p(out)))
+        return out
+
+    def compute_r(self, gauss=None) -> np.ndarray:
+        out = np.zeros(self.n3)
+        g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
+        self._check(self.lib.bdb_compute_r(self.h, _p(g), _p(out)))
+        return out
+
+    def step(self, K: int = 1, gauss=None) -> int:
+        g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
+        return self._check(self.lib.bdb_step(self.h, K, _p(g)))
+
+    def compute_hydro(self, gauss_attempts=None, move_attempts=None) -> int:
+        """One step with comp_step_ermak's retry loop: on an overlap the saved
+        coordinates and forces come back and a new noise vector is drawn
+        (dt halving of ermak_var is not modelled). Returns the attempts used."""
+        limit = self.deck.prm["move_attempts"] if move_attempts is None else move_attempts
+        count = 0
+        self.save_curr_coord()
+        while True:
+            g = None if gauss_attempts is None else gauss_attempts[count]
+            if not self.step(1, g):
+                return count + 1
+            self.load_coord()
+            count += 1
+            if count > limit:
+                raise BDBError(-5, "Wrong conformation, can't move")
+
+    def factor_error(self) -> float:
+        out = C.c_double()
+        self._check(self.lib.bdb_factor_error(self.h, C.byref(out)))
+        return out.value
+
+    def phase_ms(self, name="step") -> float:
+        out = C.c_double()
+        self._check(self.lib.bdb_phase_ms(self.h, name.encode(), C.byref(out)))
+        return out.value
+
+
+def open_deck(prm_path: str, overrides=None, **kw) -> System:
+    return System(_decks.read_deck(prm_path, overrides), **kw)

@@ -1,0 +1,166 @@
+/* bdb200 -- B200-native Brownian-dynamics step for BD_BOX decks (C ABI).
+ *
+ * Two layers are declared here.
+ *
+ * 1. The engine ABI (bdb_*): plain pointers and sizes, no CUDA or torch
+ *    types. One bdb_system holds one bead system (or a batch of independent
+ *    replicas) resident on the current CUDA device. Host arrays use BD_BOX's
+ *    layouts: coord is double[4N] (x, y, z, hydrodynamic radius; data.h:315),
+ *    Q double[N], LJ double[2N] (sigma_LJ/2, epsilon_LJ; data.c:97-100),
+ *    forces double[3N], energies double[BDB_E_LAST+1] indexed like
+ *    enum ENERGY_TYPE (data.h:278-289), diffusion tensors double[3N*3N]
+ *    row-major and symmetric.
+ *
+ * 2. The BD_BOX drop-in (libbdb200_bdbox.a): the reference's own extern "C"
+ *    entry points of src/diff_alg and src/potentials (diff_tensor.h:166-253,
+ *    calc_func.h:60-106), implemented on the engine and linked in place of
+ *    the CPU translation units, exactly as BD_BOX swaps its CUDA build in
+ *    (src/Makefile.am:44-78). Those symbols read BD_BOX's globals, so they
+ *    are declared at the end of this header only for BDB_DROPIN builds.
+ *
+ * Every bdb_* call returns BDB_OK (0) or a negative BDB_ERR_* code;
+ * bdb_last_error() gives the message of the last failure on this thread.
+ * No call exits the process (the reference's UNERR, err.c:48-90, does).
+ */
+#ifndef BDB200_H
+#define BDB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BDB_OK 0
+#define BDB_ERR_ARG (-1)       /* invalid argument or size */
+#define BDB_ERR_CUDA (-2)      /* CUDA runtime error */
+#define BDB_ERR_NOT_SPD (-3)   /* Cholesky met a non-positive pivot (diff_rand.c:78-79) */
+#define BDB_ERR_BOND (-4)      /* over-stretched FENE bond (bond.c:73-78) */
+#define BDB_ERR_STATE (-5)     /* call out of order (e.g. no coordinates yet) */
+#define BDB_ERR_NOMEM (-6)     /* device allocation failed */
+#define BDB_ERR_TIMEOUT (-7)   /* a bounded device wait gave up */
+#define BDB_ERR_UNSUPPORTED (-8)
+
+/* energy slots, enum ENERGY_TYPE (data.h:278-289) */
+enum { BDB_E_NONE, BDB_E_BOND, BDB_E_ANGLE, BDB_E_ANGLE_COS, BDB_E_DIHE,
+       BDB_E_DIHE_ANGLE, BDB_E_LJ, BDB_E_COULOMB, BDB_E_LAST };
+
+/* hydrodynamic methods, DIFF_* (diff_tensor.h:44-52) */
+enum { BDB_HYDRO_NONE = 0, BDB_HYDRO_CHOLESKY = 1, BDB_HYDRO_GEYER = 2 };
+
+/* arithmetic of the diffusion part of the step */
+enum {
+    BDB_PREC_FP64 = 0,   /* everything in FP64 (the plain GPU path) */
+    BDB_PREC_MIXED = 1   /* FP32 tensor and stored D/L, 3xTF32 tcgen05 Cholesky
+                            updates with FP64 diagonal tiles, FP64 sums */
+};
+
+/* noise sources */
+enum {
+    BDB_NOISE_PHILOX = 0,  /* Philox-4x32-10 Gaussians generated on the device */
+    BDB_NOISE_HOST = 1     /* caller passes 3N Gaussians per step (parity runs) */
+};
+
+/* Parameters of one system: the .prm keys the hot path reads (after BD_BOX's
+ * float rounding of DOUBLE keys, input.c:1010-1013) plus engine choices. */
+typedef struct {
+    int n;                    /* beads */
+    int bc;                   /* 0 none, 1 periodic box (trans.h:43-63) */
+    double box[3];            /* xbox, ybox, zbox */
+    int hydro;                /* BDB_HYDRO_* */
+    int ewald;                /* 1: Beenakker Ewald tensor (periodic, hydro != none) */
+    int ewald_real;           /* lattice radius R (ewald_real == ewald_recip, 0..5) */
+    double T, visc, vfactor, dt;
+    int elec;                 /* Debye-Hueckel on */
+    double epsilon_c, kappa_c, gamma_c, cutoff_c;
+    double alpha_lj, cutoff_lj;
+    int lj_6_term;
+    double bond_lj_scale, bond_c_scale;
+    int check_overlap;
+    int nb_list;              /* 0 all pairs, otherwise cell list */
+    double max_force_cutoff;  /* cell size (init_cutoff, pre_func.c:197-232) */
+    /* engine choices; no reference counterpart */
+    int precision;            /* BDB_PREC_* */
+    int refresh;              /* rebuild D and its factor every `refresh` steps (>= 1) */
+    int noise;                /* BDB_NOISE_* */
+    uint64_t seed;            /* Philox key */
+} bdb_params;
+
+typedef struct bdb_system bdb_system;
+
+/* Library identity and the last error message on this thread. */
+const char* bdb_version(void);
+const char* bdb_last_error(void);
+
+/* Create a system on the current device from host arrays (copied).
+ * Replaces init_diff_tensor (diff_decl.c:83-175) + init_forces
+ * (calc_func.c:411-415) + init_cuda (cuda.c:88-148). */
+int bdb_create(bdb_system** out, const bdb_params* p, const double* coord,
+               const double* Q, const double* LJ);
+int bdb_destroy(bdb_system* s);   /* free_diff_tensor + free_forces + free_cuda */
+
+/* Bonded terms, BD_BOX's arrays as read by read_str_file (input.c:567-641):
+ * bond_pairs int[2B], bond_parms double[3B] (r0, rmax, H) (bond.c:94-111);
+ * angle_pairs int[3A], angle_parms double[2A] (phi0 [rad], k) (angle.c:88-100);
+ * angle_cos_* (cos phi0, k) (angle_cos.c:84-97); dihe_pairs int[4D],
+ * dihe_parms (-k*delta, m) (dihe.c:188-209); dihe_angle_* (k, theta0 [rad])
+ * (dihe_angle.c:257-276). Counts may be 0 and pointers NULL. */
+int bdb_set_bonded(bdb_system* s,
+                   int n_bond, const int* bond_pairs, const double* bond_parms,
+                   int n_angle, const int* angle_pairs, const double* angle_parms,
+                   int n_angle_cos, const int* angle_cos_pairs, const double* angle_cos_parms,
+                   int n_dihe, const int* dihe_pairs, const double* dihe_parms,
+                   int n_dihe_angle, const int* dihe_angle_pairs, const double* dihe_angle_parms);
+
+/* Host <-> device coordinates (double[4N]); save_curr_coord/load_coord
+ * (diff_decl.c:219-237) keep a device copy instead. */
+int bdb_set_coord(bdb_system* s, const double* coord);
+int bdb_get_coord(bdb_system* s, double* coord);
+int bdb_save_state(bdb_system* s);     /* save_curr_coord + save_curr_forces */
+int bdb_load_state(bdb_system* s);     /* load_coord + load_forces */
+
+/* compute_forces (calc_func.c:106-186): forces at the current coordinates
+ * into the device force buffer; optional host copies of F (3N), E
+ * (BDB_E_LAST+1) and the pair counts {pairs with r <= cutoff_c, pairs in the
+ * LJ range of force_single (calc_func.c:378-395)}. Returns the overlap/NaN
+ * flag (0 or 1) or a negative error. */
+int bdb_compute_forces(bdb_system* s, double* F, double* E, long long* counts);
+
+/* compute_D / compute_single_D (diff_tensor.c:472-544): the full symmetric
+ * 3N x 3N tensor at the current coordinates, row-major, into host D. */
+int bdb_compute_D(bdb_system* s, double* D);
+
+/* compute_Dij (diff_tensor.c:437-470): one 3x3 tile, row-major. */
+int bdb_compute_Dij(bdb_system* s, int i, int j, double* tD);
+
+/* compute_Rf (diff_equation.c:119-214): Rf = dt/(kB T) D.F with the current
+ * forces, into host Rf (3N). Cholesky systems use the stored D (rebuilt if
+ * stale), Geyer/none recompute the tiles on the fly. */
+int bdb_compute_Rf(bdb_system* s, double* Rf);
+
+/* compute_r (diff_rand.c:47-236): random displacement Rs (3N) from 3N unit
+ * Gaussians `gauss` (host; NULL draws Philox), into host Rs. */
+int bdb_compute_r(bdb_system* s, const double* gauss, double* Rs);
+
+/* Ermak-McCammon steps (comp_step_ermak + compute_hydro_ermak,
+ * diff_comp.c:152-179, diff_equation.c:216-286): K steps on the device.
+ * gauss: K*3N host Gaussians when noise == BDB_NOISE_HOST, else NULL.
+ * Returns the OR of the overlap flags of the steps (retries are the
+ * caller's, as in comp_step_ermak) or a negative error. */
+int bdb_step(bdb_system* s, int K, const double* gauss);
+
+/* Cholesky of the stored tensor at the current coordinates (diagnostics):
+ * rel_err = ||L L^T - D||_F / ||D||_F evaluated on the device in FP64. */
+int bdb_factor_error(bdb_system* s, double* rel_err);
+
+/* Timing hooks for measurement: last-call device durations in ms of the
+ * named phases ("build", "factor", "matvec", "forces", "tea", "step"). */
+int bdb_phase_ms(bdb_system* s, const char* phase, double* ms);
+
+/* The CUDA stream all work of this system is issued on (cudaStream_t). */
+void* bdb_stream(bdb_system* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BDB200_H */
