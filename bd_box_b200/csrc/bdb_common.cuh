@@ -124,10 +124,15 @@ struct bdb_system {
     // noise
     uint64_t philox_counter = 0;
 
-    // timing
-    cudaEvent_t ev[8];
-    bool events = false;
-    double phase_ms[8] = {0};
+    // measurement: CUDA-event pairs per phase, kernel launch count
+    struct PhaseRec {
+        std::vector<cudaEvent_t> ev;   // begin/end pairs
+        size_t used = 0;
+    };
+    PhaseRec phases[16];
+    bool profiling = false;
+    long long launches = 0;
+    bdb::DevBuf<double> gbuf;          // device copy of caller Gaussians
 };
 
 namespace bdb {
@@ -162,6 +167,8 @@ __device__ __forceinline__ double sq3(const double* v)
 
 // kernel entry points used across translation units
 namespace bdb {
+enum Phase { P_STEP, P_REFRESH, P_BUILD, P_FACTOR, P_MATVEC, P_TEA, P_FORCES, P_NOISE, P_UPDATE, P_COUNT };
+void phase_mark(bdb_system* s, int phase);   // records begin/end events when profiling
 int forces_setup(bdb_system* s);
 int forces_run(bdb_system* s, bool want_energy, bool want_counts);
 int bonded_setup(bdb_system* s);

@@ -162,36 +162,69 @@ int factor_run(bdb_system* s)
             }
         }
     }
+    s->launches += 3 * nb - 2;
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;
 }
 
-// ||L L^T - D||_F / ||D||_F with L from the lower triangle and D from the
-// upper triangle + dD; one thread per (row, column >= row) element, FP64.
+// ||L L^T - D||_F / ||D||_F in FP64 over 64x64 tiles (bi >= bj) of the
+// lower triangle: L from the lower triangle of M, D from its upper triangle
+// (mirrored) and dD on the diagonal.
 template <typename T>
-__global__ void k_factor_err(const T* __restrict__ M, const double* __restrict__ dD, int n3, int npad,
-                             double* __restrict__ acc)
+__global__ void __launch_bounds__(256) k_llt_err(const T* __restrict__ M, const double* __restrict__ dD, int n3,
+                                                 int npad, double* __restrict__ acc)
 {
-    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    double num = 0, den = 0;
-    if (idx < (size_t)n3 * n3) {
-        const int r = (int)(idx / n3), c = (int)(idx % n3);
-        if (c >= r) {
-            double s = 0;
-            for (int m = 0; m <= r; ++m) s += (double)M[(size_t)r * npad + m] * (double)M[(size_t)c * npad + m];
-            const double d = c == r ? dD[r] : (double)M[(size_t)r * npad + c];
-            const double w = c == r ? 1.0 : 2.0;
-            num = w * (s - d) * (s - d);
-            den = w * d * d;
+    const int bi = blockIdx.y, bj = blockIdx.x;
+    if (bj > bi) return;
+    constexpr int KC = 32;
+    __shared__ double As[KC][NB + 1];
+    __shared__ double Bs[KC][NB + 1];
+    __shared__ double red[2][8];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    double s[4][4];
+    for (int q = 0; q < 4; ++q)
+        for (int p = 0; p < 4; ++p) s[q][p] = 0;
+    const int mend = (bj + 1) * NB;   // L[c][m] = 0 beyond the column block's diagonal
+    for (int m0 = 0; m0 < mend; m0 += KC) {
+        __syncthreads();
+        for (int idx = tid; idx < NB * KC; idx += 256) {
+            const int r = idx / KC, m = idx % KC;
+            const int gr = bi * NB + r, gc = bj * NB + r, gm = m0 + m;
+            As[m][r] = (gm <= gr && gr < n3) ? (double)M[(size_t)gr * npad + gm] : 0.0;
+            Bs[m][r] = (gm <= gc && gc < n3) ? (double)M[(size_t)gc * npad + gm] : 0.0;
         }
+        __syncthreads();
+        for (int m = 0; m < KC; ++m)
+            for (int q = 0; q < 4; ++q)
+                for (int p = 0; p < 4; ++p) s[q][p] += As[m][ty + 16 * q] * Bs[m][tx + 16 * p];
     }
+    double num = 0, den = 0;
+    for (int q = 0; q < 4; ++q)
+        for (int p = 0; p < 4; ++p) {
+            const int r = bi * NB + ty + 16 * q, c = bj * NB + tx + 16 * p;
+            if (r >= n3 || c >= n3 || c > r) continue;
+            const double d = r == c ? dD[r] : (double)M[(size_t)c * npad + r];
+            const double w = r == c ? 1.0 : 2.0;
+            num += w * (s[q][p] - d) * (s[q][p] - d);
+            den += w * d * d;
+        }
     for (int o = 16; o > 0; o >>= 1) {
         num += __shfl_xor_sync(0xffffffffu, num, o);
         den += __shfl_xor_sync(0xffffffffu, den, o);
     }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&acc[0], num);
-        atomicAdd(&acc[1], den);
+    if ((tid & 31) == 0) {
+        red[0][tid >> 5] = num;
+        red[1][tid >> 5] = den;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double a = 0, b = 0;
+        for (int w = 0; w < 8; ++w) {
+            a += red[0][w];
+            b += red[1][w];
+        }
+        atomicAdd(&acc[0], a);
+        atomicAdd(&acc[1], b);
     }
 }
 
@@ -199,12 +232,12 @@ int factor_error(bdb_system* s, double* rel)
 {
     double* acc = s->scal.p + 40;
     BDB_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(double), s->stream));
-    const size_t tot = (size_t)s->n3 * s->n3;
-    const int blocks = (int)((tot + 255) / 256);
+    const int nb = (s->n3 + NB - 1) / NB;
+    dim3 grid(nb, nb);
     if (s->p.precision == BDB_PREC_FP64)
-        k_factor_err<double><<<blocks, 256, 0, s->stream>>>(s->M64.p, s->dD.p, s->n3, s->npad, acc);
+        k_llt_err<double><<<grid, 256, 0, s->stream>>>(s->M64.p, s->dD.p, s->n3, s->npad, acc);
     else
-        k_factor_err<float><<<blocks, 256, 0, s->stream>>>(s->M32.p, s->dD.p, s->n3, s->npad, acc);
+        k_llt_err<float><<<grid, 256, 0, s->stream>>>(s->M32.p, s->dD.p, s->n3, s->npad, acc);
     BDB_CUDA(cudaGetLastError());
     double h[2];
     BDB_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s->stream));

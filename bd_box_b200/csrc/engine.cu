@@ -69,6 +69,21 @@ template struct DevBuf<int4>;
 template struct DevBuf<Segment>;
 template struct DevBuf<TileJob>;
 
+static const char* kPhaseNames[P_COUNT] = {"step", "refresh", "build", "factor", "matvec",
+                                           "tea", "forces", "noise", "update"};
+
+void phase_mark(bdb_system* s, int ph)
+{
+    if (!s->profiling) return;
+    auto& r = s->phases[ph];
+    if (r.used == r.ev.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        r.ev.push_back(e);
+    }
+    cudaEventRecord(r.ev[r.used++], s->stream);
+}
+
 static int check_status(bdb_system* s, bool* overlap)
 {
     unsigned st = 0;
@@ -107,41 +122,56 @@ static int refresh_factor(bdb_system* s)
 {
     int rc = ensure_matrix(s);
     if (rc) return rc;
+    phase_mark(s, P_REFRESH);
+    phase_mark(s, P_BUILD);
     rc = tensor_build(s);
     if (rc) return rc;
+    phase_mark(s, P_BUILD);
+    phase_mark(s, P_FACTOR);
     rc = factor_run(s);
     if (rc) return rc;
+    phase_mark(s, P_FACTOR);
+    phase_mark(s, P_REFRESH);
     s->factor_valid = true;
     s->steps_since_refresh = 0;
     return BDB_OK;
 }
 
+static int forces_phase(bdb_system* s)
+{
+    phase_mark(s, P_FORCES);
+    int rc = forces_run(s, false, false);
+    phase_mark(s, P_FORCES);
+    return rc;
+}
+
 static int one_step(bdb_system* s, const double* dev_gauss)
 {
     int rc;
-    if (!s->have_forces) {
-        rc = forces_run(s, false, false);
-        if (rc) return rc;
-    }
+    if (!s->have_forces && (rc = forces_phase(s))) return rc;
     if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
         if (!s->factor_valid || s->steps_since_refresh >= std::max(1, s->p.refresh)) {
             rc = refresh_factor(s);
             if (rc) return rc;
         }
-        rc = noise_fill(s, dev_gauss);
-        if (rc) return rc;
-        rc = stored_matvec(s, true);
-        if (rc) return rc;
+    }
+    phase_mark(s, P_NOISE);
+    if ((rc = noise_fill(s, dev_gauss))) return rc;
+    phase_mark(s, P_NOISE);
+    if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
+        phase_mark(s, P_MATVEC);
+        if ((rc = stored_matvec(s, true))) return rc;
+        phase_mark(s, P_MATVEC);
         s->steps_since_refresh++;
     } else {
-        rc = noise_fill(s, dev_gauss);
-        if (rc) return rc;
-        rc = tea_run(s, true);
-        if (rc) return rc;
+        phase_mark(s, P_TEA);
+        if ((rc = tea_run(s, true))) return rc;
+        phase_mark(s, P_TEA);
     }
-    rc = update_positions(s);
-    if (rc) return rc;
-    return forces_run(s, false, false);
+    phase_mark(s, P_UPDATE);
+    if ((rc = update_positions(s))) return rc;
+    phase_mark(s, P_UPDATE);
+    return forces_phase(s);
 }
 
 }  // namespace bdb
@@ -225,8 +255,6 @@ int bdb_create(bdb_system** out, const bdb_params* p, const double* coord, const
     TRY(forces_setup(s));
     TRY(bonded_setup(s));
     BDB_CUDA(cudaMemset(s->status.p, 0, sizeof(unsigned) * 4));
-    for (int k = 0; k < 8; ++k) cudaEventCreate(&s->ev[k]);
-    s->events = true;
 #undef TRY
 #undef TRYA
     *out = s;
@@ -237,8 +265,8 @@ int bdb_destroy(bdb_system* s)
 {
     if (!s) return BDB_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
-    if (s->events)
-        for (int k = 0; k < 8; ++k) cudaEventDestroy(s->ev[k]);
+    for (auto& r : s->phases)
+        for (auto e : r.ev) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return BDB_OK;
@@ -423,24 +451,21 @@ int bdb_step(bdb_system* s, int K, const double* gauss)
 {
     if (!s || K < 0) return fail(BDB_ERR_ARG, "bad arguments");
     if (s->p.noise == BDB_NOISE_HOST && !gauss) return fail(BDB_ERR_ARG, "host noise mode needs Gaussians");
-    DevBuf<double> g;
+    phase_mark(s, P_STEP);
     if (gauss) {
-        if (g.alloc((size_t)K * s->n3)) return BDB_ERR_NOMEM;
-        BDB_CUDA(cudaMemcpyAsync(g.p, gauss, sizeof(double) * K * s->n3, cudaMemcpyHostToDevice, s->stream));
+        const size_t need = (size_t)K * s->n3;
+        if (s->gbuf.n < need && s->gbuf.alloc(need)) return BDB_ERR_NOMEM;
+        BDB_CUDA(cudaMemcpyAsync(s->gbuf.p, gauss, sizeof(double) * need, cudaMemcpyHostToDevice, s->stream));
     }
     BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
-    BDB_CUDA(cudaEventRecord(s->ev[0], s->stream));
     for (int k = 0; k < K; ++k) {
-        int rc = one_step(s, gauss ? g.p + (size_t)k * s->n3 : nullptr);
+        int rc = one_step(s, gauss ? s->gbuf.p + (size_t)k * s->n3 : nullptr);
         if (rc) return rc;
     }
-    BDB_CUDA(cudaEventRecord(s->ev[1], s->stream));
+    phase_mark(s, P_STEP);
     bool ov = false;
     int rc = check_status(s, &ov);
     if (rc) return rc;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
-    s->phase_ms[0] = ms;
     return ov ? 1 : 0;
 }
 
@@ -455,14 +480,47 @@ int bdb_factor_error(bdb_system* s, double* rel_err)
     return factor_error(s, rel_err);
 }
 
-int bdb_phase_ms(bdb_system* s, const char* phase, double* ms)
+int bdb_profile(bdb_system* s, int enable)
 {
-    if (!s || !phase || !ms) return fail(BDB_ERR_ARG, "null argument");
-    if (!strcmp(phase, "step")) {
-        *ms = s->phase_ms[0];
-        return BDB_OK;
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    s->profiling = enable != 0;
+    return BDB_OK;
+}
+
+int bdb_phase_stats(bdb_system* s, const char* phase, double* total_ms, long long* calls)
+{
+    if (!s || !phase || !total_ms || !calls) return fail(BDB_ERR_ARG, "null argument");
+    int ph = -1;
+    for (int k = 0; k < P_COUNT; ++k)
+        if (!strcmp(phase, kPhaseNames[k])) ph = k;
+    if (ph < 0) return fail(BDB_ERR_ARG, "unknown phase");
+    BDB_CUDA(cudaStreamSynchronize(s->stream));
+    auto& r = s->phases[ph];
+    double tot = 0;
+    for (size_t k = 0; k + 1 < r.used; k += 2) {
+        float ms = 0;
+        BDB_CUDA(cudaEventElapsedTime(&ms, r.ev[k], r.ev[k + 1]));
+        tot += ms;
     }
-    return fail(BDB_ERR_ARG, "unknown phase");
+    *total_ms = tot;
+    *calls = (long long)(r.used / 2);
+    return BDB_OK;
+}
+
+int bdb_reset_stats(bdb_system* s)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    BDB_CUDA(cudaStreamSynchronize(s->stream));
+    for (auto& r : s->phases) r.used = 0;
+    s->launches = 0;
+    return BDB_OK;
+}
+
+int bdb_launches(bdb_system* s, long long* count)
+{
+    if (!s || !count) return fail(BDB_ERR_ARG, "null argument");
+    *count = s->launches;
+    return BDB_OK;
 }
 
 void* bdb_stream(bdb_system* s) { return s ? (void*)s->stream : nullptr; }

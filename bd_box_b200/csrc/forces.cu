@@ -884,6 +884,7 @@ int forces_run(bdb_system* s, bool want_energy, bool want_counts)
         k_energy_reduce<<<1, 256, 0, st>>>(nblk, s->e_part.p, s->term_energy.p, tr, s->scal.p + 16);
         BDB_CUDA(cudaGetLastError());
     }
+    s->launches += 2 + (s->n_terms ? 2 : 0) + (want_energy ? 1 : 0);
     s->have_forces = true;
     return BDB_OK;
 }

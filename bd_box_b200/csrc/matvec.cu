@@ -194,6 +194,7 @@ int stored_matvec(bdb_system* s, bool want_rs)
         k_strip_mv<float><<<blocks, 32 * WARPS, 0, s->stream>>>(s->M32.p, n3, s->npad, nseg, seg_cols, s->F.p, X,
                                                                 rowp, colp);
     BDB_CUDA(cudaGetLastError());
+    s->launches += 2;
     const double pre = s->p.dt / (BDB_KB * s->p.T);
     k_mv_finish<<<(n3 + 255) / 256, 256, 0, s->stream>>>(n3, nseg, rowp, colp, s->dD.p, s->F.p, pre, s->Rf.p, s->Rs.p,
                                                          want_rs);

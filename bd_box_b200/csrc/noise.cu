@@ -89,6 +89,7 @@ int noise_fill(bdb_system* s, const double* dev_gauss)
     k_noise<<<(threads + 255) / 256, 256, 0, s->stream>>>(n3, s->p.hydro, s->p.dt, s->preDii, s->pos.p, dev_gauss,
                                                           s->p.seed, s->philox_counter, s->X.p);
     BDB_CUDA(cudaGetLastError());
+    s->launches += 1;
     s->philox_counter++;
     return BDB_OK;
 }
@@ -116,6 +117,7 @@ int update_positions(bdb_system* s)
     k_update<<<(s->n + 127) / 128, 128, 0, s->stream>>>(
         s->n, s->p.bc == 1, make_double3(s->p.box[0], s->p.box[1], s->p.box[2]),
         make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]), s->Rf.p, s->Rs.p, s->pos.p);
+    s->launches += 1;
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;
 }

@@ -134,6 +134,7 @@ int tensor_build(bdb_system* s)
     } else {
         k_build<float><<<grid, 256, build_smem_bytes<float>(), s->stream>>>(A, s->pos.p, s->M32.p, s->dD.p);
     }
+    s->launches += 1;
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;
 }
@@ -382,6 +383,7 @@ int tea_run(bdb_system* s, bool want_rs)
             BDB_CUDA(cudaGetLastError());
         }
     }
+    s->launches += 1 + ((s->p.hydro && s->n_jobs) ? (want_rs ? 2 : 1) : 0);
     const double pre_f = s->p.dt / (BDB_KB * s->p.T);
     k_tea_finish<<<(s->n + 127) / 128, 128, 0, s->stream>>>(A, s->n, tsegs, s->d_bead_seg.p, s->part.p, s->scal.p + 64,
                                                             s->pos.p, s->F.p, s->X.p, pre_f, want_rs,

@@ -40,7 +40,8 @@ EXPORTS = [
     "bdb_version", "bdb_last_error", "bdb_create", "bdb_destroy", "bdb_set_bonded",
     "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
-    "bdb_compute_r", "bdb_step", "bdb_factor_error", "bdb_phase_ms", "bdb_stream",
+    "bdb_compute_r", "bdb_step", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
+    "bdb_reset_stats", "bdb_launches", "bdb_stream",
 ]
 
 
@@ -94,7 +95,10 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_compute_r.argtypes = [C.c_void_p, _dp, _dp]
     lib.bdb_step.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.bdb_factor_error.argtypes = [C.c_void_p, _dp]
-    lib.bdb_phase_ms.argtypes = [C.c_void_p, C.c_char_p, _dp]
+    lib.bdb_profile.argtypes = [C.c_void_p, C.c_int]
+    lib.bdb_phase_stats.argtypes = [C.c_void_p, C.c_char_p, _dp, C.POINTER(C.c_longlong)]
+    lib.bdb_reset_stats.argtypes = [C.c_void_p]
+    lib.bdb_launches.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
     lib.bdb_stream.argtypes = [C.c_void_p]
     lib.bdb_stream.restype = C.c_void_p
     _lib = lib
@@ -251,9 +255,22 @@ class System:
         self._check(self.lib.bdb_factor_error(self.h, C.byref(out)))
         return out.value
 
-    def phase_ms(self, name="step") -> float:
-        out = C.c_double()
-        self._check(self.lib.bdb_phase_ms(self.h, name.encode(), C.byref(out)))
+    def profile(self, enable: bool = True):
+        self._check(self.lib.bdb_profile(self.h, int(enable)))
+
+    def phase_stats(self, name="step"):
+        """(total device ms, calls) of a profiled phase since the last reset."""
+        tot = C.c_double()
+        calls = C.c_longlong()
+        self._check(self.lib.bdb_phase_stats(self.h, name.encode(), C.byref(tot), C.byref(calls)))
+        return tot.value, calls.value
+
+    def reset_stats(self):
+        self._check(self.lib.bdb_reset_stats(self.h))
+
+    def launches(self) -> int:
+        out = C.c_longlong()
+        self._check(self.lib.bdb_launches(self.h, C.byref(out)))
         return out.value
 
 

@@ -1,0 +1,397 @@
+"""Benchmark: Brownian-dynamics steps/s of BD_BOX's Ermak-McCammon step.
+
+Workload (one GPU): a linear bead-spring chain of N=4096 beads (3N=12288),
+the chain force field (harmonic bonds, LJ + Debye-Hueckel, cutoff 12 A),
+free-space RPY hydrodynamics with Cholesky noise, D and its factor rebuilt
+every 10 steps, mixed precision (FP32 tensor and stored D/L, 3xTF32
+Cholesky updates with FP64 diagonal tiles and FP64 sums). Inputs are
+synthetic (seeded self-avoiding walk, seeded charges).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0. ``value`` is steps/s of the whole job with
+all state resident in HBM (K steps bracketed by a barrier and device
+synchronisation, CUDA events on the engine's stream, max over ranks).
+``e2e`` drives the same steps through the C ABI with host buffers: each
+step copies its 3N Gaussians from pinned host memory and reads the 4N
+coordinates back. With N > 1 every rank advances its own independent chain
+(replicas; no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BEADS = 4096
+REFRESH = 10
+SEED = 2
+METRIC = "BD steps/s at N=4096, mixed vs FP64 GPU at stated error; Cholesky TFLOP/s"
+
+
+def make_deck(tmp: str):
+    from bd_box_b200 import decks
+    p = decks.write_chain_deck(tmp, "chain4096", N_BEADS, seed=SEED, hydro="cholesky", steps=1000)
+    return p, decks.read_deck(p)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[4 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------- CPU baseline
+def reference_cpu(prm_path: str, deck, steps: int):
+    """The reference's own CPU build (oracle/_ref/ref_harness: BD_BOX sources,
+    -O3, OpenMP, LAPACK via OpenBLAS) on this host's cores, `steps` steps
+    with D and its Cholesky factor rebuilt every REFRESH steps. Falls back to
+    the C restatement of the oracle if the reference build is absent."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    cores = os.cpu_count() or 1
+    n3 = 3 * deck.n
+    d = os.path.dirname(prm_path)
+    g = np.random.default_rng(7).standard_normal(n3 * (steps + 1))
+    gpath = os.path.join(d, "gauss.bin")
+    g.tofile(gpath)
+    env = dict(os.environ, BDB_GAUSS_FILE=gpath, OMP_NUM_THREADS=str(cores),
+               OPENBLAS_NUM_THREADS=str(cores))
+    if os.path.exists(harness):
+        def run(k):
+            t0 = time.perf_counter()
+            subprocess.run([harness, os.path.basename(prm_path), "steps", "out.bin", str(k), str(REFRESH)],
+                           cwd=d, env=env, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            return time.perf_counter() - t0
+        t = run(steps)
+        # start-up (reading the deck, first forces) is timed separately and removed
+        t0 = time.perf_counter()
+        subprocess.run([harness, os.path.basename(prm_path), "forces", "f.bin"], cwd=d, env=env, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        t_init = time.perf_counter() - t0
+        return {"value": steps / max(t - t_init, 1e-9), "unit": "steps/s", "cores": cores, "kind": "reference",
+                "sample": f"{steps} steps of the N={deck.n} chain with one D build + LAPACK dpotrf per {REFRESH} "
+                          f"steps (BD_BOX CPU sources, OpenMP + OpenBLAS, {cores} threads)"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    o = pyoracle.Oracle(deck)
+    t0 = time.perf_counter()
+    o.run_steps(steps, g, refresh=REFRESH)
+    t = time.perf_counter() - t0
+    return {"value": steps / t, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} steps, oracle restatement (OpenMP {cores} threads)"}
+
+
+# ------------------------------------------------------------------- GPU
+def time_steps(torch, sysm, K):
+    stream = torch.cuda.ExternalStream(sysm.lib.bdb_stream(sysm.h))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        sysm.step(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def phase(sysm, name):
+    import ctypes as C
+    tot = C.c_double()
+    calls = C.c_longlong()
+    sysm._check(sysm.lib.bdb_phase_stats(sysm.h, name.encode(), C.byref(tot), C.byref(calls)))
+    return tot.value, calls.value
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+def profile_traffic(name: str):
+    """dram bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/<name>.md, line 'traffic_bytes_per_launch: X')."""
+    p = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for ln in f:
+            if ln.startswith("traffic_bytes_per_launch:"):
+                try:
+                    return float(ln.split(":", 1)[1])
+                except ValueError:
+                    return None
+    return None
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import torch
+    from bd_box_b200 import engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    tmp = tempfile.mkdtemp(prefix="bdb_bench_")
+    try:
+        prm, deck = make_deck(tmp)
+        n3 = 3 * deck.n
+        sysm = engine.System(deck, precision=engine.PREC_MIXED, refresh=REFRESH,
+                             noise=engine.NOISE_PHILOX, seed=SEED + 1000 * rank)
+        for _ in range(args.warmup):
+            sysm.step(1)
+        sysm.lib.bdb_reset_stats(sysm.h)
+        sysm.lib.bdb_profile(sysm.h, 1)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            ms = time_steps(torch, sysm, args.steps)
+        sysm.lib.bdb_profile(sysm.h, 0)
+        launches = C.c_longlong()
+        sysm.lib.bdb_launches(sysm.h, C.byref(launches))
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        value = world * args.steps / (ms / 1e3)
+        fac_ms, fac_calls = phase(sysm, "factor")
+        mv_ms, mv_calls = phase(sysm, "matvec")
+        ref_ms, _ = phase(sysm, "refresh")
+        bld_ms, bld_calls = phase(sysm, "build")
+        frc_ms, frc_calls = phase(sysm, "forces")
+
+        # e2e through the C ABI with host buffers (pinned)
+        gh = torch.randn(args.steps * n3, dtype=torch.float64).pin_memory()
+        ch = torch.empty(4 * deck.n, dtype=torch.float64).pin_memory()
+        hsys = engine.System(deck, precision=engine.PREC_MIXED, refresh=REFRESH,
+                             noise=engine.NOISE_HOST, seed=SEED + 1000 * rank)
+        gp = C.cast(gh.data_ptr(), C.POINTER(C.c_double))
+        cp = C.cast(ch.data_ptr(), C.POINTER(C.c_double))
+        for k in range(min(args.warmup, 3)):
+            hsys.lib.bdb_step(hsys.h, 1, gp)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            rc = hsys.lib.bdb_step(hsys.h, 1, C.cast(gh.data_ptr() + 8 * k * n3, C.POINTER(C.c_double)))
+            hsys._check(rc)
+            hsys._check(hsys.lib.bdb_get_coord(hsys.h, cp))
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * args.steps / e2e_s, "unit": "steps/s",
+               "h2d_bytes_per_step": 8 * n3, "d2h_bytes_per_step": 8 * 4 * deck.n}
+        hsys.close()
+
+        # plain FP64 GPU path (full Cholesky every step, the reference schedule)
+        fp64 = None
+        if rank == 0 and not args.skip_fp64:
+            s64 = engine.System(deck, precision=engine.PREC_FP64, refresh=1, noise=engine.NOISE_PHILOX, seed=5)
+            s64.step(1)
+            k64 = 3
+            ms64 = time_steps(torch, s64, k64)
+            fp64 = {"value": k64 / (ms64 / 1e3), "unit": "steps/s",
+                    "note": "FP64 everywhere, D and Cholesky rebuilt every step"}
+            s64.close()
+
+        errors = None
+        if rank == 0 and not args.skip_errors:
+            errors = accuracy(torch, engine, deck)
+
+        hbm, bf16, bf16s, src = peaks()
+        # dominant phase: the Cholesky factorisation (amortised over REFRESH steps)
+        n = 3 * deck.n
+        flops = n ** 3 / 3.0
+        fac_avg = fac_ms / max(fac_calls, 1)
+        mv_avg = mv_ms / max(mv_calls, 1)
+        share_fac = fac_ms / ms if ms else 0
+        share_mv = mv_ms / ms if ms else 0
+        if share_fac >= share_mv:
+            ach = flops / (fac_avg / 1e3) / 1e12
+            roof = {"kernel": "cholesky (k_chol_tc trailing updates + FP64 panels)", "bound": "tensor",
+                    "achieved": ach, "peak": bf16s, "unit": "TFLOP/s", "frac": ach / bf16s,
+                    "traffic": profile_traffic("cholesky_n12288"),
+                    "peak_source": f"{src} bf16 sustained", "ms_per_launch": fac_avg, "share_of_step_time": share_fac}
+        else:
+            bytes_ = 4.0 * n * n
+            ach = bytes_ / (mv_avg / 1e3) / 1e9
+            roof = {"kernel": "k_strip_mv (D.F + L.X)", "bound": "hbm", "achieved": ach, "peak": hbm,
+                    "unit": "GB/s", "frac": ach / hbm, "traffic": profile_traffic("strip_mv_n12288"),
+                    "peak_source": f"{src} hbm", "ms_per_launch": mv_avg, "share_of_step_time": share_mv}
+        roof["phases_ms_per_call"] = {"factor": fac_avg, "build": bld_ms / max(bld_calls, 1),
+                                      "matvec": mv_avg, "forces": frc_ms / max(frc_calls, 1)}
+        cpu = None
+        if rank == 0 and world == 1 and not args.skip_cpu:
+            cpu = reference_cpu(prm, deck, args.cpu_steps)
+        out = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded self-avoiding chain, seeded charges; Philox noise)",
+            "config": {"workload": f"chain N={deck.n} (3N={n}), free-space RPY + Cholesky noise, D and L rebuilt "
+                                   f"every {REFRESH} steps, mixed precision",
+                       "beads": deck.n, "refresh": REFRESH, "precision": "mixed (FP32 D/L, 3xTF32 updates, FP64 "
+                                                                         "diagonal tiles and sums)",
+                       "l2": "inputs larger than L2 (stored D/L 604 MB read every step)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches.value),
+            "clocks": clk.summary(), "fp64_gpu": fp64, "errors": errors,
+        }
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        sysm.close()
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def accuracy(torch, engine, deck):
+    """Relative errors of the mixed path against the FP64 GPU path (itself
+    checked against the oracle in the parity tests): ||B B^T - D||/||D||,
+    D.F and one step's displacement from the same state and noise."""
+    n3 = 3 * deck.n
+    g = np.random.default_rng(11).standard_normal(n3)
+    sm = engine.System(deck, precision=engine.PREC_MIXED, refresh=REFRESH, noise=engine.NOISE_HOST)
+    s64 = engine.System(deck, precision=engine.PREC_FP64, refresh=REFRESH, noise=engine.NOISE_HOST)
+    out = {}
+    try:
+        out["factor_rel"] = sm.factor_error()
+    except Exception as e:  # noqa: BLE001
+        out["factor_rel"] = f"unavailable: {e}"
+    rf_m, rf_d = sm.compute_Rf(), s64.compute_Rf()
+    out["df_rel"] = float(np.linalg.norm(rf_m - rf_d) / np.linalg.norm(rf_d))
+    x0 = s64.get_coord()
+    sm.step(1, g)
+    s64.step(1, g)
+    dm = sm.get_coord()[:, :3] - x0[:, :3]
+    dd = s64.get_coord()[:, :3] - x0[:, :3]
+    out["displacement_rel"] = float(np.linalg.norm(dm - dd) / np.linalg.norm(dd))
+    sm.close()
+    s64.close()
+    return out
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    tmp = tempfile.mkdtemp(prefix="bdb_ref_")
+    try:
+        prm, deck = make_deck(tmp)
+        steps = max(1, min(args.steps, args.cpu_steps))
+        cpu = reference_cpu(prm, deck, steps)
+        out = {"metric": METRIC, "value": cpu["value"], "unit": "steps/s", "n_gpus": world, "steps": steps,
+               "warmup": 0, "ms_per_step": 1e3 / cpu["value"], "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded self-avoiding chain)",
+               "config": {"workload": f"chain N={deck.n}, free-space RPY + Cholesky noise, D and L rebuilt every "
+                                      f"{REFRESH} steps", "beads": deck.n, "refresh": REFRESH},
+               "impl": "reference", "cpu_baseline": cpu,
+               "e2e": {"value": cpu["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-errors", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -153,9 +153,17 @@ int bdb_step(bdb_system* s, int K, const double* gauss);
  * rel_err = ||L L^T - D||_F / ||D||_F evaluated on the device in FP64. */
 int bdb_factor_error(bdb_system* s, double* rel_err);
 
-/* Timing hooks for measurement: last-call device durations in ms of the
- * named phases ("build", "factor", "matvec", "forces", "tea", "step"). */
-int bdb_phase_ms(bdb_system* s, const char* phase, double* ms);
+/* Measurement hooks (no reference counterpart). With profiling on, every
+ * phase of a step is bracketed by CUDA events on the system's stream;
+ * bdb_phase_stats returns the summed device time in ms and the number of
+ * calls of a phase since the last reset: "step" (whole bdb_step calls),
+ * "refresh" (tensor build + Cholesky), "build", "factor", "matvec", "tea",
+ * "forces", "noise", "update". bdb_launches counts kernel launches issued
+ * since the system was created (or the last reset). */
+int bdb_profile(bdb_system* s, int enable);
+int bdb_phase_stats(bdb_system* s, const char* phase, double* total_ms, long long* calls);
+int bdb_reset_stats(bdb_system* s);
+int bdb_launches(bdb_system* s, long long* count);
 
 /* The CUDA stream all work of this system is issued on (cudaStream_t). */
 void* bdb_stream(bdb_system* s);
