@@ -244,6 +244,14 @@ void orc_D(const orc_system* s, double* D)
     int n3 = 3 * s->n;
     int i;
     memset(D, 0, sizeof(double) * (size_t)n3 * n3);
+    if (!s->hydro) {
+        /* compute_D returns at once without hydrodynamics (diff_tensor.c:477);
+         * the tensor is diag_D (single_point_print, main_loop.c:161-175) */
+        double preDii, preDij;
+        orc_prefactors(s, &preDii, &preDij);
+        for (i = 0; i < n3; ++i) D[(size_t)i * n3 + i] = preDii / s->coord[4 * (i / 3) + 3];
+        return;
+    }
 #pragma omp parallel for schedule(dynamic)
     for (i = 0; i < s->n; ++i) {
         int j, k, l;
