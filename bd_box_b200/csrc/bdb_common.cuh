@@ -119,6 +119,9 @@ struct bdb_system {
     bdb::DevBuf<float> M32;                    // same, FP32 (mixed path)
     bdb::DevBuf<double> panel64;               // Cholesky workspace
     bool factor_valid = false;
+    alignas(64) unsigned char tc_map[512];     // CUtensorMaps: TF32 hi / lo panel buffers, FP32 matrix
+    bool tc_map_ok = false;
+    int sm_count = 148;
     int steps_since_refresh = 0;
 
     // noise

@@ -11,7 +11,10 @@
 // T = double is the plain FP64 path; T = float stores FP32 and keeps the
 // diagonal blocks and substitutions in FP64 (the SIMT fallback of the
 // mixed path; the tcgen05 kernel in chol_tc.cu replaces its k_syrk).
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <cstdlib>
 
 #include "bdb_common.cuh"
 
@@ -90,12 +93,15 @@ __global__ void __launch_bounds__(128) k_trsm(T* __restrict__ M, int npad, int k
 }
 
 // trailing update of the lower triangle: tile (bi, bj), bi >= bj > k
+// (only_next: column block k+1 alone, the in-panel update of a 128-wide
+// super-panel)
 template <typename T>
-__global__ void __launch_bounds__(256) k_syrk(T* __restrict__ M, int npad, int k)
+__global__ void __launch_bounds__(256) k_syrk(T* __restrict__ M, int npad, int k, int only_next)
 {
     const int nb_rem = npad / NB - k - 1;
     const int bi = k + 1 + blockIdx.y, bj = k + 1 + blockIdx.x;
     if (blockIdx.x > blockIdx.y || blockIdx.y >= nb_rem) return;
+    if (only_next && blockIdx.x != 0) return;
     constexpr int KC = 32;           // panel columns staged per pass
     __shared__ T As[KC][NB + 1];     // As[m][row]
     __shared__ T Bs[KC][NB + 1];
@@ -141,8 +147,12 @@ __global__ void __launch_bounds__(256) k_syrk(T* __restrict__ M, int npad, int k
     }
 }
 
+int factor_mixed_tc(bdb_system* s);   // chol_tc.cu
+
 int factor_run(bdb_system* s)
 {
+    const bool no_tc = getenv("BDB_NO_TC") != nullptr;   // diagnostics: SIMT FP32 trailing update
+    if (s->p.precision == BDB_PREC_MIXED && !no_tc && s->npad % 128 == 0) return factor_mixed_tc(s);
     const int nb = s->npad / NB;
     for (int k = 0; k < nb; ++k) {
         const int rows_below = s->npad - (k + 1) * NB;
@@ -151,14 +161,14 @@ int factor_run(bdb_system* s)
             if (rows_below > 0) {
                 k_trsm<double><<<(rows_below + 127) / 128, 128, 0, s->stream>>>(s->M64.p, s->npad, k);
                 dim3 g(nb - k - 1, nb - k - 1);
-                k_syrk<double><<<g, 256, 0, s->stream>>>(s->M64.p, s->npad, k);
+                k_syrk<double><<<g, 256, 0, s->stream>>>(s->M64.p, s->npad, k, 0);
             }
         } else {
             k_potrf<float><<<1, NB, 0, s->stream>>>(s->M32.p, s->npad, k, s->status.p);
             if (rows_below > 0) {
                 k_trsm<float><<<(rows_below + 127) / 128, 128, 0, s->stream>>>(s->M32.p, s->npad, k);
                 dim3 g(nb - k - 1, nb - k - 1);
-                k_syrk<float><<<g, 256, 0, s->stream>>>(s->M32.p, s->npad, k);
+                k_syrk<float><<<g, 256, 0, s->stream>>>(s->M32.p, s->npad, k, 0);
             }
         }
     }

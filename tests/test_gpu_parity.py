@@ -183,3 +183,19 @@ def test_philox_moments(chain_none):
     xs = np.concatenate([s.compute_r() / np.sqrt(2 * d * diag) for _ in range(200)])
     assert abs(xs.mean()) < 0.02
     assert abs(xs.var() - 1) < 0.03
+
+
+def test_tensor_core_factor_large(deck_dir):
+    """3xTF32 tcgen05 trailing updates over many tiles (3N = 2100, 17 super
+    panels): ||L L^T - D||/||D|| within the stated 1e-5, and close to the
+    SIMT FP32 factor of the same matrix."""
+    deck = decks.read_deck(decks.write_chain_deck(deck_dir, "big_chol", 700, seed=31, hydro="cholesky"))
+    s = engine.System(deck, precision=engine.PREC_MIXED)
+    err_tc = s.factor_error()
+    os.environ["BDB_NO_TC"] = "1"
+    try:
+        err_simt = engine.System(deck, precision=engine.PREC_MIXED).factor_error()
+    finally:
+        del os.environ["BDB_NO_TC"]
+    assert err_tc <= 1e-5, err_tc
+    assert err_tc <= 10 * err_simt + 1e-7, (err_tc, err_simt)
