@@ -99,7 +99,12 @@ struct bdb_system {
     bdb::DevBuf<int> sorted_idx;
     bdb::DevBuf<double4> grid;                 // per segment: origin xyz, cell size
     bdb::DevBuf<int4> grid_dims;               // per segment: nx, ny, nz, brute flag
+    bdb::DevBuf<double4> pos_build;            // positions when the cell list was last sorted
+    bdb::DevBuf<int2> cell_range;              // dense per-segment table: [first, end) of each cell
+    bdb::DevBuf<long long> cell_off;           // per segment: offset of its table, capacity
+    bdb::DevBuf<int> cells_built;              // per segment: 1 once sorted
     double cell_size = 0;
+    double skin = 0;
 
     // force outputs
     bdb::DevBuf<double> e_part;                // energy partials

@@ -66,6 +66,8 @@ template struct DevBuf<unsigned char>;
 template struct DevBuf<double2>;
 template struct DevBuf<double4>;
 template struct DevBuf<int4>;
+template struct DevBuf<int2>;
+template struct DevBuf<long long>;
 template struct DevBuf<Segment>;
 template struct DevBuf<TileJob>;
 
@@ -315,6 +317,7 @@ int bdb_set_coord(bdb_system* s, const double* coord)
 {
     if (!s || !coord) return fail(BDB_ERR_ARG, "null argument");
     BDB_CUDA(cudaMemcpyAsync(s->pos.p, coord, sizeof(double) * 4 * s->n, cudaMemcpyHostToDevice, s->stream));
+    BDB_CUDA(cudaMemsetAsync(s->cells_built.p, 0, sizeof(int) * s->segs.size(), s->stream));
     s->have_forces = false;
     s->factor_valid = false;
     return BDB_OK;
@@ -341,6 +344,7 @@ int bdb_load_state(bdb_system* s)
     if (!s) return fail(BDB_ERR_ARG, "null system");
     BDB_CUDA(cudaMemcpyAsync(s->pos.p, s->pos_save.p, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
     BDB_CUDA(cudaMemcpyAsync(s->F.p, s->F_save.p, sizeof(double) * s->n3, cudaMemcpyDeviceToDevice, s->stream));
+    BDB_CUDA(cudaMemsetAsync(s->cells_built.p, 0, sizeof(int) * s->segs.size(), s->stream));
     s->have_forces = true;
     return BDB_OK;
 }

@@ -5,6 +5,10 @@
 //   bead by its cell and sorts (cell, bead) pairs in shared memory. A bead
 //   then finds each of its 27 neighbour cells by binary search in the sorted
 //   keys -- no per-cell arrays, so a sparse free-space chain costs O(N).
+//   Cells are the widest cutoff plus a skin, and a segment is re-sorted only
+//   after some bead has moved more than skin/2 since the last sort (each bead
+//   looks up its current cell, and every partner within the cutoff is still
+//   in an adjacent cell of the stored list), so most steps skip the sort.
 //   This replaces bucket_space / bucket_list (potentials/bucket.c); the pair
 //   set is the reference's: every pair inside the cutoffs of force_single.
 // * Non-bonded (force_single, calc_func.c:370-409; LJ_force LJ.c:37-64;
@@ -70,16 +74,38 @@ static ForceParams make_fp(const bdb_system* s)
 // ---------------------------------------------------------------- cell list
 
 __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restrict__ segs,
-                        double cell, int periodic, double3 box,
+                        double cell, double skin, int periodic, double3 box,
                         unsigned long long* __restrict__ keys_out, int* __restrict__ idx_out,
-                        double4* __restrict__ grid, int4* __restrict__ dims)
+                        double4* __restrict__ grid, int4* __restrict__ dims, double4* __restrict__ pos_build,
+                        int* __restrict__ built, int2* __restrict__ cell_range, const long long* __restrict__ cell_off)
 {
     extern __shared__ unsigned long long sk[];
     __shared__ double red[6][32];
     __shared__ double g_origin[3];
     __shared__ int g_n[3];
+    __shared__ int moved;
     const Segment sg = segs[blockIdx.x];
     const int tid = threadIdx.x, nt = blockDim.x;
+    if (built[blockIdx.x]) {
+        // re-sort only when a bead has moved more than skin/2 since the last sort
+        if (tid == 0) moved = 0;
+        __syncthreads();
+        const double lim = 0.25 * skin * skin;
+        bool far = false;
+        for (int i = tid; i < sg.count; i += nt) {
+            const double4 a = pos[sg.begin + i], b = pos_build[sg.begin + i];
+            double d[3] = {a.x - b.x, a.y - b.y, a.z - b.z};
+            if (periodic) {
+                d[0] -= box.x * floor(d[0] / box.x + 0.5);
+                d[1] -= box.y * floor(d[1] / box.y + 0.5);
+                d[2] -= box.z * floor(d[2] / box.z + 0.5);
+            }
+            if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] > lim) far = true;
+        }
+        if (far) moved = 1;
+        __syncthreads();
+        if (!moved) return;
+    }
     if (sg.count > SORT_MAX) {
         if (tid == 0) dims[blockIdx.x] = make_int4(0, 0, 0, 1);   // brute force
         return;
@@ -112,12 +138,13 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
                     H[k] = fmax(H[k], red[3 + k][w]);
                 }
             }
-            // grow the cell until the grid stays below 2^24 cells
+            // grow the cell until the grid fits the segment's cell table
+            const long long cap = cell_off[2 * blockIdx.x + 1];
             double c = cell;
             for (;;) {
                 long long tot = 1;
                 for (int k = 0; k < 3; ++k) tot *= (long long)floor((H[k] - L[k]) / c) + 1;
-                if (tot < (1ll << 24)) break;
+                if (tot <= cap) break;
                 c *= 1.25;
             }
             for (int k = 0; k < 3; ++k) {
@@ -131,8 +158,16 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
         int nn[3];
         double bx[3] = {box.x, box.y, box.z};
         int brute = 0;
+        const long long cap = cell_off[2 * blockIdx.x + 1];
+        double cw = cell;
+        for (;;) {
+            long long tot = 1;
+            for (int k = 0; k < 3; ++k) tot *= (long long)floor(bx[k] / cw);
+            if (tot <= cap) break;
+            cw *= 1.25;
+        }
         for (int k = 0; k < 3; ++k) {
-            nn[k] = (int)floor(bx[k] / cell);
+            nn[k] = (int)floor(bx[k] / cw);
             if (nn[k] < 3) brute = 1;
             g_n[k] = nn[k];
             g_origin[k] = -0.5 * bx[k];
@@ -183,10 +218,20 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
             __syncthreads();
         }
     }
+    // dense cell table: [first, end) of every cell, empty cells {0, 0}
+    int2* tab = cell_range + cell_off[2 * blockIdx.x];
+    const long long ncell = (long long)g_n[0] * g_n[1] * g_n[2];
+    for (long long k = tid; k < ncell; k += nt) tab[k] = make_int2(0, 0);
+    __syncthreads();
     for (int i = tid; i < sg.count; i += nt) {
-        keys_out[sg.begin + i] = sk[i] >> 24;
+        const unsigned long long key = sk[i] >> 24;
+        keys_out[sg.begin + i] = key;
         idx_out[sg.begin + i] = sg.begin + (int)(sk[i] & 0xffffffull);
+        pos_build[sg.begin + i] = pos[sg.begin + i];
+        if (i == 0 || (sk[i - 1] >> 24) != key) tab[key].x = sg.begin + i;
+        if (i == sg.count - 1 || (sk[i + 1] >> 24) != key) tab[key].y = sg.begin + i + 1;
     }
+    if (tid == 0) built[blockIdx.x] = 1;
 }
 
 __device__ __forceinline__ int lower_bound_key(const unsigned long long* keys, int lo, int hi,
@@ -283,110 +328,102 @@ __device__ __forceinline__ void pair_term(const ForceParams& fp, const double4* 
     if (fp.check_overlap && r) rep = 1;
 }
 
+// One warp per bead i: the lanes split the candidate beads of the 27
+// neighbour cells (or of the whole segment for brute-force segments); each
+// lane accumulates in a fixed order and the warp combines the lanes with a
+// fixed xor tree, so the result is deterministic.
 __global__ void __launch_bounds__(NB_THREADS)
 k_nonbonded(ForceParams fp, int n, const double4* __restrict__ pos, const double* __restrict__ Q,
             const double2* __restrict__ LJ, const int* __restrict__ bead_seg,
-            const Segment* __restrict__ segs, const unsigned long long* __restrict__ keys,
-            const int* __restrict__ sidx, const double4* __restrict__ grid,
-            const int4* __restrict__ dims, const int* __restrict__ conn_ptr,
+            const Segment* __restrict__ segs, const int2* __restrict__ cell_range,
+            const long long* __restrict__ cell_off, const int* __restrict__ sidx,
+            const double4* __restrict__ grid, const int4* __restrict__ dims, const int* __restrict__ conn_ptr,
             const int* __restrict__ conn_list, const double* __restrict__ F_bonded,
             double* __restrict__ F, double* __restrict__ e_part,
             unsigned long long* __restrict__ counts, unsigned* __restrict__ status)
 {
-    __shared__ double sred[2][NB_THREADS / 32];
-    __shared__ unsigned scnt[2];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    double f[3] = {0, 0, 0};
     double e_lj = 0, e_c = 0;
     unsigned cnt_c = 0, cnt_lj = 0, rep = 0;
-    if (threadIdx.x < 2) scnt[threadIdx.x] = 0;
-    if (i < n) {
-        double f[3] = {F_bonded[3 * i], F_bonded[3 * i + 1], F_bonded[3 * i + 2]};
-        const int sgi = bead_seg[i];
-        const Segment sg = segs[sgi];
-        const int4 gd = dims[sgi];
-        if (fp.elec || fp.alpha_lj != 0.0) {
-            if (gd.w) {
-                for (int j = sg.begin; j < sg.begin + sg.count; ++j) {
+    const int sgi = bead_seg[i];
+    const Segment sg = segs[sgi];
+    const int4 gd = dims[sgi];
+    if (fp.elec || fp.alpha_lj != 0.0) {
+        if (gd.w) {
+            for (int j = sg.begin + lane; j < sg.begin + sg.count; j += 32) {
+                if (j == i) continue;
+                const int a = i < j ? i : j, b = i < j ? j : i;
+                pair_term(fp, pos, Q, LJ, conn_ptr, conn_list, a, b, i, f, e_lj, e_c, cnt_c, cnt_lj, rep);
+            }
+        } else {
+            const double4 gr = grid[sgi];
+            const double4 p = pos[i];
+            const double x[3] = {p.x, p.y, p.z};
+            int c[3];
+            const int nn[3] = {gd.x, gd.y, gd.z};
+            for (int k = 0; k < 3; ++k) {
+                const double w = fp.periodic ? (&gr.x)[k] : gr.w;
+                const double o = fp.periodic ? -0.5 * fp.box[k] : (&gr.x)[k];
+                const int ci = (int)floor((x[k] - o) / w);
+                c[k] = ci < 0 ? 0 : (ci >= nn[k] ? nn[k] - 1 : ci);
+            }
+            const int2* tab = cell_range + cell_off[2 * sgi];
+            // lanes 0..26 fetch the [first, end) range of one neighbour cell each
+            int2 rg = make_int2(0, 0);
+            if (lane < 27) {
+                int cc[3] = {c[0] + lane % 3 - 1, c[1] + (lane / 3) % 3 - 1, c[2] + lane / 9 - 1};
+                bool skip = false;
+                for (int k = 0; k < 3; ++k) {
+                    if (cc[k] < 0 || cc[k] >= nn[k]) {
+                        if (!fp.periodic) skip = true;
+                        else cc[k] = (cc[k] + nn[k]) % nn[k];
+                    }
+                }
+                if (!skip) rg = tab[((long long)cc[2] * nn[1] + cc[1]) * nn[0] + cc[0]];
+            }
+            for (int nc = 0; nc < 27; ++nc) {
+                const int lo = __shfl_sync(0xffffffffu, rg.x, nc);
+                const int hi = __shfl_sync(0xffffffffu, rg.y, nc);
+                for (int q = lo + lane; q < hi; q += 32) {
+                    const int j = sidx[q];
                     if (j == i) continue;
                     const int a = i < j ? i : j, b = i < j ? j : i;
                     pair_term(fp, pos, Q, LJ, conn_ptr, conn_list, a, b, i, f, e_lj, e_c, cnt_c, cnt_lj, rep);
                 }
-            } else {
-                const double4 gr = grid[sgi];
-                const double4 p = pos[i];
-                const double x[3] = {p.x, p.y, p.z};
-                int c[3];
-                int nn[3] = {gd.x, gd.y, gd.z};
-                for (int k = 0; k < 3; ++k) {
-                    double w = fp.periodic ? (&gr.x)[k] : gr.w;
-                    double o = fp.periodic ? -0.5 * fp.box[k] : (&gr.x)[k];
-                    int ci = (int)floor((x[k] - o) / w);
-                    c[k] = ci < 0 ? 0 : (ci >= nn[k] ? nn[k] - 1 : ci);
-                }
-                for (int dz = -1; dz <= 1; ++dz)
-                    for (int dy = -1; dy <= 1; ++dy)
-                        for (int dx = -1; dx <= 1; ++dx) {
-                            int cc[3] = {c[0] + dx, c[1] + dy, c[2] + dz};
-                            bool skip = false;
-                            for (int k = 0; k < 3; ++k) {
-                                if (cc[k] < 0 || cc[k] >= nn[k]) {
-                                    if (!fp.periodic) skip = true;
-                                    else cc[k] = (cc[k] + nn[k]) % nn[k];
-                                }
-                            }
-                            if (skip) continue;
-                            const unsigned long long key =
-                                ((unsigned long long)cc[2] * nn[1] + cc[1]) * nn[0] + cc[0];
-                            int lo = lower_bound_key(keys, sg.begin, sg.begin + sg.count, key);
-                            for (int q = lo; q < sg.begin + sg.count && keys[q] == key; ++q) {
-                                const int j = sidx[q];
-                                if (j == i) continue;
-                                const int a = i < j ? i : j, b = i < j ? j : i;
-                                pair_term(fp, pos, Q, LJ, conn_ptr, conn_list, a, b, i, f, e_lj, e_c,
-                                          cnt_c, cnt_lj, rep);
-                            }
-                        }
-            }
-        } else if (fp.check_overlap) {
-            for (int j = sg.begin; j < sg.begin + sg.count; ++j) {
-                if (j == i) continue;
-                const int a = i < j ? i : j, b = i < j ? j : i;
-                double v[3];
-                dist_vec(pos[a], pos[b], fp.periodic, fp.box, fp.inv_L, v);
-                const double sig = LJ[a].x + LJ[b].x;
-                if (sig * sig > sq3(v)) rep = 1;
             }
         }
-        F[3 * i] = f[0];
-        F[3 * i + 1] = f[1];
-        F[3 * i + 2] = f[2];
+    } else if (fp.check_overlap) {
+        for (int j = sg.begin + lane; j < sg.begin + sg.count; j += 32) {
+            if (j == i) continue;
+            const int a = i < j ? i : j, b = i < j ? j : i;
+            double v[3];
+            dist_vec(pos[a], pos[b], fp.periodic, fp.box, fp.inv_L, v);
+            const double sig = LJ[a].x + LJ[b].x;
+            if (sig * sig > sq3(v)) rep = 1;
+        }
     }
-    // block reduction of energies (fixed tree) and counts
     for (int o = 16; o > 0; o >>= 1) {
+        f[0] += __shfl_xor_sync(0xffffffffu, f[0], o);
+        f[1] += __shfl_xor_sync(0xffffffffu, f[1], o);
+        f[2] += __shfl_xor_sync(0xffffffffu, f[2], o);
         e_lj += __shfl_xor_sync(0xffffffffu, e_lj, o);
         e_c += __shfl_xor_sync(0xffffffffu, e_c, o);
         cnt_c += __shfl_xor_sync(0xffffffffu, cnt_c, o);
         cnt_lj += __shfl_xor_sync(0xffffffffu, cnt_lj, o);
+        rep |= __shfl_xor_sync(0xffffffffu, rep, o);
     }
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) {
-        sred[0][threadIdx.x >> 5] = e_lj;
-        sred[1][threadIdx.x >> 5] = e_c;
-        atomicAdd(&scnt[0], cnt_c);
-        atomicAdd(&scnt[1], cnt_lj);
-    }
-    if (rep) atomicOr(status, ST_OVERLAP);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0, b = 0;
-        for (int w = 0; w < NB_THREADS / 32; ++w) {
-            a += sred[0][w];
-            b += sred[1][w];
-        }
-        e_part[2 * blockIdx.x] = a;
-        e_part[2 * blockIdx.x + 1] = b;
-        if (scnt[0]) atomicAdd(&counts[0], (unsigned long long)scnt[0]);
-        if (scnt[1]) atomicAdd(&counts[1], (unsigned long long)scnt[1]);
+    if (lane == 0) {
+        F[3 * i] = F_bonded[3 * i] + f[0];
+        F[3 * i + 1] = F_bonded[3 * i + 1] + f[1];
+        F[3 * i + 2] = F_bonded[3 * i + 2] + f[2];
+        e_part[2 * i] = e_lj;
+        e_part[2 * i + 1] = e_c;
+        if (cnt_c) atomicAdd(&counts[0], (unsigned long long)cnt_c);
+        if (cnt_lj) atomicAdd(&counts[1], (unsigned long long)cnt_lj);
+        if (rep) atomicOr(status, ST_OVERLAP);
     }
 }
 
@@ -791,8 +828,20 @@ int forces_setup(bdb_system* s)
     if (s->sorted_idx.alloc(s->n)) return BDB_ERR_NOMEM;
     if (s->grid.alloc(nseg)) return BDB_ERR_NOMEM;
     if (s->grid_dims.alloc(nseg)) return BDB_ERR_NOMEM;
-    const int nblk = (s->n + NB_THREADS - 1) / NB_THREADS;
-    if (s->e_part.alloc(2 * nblk + 16)) return BDB_ERR_NOMEM;
+    if (s->pos_build.alloc(s->n) || s->cells_built.alloc(nseg)) return BDB_ERR_NOMEM;
+    BDB_CUDA(cudaMemset(s->cells_built.p, 0, sizeof(int) * nseg));
+    // dense cell tables: 32 cells per bead (at least 4096) per segment
+    std::vector<long long> off(2 * nseg);
+    long long tot = 0;
+    for (int g = 0; g < nseg; ++g) {
+        const long long cap = std::max<long long>(4096, 32ll * s->segs[g].count);
+        off[2 * g] = tot;
+        off[2 * g + 1] = cap;
+        tot += cap;
+    }
+    if (s->cell_range.alloc(tot) || s->cell_off.alloc(2 * nseg)) return BDB_ERR_NOMEM;
+    BDB_CUDA(cudaMemcpy(s->cell_off.p, off.data(), sizeof(long long) * 2 * nseg, cudaMemcpyHostToDevice));
+    if (s->e_part.alloc(2 * s->n + 16)) return BDB_ERR_NOMEM;
     if (s->status.alloc(4)) return BDB_ERR_NOMEM;
     if (s->counts.alloc(2)) return BDB_ERR_NOMEM;
     if (s->F.alloc(3 * s->n) || s->F_save.alloc(3 * s->n) || s->work.alloc(3 * s->n + 16)) return BDB_ERR_NOMEM;
@@ -808,7 +857,8 @@ int forces_setup(bdb_system* s)
     if (s->p.elec) c = std::max(c, s->p.cutoff_c);
     if (s->p.alpha_lj != 0) c = std::max(c, s->p.cutoff_lj > 0 ? s->p.cutoff_lj : (double)1.122462f * 2 * maxsig);
     c = std::max(c, s->p.max_force_cutoff);
-    s->cell_size = c * (1 + 1e-12) + 1e-9;
+    s->skin = std::max(0.5, 0.1 * c);
+    s->cell_size = (c + s->skin) * (1 + 1e-12) + 1e-9;
     return BDB_OK;
 }
 
@@ -852,8 +902,9 @@ int forces_run(bdb_system* s, bool want_energy, bool want_counts)
     int np = 1;
     while (np < smax) np <<= 1;
     size_t shm = sizeof(unsigned long long) * (size_t)std::min(np, SORT_MAX);
-    k_cells<<<nseg, 1024, shm, st>>>(s->pos.p, s->d_segs.p, s->cell_size, s->p.bc == 1, box,
-                                      s->sorted_keys.p, s->sorted_idx.p, s->grid.p, s->grid_dims.p);
+    k_cells<<<nseg, 1024, shm, st>>>(s->pos.p, s->d_segs.p, s->cell_size, s->skin, s->p.bc == 1, box,
+                                      s->sorted_keys.p, s->sorted_idx.p, s->grid.p, s->grid_dims.p,
+                                      s->pos_build.p, s->cells_built.p, s->cell_range.p, s->cell_off.p);
     BDB_CUDA(cudaGetLastError());
     double* Fb = s->work.p;
     if (s->n_terms) {
@@ -867,9 +918,9 @@ int forces_run(bdb_system* s, bool want_energy, bool want_counts)
         BDB_CUDA(cudaMemsetAsync(Fb, 0, sizeof(double) * 3 * s->n, st));
     }
     BDB_CUDA(cudaGetLastError());
-    const int nblk = (s->n + NB_THREADS - 1) / NB_THREADS;
+    const int nblk = (s->n * 32 + NB_THREADS - 1) / NB_THREADS;
     k_nonbonded<<<nblk, NB_THREADS, 0, st>>>(make_fp(s), s->n, s->pos.p, s->Q.p, s->LJ.p, s->d_bead_seg.p,
-                                             s->d_segs.p, s->sorted_keys.p, s->sorted_idx.p, s->grid.p,
+                                             s->d_segs.p, s->cell_range.p, s->cell_off.p, s->sorted_idx.p, s->grid.p,
                                              s->grid_dims.p, s->conn_ptr.p, s->conn_list.p, Fb, s->F.p,
                                              s->e_part.p, s->counts.p, s->status.p);
     BDB_CUDA(cudaGetLastError());
@@ -881,7 +932,7 @@ int forces_run(bdb_system* s, bool want_energy, bool want_counts)
         tr.lim[3] = tr.lim[2] + s->n_angle_cos;
         tr.lim[4] = tr.lim[3] + s->n_dihe;
         tr.lim[5] = tr.lim[4] + s->n_dihe_angle;
-        k_energy_reduce<<<1, 256, 0, st>>>(nblk, s->e_part.p, s->term_energy.p, tr, s->scal.p + 16);
+        k_energy_reduce<<<1, 256, 0, st>>>(s->n, s->e_part.p, s->term_energy.p, tr, s->scal.p + 16);
         BDB_CUDA(cudaGetLastError());
     }
     s->launches += 2 + (s->n_terms ? 2 : 0) + (want_energy ? 1 : 0);

@@ -8,7 +8,7 @@
 // Work item = one warp on (strip of 32 rows) x (column segment). A lane
 // owns 4 consecutive columns of every 128-column tile (one 16-byte load of
 // FP32 or two of FP64 per row). For each tile the 32 per-row lane partials
-// are combined by a 31-shuffle reduce-scatter, after which lane q holds
+// go through a per-warp shared-memory transpose, after which lane q adds
 // row q's sum. The transposed part of D F (left of the diagonal)
 // accumulates per column over the strip's 32 rows and is written as one
 // partial per (strip, column); k_mv_finish adds all partials in a fixed
@@ -44,22 +44,6 @@ __device__ __forceinline__ void load4(const double* p, double* o)
     o[3] = b.y;
 }
 
-// v[q] per lane -> returns sum over lanes of v[lane]
-__device__ __forceinline__ double reduce_scatter32(double* v, int lane)
-{
-#pragma unroll
-    for (int w = 16; w >= 1; w >>= 1) {
-        const bool hi = (lane & w) != 0;
-#pragma unroll
-        for (int k = 0; k < w; ++k) {
-            const double send = hi ? v[k] : v[k + w];
-            const double keep = hi ? v[k + w] : v[k];
-            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, w);
-        }
-    }
-    return v[0];
-}
-
 // rowp: [nseg][n3][2] row partials (Rs, Rf right part); colp: [nstrip][n3]
 template <typename T>
 __global__ void __launch_bounds__(32 * WARPS)
@@ -68,6 +52,7 @@ k_strip_mv(const T* __restrict__ M, int n3, int npad, int nseg, int seg_cols,
            double* __restrict__ colp)
 {
     __shared__ double sF[WARPS][STRIP];
+    __shared__ double red[WARPS][32][STRIP + 1];   // [lane][row] partials of one tile
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int item = blockIdx.x * WARPS + warp;
     const int nstrip = (n3 + STRIP - 1) / STRIP;
@@ -78,6 +63,7 @@ k_strip_mv(const T* __restrict__ M, int n3, int npad, int nseg, int seg_cols,
     const int c_beg = seg * seg_cols, c_end = min(n3, c_beg + seg_cols);
     sF[warp][lane] = lane < nrow ? F[r0 + lane] : 0.0;
     __syncwarp();
+    double (*rd)[STRIP + 1] = red[warp];
     double rs_acc = 0, rf_acc = 0;
     for (int c0 = c_beg; c0 < c_end; c0 += 128) {
         const int c = c0 + 4 * lane;
@@ -88,56 +74,60 @@ k_strip_mv(const T* __restrict__ M, int n3, int npad, int nseg, int seg_cols,
             x[v] = ok ? X[c + v] : 0.0;
             f[v] = ok ? F[c + v] : 0.0;
         }
-        const bool full = c + 3 < c_end;
         const bool lower = c0 + 127 < r0;
         const bool upper = c0 > r0 + STRIP - 1;
-        double pr[STRIP];
-        if (lower || upper) {
+        // warp-uniform choice: every lane of an interior tile has 4 columns
+        if ((lower || upper) && nrow == STRIP && c0 + 127 < c_end) {
+            // interior tile: 8 rows of loads in flight at a time
             const double* w = lower ? x : f;
+            double (*dst)[STRIP + 1] = rd;
 #pragma unroll 8
             for (int q = 0; q < STRIP; ++q) {
-                double m[4] = {0, 0, 0, 0};
-                if (q < nrow) {
-                    const T* rp = M + (size_t)(r0 + q) * npad + c;
-                    if (full) load4(rp, m);
-                    else
-                        for (int v = 0; v < 4; ++v)
-                            if (c + v < c_end) m[v] = (double)rp[v];
-                }
-                pr[q] = m[0] * w[0] + m[1] * w[1] + m[2] * w[2] + m[3] * w[3];
+                double m[4];
+                load4(M + (size_t)(r0 + q) * npad + c, m);
+                dst[lane][q] = m[0] * w[0] + m[1] * w[1] + m[2] * w[2] + m[3] * w[3];
                 if (upper) {
                     const double fq = sF[warp][q];
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) pc[v] += m[v] * fq;
+                    pc[0] += m[0] * fq;
+                    pc[1] += m[1] * fq;
+                    pc[2] += m[2] * fq;
+                    pc[3] += m[3] * fq;
                 }
             }
-            const double red = reduce_scatter32(pr, lane);
-            if (lower) rs_acc += red; else rf_acc += red;
+            __syncwarp();
+            double sum = 0;
+#pragma unroll 8
+            for (int l = 0; l < 32; ++l) sum += dst[l][lane];
+            if (lower) rs_acc += sum; else rf_acc += sum;
+            __syncwarp();
         } else {
-            // tile crossing the diagonal: per element
-            double ps[STRIP];
-#pragma unroll 4
-            for (int q = 0; q < STRIP; ++q) {
-                const int r = r0 + q;
-                double m[4] = {0, 0, 0, 0};
-                if (q < nrow)
-                    for (int v = 0; v < 4; ++v)
-                        if (c + v < c_end) m[v] = (double)M[(size_t)r * npad + c + v];
-                double s = 0, t = 0;
-                const double fq = sF[warp][q];
+            // edge tile or tile crossing the diagonal: per element, the L
+            // part (columns <= row) first, then the D part
+            for (int part = 0; part < 2; ++part) {
+                for (int q = 0; q < STRIP; ++q) {
+                    const int r = r0 + q;
+                    double m[4] = {0, 0, 0, 0};
+                    if (q < nrow)
+                        for (int v = 0; v < 4; ++v)
+                            if (c + v < c_end) m[v] = (double)M[(size_t)r * npad + c + v];
+                    double a = 0;
+                    const double fq = sF[warp][q];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    if (c + v <= r) s += m[v] * x[v];
-                    else {
-                        t += m[v] * f[v];
-                        pc[v] += m[v] * fq;
+                    for (int v = 0; v < 4; ++v) {
+                        if (part == 0 && c + v <= r) a += m[v] * x[v];
+                        if (part == 1 && c + v > r) {
+                            a += m[v] * f[v];
+                            pc[v] += m[v] * fq;
+                        }
                     }
+                    rd[lane][q] = a;
                 }
-                ps[q] = s;
-                pr[q] = t;
+                __syncwarp();
+                double sa = 0;
+                for (int l = 0; l < 32; ++l) sa += rd[l][lane];
+                if (part == 0) rs_acc += sa; else rf_acc += sa;
+                __syncwarp();
             }
-            rs_acc += reduce_scatter32(ps, lane);
-            rf_acc += reduce_scatter32(pr, lane);
         }
         if (!lower) {
 #pragma unroll
