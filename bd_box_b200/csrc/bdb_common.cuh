@@ -70,6 +70,8 @@ struct bdb_system {
     int n3 = 0;      // 3n
     int npad = 0;    // stored-matrix dimension (3n rounded up to the tile)
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;            // look-ahead panel factorisation
+    cudaEvent_t la_ev[2] = {nullptr, nullptr};
     double inv_L[3] = {0, 0, 0};
     double preDii = 0, preDij = 0;
 
@@ -124,7 +126,7 @@ struct bdb_system {
     bdb::DevBuf<float> M32;                    // same, FP32 (mixed path)
     bdb::DevBuf<double> panel64;               // Cholesky workspace
     bool factor_valid = false;
-    alignas(64) unsigned char tc_map[512];     // CUtensorMaps: TF32 hi / lo panel buffers, FP32 matrix
+    alignas(64) unsigned char tc_map[640];     // CUtensorMaps: TF32 hi / lo panel buffers (x2), FP32 matrix
     bool tc_map_ok = false;
     int sm_count = 148;
     int steps_since_refresh = 0;

@@ -3,15 +3,15 @@
 //
 // M is FP32 (lower triangle: the factor, upper: D, never written here).
 // Super-panel P covers columns p0 = 128P .. p0+127:
-//   k_potrf128  one CTA factors the 128x128 diagonal block in FP64 (blocked
-//               by 16 columns: one warp factors each 16x16 pivot block with
-//               shuffles, then all threads solve and update the rest of the
-//               block in shared memory); L_PP goes to M (FP32) and, in FP64
-//               and transposed, to a 128x128 scratch block for the panel solve;
-//   k_trsm128   one warp per row below the block solves x L_PP^T = a in FP64
-//               (lane l owns columns 4l..4l+3); writes the row to M and its
-//               TF32 split L = L_hi + L_lo (L_hi: low 13 mantissa bits
-//               cleared, exactly TF32; L_lo = L - L_hi) to two panel buffers;
+//   k_potrf128  one CTA factors the 128x128 diagonal block in FP64,
+//               right-looking by 8 columns with the 8x8 pivot blocks factored
+//               in registers by one thread while the others update; L_PP goes
+//               to M (FP32) and, in FP64 and transposed, to a scratch block;
+//   k_trsm128   slabs of 64 rows below the block solve X L_PP^T = A in FP64
+//               (right-looking by 8 columns, 4x4 register tiles); each row
+//               goes to M and its TF32 split L = L_hi + L_lo (L_hi: low 13
+//               mantissa bits cleared, exactly TF32; L_lo = L - L_hi) to two
+//               panel buffers;
 //   k_syrk_tc   C -= L_i L_j^T over all 128x128 tiles ti >= tj > P of the
 //               trailing lower triangle, with
 //               L_i L_j^T ~= Lhi_i Lhi_j^T + Lhi_i Llo_j^T + Llo_i Lhi_j^T
@@ -162,186 +162,252 @@ __device__ __forceinline__ void tri_index(int idx, int& ti, int& tj)
     tj = idx - i * (i + 1) / 2;
 }
 
+// tile t of a launch -> (ti, tj) relative to the first trailing block:
+// mode 0 all tiles of the lower triangle, 1 only block column 0,
+// 2 all but block column 0
+__device__ __forceinline__ void tile_of_mode(int t, int mode, int& ti, int& tj)
+{
+    if (mode == 1) {
+        ti = t;
+        tj = 0;
+    } else {
+        tri_index(t, ti, tj);
+        if (mode == 2) {
+            ++ti;
+            ++tj;
+        }
+    }
+}
+
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 
 // ------------------------------------------------------------ FP64 panel
 
+// 1/sqrt(x) for x > 0 in FP64: a single-precision estimate refined by two
+// Newton-Raphson steps y <- y (3 - x y^2) / 2 (quadratic convergence:
+// ~2^-22 -> ~2^-44 -> full double precision), a shorter dependency chain
+// than a general double-precision reciprocal square root.
+__device__ __forceinline__ double rsqrt_nr(double x)
+{
+    double y = (double)rsqrtf((float)x);
+    y = y * (1.5 - 0.5 * x * y * y);
+    y = y * (1.5 - 0.5 * x * y * y);
+    return y;
+}
+
+// Pivot block of 8 columns at (c0, c0) of the shared FP64 block, factored
+// by one thread in registers; also leaves 1/L_jj in dinv[c0..c0+7].
+__device__ __forceinline__ bool pivot8(double* S, int c0, double* dinv)
+{
+    double a[8][8];
+    bool ok = true;
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c <= r; ++c) a[r][c] = S[(c0 + r) * LDS + c0 + c];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const double piv = a[j][j];
+        if (!(piv > 0.0)) ok = false;
+        const double inv = rsqrt_nr(piv);
+        a[j][j] = piv * inv;
+        dinv[c0 + j] = inv;
+#pragma unroll
+        for (int r = j + 1; r < 8; ++r) a[r][j] *= inv;
+#pragma unroll
+        for (int r = j + 1; r < 8; ++r)
+#pragma unroll
+            for (int c = j + 1; c <= r; ++c) a[r][c] -= a[r][j] * a[c][j];
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c <= r; ++c) S[(c0 + r) * LDS + c0 + c] = a[r][c];
+    return ok;
+}
+
+// rank-8 update of the lower triangle of the block over rows [rlo, 128) and
+// columns [clo, chi), with the 8 columns c0.. as the update panel. Warps
+// take groups of 4 rows (the row values are broadcast reads), lanes take
+// consecutive columns (conflict-free reads and writes); warps [w0, w0 + nw).
+__device__ __forceinline__ void update8(double* S, int c0, int rlo, int clo, int chi, int w0, int nw)
+{
+    const int warp = (threadIdx.x >> 5) - w0, lane = threadIdx.x & 31;
+    if (warp < 0 || warp >= nw) return;
+    const int ncol = chi - clo;
+    for (int rb = rlo + 4 * warp; rb < PW; rb += 4 * nw) {
+        for (int cb = 0; cb < ncol; cb += 128) {
+            double acc[4][4] = {};
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                double x[4], y[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) x[q] = S[(rb + q) * LDS + c0 + m];
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const int k = clo + cb + lane + 32 * p;
+                    y[p] = k < chi ? S[k * LDS + c0 + m] : 0.0;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) acc[q][p] += x[q] * y[p];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const int k = clo + cb + lane + 32 * p;
+                    if (k < chi && k <= rb + q) S[(rb + q) * LDS + k] -= acc[q][p];
+                }
+        }
+    }
+}
+
+// FP64 factorisation of the 128x128 diagonal block (P, P), right-looking by
+// 8 columns: thread 0 factors the 8x8 pivot block in registers while the
+// other threads finish the previous trailing update (look-ahead inside the
+// block), then all threads solve the rows below it and update the next 8
+// columns.
 __global__ void __launch_bounds__(256) k_potrf128(float* __restrict__ M, int npad, int P, double* __restrict__ Lkk,
                                                   unsigned* __restrict__ status)
 {
     extern __shared__ double S[];   // [PW][LDS]
-    __shared__ double dinv16[16];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    __shared__ double dinv[PW];
+    const int tid = threadIdx.x;
     const size_t base = (size_t)P * PW;
     for (int idx = tid; idx < PW * PW; idx += blockDim.x) {
         const int r = idx / PW, c = idx % PW;
         S[r * LDS + c] = c <= r ? (double)M[(base + r) * npad + base + c] : 0.0;
     }
     __syncthreads();
-    bool bad = false;
-    for (int c0 = 0; c0 < PW; c0 += 16) {
-        // 1. 16x16 pivot block by warp 0 (lane & 15 = row)
-        if (warp == 0) {
-            const int lr = lane & 15;
-            const int r = c0 + lr;
-            double a[16];
-#pragma unroll
-            for (int c = 0; c < 16; ++c) a[c] = S[r * LDS + c0 + c];
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const double piv = __shfl_sync(0xffffffffu, a[j], j);
-                if (!(piv > 0.0)) bad = true;
-                const double inv = rsqrt(piv), d = piv * inv;
-                const double lj = lr == j ? d : (lr > j ? a[j] * inv : a[j]);
-                a[j] = lj;
-#pragma unroll
-                for (int c = j + 1; c < 16; ++c) {
-                    const double lcj = __shfl_sync(0xffffffffu, lj, c);
-                    if (lr >= c) a[c] -= lj * lcj;
-                }
-            }
-            if (lane < 16) {
-#pragma unroll
-                for (int c = 0; c < 16; ++c)
-                    if (c <= lr) S[r * LDS + c0 + c] = a[c];
-            }
-        }
-        if (tid < 16) dinv16[tid] = 1.0 / S[(c0 + tid) * LDS + c0 + tid];
-        __syncthreads();
-        // 2. rows below inside the block: x L16^T = a
-        const int nrow = PW - c0 - 16;
+    bool ok = true;
+    if (tid == 0) ok = pivot8(S, 0, dinv);
+    __syncthreads();
+    for (int c0 = 0; c0 < PW; c0 += 8) {
+        // rows below the pivot block: x L8^T = a
+        const int nrow = PW - c0 - 8;
         if (tid < nrow) {
-            const int r = c0 + 16 + tid;
-            double x[16];
+            const int r = c0 + 8 + tid;
+            double x[8];
 #pragma unroll
-            for (int c = 0; c < 16; ++c) x[c] = S[r * LDS + c0 + c];
+            for (int c = 0; c < 8; ++c) x[c] = S[r * LDS + c0 + c];
 #pragma unroll
-            for (int m = 0; m < 16; ++m) {
-                x[m] *= dinv16[m];
+            for (int m = 0; m < 8; ++m) {
+                x[m] *= dinv[c0 + m];
 #pragma unroll
-                for (int c = m + 1; c < 16; ++c) x[c] -= S[(c0 + c) * LDS + c0 + m] * x[m];
+                for (int c = m + 1; c < 8; ++c) x[c] -= S[(c0 + c) * LDS + c0 + m] * x[m];
             }
 #pragma unroll
-            for (int c = 0; c < 16; ++c) S[r * LDS + c0 + c] = x[c];
+            for (int c = 0; c < 8; ++c) S[r * LDS + c0 + c] = x[c];
         }
         __syncthreads();
-        // 3. trailing update of the block, 4x4 register tiles (lower triangle)
-        const int nb4 = nrow / 4;
-        const int cnt = nb4 * (nb4 + 1) / 2;
-        for (int e = tid; e < cnt; e += blockDim.x) {
-            int br, bc;
-            tri_index(e, br, bc);
-            const int r0 = c0 + 16 + 4 * br, k0 = c0 + 16 + 4 * bc;
-            double acc[4][4] = {};
-#pragma unroll 4
-            for (int m = 0; m < 16; ++m) {
-                double a[4], b[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    a[q] = S[(r0 + q) * LDS + c0 + m];
-                    b[q] = S[(k0 + q) * LDS + c0 + m];
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-#pragma unroll
-                    for (int p = 0; p < 4; ++p) acc[q][p] += a[q] * b[p];
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int p = 0; p < 4; ++p)
-                    if (k0 + p <= r0 + q) S[(r0 + q) * LDS + k0 + p] -= acc[q][p];
+        if (nrow == 0) break;
+        // the next 8 columns first (they hold the next pivot block) ...
+        update8(S, c0, c0 + 8, c0 + 8, c0 + 16, 0, 8);
+        __syncthreads();
+        // ... then the next pivot (thread 0) beside the rest of the update (warps 1-7)
+        if (tid == 0) {
+            ok = pivot8(S, c0 + 8, dinv) && ok;
+        } else if (c0 + 16 < PW) {
+            update8(S, c0, c0 + 16, c0 + 16, PW, 1, 7);
         }
         __syncthreads();
     }
-    if (bad) atomicOr(status, ST_NOT_SPD);
+    if (!ok) atomicOr(status, ST_NOT_SPD);
     // L_PP to M (FP32, lower) and, transposed, to the FP64 scratch block:
     // LkkT[m][c] = L[c][m], the layout the panel solve reads
     for (int idx = tid; idx < PW * PW; idx += blockDim.x) {
         const int r = idx / PW, c = idx % PW;
         if (c <= r) M[(base + r) * npad + base + c] = (float)S[r * LDS + c];
-        const int m = idx / PW, cc = idx % PW;
-        Lkk[idx] = cc >= m ? S[cc * LDS + m] : 0.0;
+        Lkk[idx] = c >= r ? S[c * LDS + r] : 0.0;
     }
 }
 
-// rows below block P: x L_PP^T = a; each warp solves R = 4 rows at once so
-// every row of L_PP read from shared memory serves four rows; writes M and
-// the split panel
-static constexpr int TRSM_R = 4;
+// Rows below block P: X L_PP^T = A for a slab of 64 rows per CTA, in FP64
+// in shared memory, right-looking by 8 columns: each row solves its 8
+// columns (one thread per row), then 4x4 register tiles update the columns
+// to the right. Writes the rows to M and their TF32 split to the panel
+// buffers.
+static constexpr int TRSM_ROWS = 64;
+static constexpr int TRSM_LDX = PW + 1;
+static constexpr int TRSM_SMEM = (PW * PW + TRSM_ROWS * TRSM_LDX + PW) * 8;
 
-__global__ void __launch_bounds__(512) k_trsm128(float* __restrict__ M, int npad, int P, const double* __restrict__ Lkk,
+__global__ void __launch_bounds__(256) k_trsm128(float* __restrict__ M, int npad, int P, const double* __restrict__ LkkT,
                                                  float* __restrict__ Lhi, float* __restrict__ Llo)
 {
-    extern __shared__ double Lt[];   // Lt[m][c] = L[c][m], [PW][PW]
-    __shared__ double dinv[PW];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int idx = tid; idx < PW * PW / 2; idx += blockDim.x)
-        reinterpret_cast<double2*>(Lt)[idx] = reinterpret_cast<const double2*>(Lkk)[idx];   // already transposed
-    if (tid < PW) dinv[tid] = 1.0 / Lkk[tid * PW + tid];
-    __syncthreads();
+    extern __shared__ double sh[];
+    double* Lt = sh;                              // Lt[m][c] = L[c][m]
+    double* X = sh + PW * PW;                     // [TRSM_ROWS][TRSM_LDX]
+    double* dinv = X + TRSM_ROWS * TRSM_LDX;
+    const int tid = threadIdx.x;
     const size_t base = (size_t)P * PW;
-    const int nw = blockDim.x >> 5;
-    const size_t first = base + PW;
-    for (size_t row0 = first + ((size_t)blockIdx.x * nw + warp) * TRSM_R; row0 < (size_t)npad;
-         row0 += (size_t)gridDim.x * nw * TRSM_R) {
-        double x[TRSM_R][4];
+    const size_t row0 = base + PW + (size_t)blockIdx.x * TRSM_ROWS;
+    const int nrow = (int)min((size_t)TRSM_ROWS, (size_t)npad - row0);
+    for (int idx = tid; idx < PW * PW / 2; idx += blockDim.x)
+        reinterpret_cast<double2*>(Lt)[idx] = reinterpret_cast<const double2*>(LkkT)[idx];
+    for (int idx = tid; idx < TRSM_ROWS * PW; idx += blockDim.x) {
+        const int r = idx / PW, c = idx % PW;
+        X[r * TRSM_LDX + c] = r < nrow ? (double)M[(row0 + r) * npad + base + c] : 0.0;
+    }
+    if (tid < PW) dinv[tid] = 1.0 / LkkT[tid * PW + tid];
+    __syncthreads();
+    for (int c0 = 0; c0 < PW; c0 += 8) {
+        if (tid < TRSM_ROWS) {
+            double x[8];
 #pragma unroll
-        for (int q = 0; q < TRSM_R; ++q) {
-            const size_t row = row0 + q;
-            float4 a4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (row < (size_t)npad) a4 = reinterpret_cast<const float4*>(M + row * npad + base)[lane];
-            x[q][0] = a4.x;
-            x[q][1] = a4.y;
-            x[q][2] = a4.z;
-            x[q][3] = a4.w;
+            for (int c = 0; c < 8; ++c) x[c] = X[tid * TRSM_LDX + c0 + c];
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                x[m] *= dinv[c0 + m];
+#pragma unroll
+                for (int c = m + 1; c < 8; ++c) x[c] -= Lt[(c0 + m) * PW + c0 + c] * x[m];
+            }
+#pragma unroll
+            for (int c = 0; c < 8; ++c) X[tid * TRSM_LDX + c0 + c] = x[c];
         }
-#pragma unroll 1
-        for (int mb = 0; mb < PW / 4; ++mb) {
+        __syncthreads();
+        const int ncol = PW - c0 - 8;
+        if (ncol == 0) break;
+        // X[:, c0+8:] -= X[:, c0:c0+8] L[c0+8:, c0:c0+8]^T: each warp takes 8
+        // rows (broadcast reads of X), lanes take consecutive columns
+        // (conflict-free reads of L^T and writes of X)
+        {
+            const int warp = tid >> 5, lane = tid & 31;
+            const int rbase = 8 * warp;
+            double acc[8][4] = {};
 #pragma unroll
-            for (int qq = 0; qq < 4; ++qq) {
-                const int m = 4 * mb + qq;
-                const double dm = dinv[m];
-                const double2 l01 = *reinterpret_cast<const double2*>(&Lt[m * PW + 4 * lane]);
-                const double2 l23 = *reinterpret_cast<const double2*>(&Lt[m * PW + 4 * lane + 2]);
+            for (int m = 0; m < 8; ++m) {
+                double y[4];
 #pragma unroll
-                for (int q = 0; q < TRSM_R; ++q) {
-                    if (lane == mb) x[q][qq] *= dm;
-                    const double xm = __shfl_sync(0xffffffffu, x[q][qq], mb);
-                    if (lane > mb) {
-                        x[q][0] -= l01.x * xm;
-                        x[q][1] -= l01.y * xm;
-                        x[q][2] -= l23.x * xm;
-                        x[q][3] -= l23.y * xm;
-                    } else if (lane == mb) {
-                        if (qq < 1) x[q][1] -= l01.y * xm;
-                        if (qq < 2) x[q][2] -= l23.x * xm;
-                        if (qq < 3) x[q][3] -= l23.y * xm;
-                    }
+                for (int p = 0; p < 4; ++p) {
+                    const int k = c0 + 8 + lane + 32 * p;
+                    y[p] = k < PW ? Lt[(c0 + m) * PW + k] : 0.0;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const double x = X[(rbase + q) * TRSM_LDX + c0 + m];
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) acc[q][p] += x * y[p];
                 }
             }
-        }
 #pragma unroll
-        for (int q = 0; q < TRSM_R; ++q) {
-            const size_t row = row0 + q;
-            if (row >= (size_t)npad) break;
-            float4 o, h, l;
-            o.x = (float)x[q][0];
-            o.y = (float)x[q][1];
-            o.z = (float)x[q][2];
-            o.w = (float)x[q][3];
-            h.x = tf32_hi(o.x);
-            h.y = tf32_hi(o.y);
-            h.z = tf32_hi(o.z);
-            h.w = tf32_hi(o.w);
-            l.x = o.x - h.x;
-            l.y = o.y - h.y;
-            l.z = o.z - h.z;
-            l.w = o.w - h.w;
-            reinterpret_cast<float4*>(M + row * npad + base)[lane] = o;
-            reinterpret_cast<float4*>(Lhi + row * PW)[lane] = h;
-            reinterpret_cast<float4*>(Llo + row * PW)[lane] = l;
+            for (int q = 0; q < 8; ++q)
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const int k = c0 + 8 + lane + 32 * p;
+                    if (k < PW) X[(rbase + q) * TRSM_LDX + k] -= acc[q][p];
+                }
         }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < nrow * PW; idx += blockDim.x) {
+        const int r = idx / PW, c = idx % PW;
+        const float o = (float)X[r * TRSM_LDX + c];
+        const float h = tf32_hi(o);
+        M[(row0 + r) * npad + base + c] = o;
+        Lhi[(row0 + r) * PW + c] = h;
+        Llo[(row0 + r) * PW + c] = o - h;
     }
 }
 
@@ -361,7 +427,7 @@ __device__ __forceinline__ float4* c_chunk(unsigned char* cbuf, int cc, int r, i
 
 __global__ void __launch_bounds__(192, 1)
 k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
-          const __grid_constant__ CUtensorMap map_c, int t0, int ntiles, unsigned* __restrict__ status)
+          const __grid_constant__ CUtensorMap map_c, int t0, int ntiles, int mode, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -402,7 +468,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             uint32_t g = 0;
             for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
                 int ti, tj;
-                tri_index(t, ti, tj);
+                tile_of_mode(t, mode, ti, tj);
                 const int ra = (t0 + ti) * PW, rb = (t0 + tj) * PW;
                 for (int kc = 0; kc < NCHUNK; ++kc, ++g) {
                     const int s = g % STAGES;
@@ -421,7 +487,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             uint32_t tl = 0;
             for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++tl) {
                 int ti, tj;
-                tri_index(t, ti, tj);
+                tile_of_mode(t, mode, ti, tj);
                 const int ra = (t0 + ti) * PW, rb = (t0 + tj) * PW;
                 if (!mbar_wait(smem_u32(&bars.cempty), (tl & 1) ^ 1, &abort_flag)) break;
                 const uint32_t cb = smem_u32(&bars.cfull);
@@ -470,7 +536,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
         uint32_t tl = 0;
         for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++tl) {
             int ti, tj;
-            tri_index(t, ti, tj);
+            tile_of_mode(t, mode, ti, tj);
             const uint32_t b = tl & 1;
             if (!mbar_wait(smem_u32(&bars.accfull[b]), (tl >> 1) & 1, &abort_flag)) break;
             if (!mbar_wait(smem_u32(&bars.cfull), tl & 1, &abort_flag)) break;
@@ -562,26 +628,39 @@ static int make_panel_map(float* buf, int rows, CUtensorMap* map, int cols = PW)
     return BDB_OK;
 }
 
+// scratch layout in panel64: two panel buffers (hi, lo: FP32 [npad][128]
+// each), then two FP64 128x128 blocks L_PP^T, for even and odd panels
+static void panel_ptrs(bdb_system* s, int par, float** hi, float** lo, double** lkk)
+{
+    const size_t pan = (size_t)s->npad * PW;
+    float* base = reinterpret_cast<float*>(s->panel64.p);
+    *hi = base + (size_t)par * 2 * pan;
+    *lo = *hi + pan;
+    *lkk = reinterpret_cast<double*>(base + 4 * pan) + (size_t)par * PW * PW;
+}
+
 static int tc_setup(bdb_system* s)
 {
     if (s->tc_map_ok) return BDB_OK;
     const size_t pan = (size_t)s->npad * PW;
-    if (s->panel64.alloc(pan + PW * PW + 64)) return BDB_ERR_NOMEM;   // hi + lo (FP32 each) + L_PP (FP64)
-    float* hi = reinterpret_cast<float*>(s->panel64.p);
-    float* lo = hi + pan;
+    if (s->panel64.alloc(2 * pan + 2 * PW * PW + 64)) return BDB_ERR_NOMEM;
     BDB_CUDA(cudaMemset(s->panel64.p, 0, s->panel64.n * sizeof(double)));
-    CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(s->tc_map);
-    int rc = make_panel_map(hi, s->npad, &maps[0]);
-    if (rc) return rc;
-    rc = make_panel_map(lo, s->npad, &maps[1]);
-    if (rc) return rc;
-    rc = make_panel_map(s->M32.p, s->npad, &maps[2], s->npad);
+    CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(s->tc_map);   // hi0, lo0, hi1, lo1, M
+    for (int par = 0; par < 2; ++par) {
+        float *hi, *lo;
+        double* lkk;
+        panel_ptrs(s, par, &hi, &lo, &lkk);
+        int rc = make_panel_map(hi, s->npad, &maps[2 * par]);
+        if (rc) return rc;
+        rc = make_panel_map(lo, s->npad, &maps[2 * par + 1]);
+        if (rc) return rc;
+    }
+    int rc = make_panel_map(s->M32.p, s->npad, &maps[4], s->npad);
     if (rc) return rc;
     BDB_CUDA(cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_potrf128, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(PW * LDS * sizeof(double))));
-    BDB_CUDA(cudaFuncSetAttribute(k_trsm128, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(PW * PW * sizeof(double))));
+    BDB_CUDA(cudaFuncSetAttribute(k_trsm128, cudaFuncAttributeMaxDynamicSharedMemorySize, TRSM_SMEM));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -590,29 +669,50 @@ static int tc_setup(bdb_system* s)
     return BDB_OK;
 }
 
+// Factorisation with one panel of look-ahead. For panel P the trailing
+// update is split: block column P+1 first (main stream), then the FP64
+// diagonal factorisation of block P+1 runs on the second stream on an SM
+// that the persistent update of the remaining tiles leaves free; the panel
+// solve of P+1 follows once both are done. Panel buffers alternate between
+// even and odd panels so the two never share one.
 int factor_mixed_tc(bdb_system* s)
 {
     int rc = tc_setup(s);
     if (rc) return rc;
     const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(s->tc_map);
-    const size_t pan = (size_t)s->npad * PW;
-    float* hi = reinterpret_cast<float*>(s->panel64.p);
-    float* lo = hi + pan;
-    double* Lkk = reinterpret_cast<double*>(lo + pan);
     const int nt = s->npad / PW;
-    for (int P = 0; P < nt; ++P) {
-        k_potrf128<<<1, 256, PW * LDS * sizeof(double), s->stream>>>(s->M32.p, s->npad, P, Lkk, s->status.p);
-        s->launches += 1;
+    cudaStream_t st = s->stream, st2 = s->stream2;
+    float *hi, *lo;
+    double* lkk;
+    panel_ptrs(s, 0, &hi, &lo, &lkk);
+    k_potrf128<<<1, 256, PW * LDS * sizeof(double), st>>>(s->M32.p, s->npad, 0, lkk, s->status.p);
+    s->launches += 1;
+    for (int P = 0; P + 1 < nt; ++P) {
+        const int par = P & 1;
+        panel_ptrs(s, par, &hi, &lo, &lkk);
         const int rows_below = s->npad - (P + 1) * PW;
-        if (rows_below <= 0) break;
-        const int warps = 16;
-        const int blocks = std::min(s->sm_count, (rows_below + warps * TRSM_R - 1) / (warps * TRSM_R));
-        k_trsm128<<<blocks, 32 * warps, PW * PW * sizeof(double), s->stream>>>(s->M32.p, s->npad, P, Lkk, hi, lo);
+        k_trsm128<<<(rows_below + TRSM_ROWS - 1) / TRSM_ROWS, 256, TRSM_SMEM, st>>>(s->M32.p, s->npad, P, lkk, hi, lo);
         const int rem = nt - P - 1;
-        const int tiles = rem * (rem + 1) / 2;
-        const int grid = std::min(s->sm_count, tiles);
-        k_syrk_tc<<<grid, 192, SYRK_SMEM, s->stream>>>(maps[0], maps[1], maps[2], P + 1, tiles, s->status.p);
+        // block column P+1 of the trailing matrix
+        k_syrk_tc<<<std::min(s->sm_count, rem), 192, SYRK_SMEM, st>>>(maps[2 * par], maps[2 * par + 1], maps[4], P + 1,
+                                                                      rem, 1, s->status.p);
         s->launches += 2;
+        // diagonal block P+1 on the side stream, beside the rest of the update
+        float *hi2, *lo2;
+        double* lkk2;
+        panel_ptrs(s, par ^ 1, &hi2, &lo2, &lkk2);
+        BDB_CUDA(cudaEventRecord(s->la_ev[0], st));
+        BDB_CUDA(cudaStreamWaitEvent(st2, s->la_ev[0], 0));
+        k_potrf128<<<1, 256, PW * LDS * sizeof(double), st2>>>(s->M32.p, s->npad, P + 1, lkk2, s->status.p);
+        BDB_CUDA(cudaEventRecord(s->la_ev[1], st2));
+        s->launches += 1;
+        const int rest = rem * (rem + 1) / 2 - rem;
+        if (rest > 0) {
+            k_syrk_tc<<<std::min(s->sm_count - 1, rest), 192, SYRK_SMEM, st>>>(maps[2 * par], maps[2 * par + 1], maps[4],
+                                                                           P + 1, rest, 2, s->status.p);
+            s->launches += 1;
+        }
+        BDB_CUDA(cudaStreamWaitEvent(st, s->la_ev[1], 0));
     }
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;

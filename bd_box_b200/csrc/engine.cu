@@ -225,9 +225,12 @@ int bdb_create(bdb_system** out, const bdb_params* p, const double* coord, const
             return BDB_ERR_NOMEM;                \
         }                                        \
     } while (0)
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        delete s;
-        return fail(BDB_ERR_CUDA, "cudaStreamCreate failed");
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->la_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->la_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        bdb_destroy(s);
+        return fail(BDB_ERR_CUDA, "stream/event creation failed");
     }
     s->segs.push_back(Segment{0, s->n, 0});
     TRYA(s->d_segs, 1);
@@ -269,6 +272,10 @@ int bdb_destroy(bdb_system* s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& r : s->phases)
         for (auto e : r.ev) cudaEventDestroy(e);
+    if (s->stream2) cudaStreamSynchronize(s->stream2);
+    for (auto e : s->la_ev)
+        if (e) cudaEventDestroy(e);
+    if (s->stream2) cudaStreamDestroy(s->stream2);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return BDB_OK;
