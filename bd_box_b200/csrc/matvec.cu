@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <string>
 
 #include "bdb_common.cuh"
 
@@ -192,4 +193,60 @@ int stored_matvec(bdb_system* s, bool want_rs)
     return BDB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// No-allocation entry point: the same two products on caller-owned device
+// buffers, with the partial sums kept in a fixed-size array in this file's
+// device memory instead of a buffer obtained from cudaMalloc.
+
+static constexpr int NOALLOC_MAX_N3 = 3072;              // 1024 beads
+static constexpr int NOALLOC_MAX_SEG = 4;
+static constexpr size_t NOALLOC_SCRATCH =
+    (size_t)NOALLOC_MAX_SEG * NOALLOC_MAX_N3 * 2 + (size_t)(NOALLOC_MAX_N3 / STRIP) * NOALLOC_MAX_N3;
+
+// Scratch for row and column partial sums (2.5 MB of doubles), one copy on
+// every device that loads the library, kept until the process exits.
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH];
+
+static constexpr int NOALLOC_MAX_DEVICES = 64;
+static double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
 }  // namespace bdb
+
+using bdb::g_noalloc_scratch;
+
+extern "C" int bdb_stored_matvec_noalloc(const float* M, int n3, int ld, const double* dD, const double* F,
+                                         const double* X, double pre, double* Rf, double* Rs, void* stream)
+{
+    using namespace bdb;
+    if (!M || !dD || !F || !X || !Rf || !Rs) return fail(BDB_ERR_ARG, "null device pointer");
+    if (n3 <= 0 || n3 > NOALLOC_MAX_N3)
+        return fail(BDB_ERR_ARG, "bdb_stored_matvec_noalloc: 3N must be in 1.." + std::to_string(NOALLOC_MAX_N3) +
+                                     " (its scratch array has a fixed size), got " + std::to_string(n3));
+    if (ld < n3 || ld % 4 != 0 || reinterpret_cast<uintptr_t>(M) % 16 != 0)
+        return fail(BDB_ERR_ARG, "bdb_stored_matvec_noalloc: ld must be >= 3N and a multiple of 4, M 16-byte aligned");
+    int dev = 0;
+    BDB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(BDB_ERR_ARG, "device index out of range");
+    if (!g_noalloc_ptr[dev]) {
+        // set-up, once per device with that device current: the host-side
+        // symbol is only a stand-in, the kernels need its device address
+        void* p = nullptr;
+        BDB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nstrip = (n3 + STRIP - 1) / STRIP;
+    int nseg = std::min(NOALLOC_MAX_SEG, std::max(1, (148 * 16 + nstrip - 1) / nstrip));
+    const int seg_cols = ((n3 + nseg - 1) / nseg + 127) / 128 * 128;
+    nseg = (n3 + seg_cols - 1) / seg_cols;
+    // every partial that k_mv_finish reads is written first by k_strip_mv,
+    // so nothing in the scratch has to start at zero
+    double* rowp = g_noalloc_ptr[dev];
+    double* colp = rowp + (size_t)nseg * n3 * 2;
+    const int blocks = (nstrip * nseg + WARPS - 1) / WARPS;
+    k_strip_mv<float><<<blocks, 32 * WARPS, 0, st>>>(M, n3, ld, nseg, seg_cols, F, X, rowp, colp);
+    BDB_CUDA(cudaGetLastError());
+    k_mv_finish<<<(n3 + 255) / 256, 256, 0, st>>>(n3, nseg, rowp, colp, dD, F, pre, Rf, Rs, 1);
+    BDB_CUDA(cudaGetLastError());
+    return BDB_OK;
+}

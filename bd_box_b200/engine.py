@@ -41,7 +41,7 @@ EXPORTS = [
     "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
     "bdb_compute_r", "bdb_step", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
-    "bdb_reset_stats", "bdb_launches", "bdb_stream",
+    "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc",
 ]
 
 
@@ -101,6 +101,8 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_launches.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
     lib.bdb_stream.argtypes = [C.c_void_p]
     lib.bdb_stream.restype = C.c_void_p
+    lib.bdb_stored_matvec_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
 

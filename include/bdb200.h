@@ -168,6 +168,28 @@ int bdb_launches(bdb_system* s, long long* count);
 /* The CUDA stream all work of this system is issued on (cudaStream_t). */
 void* bdb_stream(bdb_system* s);
 
+/* No-allocation variant of the Cholesky path's per-step products; it has no
+ * counterpart in the reference. For callers that cannot call cudaMalloc --
+ * a host whose device memory is entirely owned by its own pool allocator, or
+ * a real-time loop that must not allocate -- this computes, on buffers the
+ * caller already owns (all device pointers):
+ *     Rf = pre * (D F)   and   Rs = L X
+ * from an FP32 matrix M (ld floats per row, 16-byte aligned, ld a multiple
+ * of 4) whose strict upper triangle holds D, whose lower triangle including
+ * the diagonal holds its Cholesky factor L, and from dD = diag(D). It
+ * allocates nothing: its partial sums live in a fixed array in the
+ * library's device memory (2.5 MB on every device that loads the library,
+ * held until the process exits), so 3N is limited to 3072 (1024 beads) and
+ * larger sizes are rejected with BDB_ERR_ARG. The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture. All calls share the array: calls
+ * whose work overlaps on the GPU (different streams, or different host
+ * threads) race and must be serialised by the caller. `stream` is a
+ * cudaStream_t or NULL for the default stream. */
+int bdb_stored_matvec_noalloc(const float* M, int n3, int ld, const double* dD,
+                              const double* F, const double* X, double pre,
+                              double* Rf, double* Rs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
