@@ -480,6 +480,13 @@ int bdb_step(bdb_system* s, int K, const double* gauss)
     return ov ? 1 : 0;
 }
 
+int bdb_set_dt(bdb_system* s, double dt)
+{
+    if (!s || !(dt > 0.0)) return fail(BDB_ERR_ARG, "time step must be positive");
+    s->p.dt = dt;
+    return BDB_OK;
+}
+
 int bdb_factor_error(bdb_system* s, double* rel_err)
 {
     if (!s || !rel_err) return fail(BDB_ERR_ARG, "null argument");

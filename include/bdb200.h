@@ -15,8 +15,9 @@
  *    entry points of src/diff_alg and src/potentials (diff_tensor.h:166-253,
  *    calc_func.h:60-106), implemented on the engine and linked in place of
  *    the CPU translation units, exactly as BD_BOX swaps its CUDA build in
- *    (src/Makefile.am:44-78). Those symbols read BD_BOX's globals, so they
- *    are declared at the end of this header only for BDB_DROPIN builds.
+ *    (src/Makefile.am:44-78). Those symbols read and write BD_BOX's
+ *    globals, so their declarations are BD_BOX's own headers; they are
+ *    defined in bd_box_b200/dropin/bdbox_dropin.c.
  *
  * Every bdb_* call returns BDB_OK (0) or a negative BDB_ERR_* code;
  * bdb_last_error() gives the message of the last failure on this thread.
@@ -148,6 +149,10 @@ int bdb_compute_r(bdb_system* s, const double* gauss, double* Rs);
  * Returns the OR of the overlap flags of the steps (retries are the
  * caller's, as in comp_step_ermak) or a negative error. */
 int bdb_step(bdb_system* s, int K, const double* gauss);
+
+/* Time step of the following steps (curr_dt, diff_decl.c:68): the variable
+ * step of comp_step_ermak halves it on overlap (diff_comp.c:162-165). */
+int bdb_set_dt(bdb_system* s, double dt);
 
 /* Cholesky of the stored tensor at the current coordinates (diagnostics):
  * rel_err = ||L L^T - D||_F / ||D||_F evaluated on the device in FP64. */
