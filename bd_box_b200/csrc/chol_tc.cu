@@ -6,9 +6,10 @@
 //   k_potrf128  one CTA factors the 128x128 diagonal block in FP64,
 //               right-looking by 8 columns with the 8x8 pivot blocks factored
 //               in registers by one thread while the others update; L_PP goes
-//               to M (FP32) and, in FP64 and transposed, to a scratch block;
+//               to M (FP32), and its inverse W = L_PP^-1 (FP64, blocked
+//               forward substitution) transposed to a scratch block;
 //   k_trsm128   slabs of 64 rows below the block solve X L_PP^T = A in FP64
-//               (right-looking by 8 columns, 4x4 register tiles); each row
+//               as the product X = A W^T (no sequential dependency); each row
 //               goes to M and its TF32 split L = L_hi + L_lo (L_hi: low 13
 //               mantissa bits cleared, exactly TF32; L_lo = L - L_hi) to two
 //               panel buffers;
@@ -226,188 +227,265 @@ __device__ __forceinline__ bool pivot8(double* S, int c0, double* dinv)
     return ok;
 }
 
-// rank-8 update of the lower triangle of the block over rows [rlo, 128) and
-// columns [clo, chi), with the 8 columns c0.. as the update panel. Warps
-// take groups of 4 rows (the row values are broadcast reads), lanes take
-// consecutive columns (conflict-free reads and writes); warps [w0, w0 + nw).
-__device__ __forceinline__ void update8(double* S, int c0, int rlo, int clo, int chi, int w0, int nw)
+// W_kk = L_kk^-1 for the 8x8 diagonal block at c0 (lanes 0-7, one column
+// each, forward substitution); stored transposed in the strict upper
+// triangle of the block (S[c0+c][c0+i] = W[i][c], c < i), diagonal in dinv.
+__device__ __forceinline__ void inverse8(double* S, int c0, const double* dinv, int lane)
 {
-    const int warp = (threadIdx.x >> 5) - w0, lane = threadIdx.x & 31;
-    if (warp < 0 || warp >= nw) return;
-    const int ncol = chi - clo;
-    for (int rb = rlo + 4 * warp; rb < PW; rb += 4 * nw) {
-        for (int cb = 0; cb < ncol; cb += 128) {
-            double acc[4][4] = {};
+    if (lane < 8) {
+        const int c = lane;
+        double w[8];
 #pragma unroll
-            for (int m = 0; m < 8; ++m) {
-                double x[4], y[4];
+        for (int i = 0; i < 8; ++i) {
+            double v = i == c ? 1.0 : 0.0;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) x[q] = S[(rb + q) * LDS + c0 + m];
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const int k = clo + cb + lane + 32 * p;
-                    y[p] = k < chi ? S[k * LDS + c0 + m] : 0.0;
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-#pragma unroll
-                    for (int p = 0; p < 4; ++p) acc[q][p] += x[q] * y[p];
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const int k = clo + cb + lane + 32 * p;
-                    if (k < chi && k <= rb + q) S[(rb + q) * LDS + k] -= acc[q][p];
-                }
+            for (int m = 0; m < i; ++m) v -= S[(c0 + i) * LDS + c0 + m] * w[m];
+            w[i] = i >= c ? v * dinv[c0 + i] : 0.0;
         }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (i > c) S[(c0 + c) * LDS + c0 + i] = w[i];
     }
 }
 
-// FP64 factorisation of the 128x128 diagonal block (P, P), right-looking by
-// 8 columns: thread 0 factors the 8x8 pivot block in registers while the
-// other threads finish the previous trailing update (look-ahead inside the
-// block), then all threads solve the rows below it and update the next 8
-// columns.
-__global__ void __launch_bounds__(256) k_potrf128(float* __restrict__ M, int npad, int P, double* __restrict__ Lkk,
-                                                  unsigned* __restrict__ status)
+// Row i of block column c0 below the diagonal: L[i][c0+c] = sum_{m <= c}
+// A[i][c0+m] W_kk[c][m] (X L_kk^T = A solved with the inverse). Warp 0 and
+// the bulk warps both call this, so a row gets the same bits from either.
+__device__ __forceinline__ void solve_row8(const double* S, int c0, int i, const double* dinv, double* l)
 {
-    extern __shared__ double S[];   // [PW][LDS]
-    __shared__ double dinv[PW];
-    const int tid = threadIdx.x;
+    double a[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[c] = S[i * LDS + c0 + c];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        double v = a[c] * dinv[c0 + c];
+#pragma unroll
+        for (int m = 0; m < c; ++m) v += a[m] * S[(c0 + m) * LDS + c0 + c];
+        l[c] = v;
+    }
+}
+
+static constexpr int POTRF_THREADS = 512;
+static constexpr int POTRF_SMEM = (PW * LDS + 8 * PW + PW) * 8;
+
+// FP64 factorisation of the 128x128 diagonal block (P, P) and its inverse,
+// right-looking over 16 blocks of 8 columns. In iteration k warp 0 runs the
+// critical path: the next 8 rows of block column k, the update of diagonal
+// block k+1 and its factorisation (one thread, in registers) and inverse.
+// Warps 1-15 meanwhile solve the other rows of block column k, form row
+// block k of W = L^-1, and apply the rank-8 update of block column k to the
+// trailing lower triangle (L) and to the partial sums of W (upper triangle,
+// transposed: S[j][i] accumulates -sum_m L[i][m] W[m][j] until row block
+// i/8 of W is formed). Bk[m][j] stages the update's right-hand operand:
+// W[c0+m][j] for j < c0+8, L[j][c0+m] for j >= c0+8.
+__global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict__ M, int npad, int P,
+                                                            double* __restrict__ Wt, unsigned* __restrict__ status)
+{
+    extern __shared__ double S[];   // [PW][LDS], then Bk [8][PW], dinv [PW]
+    double* Bk = S + PW * LDS;
+    double* dinv = Bk + 8 * PW;
+    __shared__ int bad;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const size_t base = (size_t)P * PW;
-    for (int idx = tid; idx < PW * PW; idx += blockDim.x) {
-        const int r = idx / PW, c = idx % PW;
-        S[r * LDS + c] = c <= r ? (double)M[(base + r) * npad + base + c] : 0.0;
+    for (int idx = tid; idx < PW * PW / 4; idx += blockDim.x) {
+        const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
+        const float4 v = *reinterpret_cast<const float4*>(M + (base + r) * npad + base + c);
+        double* s = S + r * LDS + c;
+        s[0] = c <= r ? (double)v.x : 0.0;
+        s[1] = c + 1 <= r ? (double)v.y : 0.0;
+        s[2] = c + 2 <= r ? (double)v.z : 0.0;
+        s[3] = c + 3 <= r ? (double)v.w : 0.0;
+    }
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    if (warp == 0) {
+        if (lane == 0 && !pivot8(S, 0, dinv)) bad = 1;
+        __syncwarp();
+        inverse8(S, 0, dinv, lane);
     }
     __syncthreads();
-    bool ok = true;
-    if (tid == 0) ok = pivot8(S, 0, dinv);
-    __syncthreads();
-    for (int c0 = 0; c0 < PW; c0 += 8) {
-        // rows below the pivot block: x L8^T = a
-        const int nrow = PW - c0 - 8;
-        if (tid < nrow) {
-            const int r = c0 + 8 + tid;
-            double x[8];
+    for (int k = 0; k < PW / 8; ++k) {
+        const int c0 = 8 * k;
+        const bool last = k == PW / 8 - 1;
+        if (warp == 0) {
+            if (!last) {
+                // rows c0+8..c0+15 of block column k
+                if (lane < 8) {
+                    const int i = c0 + 8 + lane;
+                    double l[8];
+                    solve_row8(S, c0, i, dinv, l);
 #pragma unroll
-            for (int c = 0; c < 8; ++c) x[c] = S[r * LDS + c0 + c];
+                    for (int c = 0; c < 8; ++c) {
+                        S[i * LDS + c0 + c] = l[c];
+                        Bk[c * PW + i] = l[c];
+                    }
+                }
+                __syncwarp();
+                asm volatile("bar.arrive 2, %0;" ::"r"(POTRF_THREADS) : "memory");
+                // diagonal block k+1 -= L[k+1][k] L[k+1][k]^T (lower triangle)
+                for (int e = lane; e < 36; e += 32) {
+                    int r = 0;
+                    while ((r + 1) * (r + 2) / 2 <= e) ++r;
+                    const int c = e - r * (r + 1) / 2;
+                    const int ri = c0 + 8 + r, ci = c0 + 8 + c;
+                    double acc = 0.0;
 #pragma unroll
-            for (int m = 0; m < 8; ++m) {
-                x[m] *= dinv[c0 + m];
-#pragma unroll
-                for (int c = m + 1; c < 8; ++c) x[c] -= S[(c0 + c) * LDS + c0 + m] * x[m];
+                    for (int m = 0; m < 8; ++m) acc += S[ri * LDS + c0 + m] * S[ci * LDS + c0 + m];
+                    S[ri * LDS + ci] -= acc;
+                }
+                __syncwarp();
+                if (lane == 0 && !pivot8(S, c0 + 8, dinv)) bad = 1;
+                __syncwarp();
+                inverse8(S, c0 + 8, dinv, lane);
             }
+        } else {
+            const int bt = tid - 32;   // 0 .. POTRF_THREADS-33
+            if (bt < PW - c0 - 16) {
+                // rows c0+16.. of block column k
+                const int i = c0 + 16 + bt;
+                double l[8];
+                solve_row8(S, c0, i, dinv, l);
 #pragma unroll
-            for (int c = 0; c < 8; ++c) S[r * LDS + c0 + c] = x[c];
-        }
-        __syncthreads();
-        if (nrow == 0) break;
-        // the next 8 columns first (they hold the next pivot block) ...
-        update8(S, c0, c0 + 8, c0 + 8, c0 + 16, 0, 8);
-        __syncthreads();
-        // ... then the next pivot (thread 0) beside the rest of the update (warps 1-7)
-        if (tid == 0) {
-            ok = pivot8(S, c0 + 8, dinv) && ok;
-        } else if (c0 + 16 < PW) {
-            update8(S, c0, c0 + 16, c0 + 16, PW, 1, 7);
+                for (int c = 0; c < 8; ++c) {
+                    S[i * LDS + c0 + c] = l[c];
+                    Bk[c * PW + i] = l[c];
+                }
+            } else if (bt >= 128 && bt < 128 + c0) {
+                // row block k of W: W[c0+m][j] = sum_{c <= m} W_kk[m][c] T[c0+c][j]
+                const int j = bt - 128;
+                double t[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) t[c] = S[j * LDS + c0 + c];
+#pragma unroll
+                for (int m = 0; m < 8; ++m) {
+                    double v = t[m] * dinv[c0 + m];
+#pragma unroll
+                    for (int c = 0; c < m; ++c) v += S[(c0 + c) * LDS + c0 + m] * t[c];
+                    S[j * LDS + c0 + m] = v;
+                    Bk[m * PW + j] = v;
+                }
+            } else if (bt >= 256 && bt < 256 + 64) {
+                // W_kk into the staging rows
+                const int m = (bt - 256) >> 3, jj = (bt - 256) & 7;
+                Bk[m * PW + c0 + jj] = jj < m ? S[(c0 + jj) * LDS + c0 + m] : (jj == m ? dinv[c0 + m] : 0.0);
+            }
+            if (!last) {
+                asm volatile("bar.sync 2, %0;" ::"r"(POTRF_THREADS) : "memory");
+                // rank-8 update of row group g (rows 8g..8g+7), columns j <= i:
+                // j < c0+8 -> partial sums of W (S[j][i]); j >= c0+8 -> L (S[i][j]);
+                // the diagonal block k+1 is warp 0's
+                const int g = k + warp;   // warps 1..15 -> g = k+1 ..
+                if (g < PW / 8) {
+                    const int i0 = 8 * g;
+                    const int jmax = g == k + 1 ? c0 + 8 : i0 + 8;
+                    double acc[8][4] = {};
+#pragma unroll
+                    for (int m = 0; m < 8; ++m) {
+                        double b[4];
+#pragma unroll
+                        for (int p = 0; p < 4; ++p) {
+                            const int j = lane + 32 * p;
+                            b[p] = j < jmax ? Bk[m * PW + j] : 0.0;
+                        }
+#pragma unroll
+                        for (int r = 0; r < 8; ++r) {
+                            const double a = Bk[m * PW + i0 + r];
+#pragma unroll
+                            for (int p = 0; p < 4; ++p) acc[r][p] += a * b[p];
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) {
+                        const int i = i0 + r;
+#pragma unroll
+                        for (int p = 0; p < 4; ++p) {
+                            const int j = lane + 32 * p;
+                            if (j < jmax && j <= i) {
+                                if (j < c0 + 8) S[j * LDS + i] -= acc[r][p];
+                                else S[i * LDS + j] -= acc[r][p];
+                            }
+                        }
+                    }
+                }
+            }
         }
         __syncthreads();
     }
-    if (!ok) atomicOr(status, ST_NOT_SPD);
-    // L_PP to M (FP32, lower) and, transposed, to the FP64 scratch block:
-    // LkkT[m][c] = L[c][m], the layout the panel solve reads
+    if (tid == 0 && bad) atomicOr(status, ST_NOT_SPD);
+    // L_PP to M (FP32, lower triangle); Wt[m][c] = W[c][m] (upper triangular,
+    // row-major), the layout the panel solve X = A W^T reads
     for (int idx = tid; idx < PW * PW; idx += blockDim.x) {
         const int r = idx / PW, c = idx % PW;
         if (c <= r) M[(base + r) * npad + base + c] = (float)S[r * LDS + c];
-        Lkk[idx] = c >= r ? S[c * LDS + r] : 0.0;
+        Wt[idx] = r < c ? S[r * LDS + c] : (r == c ? dinv[c] : 0.0);
     }
 }
 
-// Rows below block P: X L_PP^T = A for a slab of 64 rows per CTA, in FP64
-// in shared memory, right-looking by 8 columns: each row solves its 8
-// columns (one thread per row), then 4x4 register tiles update the columns
-// to the right. Writes the rows to M and their TF32 split to the panel
-// buffers.
+// Rows below block P: X L_PP^T = A, i.e. X = A W^T with W = L_PP^-1 from
+// k_potrf128, for a slab of 64 rows per CTA in FP64. Wt = W^T is upper
+// triangular, so X[r][c] = sum_{m <= c} A[r][m] Wt[m][c]: a product with no
+// sequential dependency. Warp w owns rows 8w..8w+7, lane l the columns
+// l + 32p (p = 0..3); column group p only needs m < 32(p+1). Writes the
+// rows to M and their TF32 split to the panel buffers.
 static constexpr int TRSM_ROWS = 64;
 static constexpr int TRSM_LDX = PW + 1;
-static constexpr int TRSM_SMEM = (PW * PW + TRSM_ROWS * TRSM_LDX + PW) * 8;
+static constexpr int TRSM_SMEM = (PW * PW + TRSM_ROWS * TRSM_LDX) * 8;
 
-__global__ void __launch_bounds__(256) k_trsm128(float* __restrict__ M, int npad, int P, const double* __restrict__ LkkT,
+__global__ void __launch_bounds__(256) k_trsm128(float* __restrict__ M, int npad, int P, const double* __restrict__ Wt,
                                                  float* __restrict__ Lhi, float* __restrict__ Llo)
 {
     extern __shared__ double sh[];
-    double* Lt = sh;                              // Lt[m][c] = L[c][m]
-    double* X = sh + PW * PW;                     // [TRSM_ROWS][TRSM_LDX]
-    double* dinv = X + TRSM_ROWS * TRSM_LDX;
+    double* sW = sh;                              // [PW][PW], Wt
+    double* A = sh + PW * PW;                     // [TRSM_ROWS][TRSM_LDX]
     const int tid = threadIdx.x;
     const size_t base = (size_t)P * PW;
     const size_t row0 = base + PW + (size_t)blockIdx.x * TRSM_ROWS;
     const int nrow = (int)min((size_t)TRSM_ROWS, (size_t)npad - row0);
     for (int idx = tid; idx < PW * PW / 2; idx += blockDim.x)
-        reinterpret_cast<double2*>(Lt)[idx] = reinterpret_cast<const double2*>(LkkT)[idx];
-    for (int idx = tid; idx < TRSM_ROWS * PW; idx += blockDim.x) {
-        const int r = idx / PW, c = idx % PW;
-        X[r * TRSM_LDX + c] = r < nrow ? (double)M[(row0 + r) * npad + base + c] : 0.0;
+        reinterpret_cast<double2*>(sW)[idx] = reinterpret_cast<const double2*>(Wt)[idx];
+    for (int idx = tid; idx < TRSM_ROWS * PW / 4; idx += blockDim.x) {
+        const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (r < nrow) v = *reinterpret_cast<const float4*>(M + (row0 + r) * npad + base + c);
+        double* a = A + r * TRSM_LDX + c;
+        a[0] = v.x;
+        a[1] = v.y;
+        a[2] = v.z;
+        a[3] = v.w;
     }
-    if (tid < PW) dinv[tid] = 1.0 / LkkT[tid * PW + tid];
     __syncthreads();
-    for (int c0 = 0; c0 < PW; c0 += 8) {
-        if (tid < TRSM_ROWS) {
-            double x[8];
+    const int warp = tid >> 5, lane = tid & 31;
+    const int rbase = 8 * warp;
+    double acc[8][4] = {};
 #pragma unroll
-            for (int c = 0; c < 8; ++c) x[c] = X[tid * TRSM_LDX + c0 + c];
+    for (int g = 0; g < 4; ++g) {          // m in [32g, 32g + 32): column groups p >= g
+        for (int mm = 0; mm < 32; ++mm) {
+            const int m = 32 * g + mm;
+            double y[4];
 #pragma unroll
-            for (int m = 0; m < 8; ++m) {
-                x[m] *= dinv[c0 + m];
+            for (int p = 0; p < 4; ++p) y[p] = p >= g ? sW[m * PW + lane + 32 * p] : 0.0;
 #pragma unroll
-                for (int c = m + 1; c < 8; ++c) x[c] -= Lt[(c0 + m) * PW + c0 + c] * x[m];
+            for (int q = 0; q < 8; ++q) {
+                const double x = A[(rbase + q) * TRSM_LDX + m];
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+                    if (p >= g) acc[q][p] += x * y[p];
             }
-#pragma unroll
-            for (int c = 0; c < 8; ++c) X[tid * TRSM_LDX + c0 + c] = x[c];
         }
-        __syncthreads();
-        const int ncol = PW - c0 - 8;
-        if (ncol == 0) break;
-        // X[:, c0+8:] -= X[:, c0:c0+8] L[c0+8:, c0:c0+8]^T: each warp takes 8
-        // rows (broadcast reads of X), lanes take consecutive columns
-        // (conflict-free reads of L^T and writes of X)
-        {
-            const int warp = tid >> 5, lane = tid & 31;
-            const int rbase = 8 * warp;
-            double acc[8][4] = {};
-#pragma unroll
-            for (int m = 0; m < 8; ++m) {
-                double y[4];
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const int k = c0 + 8 + lane + 32 * p;
-                    y[p] = k < PW ? Lt[(c0 + m) * PW + k] : 0.0;
-                }
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const double x = X[(rbase + q) * TRSM_LDX + c0 + m];
-#pragma unroll
-                    for (int p = 0; p < 4; ++p) acc[q][p] += x * y[p];
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const int k = c0 + 8 + lane + 32 * p;
-                    if (k < PW) X[(rbase + q) * TRSM_LDX + k] -= acc[q][p];
-                }
-        }
-        __syncthreads();
     }
-    for (int idx = tid; idx < nrow * PW; idx += blockDim.x) {
-        const int r = idx / PW, c = idx % PW;
-        const float o = (float)X[r * TRSM_LDX + c];
-        const float h = tf32_hi(o);
-        M[(row0 + r) * npad + base + c] = o;
-        Lhi[(row0 + r) * PW + c] = h;
-        Llo[(row0 + r) * PW + c] = o - h;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int r = rbase + q;
+        if (r >= nrow) break;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int c = lane + 32 * p;
+            const float o = (float)acc[q][p];
+            const float h = tf32_hi(o);
+            M[(row0 + r) * npad + base + c] = o;
+            Lhi[(row0 + r) * PW + c] = h;
+            Llo[(row0 + r) * PW + c] = o - h;
+        }
     }
 }
 
@@ -658,8 +736,7 @@ static int tc_setup(bdb_system* s)
     int rc = make_panel_map(s->M32.p, s->npad, &maps[4], s->npad);
     if (rc) return rc;
     BDB_CUDA(cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
-    BDB_CUDA(cudaFuncSetAttribute(k_potrf128, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(PW * LDS * sizeof(double))));
+    BDB_CUDA(cudaFuncSetAttribute(k_potrf128, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_trsm128, cudaFuncAttributeMaxDynamicSharedMemorySize, TRSM_SMEM));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -685,7 +762,7 @@ int factor_mixed_tc(bdb_system* s)
     float *hi, *lo;
     double* lkk;
     panel_ptrs(s, 0, &hi, &lo, &lkk);
-    k_potrf128<<<1, 256, PW * LDS * sizeof(double), st>>>(s->M32.p, s->npad, 0, lkk, s->status.p);
+    k_potrf128<<<1, POTRF_THREADS, POTRF_SMEM, st>>>(s->M32.p, s->npad, 0, lkk, s->status.p);
     s->launches += 1;
     for (int P = 0; P + 1 < nt; ++P) {
         const int par = P & 1;
@@ -703,7 +780,7 @@ int factor_mixed_tc(bdb_system* s)
         panel_ptrs(s, par ^ 1, &hi2, &lo2, &lkk2);
         BDB_CUDA(cudaEventRecord(s->la_ev[0], st));
         BDB_CUDA(cudaStreamWaitEvent(st2, s->la_ev[0], 0));
-        k_potrf128<<<1, 256, PW * LDS * sizeof(double), st2>>>(s->M32.p, s->npad, P + 1, lkk2, s->status.p);
+        k_potrf128<<<1, POTRF_THREADS, POTRF_SMEM, st2>>>(s->M32.p, s->npad, P + 1, lkk2, s->status.p);
         BDB_CUDA(cudaEventRecord(s->la_ev[1], st2));
         s->launches += 1;
         const int rest = rem * (rem + 1) / 2 - rem;
