@@ -186,9 +186,23 @@ const char* bdb_version(void) { return "bdb200 1.0 (sm_100a)"; }
 
 const char* bdb_last_error(void) { return g_err.c_str(); }
 
-int bdb_create(bdb_system** out, const bdb_params* p, const double* coord, const double* Q, const double* LJ)
+}  // extern "C"
+
+// One system of nseg independent segments (replicas) of counts[g] beads,
+// stored back to back; nseg = 1 is a single system.
+static int create_system(bdb_system** out, const bdb_params* p, int nseg, const int* counts, const double* coord,
+                         const double* Q, const double* LJ)
 {
-    if (!out || !p || !coord || !Q || !LJ) return fail(BDB_ERR_ARG, "null argument");
+    if (!out || !p || !coord || !Q || !LJ || !counts) return fail(BDB_ERR_ARG, "null argument");
+    if (nseg < 1) return fail(BDB_ERR_ARG, "need at least one segment");
+    long long total = 0;
+    for (int g = 0; g < nseg; ++g) {
+        if (counts[g] < 2) return fail(BDB_ERR_ARG, "every segment needs at least two beads");
+        total += counts[g];
+    }
+    if (total != p->n) return fail(BDB_ERR_ARG, "params.n must equal the sum of the segment bead counts");
+    if (nseg > 1 && p->hydro == BDB_HYDRO_CHOLESKY)
+        return fail(BDB_ERR_UNSUPPORTED, "batched segments need hydro none or geyer (the stored tensor holds one system)");
     if (p->n <= 1) return fail(BDB_ERR_ARG, "need at least two beads");
     if (p->hydro < 0 || p->hydro > 2) return fail(BDB_ERR_ARG, "hydro must be none, cholesky or geyer");
     if (p->bc == 1 && (p->box[0] <= 0 || p->box[1] <= 0 || p->box[2] <= 0))
@@ -232,8 +246,14 @@ int bdb_create(bdb_system** out, const bdb_params* p, const double* coord, const
         bdb_destroy(s);
         return fail(BDB_ERR_CUDA, "stream/event creation failed");
     }
-    s->segs.push_back(Segment{0, s->n, 0});
-    TRYA(s->d_segs, 1);
+    {
+        int b = 0;
+        for (int g = 0; g < nseg; ++g) {
+            s->segs.push_back(Segment{b, counts[g], 0});
+            b += counts[g];
+        }
+    }
+    TRYA(s->d_segs, nseg);
     TRYA(s->d_bead_seg, s->n);
     TRYA(s->pos, s->n);
     TRYA(s->pos_save, s->n);
@@ -243,9 +263,14 @@ int bdb_create(bdb_system** out, const bdb_params* p, const double* coord, const
     TRYA(s->Rs, s->n3);
     TRYA(s->X, s->n3);
     TRYA(s->dD, s->npad);
-    TRYA(s->scal, 64 + 4 * 1 + 64);
-    BDB_CUDA(cudaMemcpy(s->d_segs.p, s->segs.data(), sizeof(Segment), cudaMemcpyHostToDevice));
-    BDB_CUDA(cudaMemset(s->d_bead_seg.p, 0, sizeof(int) * s->n));
+    TRYA(s->scal, 64 + 4 * (size_t)nseg + 64);
+    BDB_CUDA(cudaMemcpy(s->d_segs.p, s->segs.data(), sizeof(Segment) * nseg, cudaMemcpyHostToDevice));
+    {
+        std::vector<int> bs(s->n);
+        for (int g = 0; g < nseg; ++g)
+            for (int i = 0; i < counts[g]; ++i) bs[s->segs[g].begin + i] = g;
+        BDB_CUDA(cudaMemcpy(s->d_bead_seg.p, bs.data(), sizeof(int) * s->n, cudaMemcpyHostToDevice));
+    }
     BDB_CUDA(cudaMemcpy(s->pos.p, coord, sizeof(double) * 4 * s->n, cudaMemcpyHostToDevice));
     BDB_CUDA(cudaMemcpy(s->Q.p, Q, sizeof(double) * s->n, cudaMemcpyHostToDevice));
     BDB_CUDA(cudaMemcpy(s->LJ.p, LJ, sizeof(double) * 2 * s->n, cudaMemcpyHostToDevice));
@@ -264,6 +289,20 @@ int bdb_create(bdb_system** out, const bdb_params* p, const double* coord, const
 #undef TRYA
     *out = s;
     return BDB_OK;
+}
+
+extern "C" {
+
+int bdb_create(bdb_system** out, const bdb_params* p, const double* coord, const double* Q, const double* LJ)
+{
+    if (!p) return fail(BDB_ERR_ARG, "null argument");
+    return create_system(out, p, 1, &p->n, coord, Q, LJ);
+}
+
+int bdb_create_batch(bdb_system** out, const bdb_params* p, int nseg, const int* counts, const double* coord,
+                     const double* Q, const double* LJ)
+{
+    return create_system(out, p, nseg, counts, coord, Q, LJ);
 }
 
 int bdb_destroy(bdb_system* s)
@@ -302,10 +341,17 @@ int bdb_set_bonded(bdb_system* s, int n_bond, const int* bond_pairs, const doubl
         {n_dihe_angle, 4, 2, dihe_angle_pairs, dihe_angle_parms, &s->dihe_angle_pairs, &s->dihe_angle_parms,
          &s->n_dihe_angle},
     };
+    std::vector<int> seg_of(s->n);
+    for (size_t g = 0; g < s->segs.size(); ++g)
+        for (int i = 0; i < s->segs[g].count; ++i) seg_of[s->segs[g].begin + i] = (int)g;
     for (auto& t : terms) {
         if (t.cnt < 0 || (t.cnt && (!t.idx || !t.par))) return fail(BDB_ERR_ARG, "bonded term arrays");
         for (int k = 0; k < t.cnt * t.members; ++k)
             if (t.idx[k] < 0 || t.idx[k] >= s->n) return fail(BDB_ERR_ARG, "bonded term references a missing bead");
+        for (int k = 0; k < t.cnt; ++k)
+            for (int m = 1; m < t.members; ++m)
+                if (seg_of[t.idx[k * t.members + m]] != seg_of[t.idx[k * t.members]])
+                    return fail(BDB_ERR_ARG, "bonded term joins beads of two segments");
     }
     for (auto& t : terms) {
         *t.store = t.cnt;
@@ -380,6 +426,7 @@ int bdb_compute_forces(bdb_system* s, double* F, double* E, long long* counts)
 int bdb_compute_D(bdb_system* s, double* D)
 {
     if (!s || !D) return fail(BDB_ERR_ARG, "null argument");
+    if (s->segs.size() > 1) return fail(BDB_ERR_UNSUPPORTED, "the full tensor of a batch is not formed (segments are independent)");
     const int n3 = s->n3;
     if (s->p.hydro == BDB_HYDRO_NONE) {
         // compute_D does nothing without hydrodynamics; the tensor is diag_D
@@ -416,6 +463,18 @@ int bdb_compute_D(bdb_system* s, double* D)
 int bdb_compute_Dij(bdb_system* s, int i, int j, double* tD)
 {
     if (!s || !tD || i < 0 || j < 0 || i >= s->n || j >= s->n) return fail(BDB_ERR_ARG, "bad tile index");
+    if (s->segs.size() > 1) {
+        // beads of different segments do not interact
+        auto seg = [&](int b) {
+            int g = 0;
+            while (g + 1 < (int)s->segs.size() && s->segs[g + 1].begin <= b) ++g;
+            return g;
+        };
+        if (seg(i) != seg(j)) {
+            for (int k = 0; k < 9; ++k) tD[k] = 0.0;
+            return BDB_OK;
+        }
+    }
     return tensor_tile_host(s, i, j, tD);
 }
 

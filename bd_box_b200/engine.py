@@ -37,7 +37,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 NOISE_PHILOX, NOISE_HOST = 0, 1
 
 EXPORTS = [
-    "bdb_version", "bdb_last_error", "bdb_create", "bdb_destroy", "bdb_set_bonded",
+    "bdb_version", "bdb_last_error", "bdb_create", "bdb_create_batch", "bdb_destroy", "bdb_set_bonded",
     "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
     "bdb_compute_r", "bdb_step", "bdb_set_dt", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
@@ -82,6 +82,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_version.restype = C.c_char_p
     lib.bdb_last_error.restype = C.c_char_p
     lib.bdb_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Params), _dp, _dp, _dp]
+    lib.bdb_create_batch.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Params), C.c_int, _ip, _dp, _dp, _dp]
     lib.bdb_destroy.argtypes = [C.c_void_p]
     lib.bdb_set_bonded.argtypes = [C.c_void_p] + [C.c_int, _ip, _dp] * 5
     for name in ("bdb_set_coord", "bdb_get_coord"):
@@ -142,26 +143,38 @@ def params_from_deck(deck, precision=PREC_FP64, refresh=1, noise=NOISE_PHILOX, s
 
 
 class System:
-    """One bead system resident on the current CUDA device."""
+    """One bead system resident on the current CUDA device, or, given a list
+    of decks, a batch of independent replicas advanced together
+    (bdb_create_batch; the parameters come from the first deck)."""
 
     def __init__(self, deck, precision=PREC_FP64, refresh=1, noise=NOISE_PHILOX, seed=None):
         self.lib = load_library()
-        self.deck = deck
-        self.n = deck.n
-        self.params = params_from_deck(deck, precision, refresh, noise, seed)
+        decks = list(deck) if isinstance(deck, (list, tuple)) else [deck]
+        self.decks = decks
+        self.deck = decks[0]
+        self.counts = np.array([d.n for d in decks], dtype=np.int32)
+        self.begins = np.concatenate([[0], np.cumsum(self.counts)[:-1]]).astype(np.int64)
+        self.n = int(self.counts.sum())
+        self.params = params_from_deck(self.deck, precision, refresh, noise, seed)
+        self.params.n = self.n
         h = C.c_void_p()
-        coord = np.ascontiguousarray(deck.coord, dtype=np.float64)
-        rc = self.lib.bdb_create(C.byref(h), C.byref(self.params), _p(coord),
-                                 _p(np.ascontiguousarray(deck.Q, dtype=np.float64)),
-                                 _p(np.ascontiguousarray(deck.LJ, dtype=np.float64)))
+        coord = np.ascontiguousarray(np.concatenate([d.coord for d in decks]), dtype=np.float64)
+        Q = np.ascontiguousarray(np.concatenate([d.Q for d in decks]), dtype=np.float64)
+        LJ = np.ascontiguousarray(np.concatenate([d.LJ for d in decks]), dtype=np.float64)
+        if len(decks) == 1:
+            rc = self.lib.bdb_create(C.byref(h), C.byref(self.params), _p(coord), _p(Q), _p(LJ))
+        else:
+            rc = self.lib.bdb_create_batch(C.byref(h), C.byref(self.params), len(decks),
+                                           self.counts.ctypes.data_as(_ip), _p(coord), _p(Q), _p(LJ))
         self._check(rc)
         self.h = h
-        self._bonded = [np.ascontiguousarray(a, dtype=t) for a, t in (
-            (deck.bond_pairs, np.int32), (deck.bond_parms, np.float64),
-            (deck.angle_pairs, np.int32), (deck.angle_parms, np.float64),
-            (deck.angle_cos_pairs, np.int32), (deck.angle_cos_parms, np.float64),
-            (deck.dihe_pairs, np.int32), (deck.dihe_parms, np.float64),
-            (deck.dihe_angle_pairs, np.int32), (deck.dihe_angle_parms, np.float64))]
+        names = ("bond", "angle", "angle_cos", "dihe", "dihe_angle")
+        self._bonded = []
+        for nm in names:
+            pairs = [np.asarray(getattr(d, nm + "_pairs"), dtype=np.int32) + b for d, b in zip(decks, self.begins)]
+            parms = [np.asarray(getattr(d, nm + "_parms"), dtype=np.float64) for d in decks]
+            self._bonded.append(np.ascontiguousarray(np.concatenate(pairs), dtype=np.int32))
+            self._bonded.append(np.ascontiguousarray(np.concatenate(parms), dtype=np.float64))
         b = self._bonded
         args = []
         for k in range(5):

@@ -100,6 +100,18 @@ int bdb_create(bdb_system** out, const bdb_params* p, const double* coord,
                const double* Q, const double* LJ);
 int bdb_destroy(bdb_system* s);   /* free_diff_tensor + free_forces + free_cuda */
 
+/* A batch of nseg independent systems (replicas) that share the parameters
+ * and advance together, every kernel of a step covering all of them. Beads
+ * are stored back to back: segment g holds counts[g] >= 2 beads, p->n is
+ * their sum, and coord/Q/LJ are the concatenated host arrays. Each segment
+ * has its own cell list, tensor tiles and TEA normalisation (eps, beta);
+ * bonded terms may not join two segments. Overlap flags and energies are
+ * summed over the batch. hydro cholesky is single-system only
+ * (BDB_ERR_UNSUPPORTED); bdb_compute_D is not formed for a batch. No
+ * reference counterpart: BD_BOX runs one system per process. */
+int bdb_create_batch(bdb_system** out, const bdb_params* p, int nseg, const int* counts,
+                     const double* coord, const double* Q, const double* LJ);
+
 /* Bonded terms, BD_BOX's arrays as read by read_str_file (input.c:567-641):
  * bond_pairs int[2B], bond_parms double[3B] (r0, rmax, H) (bond.c:94-111);
  * angle_pairs int[3A], angle_parms double[2A] (phi0 [rad], k) (angle.c:88-100);
