@@ -131,8 +131,16 @@ struct bdb_system {
     int sm_count = 148;
     int steps_since_refresh = 0;
 
-    // noise
-    uint64_t philox_counter = 0;
+    // noise: Philox stream index and finished-block count (device)
+    bdb::DevBuf<unsigned long long> ctr;
+
+    // CUDA graph of the steady part of a step (noise .. forces), replayed
+    // while no refresh is due; rebuilt after anything its launches captured
+    // changes (time step, bonded terms)
+    cudaGraphExec_t step_graph = nullptr;
+    long long graph_launches = 0;
+    long long eager_steps = 0;
+    bool graphs = true;
 
     // measurement: CUDA-event pairs per phase, kernel launch count
     struct PhaseRec {
@@ -179,6 +187,7 @@ __device__ __forceinline__ double sq3(const double* v)
 namespace bdb {
 enum Phase { P_STEP, P_REFRESH, P_BUILD, P_FACTOR, P_MATVEC, P_TEA, P_FORCES, P_NOISE, P_UPDATE, P_COUNT };
 void phase_mark(bdb_system* s, int phase);   // records begin/end events when profiling
+void drop_graph(bdb_system* s);              // forget the captured step
 int forces_setup(bdb_system* s);
 int forces_run(bdb_system* s, bool want_energy, bool want_counts);
 int bonded_setup(bdb_system* s);

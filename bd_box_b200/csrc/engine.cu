@@ -147,16 +147,11 @@ static int forces_phase(bdb_system* s)
     return rc;
 }
 
-static int one_step(bdb_system* s, const double* dev_gauss)
+// noise, D.F and the random displacement, the update and the new forces:
+// the part of a step that is the same every step while no refresh is due
+static int step_body(bdb_system* s, const double* dev_gauss)
 {
     int rc;
-    if (!s->have_forces && (rc = forces_phase(s))) return rc;
-    if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
-        if (!s->factor_valid || s->steps_since_refresh >= std::max(1, s->p.refresh)) {
-            rc = refresh_factor(s);
-            if (rc) return rc;
-        }
-    }
     phase_mark(s, P_NOISE);
     if ((rc = noise_fill(s, dev_gauss))) return rc;
     phase_mark(s, P_NOISE);
@@ -164,7 +159,6 @@ static int one_step(bdb_system* s, const double* dev_gauss)
         phase_mark(s, P_MATVEC);
         if ((rc = stored_matvec(s, true))) return rc;
         phase_mark(s, P_MATVEC);
-        s->steps_since_refresh++;
     } else {
         phase_mark(s, P_TEA);
         if ((rc = tea_run(s, true))) return rc;
@@ -174,6 +168,59 @@ static int one_step(bdb_system* s, const double* dev_gauss)
     if ((rc = update_positions(s))) return rc;
     phase_mark(s, P_UPDATE);
     return forces_phase(s);
+}
+
+void drop_graph(bdb_system* s)
+{
+    if (s->step_graph) cudaGraphExecDestroy(s->step_graph);
+    s->step_graph = nullptr;
+}
+
+// step_body captured once as a CUDA graph and replayed (device noise only:
+// caller Gaussians change address every step; not while profiling, whose
+// event records would be frozen into the graph)
+static int step_body_graph(bdb_system* s)
+{
+    if (!s->step_graph) {
+        const long long before = s->launches;
+        BDB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = step_body(s, nullptr);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return rc ? rc : cuda_fail(e, "cudaStreamEndCapture");
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&s->step_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            s->step_graph = nullptr;
+            return cuda_fail(ei, "cudaGraphInstantiate");
+        }
+        s->graph_launches = s->launches - before;
+        s->launches = before;
+    }
+    BDB_CUDA(cudaGraphLaunch(s->step_graph, s->stream));
+    s->launches += s->graph_launches;
+    return BDB_OK;
+}
+
+static int one_step(bdb_system* s, const double* dev_gauss)
+{
+    int rc;
+    if (!s->have_forces && (rc = forces_phase(s))) return rc;
+    if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
+        if (!s->factor_valid || s->steps_since_refresh >= std::max(1, s->p.refresh)) {
+            rc = refresh_factor(s);
+            if (rc) return rc;
+        }
+        s->steps_since_refresh++;
+    }
+    // the first step runs eagerly, so that buffers allocated on first use
+    // exist (at fixed addresses) before a graph captures them
+    if (s->graphs && !dev_gauss && !s->profiling && s->eager_steps > 0) return step_body_graph(s);
+    s->eager_steps++;
+    return step_body(s, dev_gauss);
 }
 
 }  // namespace bdb
@@ -264,6 +311,7 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     TRYA(s->X, s->n3);
     TRYA(s->dD, s->npad);
     TRYA(s->scal, 64 + 4 * (size_t)nseg + 64);
+    TRYA(s->ctr, 2);
     BDB_CUDA(cudaMemcpy(s->d_segs.p, s->segs.data(), sizeof(Segment) * nseg, cudaMemcpyHostToDevice));
     {
         std::vector<int> bs(s->n);
@@ -275,6 +323,7 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     BDB_CUDA(cudaMemcpy(s->Q.p, Q, sizeof(double) * s->n, cudaMemcpyHostToDevice));
     BDB_CUDA(cudaMemcpy(s->LJ.p, LJ, sizeof(double) * 2 * s->n, cudaMemcpyHostToDevice));
     BDB_CUDA(cudaMemset(s->scal.p, 0, sizeof(double) * s->scal.n));
+    BDB_CUDA(cudaMemset(s->ctr.p, 0, sizeof(unsigned long long) * 2));
     BDB_CUDA(cudaMemset(s->Rf.p, 0, sizeof(double) * s->n3));
     BDB_CUDA(cudaMemset(s->Rs.p, 0, sizeof(double) * s->n3));
     BDB_CUDA(cudaMemset(s->X.p, 0, sizeof(double) * s->n3));
@@ -314,6 +363,7 @@ int bdb_destroy(bdb_system* s)
     if (s->stream2) cudaStreamSynchronize(s->stream2);
     for (auto e : s->la_ev)
         if (e) cudaEventDestroy(e);
+    drop_graph(s);
     if (s->stream2) cudaStreamDestroy(s->stream2);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -363,6 +413,7 @@ int bdb_set_bonded(bdb_system* s, int n_bond, const int* bond_pairs, const doubl
         }
     }
     s->have_forces = false;
+    drop_graph(s);
     return bonded_setup(s);
 }
 
@@ -539,9 +590,18 @@ int bdb_step(bdb_system* s, int K, const double* gauss)
     return ov ? 1 : 0;
 }
 
+int bdb_set_graphs(bdb_system* s, int enable)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    s->graphs = enable != 0;
+    if (!s->graphs) drop_graph(s);
+    return BDB_OK;
+}
+
 int bdb_set_dt(bdb_system* s, double dt)
 {
     if (!s || !(dt > 0.0)) return fail(BDB_ERR_ARG, "time step must be positive");
+    if (s->p.dt != dt) drop_graph(s);
     s->p.dt = dt;
     return BDB_OK;
 }

@@ -57,28 +57,45 @@ __device__ __forceinline__ void gauss2(uint64_t seed, uint64_t stream, uint32_t 
 }
 
 // mode: 1 cholesky sqrt(2 dt); 2 TEA sqrt(2 dt / D_ii); 0 none sqrt(D_ii 2 dt)
+// The Philox stream index (one per call) lives in device memory, ctr[0],
+// so that a step captured once in a CUDA graph draws fresh noise on every
+// replay; the last block to finish advances it (ctr[1] counts finished
+// blocks).
 __global__ void k_noise(int n3, int mode, double dt, double preDii, const double4* __restrict__ pos,
-                        const double* __restrict__ host_g, uint64_t seed, uint64_t stream, double* __restrict__ X)
+                        const double* __restrict__ host_g, uint64_t seed, unsigned long long* __restrict__ ctr,
+                        double* __restrict__ X)
 {
+    const uint64_t stream = *reinterpret_cast<volatile unsigned long long*>(ctr);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i0 = 2 * t;
-    if (i0 >= n3) return;
-    double g[2];
-    if (host_g) {
-        g[0] = host_g[i0];
-        g[1] = i0 + 1 < n3 ? host_g[i0 + 1] : 0.0;
-    } else {
-        gauss2(seed, stream, (uint32_t)t, g[0], g[1]);
+    if (i0 < n3) {
+        double g[2];
+        if (host_g) {
+            g[0] = host_g[i0];
+            g[1] = i0 + 1 < n3 ? host_g[i0 + 1] : 0.0;
+        } else {
+            gauss2(seed, stream, (uint32_t)t, g[0], g[1]);
+        }
+        for (int q = 0; q < 2; ++q) {
+            const int i = i0 + q;
+            if (i >= n3) break;
+            const double d = preDii / pos[i / 3].w;   // diag_D (diff_decl.c:94-99)
+            double sc;
+            if (mode == 1) sc = sqrt(2 * dt);
+            else if (mode == 2) sc = sqrt(2 * dt * (1 / d));
+            else sc = sqrt(d * 2 * dt);
+            X[i] = g[q] * sc;
+        }
     }
-    for (int q = 0; q < 2; ++q) {
-        const int i = i0 + q;
-        if (i >= n3) break;
-        const double d = preDii / pos[i / 3].w;   // diag_D (diff_decl.c:94-99)
-        double sc;
-        if (mode == 1) sc = sqrt(2 * dt);
-        else if (mode == 2) sc = sqrt(2 * dt * (1 / d));
-        else sc = sqrt(d * 2 * dt);
-        X[i] = g[q] * sc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned done = atomicAdd(reinterpret_cast<unsigned*>(ctr + 1), 1u);
+        if (done == gridDim.x - 1) {
+            ctr[1] = 0;
+            ctr[0] = stream + 1;
+            __threadfence();
+        }
     }
 }
 
@@ -87,10 +104,9 @@ int noise_fill(bdb_system* s, const double* dev_gauss)
     const int n3 = s->n3;
     const int threads = (n3 + 1) / 2;
     k_noise<<<(threads + 255) / 256, 256, 0, s->stream>>>(n3, s->p.hydro, s->p.dt, s->preDii, s->pos.p, dev_gauss,
-                                                          s->p.seed, s->philox_counter, s->X.p);
+                                                          s->p.seed, s->ctr.p, s->X.p);
     BDB_CUDA(cudaGetLastError());
     s->launches += 1;
-    s->philox_counter++;
     return BDB_OK;
 }
 

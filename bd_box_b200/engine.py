@@ -40,7 +40,7 @@ EXPORTS = [
     "bdb_version", "bdb_last_error", "bdb_create", "bdb_create_batch", "bdb_destroy", "bdb_set_bonded",
     "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
-    "bdb_compute_r", "bdb_step", "bdb_set_dt", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
+    "bdb_compute_r", "bdb_step", "bdb_set_graphs", "bdb_set_dt", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc",
 ]
 
@@ -96,6 +96,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_compute_r.argtypes = [C.c_void_p, _dp, _dp]
     lib.bdb_step.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.bdb_set_dt.argtypes = [C.c_void_p, C.c_double]
+    lib.bdb_set_graphs.argtypes = [C.c_void_p, C.c_int]
     lib.bdb_factor_error.argtypes = [C.c_void_p, _dp]
     lib.bdb_profile.argtypes = [C.c_void_p, C.c_int]
     lib.bdb_phase_stats.argtypes = [C.c_void_p, C.c_char_p, _dp, C.POINTER(C.c_longlong)]

@@ -162,6 +162,13 @@ int bdb_compute_r(bdb_system* s, const double* gauss, double* Rs);
  * caller's, as in comp_step_ermak) or a negative error. */
 int bdb_step(bdb_system* s, int K, const double* gauss);
 
+/* Device-noise steps (BDB_NOISE_PHILOX, profiling off) replay the steady
+ * part of a step -- noise, D.F and the random displacement, the update, the
+ * forces -- from a CUDA graph captured on the second step; refreshes of D
+ * and its factor run outside it. On by default; 0 turns it off. No
+ * reference counterpart. */
+int bdb_set_graphs(bdb_system* s, int enable);
+
 /* Time step of the following steps (curr_dt, diff_decl.c:68): the variable
  * step of comp_step_ermak halves it on overlap (diff_comp.c:162-165). */
 int bdb_set_dt(bdb_system* s, double dt);
