@@ -200,4 +200,6 @@ int noise_fill(bdb_system* s, const double* host_gauss);   // X = unit Gaussians
 int update_positions(bdb_system* s);  // pos += Rf + Rs, periodic wrap
 int diag_noise(bdb_system* s);        // hydro none: Rs = X sqrt(2 dt D_ii)
 int factor_error(bdb_system* s, double* rel);
+int ensure_matrix(bdb_system* s);    // allocate the stored matrix (identity padding)
+int engine_step(bdb_system* s);      // one Ermak-McCammon step, device noise
 }  // namespace bdb

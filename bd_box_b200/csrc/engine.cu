@@ -98,7 +98,7 @@ static int check_status(bdb_system* s, bool* overlap)
     return BDB_OK;
 }
 
-static int ensure_matrix(bdb_system* s)
+int ensure_matrix(bdb_system* s)
 {
     const size_t nn = (size_t)s->npad * s->npad;
     if (s->p.precision == BDB_PREC_FP64) {
@@ -222,6 +222,8 @@ static int one_step(bdb_system* s, const double* dev_gauss)
     s->eager_steps++;
     return step_body(s, dev_gauss);
 }
+
+int engine_step(bdb_system* s) { return one_step(s, nullptr); }
 
 }  // namespace bdb
 

@@ -40,7 +40,7 @@ EXPORTS = [
     "bdb_version", "bdb_last_error", "bdb_create", "bdb_create_batch", "bdb_destroy", "bdb_set_bonded",
     "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
-    "bdb_compute_r", "bdb_step", "bdb_set_graphs", "bdb_set_dt", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
+    "bdb_compute_r", "bdb_step", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc",
 ]
 
@@ -97,6 +97,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_step.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.bdb_set_dt.argtypes = [C.c_void_p, C.c_double]
     lib.bdb_set_graphs.argtypes = [C.c_void_p, C.c_int]
+    lib.bdb_adjoint.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _ip, _dp, _dp, _dp, _dp]
     lib.bdb_factor_error.argtypes = [C.c_void_p, _dp]
     lib.bdb_profile.argtypes = [C.c_void_p, C.c_int]
     lib.bdb_phase_stats.argtypes = [C.c_void_p, C.c_char_p, _dp, C.POINTER(C.c_longlong)]
@@ -266,6 +267,18 @@ class System:
             count += 1
             if count > limit:
                 raise BDBError(-5, "Wrong conformation, can't move")
+
+    def adjoint(self, K: int, checkpoint: int, pairs, targets):
+        """bdb_adjoint: (loss, dloss/dx_0 as (N, 3), dloss/d scale factors
+        (LJ epsilon, LJ sigma, bond H, Debye length))."""
+        pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        targets = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1)
+        loss = C.c_double()
+        gx = np.zeros(self.n3)
+        gp = np.zeros(4)
+        self._check(self.lib.bdb_adjoint(self.h, K, checkpoint, len(pairs), pairs.ctypes.data_as(_ip), _p(targets),
+                                         C.byref(loss), _p(gx), _p(gp)))
+        return loss.value, gx.reshape(self.n, 3), gp
 
     def factor_error(self) -> float:
         out = C.c_double()

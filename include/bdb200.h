@@ -173,6 +173,23 @@ int bdb_set_graphs(bdb_system* s, int enable);
  * step of comp_step_ermak halves it on overlap (diff_comp.c:162-165). */
 int bdb_set_dt(bdb_system* s, double dt);
 
+/* Hand-written adjoint of K Ermak-McCammon steps (no reference counterpart).
+ * From the current state, runs K device-noise steps (Philox noise, a fixed
+ * sequence given the seed and the stream position at the call), evaluates
+ * loss = (1/P) sum_p (|x_{b_p} - x_{a_p}| - targets[p])^2 at the final
+ * positions (pairs int[2P] = a_0, b_0, a_1, ...), and propagates it back
+ * through every step -- D(x) F(x), the forces and the Cholesky noise factor
+ * B(x) X -- recomputing the forward pass from the positions saved every
+ * `checkpoint` steps. Outputs: *loss, grad_coord[3N] = dloss/dx_0 and
+ * grad_params[4] = dloss/ds for scale factors s multiplying every bead's LJ
+ * epsilon, every bead's LJ sigma, every bond's H and the Debye length 1/kappa
+ * (so dloss/d epsilon = grad_params[0] / epsilon for a uniform epsilon).
+ * Leaves the system at the final positions. Needs one free-space system,
+ * hydro cholesky, BDB_PREC_FP64, refresh 1, BDB_NOISE_PHILOX, and bonds as
+ * the only bonded terms (else BDB_ERR_UNSUPPORTED). */
+int bdb_adjoint(bdb_system* s, int K, int checkpoint, int npairs, const int* pairs,
+                const double* targets, double* loss, double* grad_coord, double* grad_params);
+
 /* Cholesky of the stored tensor at the current coordinates (diagnostics):
  * rel_err = ||L L^T - D||_F / ||D||_F evaluated on the device in FP64. */
 int bdb_factor_error(bdb_system* s, double* rel_err);
