@@ -307,6 +307,12 @@ def run_ours(args):
         reps = None
         if rank == 0 and not args.skip_replicas:
             reps = replicas(torch, engine, max(3, args.steps // 5), 3)
+        adj = None
+        if rank == 0 and not args.skip_adjoint:
+            adj = adjoint_case(torch, engine)
+        ew = None
+        if rank == 0 and not args.skip_ewald:
+            ew = ewald_case(torch, engine)
         cpu = None
         if rank == 0 and world == 1 and not args.skip_cpu:
             cpu = reference_cpu(prm, deck, args.cpu_steps)
@@ -322,7 +328,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (stored D/L 604 MB read every step)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches.value),
-            "clocks": clk.summary(), "fp64_gpu": fp64, "errors": errors, "replicas": reps,
+            "clocks": clk.summary(), "fp64_gpu": fp64, "errors": errors, "replicas": reps, "adjoint": adj, "ewald_suspension": ew,
         }
         if rank == 0:
             print(json.dumps(out), flush=True)
@@ -401,6 +407,102 @@ def replicas(torch, engine, steps, warmup):
             "displacement_rel_vs_fp64": {"max": max(errs), "median": float(np.median(errs))}}
 
 
+def adjoint_case(torch, engine):
+    """Adjoint workload: an N=1024 chain with the chain force field, free-space
+    RPY with Cholesky noise (a fixed Philox sequence), 200 steps, checkpoint
+    every 20; loss = mean squared deviation of 128 seeded pair distances from
+    seeded targets in [10, 60] A. One gradient (forward, recomputation and
+    backward) is timed; one random direction of the position gradient is
+    checked against a central difference of the FP64 forward."""
+    from bd_box_b200 import decks
+    with tempfile.TemporaryDirectory() as d:
+        deck = decks.read_deck(decks.write_chain_deck(d, "adj1024", 1024, seed=21, hydro="cholesky"))
+    rng = np.random.default_rng(4)
+    pairs = np.array([rng.choice(deck.n, 2, replace=False) for _ in range(128)], dtype=np.int32)
+    targets = rng.uniform(10, 60, size=len(pairs))
+    K, ck = 200, 20
+
+    def new_sys(coord=None):
+        s = engine.System(deck, precision=engine.PREC_FP64, refresh=1, noise=engine.NOISE_PHILOX, seed=99)
+        if coord is not None:
+            s.set_coord(coord)
+        return s
+
+    s = new_sys()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss, gx, gp = s.adjoint(K, ck, pairs, targets)
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t0
+    s.close()
+    s = new_sys()
+    t0 = time.perf_counter()
+    s.step(K)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    s.close()
+
+    def loss_at(coord):
+        s = new_sys(coord)
+        s.step(K)
+        x = s.get_coord()[:, :3]
+        s.close()
+        r = np.linalg.norm(x[pairs[:, 1]] - x[pairs[:, 0]], axis=1)
+        return float(np.mean((r - targets) ** 2))
+
+    v = rng.standard_normal((deck.n, 3))
+    v /= np.linalg.norm(v)
+    # h = 1e-5 A: with the 12 A cutoffs a few of the ~5e5 pairs cross a
+    # cutoff between the two h = 1e-4 trajectories over 200 steps, and the
+    # force jump swamps that difference
+    h = 1e-5
+    c0 = deck.coord.copy()
+    cp, cm = c0.copy(), c0.copy()
+    cp[:, :3] += h * v
+    cm[:, :3] -= h * v
+    fd = (loss_at(cp) - loss_at(cm)) / (2 * h)
+    an = float(np.sum(gx * v))
+    return {"workload": "chain N=1024, Cholesky noise, 200 steps, checkpoint 20, 128 pair-distance loss, FP64",
+            "loss": loss, "seconds_per_gradient": t_grad, "seconds_forward_only": t_fwd,
+            "gradient_over_forward": t_grad / t_fwd,
+            "fd_check": {"direction": "random unit", "h": h, "fd": fd, "adjoint": an, "rel_err": abs(fd - an) / abs(fd)},
+            "grad_scale_factors": {"lj_epsilon": gp[0], "lj_sigma": gp[1], "bond_H": gp[2], "debye_length": gp[3]}}
+
+
+def ewald_case(torch, engine, steps=3):
+    """Periodic suspension: N=4096 spheres of radius 1 A at volume fraction
+    0.10, Beenakker-Ewald RPY (lattice radius 3) with TEA noise computed on
+    the fly, WCA repulsion via cell lists; steps/s of the mixed path and one
+    step's displacement error against the FP64 path with the same noise."""
+    from bd_box_b200 import decks
+    with tempfile.TemporaryDirectory() as d:
+        deck = decks.read_deck(decks.write_suspension_deck(d, "susp4096", 4096, seed=8, ewald_r=3))
+    s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_PHILOX, seed=SEED)
+    s.step(1)
+    ms = time_steps(torch, s, steps)
+    s.close()
+    g = np.random.default_rng(6).standard_normal(3 * deck.n)
+    sm = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
+    s64 = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
+    x0 = s64.get_coord()
+    t0 = time.perf_counter()
+    s64.step(1, g)
+    torch.cuda.synchronize()
+    t64 = time.perf_counter() - t0
+    sm.step(1, g)
+    dd = s64.get_coord()[:, :3] - x0[:, :3]
+    dm = sm.get_coord()[:, :3] - x0[:, :3]
+    box = deck.box[0]
+    dd -= box * np.round(dd / box)
+    dm -= box * np.round(dm / box)
+    sm.close()
+    s64.close()
+    return {"workload": "periodic suspension N=4096, phi=0.10, Beenakker Ewald R=3, TEA on the fly, mixed precision",
+            "metric": "steps/s", "value": steps / (ms / 1e3), "ms_per_step": ms / steps,
+            "fp64_steps_per_s": 1.0 / t64,
+            "displacement_rel_vs_fp64": float(np.linalg.norm(dm - dd) / np.linalg.norm(dd))}
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -434,6 +536,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-errors", action="store_true")
     ap.add_argument("--skip-replicas", action="store_true")
+    ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--skip-ewald", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
