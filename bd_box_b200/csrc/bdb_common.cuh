@@ -19,6 +19,7 @@
 #define BDB_SQRTPI 1.77245385090551602729
 #define BDB_M1_SQRTPI 0.5641895835
 #define BDB_M_PIF 3.14159265358979323846f
+#define BDB_PI_D 3.14159265358979323846
 
 namespace bdb {
 
@@ -122,6 +123,8 @@ struct bdb_system {
     bdb::DevBuf<unsigned char> tea_meta;       // TEA segment table + job offsets
     int n_jobs = 0;
     int tea_tile = 32;
+    bdb::DevBuf<double> ewald_tab;             // Ewald lattice tables (rpy_tile.cuh EwaldConst)
+    int ewald_nk = 0, ewald_nimg = 0;
     bdb::DevBuf<double> M64;                   // stored D (upper) + L (lower), FP64
     bdb::DevBuf<float> M32;                    // same, FP32 (mixed path)
     bdb::DevBuf<double> panel64;               // Cholesky workspace

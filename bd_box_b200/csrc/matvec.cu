@@ -143,22 +143,44 @@ k_strip_mv(const T* __restrict__ M, int n3, int npad, int nseg, int seg_cols,
 }
 
 // Rs = sum of row partials; Rf = pre * (row partials + dD F + column partials
-// of the strips above).
-__global__ void k_mv_finish(int n3, int nseg, const double* __restrict__ rowp, const double* __restrict__ colp,
-                            const double* __restrict__ dD, const double* __restrict__ F, double pre,
-                            double* __restrict__ Rf, double* __restrict__ Rs, int want_rs)
+// of the strips above). A block covers 32 rows; its 8 thread rows take every
+// 8th strip (4 independent sums each) and are combined in a fixed order.
+static constexpr int FIN_ROWS = 32, FIN_GROUPS = 8;
+
+__global__ void __launch_bounds__(FIN_ROWS * FIN_GROUPS)
+k_mv_finish(int n3, int nseg, const double* __restrict__ rowp, const double* __restrict__ colp,
+            const double* __restrict__ dD, const double* __restrict__ F, double pre, double* __restrict__ Rf,
+            double* __restrict__ Rs, int want_rs)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n3) return;
-    double s = 0, f = 0;
-    for (int g = 0; g < nseg; ++g) {
-        s += rowp[((size_t)g * n3 + r) * 2];
-        f += rowp[((size_t)g * n3 + r) * 2 + 1];
+    __shared__ double part[FIN_GROUPS][FIN_ROWS + 1];
+    const int tx = threadIdx.x % FIN_ROWS, ty = threadIdx.x / FIN_ROWS;
+    const int r = blockIdx.x * FIN_ROWS + tx;
+    double c[4] = {0, 0, 0, 0};
+    if (r < n3) {
+        const int nst = (r + STRIP - 1) / STRIP;   // strips st with st * STRIP < r
+        int st = ty, q = 0;
+        for (; st < nst; st += FIN_GROUPS, q = (q + 1) & 3) c[q] += colp[(size_t)st * n3 + r];
     }
-    f += dD[r] * F[r];
-    for (int st = 0; st * STRIP < r; ++st) f += colp[(size_t)st * n3 + r];
-    Rf[r] = f * pre;
-    if (want_rs) Rs[r] = s;
+    part[ty][tx] = (c[0] + c[1]) + (c[2] + c[3]);
+    __syncthreads();
+    if (ty == 0 && r < n3) {
+        double s = 0, f = 0;
+        for (int g = 0; g < nseg; ++g) {
+            s += rowp[((size_t)g * n3 + r) * 2];
+            f += rowp[((size_t)g * n3 + r) * 2 + 1];
+        }
+        f += dD[r] * F[r];
+        for (int g = 0; g < FIN_GROUPS; ++g) f += part[g][tx];
+        Rf[r] = f * pre;
+        if (want_rs) Rs[r] = s;
+    }
+}
+
+static void mv_finish(cudaStream_t st, int n3, int nseg, const double* rowp, const double* colp, const double* dD,
+                      const double* F, double pre, double* Rf, double* Rs, int want_rs)
+{
+    k_mv_finish<<<(n3 + FIN_ROWS - 1) / FIN_ROWS, FIN_ROWS * FIN_GROUPS, 0, st>>>(n3, nseg, rowp, colp, dD, F, pre, Rf,
+                                                                                Rs, want_rs);
 }
 
 int stored_matvec(bdb_system* s, bool want_rs)
@@ -187,8 +209,7 @@ int stored_matvec(bdb_system* s, bool want_rs)
     BDB_CUDA(cudaGetLastError());
     s->launches += 2;
     const double pre = s->p.dt / (BDB_KB * s->p.T);
-    k_mv_finish<<<(n3 + 255) / 256, 256, 0, s->stream>>>(n3, nseg, rowp, colp, s->dD.p, s->F.p, pre, s->Rf.p, s->Rs.p,
-                                                         want_rs);
+    mv_finish(s->stream, n3, nseg, rowp, colp, s->dD.p, s->F.p, pre, s->Rf.p, s->Rs.p, want_rs);
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;
 }
@@ -246,7 +267,7 @@ extern "C" int bdb_stored_matvec_noalloc(const float* M, int n3, int ld, const d
     const int blocks = (nstrip * nseg + WARPS - 1) / WARPS;
     k_strip_mv<float><<<blocks, 32 * WARPS, 0, st>>>(M, n3, ld, nseg, seg_cols, F, X, rowp, colp);
     BDB_CUDA(cudaGetLastError());
-    k_mv_finish<<<(n3 + 255) / 256, 256, 0, st>>>(n3, nseg, rowp, colp, dD, F, pre, Rf, Rs, 1);
+    mv_finish(st, n3, nseg, rowp, colp, dD, F, pre, Rf, Rs, 1);
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;
 }

@@ -6,7 +6,7 @@
 //  * rpy_free: diff_tensor_calc_pos (diff_alg/diff_tensor.c:45-92), the
 //    free-space Rotne-Prager-Yamakawa tensor with the overlap form for
 //    r < a_i + a_j.
-//  * rpy_beenakker: diff_tensor_calc_ewald_beenakker (diff_tensor.c:265-401)
+//  * rpy_ewald_tab: diff_tensor_calc_ewald_beenakker (diff_tensor.c:265-401)
 //    with its self term (:404-422): real-space images r + L m and
 //    reciprocal vectors over the same sphere |m|^2 <= R^2, overlap
 //    correction on the raw (not minimum-image) separation, alpha = sqrt(pi)/L
@@ -24,6 +24,14 @@ struct EwaldConst {
     double four_pif2;    // 4*M_PIF*M_PIF evaluated in float
     double six_pif;      // 6*M_PIF evaluated in float
     int R, rr_sq;
+    // lattice tables (device memory, built by ewald_tables on the host):
+    // rk[12 k ..]: h, f, g, A_k, B_k, then 2(1 - e_a^2) for a = x, y, z and
+    // -2 e_a e_b for xy, xz, yz, over one half of the reciprocal sphere
+    // (k and -k contribute alike); img[m]: the real-space image offsets L m
+    const double* rk = nullptr;
+    const double4* img = nullptr;
+    int nk = 0, nimg = 0;
+    float rcut_sq = 0.f;   // mixed precision: real-space images beyond this are dropped
 };
 
 inline EwaldConst make_ewald(double L, double inv_L, int R)
@@ -88,10 +96,15 @@ __device__ __forceinline__ void rpy_free(const double4& pi, const double4& pj, T
     }
 }
 
-// diff_tensor_calc_ewald_beenakker(i, j) (+ _diag for i == j), FP64.
-__device__ __forceinline__ void rpy_beenakker(const double4& pi, const double4& pj, bool self,
-                                              double preDii, double preDij, const EwaldConst& ec,
-                                              double* t)
+// diff_tensor_calc_ewald_beenakker(i, j) (+ _diag for i == j) from the
+// lattice tables: each reciprocal vector once for the pair k, -k, with its
+// k-only factors precomputed. The FP64 path keeps every real-space image
+// and the reference's cos(2 pi_f k.r). With MIXED the real-space images are
+// summed in FP32 (images beyond rcut dropped) and the reciprocal phases
+// taken as FP32 cosines of the same argument, both accumulated in FP64.
+template <bool MIXED>
+__device__ __forceinline__ void rpy_ewald_tab(const double4& pi, const double4& pj, bool self, double preDii,
+                                              double preDij, const EwaldConst& ec, double* t)
 {
     const double sigma_i = pj.w, sigma_j = pi.w;
     const double r0 = pj.x - pi.x, r1 = pj.y - pi.y, r2 = pj.z - pi.z;
@@ -114,60 +127,81 @@ __device__ __forceinline__ void rpy_beenakker(const double4& pi, const double4& 
         for (int k = 3; k < 6; ++k)
             t[k] += pre * 3 * e[ia[k]] * e[ib[k]] * r / (32 * sigma) - pre2 * e[ia[k]] * e[ib[k]] * (1 - sigm_r);
     }
-    const double v0 = r0 * ec.inv_L, v1 = r1 * ec.inv_L, v2 = r2 * ec.inv_L;
-    const double a = ec.alpha, a2 = ec.alpha2, a3 = ec.alpha3;
-    for (int h = -ec.R; h <= ec.R; ++h) {
-        const int nf = (int)sqrt((double)(ec.rr_sq - h * h));
-        for (int f = -nf; f <= nf; ++f) {
-            const int ng = (int)sqrt((double)(ec.rr_sq - h * h - f * f));
-            for (int g = -ng; g <= ng; ++g) {
-                // real space
-                const double x = r0 + ec.L * h, y = r1 + ec.L * f, z = r2 + ec.L * g;
-                const double r_sq = x * x + y * y + z * z;
-                if (r_sq != 0.0) {
-                    const double r = sqrt(r_sq);
-                    const double inv_r = 1 / r, inv_r2 = 1 / r_sq, inv_r3 = inv_r * inv_r2;
-                    const double e[3] = {x * inv_r, y * inv_r, z * inv_r};
-                    const double ex = exp(-a2 * r_sq);
-                    const double ec_ = erfc(r * a);
-                    double sc = a * sigma_sq * inv_r2 + 14 * a3 * sigma_sq - 4.5 * a -
-                                20 * a2 * a3 * sigma_sq * r_sq + 3 * a3 * r_sq +
-                                4 * a3 * a2 * a2 * sigma_sq * r_sq * r_sq;
-                    sc = sc * ex / BDB_SQRTPI + ec_ * (0.75 * inv_r + 0.5 * sigma_sq * inv_r3);
-                    double sc2 = -3 * a * sigma_sq * inv_r2 - 2 * a3 * sigma_sq + 1.5 * a +
-                                 16 * a2 * a3 * sigma_sq * r_sq - 3 * a3 * r_sq -
-                                 4 * a3 * a2 * a2 * sigma_sq * r_sq * r_sq;
-                    sc2 = sc2 * ex / BDB_SQRTPI + ec_ * (0.75 * inv_r - 1.5 * sigma_sq * inv_r3);
-                    O[0] += sc + sc2 * e[0] * e[0];
-                    O[1] += sc + sc2 * e[1] * e[1];
-                    O[2] += sc + sc2 * e[2] * e[2];
-                    O[3] += sc2 * e[0] * e[1];
-                    O[4] += sc2 * e[0] * e[2];
-                    O[5] += sc2 * e[1] * e[2];
-                }
-                // reciprocal space
-                const double k_sq = (double)(h * h + f * f + g * g);
-                if (k_sq != 0.0) {
-                    const double kn = sqrt(k_sq), ik = 1 / kn;
-                    const double e[3] = {h * ik, f * ik, g * ik};
-                    const double k2 = k_sq * ec.four_pif2;
-                    double sc = 1 - sigma_sq * k2 / 3;
-                    sc *= 1 + (ec.inv_alpha2 * k2 / 4) * (1 + ec.inv_alpha2 * k2 / 2);
-                    sc *= ec.six_pif * exp(-ec.inv_alpha2 * k2 / 4) / k2;
-                    sc *= cos(ec.two_pif * (v0 * h + v1 * f + v2 * g));
-                    Qr[0] += sc - sc * e[0] * e[0];
-                    Qr[1] += sc - sc * e[1] * e[1];
-                    Qr[2] += sc - sc * e[2] * e[2];
-                    Qr[3] -= sc * e[0] * e[1];
-                    Qr[4] -= sc * e[0] * e[2];
-                    Qr[5] -= sc * e[1] * e[2];
-                }
-            }
+    // real space
+    if (MIXED) {
+        const float a = (float)ec.alpha, a2 = (float)ec.alpha2, a3 = (float)ec.alpha3;
+        const float s2 = (float)sigma_sq;
+        const float a5s = 20.f * a2 * a3 * s2, a5s16 = 16.f * a2 * a3 * s2, a7s = 4.f * a3 * a2 * a2 * s2;
+        const float c0 = 14.f * a3 * s2 - 4.5f * a, c0b = -2.f * a3 * s2 + 1.5f * a;
+        const float isp = (float)(1.0 / BDB_SQRTPI);
+        const float fx = (float)r0, fy = (float)r1, fz = (float)r2;
+        float o[6] = {0, 0, 0, 0, 0, 0};
+        for (int m = 0; m < ec.nimg; ++m) {
+            const double4 off = ec.img[m];
+            const float x = fx + (float)off.x, y = fy + (float)off.y, z = fz + (float)off.z;
+            const float r_sq = x * x + y * y + z * z;
+            if (r_sq == 0.f || r_sq > ec.rcut_sq) continue;
+            const float inv_r = rsqrtf(r_sq), inv_r2 = inv_r * inv_r, inv_r3 = inv_r * inv_r2, r = r_sq * inv_r;
+            const float ex = __expf(-a2 * r_sq) * isp;
+            const float ec_ = erfcf(r * a);
+            const float sc = (a * s2 * inv_r2 + c0 - a5s * r_sq + 3.f * a3 * r_sq + a7s * r_sq * r_sq) * ex +
+                             ec_ * (0.75f * inv_r + 0.5f * s2 * inv_r3);
+            const float sc2 = (-3.f * a * s2 * inv_r2 + c0b + a5s16 * r_sq - 3.f * a3 * r_sq - a7s * r_sq * r_sq) * ex +
+                              ec_ * (0.75f * inv_r - 1.5f * s2 * inv_r3);
+            const float e0 = x * inv_r, e1 = y * inv_r, e2 = z * inv_r;
+            o[0] += sc + sc2 * e0 * e0;
+            o[1] += sc + sc2 * e1 * e1;
+            o[2] += sc + sc2 * e2 * e2;
+            o[3] += sc2 * e0 * e1;
+            o[4] += sc2 * e0 * e2;
+            o[5] += sc2 * e1 * e2;
         }
+        for (int k = 0; k < 6; ++k) O[k] = o[k];
+    } else {
+        const double a = ec.alpha, a2 = ec.alpha2, a3 = ec.alpha3;
+        for (int m = 0; m < ec.nimg; ++m) {
+            const double4 off = ec.img[m];
+            const double x = r0 + off.x, y = r1 + off.y, z = r2 + off.z;
+            const double r_sq = x * x + y * y + z * z;
+            if (r_sq == 0.0) continue;
+            const double r = sqrt(r_sq);
+            const double inv_r = 1 / r, inv_r2 = 1 / r_sq, inv_r3 = inv_r * inv_r2;
+            const double e[3] = {x * inv_r, y * inv_r, z * inv_r};
+            const double ex = exp(-a2 * r_sq);
+            const double ec_ = erfc(r * a);
+            double sc = a * sigma_sq * inv_r2 + 14 * a3 * sigma_sq - 4.5 * a - 20 * a2 * a3 * sigma_sq * r_sq +
+                        3 * a3 * r_sq + 4 * a3 * a2 * a2 * sigma_sq * r_sq * r_sq;
+            sc = sc * ex / BDB_SQRTPI + ec_ * (0.75 * inv_r + 0.5 * sigma_sq * inv_r3);
+            double sc2 = -3 * a * sigma_sq * inv_r2 - 2 * a3 * sigma_sq + 1.5 * a + 16 * a2 * a3 * sigma_sq * r_sq -
+                         3 * a3 * r_sq - 4 * a3 * a2 * a2 * sigma_sq * r_sq * r_sq;
+            sc2 = sc2 * ex / BDB_SQRTPI + ec_ * (0.75 * inv_r - 1.5 * sigma_sq * inv_r3);
+            O[0] += sc + sc2 * e[0] * e[0];
+            O[1] += sc + sc2 * e[1] * e[1];
+            O[2] += sc + sc2 * e[2] * e[2];
+            O[3] += sc2 * e[0] * e[1];
+            O[4] += sc2 * e[0] * e[2];
+            O[5] += sc2 * e[1] * e[2];
+        }
+    }
+    // reciprocal space
+    const double v0 = r0 * ec.inv_L, v1 = r1 * ec.inv_L, v2 = r2 * ec.inv_L;
+    for (int k = 0; k < ec.nk; ++k) {
+        const double* q = ec.rk + 12 * k;
+        const double ph = v0 * q[0] + v1 * q[1] + v2 * q[2];
+        double cs;
+        if (MIXED) {
+            // cos(2 pi_f ph), pi_f the float pi of the reference's constants
+            cs = (double)cospif((float)(ph * (ec.two_pif / BDB_PI_D)));
+        } else {
+            cs = cos(ec.two_pif * ph);
+        }
+        const double sc = (q[3] - sigma_sq * q[4]) * cs;
+        for (int c = 0; c < 6; ++c) Qr[c] += sc * q[5 + c];
     }
     for (int k = 0; k < 6; ++k) t[k] += preDii * (O[k] + ec.preQ * Qr[k]);
     if (self) {
         const double aw = pi.w;
+        const double a = ec.alpha, a3 = ec.alpha3;
         const double sc3 = (-6 * a / BDB_SQRTPI + 40 * a3 * aw * aw / (3 * BDB_SQRTPI)) * preDii;
         for (int k = 0; k < 3; ++k) t[k] = preDii / aw + sc3 + t[k];
         t[3] = t[4] = t[5] = 0;

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "bdb_common.cuh"
@@ -37,6 +38,45 @@ struct TensorArgs {
     EwaldConst ec;
 };
 
+// Lattice tables of the Ewald sums (see EwaldConst), built once per system
+// in the order diff_tensor_calc_ewald_beenakker walks the sphere |m|^2 <= R^2
+// (diff_tensor.c:319-326); the k-only factors of the reciprocal term are
+// evaluated as the device evaluates them per pair.
+static int ewald_tables(bdb_system* s)
+{
+    if (!s->p.ewald || s->ewald_tab.p) return BDB_OK;
+    const EwaldConst ec = make_ewald(s->p.box[0], s->inv_L[0], s->p.ewald_real);
+    std::vector<double> rk, img;
+    const int R = ec.R;
+    for (int h = -R; h <= R; ++h) {
+        const int nf = (int)std::sqrt((double)(ec.rr_sq - h * h));
+        for (int f = -nf; f <= nf; ++f) {
+            const int ng = (int)std::sqrt((double)(ec.rr_sq - h * h - f * f));
+            for (int g = -ng; g <= ng; ++g) {
+                img.insert(img.end(), {ec.L * h, ec.L * f, ec.L * g, 0.0});
+                const bool half = h > 0 || (h == 0 && (f > 0 || (f == 0 && g > 0)));
+                if (!half) continue;
+                const double k_sq = (double)(h * h + f * f + g * g);
+                const double kn = std::sqrt(k_sq), ik = 1 / kn;
+                const double e[3] = {h * ik, f * ik, g * ik};
+                const double k2 = k_sq * ec.four_pif2;
+                double P = 1 + (ec.inv_alpha2 * k2 / 4) * (1 + ec.inv_alpha2 * k2 / 2);
+                P *= ec.six_pif * std::exp(-ec.inv_alpha2 * k2 / 4) / k2;
+                rk.insert(rk.end(), {(double)h, (double)f, (double)g, P, k2 / 3 * P, 2 * (1 - e[0] * e[0]),
+                                     2 * (1 - e[1] * e[1]), 2 * (1 - e[2] * e[2]), -2 * e[0] * e[1], -2 * e[0] * e[2],
+                                     -2 * e[1] * e[2], 0.0});
+            }
+        }
+    }
+    s->ewald_nk = (int)(rk.size() / 12);
+    s->ewald_nimg = (int)(img.size() / 4);
+    if (s->ewald_tab.alloc(rk.size() + img.size())) return BDB_ERR_NOMEM;
+    if (!rk.empty())
+        BDB_CUDA(cudaMemcpy(s->ewald_tab.p, rk.data(), sizeof(double) * rk.size(), cudaMemcpyHostToDevice));
+    BDB_CUDA(cudaMemcpy(s->ewald_tab.p + rk.size(), img.data(), sizeof(double) * img.size(), cudaMemcpyHostToDevice));
+    return BDB_OK;
+}
+
 static TensorArgs targs(const bdb_system* s)
 {
     TensorArgs a;
@@ -46,6 +86,14 @@ static TensorArgs targs(const bdb_system* s)
     a.preDij = s->preDij;
     a.ewald = s->p.ewald;
     a.ec = make_ewald(s->p.box[0], s->inv_L[0], s->p.ewald_real);
+    if (s->p.ewald) {
+        a.ec.rk = s->ewald_tab.p;
+        a.ec.nk = s->ewald_nk;
+        a.ec.img = reinterpret_cast<const double4*>(s->ewald_tab.p + 12 * (size_t)s->ewald_nk);
+        a.ec.nimg = s->ewald_nimg;
+        const double rc = 2.5 * s->p.box[0];   // erfc(2.5 sqrt(pi)) ~ 3e-10
+        a.ec.rcut_sq = (float)(rc * rc);
+    }
     return a;
 }
 
@@ -55,7 +103,7 @@ __device__ __forceinline__ void tile_of(const TensorArgs& A, const double4* pos,
     const double4 pi = pos[i], pj = pos[j];
     if (A.ewald) {
         double d[6];
-        rpy_beenakker(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
+        rpy_ewald_tab<sizeof(T) == 4>(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
         for (int k = 0; k < 6; ++k) t[k] = (T)d[k];
     } else if (i == j) {
         const T d = (T)(A.preDii / pi.w);
@@ -126,6 +174,7 @@ int tensor_build(bdb_system* s)
 {
     int rc = tensor_attrs();
     if (rc) return rc;
+    if (int rc_e = ewald_tables(s)) return rc_e;
     const TensorArgs A = targs(s);
     const int nt = (s->n + TB - 1) / TB;
     dim3 grid(nt, nt);
@@ -153,6 +202,7 @@ __global__ void k_one_tile(TensorArgs A, const double4* pos, int i, int j, doubl
 
 int tensor_tile_host(bdb_system* s, int i, int j, double* tD)
 {
+    if (int rc_e = ewald_tables(s)) return rc_e;
     const TensorArgs A = targs(s);
     double* d = s->work.p;
     k_one_tile<<<1, 1, 0, s->stream>>>(A, s->pos.p, i, j, d);
@@ -366,10 +416,11 @@ int tea_run(bdb_system* s, bool want_rs)
     }
     int rc0 = tensor_attrs();
     if (rc0) return rc0;
+    if (int rc_e = ewald_tables(s)) return rc_e;
     const TensorArgs A = targs(s);
     TeaSeg* tsegs = reinterpret_cast<TeaSeg*>(s->tea_meta.p);
     if (s->p.hydro && s->n_jobs) {
-        if (s->p.precision == BDB_PREC_FP64 || s->p.ewald)
+        if (s->p.precision == BDB_PREC_FP64)
             k_tea<double><<<s->n_jobs, 256, tea_smem_bytes<double>(), s->stream>>>(A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p,
                                                            s->part.p, s->eps_part.p, want_rs);
         else

@@ -199,3 +199,20 @@ def test_tensor_core_factor_large(deck_dir):
         del os.environ["BDB_NO_TC"]
     assert err_tc <= 1e-5, err_tc
     assert err_tc <= 10 * err_simt + 1e-7, (err_tc, err_simt)
+
+
+@pytest.mark.parametrize("name", ["chain_tea", "susp"])
+def test_tea_mixed_within_bound(name, request):
+    """Mixed precision TEA (FP32 tiles; for Ewald FP32 real-space images and
+    reciprocal phases, FP64 sums) against the FP64 oracle: D.F and the noise
+    within the method's 1e-5 bound."""
+    deck = request.getfixturevalue(name)
+    o = pyoracle.Oracle(deck)
+    n3 = 3 * deck.n
+    F, _, _, _ = o.forces()
+    Rf_o = o.df(F, deck.prm["dt"])
+    g = gauss(n3, 1, seed=9)
+    Rs_o, _, _ = o.tea(g, deck.prm["dt"])
+    s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
+    assert rel(s.compute_Rf(), Rf_o) < 1e-5
+    assert rel(s.compute_r(g), Rs_o) < 1e-5
