@@ -39,6 +39,7 @@ enum : unsigned {
     ST_BOND = 2u,         // over-stretched FENE bond (fatal in the reference)
     ST_NOT_SPD = 4u,      // non-positive Cholesky pivot
     ST_TIMEOUT = 8u,      // a bounded wait gave up
+    ST_LAUNCH = 16u,      // a kernel found its launch shape wrong and did nothing
 };
 
 // A bead segment: one independent system inside a batch.

@@ -285,6 +285,15 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
     double* Bk = S + PW * LDS;
     double* dinv = Bk + 8 * PW;
     __shared__ int bad;
+    {
+        // the warp roles and barrier counts assume this exact launch shape
+        uint32_t dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (blockDim.x != POTRF_THREADS || dyn < (uint32_t)POTRF_SMEM) {
+            if (threadIdx.x == 0) atomicOr(status, ST_LAUNCH);
+            return;
+        }
+    }
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const size_t base = (size_t)P * PW;
     for (int idx = tid; idx < PW * PW / 4; idx += blockDim.x) {
@@ -507,6 +516,14 @@ __global__ void __launch_bounds__(192, 1)
 k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
           const __grid_constant__ CUtensorMap map_c, int t0, int ntiles, int mode, unsigned* __restrict__ status)
 {
+    {
+        uint32_t dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (blockDim.x != 192 || dyn < (uint32_t)SYRK_SMEM) {
+            if (threadIdx.x == 0) atomicOr(status, ST_LAUNCH);
+            return;
+        }
+    }
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ SyrkBars bars;

@@ -94,6 +94,7 @@ static int check_status(bdb_system* s, bool* overlap)
     if (st & ST_BOND) return fail(BDB_ERR_BOND, "Overstretched bond (bond.c:73-78)");
     if (st & ST_NOT_SPD) return fail(BDB_ERR_NOT_SPD, "Cholesky decomposition error: non-positive pivot");
     if (st & ST_TIMEOUT) return fail(BDB_ERR_TIMEOUT, "device wait timed out");
+    if (st & ST_LAUNCH) return fail(BDB_ERR_CUDA, "a kernel was launched with the wrong shape");
     if (overlap) *overlap = (st & ST_OVERLAP) != 0;
     return BDB_OK;
 }
