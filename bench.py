@@ -195,27 +195,21 @@ def run_ours(args):
     import torch
     from bd_box_b200 import engine
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from bd_box_b200 import ranks
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist, rank, world, local = ranks.init("nccl")
     tmp = tempfile.mkdtemp(prefix="bdb_bench_")
     try:
         prm, deck = make_deck(tmp)
         n3 = 3 * deck.n
         sysm = engine.System(deck, precision=engine.PREC_MIXED, refresh=REFRESH,
-                             noise=engine.NOISE_PHILOX, seed=SEED + 1000 * rank)
+                             noise=engine.NOISE_PHILOX, seed=ranks.replica_seed(SEED, rank))
         for _ in range(args.warmup):
             sysm.step(1)
         sysm.lib.bdb_reset_stats(sysm.h)
-        if dist:
-            dist.barrier()
+        ranks.barrier(dist)
         torch.cuda.synchronize()
         with ClockSampler(local) as clk:
             ms = time_steps(torch, sysm, args.steps)
@@ -227,11 +221,8 @@ def run_ours(args):
         sysm.lib.bdb_profile(sysm.h, 1)
         ms_prof = time_steps(torch, sysm, args.steps)
         sysm.lib.bdb_profile(sysm.h, 0)
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-            dist.barrier()
+        ms = ranks.max_over_ranks(dist, ms, "cuda")
+        ranks.barrier(dist)
         value = world * args.steps / (ms / 1e3)
         fac_ms, fac_calls = phase(sysm, "factor")
         mv_ms, mv_calls = phase(sysm, "matvec")
@@ -243,13 +234,12 @@ def run_ours(args):
         gh = torch.randn(args.steps * n3, dtype=torch.float64).pin_memory()
         ch = torch.empty(4 * deck.n, dtype=torch.float64).pin_memory()
         hsys = engine.System(deck, precision=engine.PREC_MIXED, refresh=REFRESH,
-                             noise=engine.NOISE_HOST, seed=SEED + 1000 * rank)
+                             noise=engine.NOISE_HOST, seed=ranks.replica_seed(SEED, rank))
         gp = C.cast(gh.data_ptr(), C.POINTER(C.c_double))
         cp = C.cast(ch.data_ptr(), C.POINTER(C.c_double))
         for k in range(min(args.warmup, 3)):
             hsys.lib.bdb_step(hsys.h, 1, gp)
-        if dist:
-            dist.barrier()
+        ranks.barrier(dist)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for k in range(args.steps):
@@ -258,17 +248,14 @@ def run_ours(args):
             hsys._check(hsys.lib.bdb_get_coord(hsys.h, cp))
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = ranks.max_over_ranks(dist, e2e_s, "cuda")
         e2e = {"value": world * args.steps / e2e_s, "unit": "steps/s",
                "h2d_bytes_per_step": 8 * n3, "d2h_bytes_per_step": 8 * 4 * deck.n}
         hsys.close()
 
         # plain FP64 GPU path (full Cholesky every step, the reference schedule)
         fp64 = None
-        if rank == 0 and not args.skip_fp64:
+        if rank == 0 and world == 1 and not args.skip_fp64:
             s64 = engine.System(deck, precision=engine.PREC_FP64, refresh=1, noise=engine.NOISE_PHILOX, seed=5)
             s64.step(1)
             k64 = 3
@@ -278,7 +265,7 @@ def run_ours(args):
             s64.close()
 
         errors = None
-        if rank == 0 and not args.skip_errors:
+        if rank == 0 and world == 1 and not args.skip_errors:
             errors = accuracy(torch, engine, deck)
 
         hbm, bf16, bf16s, src = peaks()
@@ -305,13 +292,13 @@ def run_ours(args):
         roof["phases_ms_per_call"] = {"factor": fac_avg, "build": bld_ms / max(bld_calls, 1),
                                       "matvec": mv_avg, "forces": frc_ms / max(frc_calls, 1)}
         reps = None
-        if rank == 0 and not args.skip_replicas:
+        if rank == 0 and world == 1 and not args.skip_replicas:
             reps = replicas(torch, engine, max(3, args.steps // 5), 3)
         adj = None
-        if rank == 0 and not args.skip_adjoint:
+        if rank == 0 and world == 1 and not args.skip_adjoint:
             adj = adjoint_case(torch, engine)
         ew = None
-        if rank == 0 and not args.skip_ewald:
+        if rank == 0 and world == 1 and not args.skip_ewald:
             ew = ewald_case(torch, engine)
         cpu = None
         if rank == 0 and world == 1 and not args.skip_cpu:
@@ -333,9 +320,7 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps(out), flush=True)
         sysm.close()
-        if dist:
-            dist.barrier()
-            dist.destroy_process_group()
+        ranks.finish(dist)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 
