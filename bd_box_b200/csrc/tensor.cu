@@ -220,6 +220,12 @@ struct TeaSeg {
     int begin, count, ntile, part_begin;
 };
 
+// One job = the tile pair (I, J) of a segment: 32 x 32 bead tiles D_ij
+// computed once into shared memory (six planes, so that row and column
+// walks both read consecutive words), then (phase 2) the row sums into the
+// beads of I and (phase 3) the column sums into the beads of J. Within a job
+// the sums run in T (FP32 on the mixed path); the records they produce and
+// every sum across jobs are FP64.
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__ segs,
@@ -227,8 +233,8 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
       double* __restrict__ part, double* __restrict__ eps_part, int want_rs)
 {
     extern __shared__ __align__(16) unsigned char tea_smem[];
-    T(*tD)[TB + 1][6] = reinterpret_cast<T(*)[TB + 1][6]>(tea_smem);
-    __shared__ double sF[2][TB][3], sX[2][TB][3], sInv[2][TB];
+    T(*tD)[TB][TB + 1] = reinterpret_cast<T(*)[TB][TB + 1]>(tea_smem);   // [6][TB][TB+1]
+    __shared__ T sF[2][TB][3], sX[2][TB][3], sInv[2][TB];
     __shared__ double sAcc[TB][9];
     __shared__ double sEps[8];
     const TileJob jb = jobs[blockIdx.x];
@@ -242,10 +248,10 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
             const int b = (side ? bj0 : bi0) + tid;
             const bool ok = tid < (side ? nj : ni);
             for (int k = 0; k < 3; ++k) {
-                sF[side][tid][k] = ok ? F[3 * b + k] : 0.0;
-                sX[side][tid][k] = ok && want_rs ? X[3 * b + k] : 0.0;
+                sF[side][tid][k] = ok ? (T)F[3 * b + k] : (T)0;
+                sX[side][tid][k] = ok && want_rs ? (T)X[3 * b + k] : (T)0;
             }
-            sInv[side][tid] = ok ? pos[b].w / A.preDii : 0.0;   // 1/diag_D (diff_decl.c:94-99)
+            sInv[side][tid] = ok ? (T)(pos[b].w / A.preDii) : (T)0;   // 1/diag_D (diff_decl.c:94-99)
         }
     }
     // phase 1: tiles
@@ -253,19 +259,19 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
         const int li = p / TB, lj = p % TB;
         T t[6] = {0, 0, 0, 0, 0, 0};
         if (li < ni && lj < nj && (!diag || lj < li)) tile_of<T>(A, pos, bi0 + li, bj0 + lj, t);
-        for (int k = 0; k < 6; ++k) tD[li][lj][k] = t[k];
+        for (int k = 0; k < 6; ++k) tD[k][li][lj] = t[k];
     }
     __syncthreads();
     // phase 2: rows (into bead i of tile I), 8 lanes per row
     const int row = tid >> 3, lane = tid & 7;
-    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    double eps = 0;
+    T acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    T eps = 0;
     for (int lj = lane; lj < TB; lj += 8) {
-        const T* t = tD[row][lj];
-        const double xx = t[0], yy = t[1], zz = t[2], xy = t[3], xz = t[4], yz = t[5];
-        const double* f = sF[1][lj];
-        const double* x = sX[1][lj];
-        const double inv = sInv[1][lj];
+        const T xx = tD[0][row][lj], yy = tD[1][row][lj], zz = tD[2][row][lj];
+        const T xy = tD[3][row][lj], xz = tD[4][row][lj], yz = tD[5][row][lj];
+        const T* f = sF[1][lj];
+        const T* x = sX[1][lj];
+        const T inv = sInv[1][lj];
         acc[0] += xx * f[0] + xy * f[1] + xz * f[2];
         acc[1] += xy * f[0] + yy * f[1] + yz * f[2];
         acc[2] += xz * f[0] + yz * f[1] + zz * f[2];
@@ -282,10 +288,10 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
         eps += __shfl_xor_sync(0xffffffffu, eps, o);
     }
     if (lane == 0)
-        for (int k = 0; k < 9; ++k) sAcc[row][k] = acc[k];
+        for (int k = 0; k < 9; ++k) sAcc[row][k] = (double)acc[k];
     // eps: one value per warp (rows 4w..4w+3), then fixed-order sum
     {
-        double e = lane == 0 ? eps : 0.0;
+        double e = lane == 0 ? (double)eps : 0.0;
         for (int o = 8; o < 32; o <<= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
         if ((tid & 31) == 0) sEps[tid >> 5] = e;
     }
@@ -307,11 +313,11 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
     const int col = tid >> 3;
     for (int k = 0; k < 9; ++k) acc[k] = 0;
     for (int li = lane; li < TB; li += 8) {
-        const T* t = tD[li][col];
-        const double xx = t[0], yy = t[1], zz = t[2], xy = t[3], xz = t[4], yz = t[5];
-        const double* f = sF[0][li];
-        const double* x = sX[0][li];
-        const double inv = sInv[0][li];
+        const T xx = tD[0][li][col], yy = tD[1][li][col], zz = tD[2][li][col];
+        const T xy = tD[3][li][col], xz = tD[4][li][col], yz = tD[5][li][col];
+        const T* f = sF[0][li];
+        const T* x = sX[0][li];
+        const T inv = sInv[0][li];
         acc[0] += xx * f[0] + xy * f[1] + xz * f[2];
         acc[1] += xy * f[0] + yy * f[1] + yz * f[2];
         acc[2] += xz * f[0] + yz * f[1] + zz * f[2];
@@ -327,9 +333,9 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
     if (lane == 0 && col < nj) {
         double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.I * g.count + jb.J * TB + col);
         if (diag) {
-            for (int k = 0; k < 9; ++k) dst[k] = acc[k] + sAcc[col][k];
+            for (int k = 0; k < 9; ++k) dst[k] = (double)acc[k] + sAcc[col][k];
         } else {
-            for (int k = 0; k < 9; ++k) dst[k] = acc[k];
+            for (int k = 0; k < 9; ++k) dst[k] = (double)acc[k];
         }
     }
 }
