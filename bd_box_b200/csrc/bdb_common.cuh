@@ -123,7 +123,9 @@ struct bdb_system {
     bdb::DevBuf<bdb::TileJob> jobs;
     bdb::DevBuf<unsigned char> tea_meta;       // TEA segment table + job offsets
     int n_jobs = 0;
-    int tea_tile = 32;
+    int tea_tile = 32;                         // TEA tile edge (16 or 32 beads)
+    int mv_warps = 16;                         // stored matvec: target warps per SM
+    bool autotune = false, tea_tuned = false, mv_tuned = false;
     bdb::DevBuf<double> ewald_tab;             // Ewald lattice tables (rpy_tile.cuh EwaldConst)
     int ewald_nk = 0, ewald_nimg = 0;
     bdb::DevBuf<double> M64;                   // stored D (upper) + L (lower), FP64

@@ -266,6 +266,7 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return fail(BDB_ERR_CUDA, "no CUDA device");
     bdb_system* s = new bdb_system();
+    cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, dev);
     s->p = *p;
     if (s->p.refresh < 1) s->p.refresh = 1;
     s->n = p->n;
@@ -591,6 +592,39 @@ int bdb_step(bdb_system* s, int K, const double* gauss)
     int rc = check_status(s, &ov);
     if (rc) return rc;
     return ov ? 1 : 0;
+}
+
+int bdb_autotune(bdb_system* s, int enable)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    s->autotune = enable != 0;
+    return BDB_OK;
+}
+
+int bdb_get_tuning(bdb_system* s, int* tea_tile, int* mv_warps_per_sm)
+{
+    if (!s || !tea_tile || !mv_warps_per_sm) return fail(BDB_ERR_ARG, "null argument");
+    *tea_tile = s->tea_tile;
+    *mv_warps_per_sm = s->mv_warps;
+    return BDB_OK;
+}
+
+int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    if (tea_tile != 0 && tea_tile != 16 && tea_tile != 32) return fail(BDB_ERR_ARG, "TEA tile must be 16 or 32");
+    if (mv_warps_per_sm < 0 || mv_warps_per_sm > 64) return fail(BDB_ERR_ARG, "matvec warps per SM out of range");
+    if (tea_tile && tea_tile != s->tea_tile) {
+        s->tea_tile = tea_tile;
+        s->tea_meta.release();   // the work list is rebuilt for the new tile at the next TEA call
+        drop_graph(s);
+    }
+    if (mv_warps_per_sm && mv_warps_per_sm != s->mv_warps) {
+        s->mv_warps = mv_warps_per_sm;
+        drop_graph(s);
+    }
+    s->tea_tuned = s->mv_tuned = true;   // pinned values are not re-tuned
+    return BDB_OK;
 }
 
 int bdb_set_graphs(bdb_system* s, int enable)

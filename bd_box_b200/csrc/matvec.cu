@@ -183,29 +183,89 @@ static void mv_finish(cudaStream_t st, int n3, int nseg, const double* rowp, con
                                                                                 Rs, want_rs);
 }
 
-int stored_matvec(bdb_system* s, bool want_rs)
+// column segmentation of the strip products: enough warps for the machine
+// (warps_per_sm per SM), columns in multiples of 128
+static void mv_split(int n3, int warps_per_sm, int sms, int* nseg_out, int* seg_cols_out)
+{
+    const int nstrip = (n3 + STRIP - 1) / STRIP;
+    int nseg = std::max(1, (sms * warps_per_sm + nstrip - 1) / nstrip);
+    const int seg_cols = ((n3 + nseg - 1) / nseg + 127) / 128 * 128;
+    nseg = (n3 + seg_cols - 1) / seg_cols;
+    *nseg_out = nseg;
+    *seg_cols_out = seg_cols;
+}
+
+static void mv_launch(bdb_system* s, int nseg, int seg_cols, const double* X, double* rowp, double* colp)
 {
     const int n3 = s->n3;
     const int nstrip = (n3 + STRIP - 1) / STRIP;
-    // enough warps for the machine: aim at >= 16 warps per SM
-    int nseg = std::max(1, (148 * 16 + nstrip - 1) / nstrip);
-    int seg_cols = ((n3 + nseg - 1) / nseg + 127) / 128 * 128;
-    nseg = (n3 + seg_cols - 1) / seg_cols;
-    const size_t need_row = (size_t)nseg * n3 * 2, need_col = (size_t)nstrip * n3;
-    if (s->part.n < need_row + need_col) {
-        if (s->part.alloc(need_row + need_col)) return BDB_ERR_NOMEM;
-    }
-    double* rowp = s->part.p;
-    double* colp = s->part.p + need_row;
-    const int items = nstrip * nseg;
-    const int blocks = (items + WARPS - 1) / WARPS;
-    const double* X = want_rs ? s->X.p : s->F.p;   // any valid vector when Rs is not wanted
+    const int blocks = (nstrip * nseg + WARPS - 1) / WARPS;
     if (s->p.precision == BDB_PREC_FP64)
         k_strip_mv<double><<<blocks, 32 * WARPS, 0, s->stream>>>(s->M64.p, n3, s->npad, nseg, seg_cols, s->F.p, X,
                                                                  rowp, colp);
     else
         k_strip_mv<float><<<blocks, 32 * WARPS, 0, s->stream>>>(s->M32.p, n3, s->npad, nseg, seg_cols, s->F.p, X,
                                                                 rowp, colp);
+}
+
+// Autotuning of the segmentation: 8, 16 or 32 warps per SM, each timed
+// twice after a warm-up; runs at the first product of a system with
+// autotuning on (before any graph capture).
+static int mv_tune(bdb_system* s, const double* X, double* part)
+{
+    const int cands[3] = {8, 16, 32};
+    float best_ms = 1e30f;
+    int best = s->mv_warps;
+    cudaEvent_t e0, e1;
+    BDB_CUDA(cudaEventCreate(&e0));
+    BDB_CUDA(cudaEventCreate(&e1));
+    for (int w : cands) {
+        int nseg, seg_cols;
+        mv_split(s->n3, w, s->sm_count, &nseg, &seg_cols);
+        double* rowp = part;
+        double* colp = part + (size_t)nseg * s->n3 * 2;
+        mv_launch(s, nseg, seg_cols, X, rowp, colp);
+        BDB_CUDA(cudaEventRecord(e0, s->stream));
+        mv_launch(s, nseg, seg_cols, X, rowp, colp);
+        mv_launch(s, nseg, seg_cols, X, rowp, colp);
+        BDB_CUDA(cudaEventRecord(e1, s->stream));
+        BDB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BDB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        s->launches += 3;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = w;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->mv_warps = best;
+    s->mv_tuned = true;
+    return BDB_OK;
+}
+
+int stored_matvec(bdb_system* s, bool want_rs)
+{
+    const int n3 = s->n3;
+    const int nstrip = (n3 + STRIP - 1) / STRIP;
+    // room for the largest segmentation any tuning candidate can pick
+    int nseg_max, cols_max;
+    mv_split(n3, 32, s->sm_count, &nseg_max, &cols_max);
+    const size_t need = (size_t)std::max(nseg_max, 1) * n3 * 2 + (size_t)nstrip * n3;
+    if (s->part.n < need) {
+        if (s->part.alloc(need)) return BDB_ERR_NOMEM;
+    }
+    const double* X = want_rs ? s->X.p : s->F.p;   // any valid vector when Rs is not wanted
+    if (s->autotune && !s->mv_tuned) {
+        int rc = mv_tune(s, X, s->part.p);
+        if (rc) return rc;
+    }
+    int nseg, seg_cols;
+    mv_split(n3, s->mv_warps, s->sm_count, &nseg, &seg_cols);
+    double* rowp = s->part.p;
+    double* colp = s->part.p + (size_t)nseg * n3 * 2;
+    mv_launch(s, nseg, seg_cols, X, rowp, colp);
     BDB_CUDA(cudaGetLastError());
     s->launches += 2;
     const double pre = s->p.dt / (BDB_KB * s->p.T);

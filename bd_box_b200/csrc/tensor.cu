@@ -162,10 +162,10 @@ static size_t build_smem_bytes()
     return sizeof(T) * 3 * TB * (3 * TB + 1);
 }
 
-template <typename T>
+template <typename T, int TT>
 static size_t tea_smem_bytes()
 {
-    return sizeof(T) * TB * (TB + 1) * 6;
+    return sizeof(T) * TT * (TT + 1) * 6;
 }
 
 static int tensor_attrs();
@@ -226,24 +226,25 @@ struct TeaSeg {
 // beads of I and (phase 3) the column sums into the beads of J. Within a job
 // the sums run in T (FP32 on the mixed path); the records they produce and
 // every sum across jobs are FP64.
-template <typename T>
+template <typename T, int TT>
 __global__ void __launch_bounds__(256)
 k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__ segs,
       const double4* __restrict__ pos, const double* __restrict__ F, const double* __restrict__ X,
       double* __restrict__ part, double* __restrict__ eps_part, int want_rs)
 {
     extern __shared__ __align__(16) unsigned char tea_smem[];
-    T(*tD)[TB][TB + 1] = reinterpret_cast<T(*)[TB][TB + 1]>(tea_smem);   // [6][TB][TB+1]
-    __shared__ T sF[2][TB][3], sX[2][TB][3], sInv[2][TB];
-    __shared__ double sAcc[TB][9];
+    constexpr int LPR = 256 / TT;   // lanes per row (phase 2) or column (phase 3)
+    T(*tD)[TT][TT + 1] = reinterpret_cast<T(*)[TT][TT + 1]>(tea_smem);   // [6][TT][TT+1]
+    __shared__ T sF[2][TT][3], sX[2][TT][3], sInv[2][TT];
+    __shared__ double sAcc[TT][9];
     __shared__ double sEps[8];
     const TileJob jb = jobs[blockIdx.x];
     const TeaSeg g = segs[jb.seg];
     const int tid = threadIdx.x;
-    const int bi0 = g.begin + jb.I * TB, bj0 = g.begin + jb.J * TB;
-    const int ni = min(TB, g.count - jb.I * TB), nj = min(TB, g.count - jb.J * TB);
+    const int bi0 = g.begin + jb.I * TT, bj0 = g.begin + jb.J * TT;
+    const int ni = min(TT, g.count - jb.I * TT), nj = min(TT, g.count - jb.J * TT);
     const bool diag = jb.I == jb.J;
-    if (tid < TB) {
+    if (tid < TT) {
         for (int side = 0; side < 2; ++side) {
             const int b = (side ? bj0 : bi0) + tid;
             const bool ok = tid < (side ? nj : ni);
@@ -255,18 +256,18 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
         }
     }
     // phase 1: tiles
-    for (int p = tid; p < TB * TB; p += blockDim.x) {
-        const int li = p / TB, lj = p % TB;
+    for (int p = tid; p < TT * TT; p += blockDim.x) {
+        const int li = p / TT, lj = p % TT;
         T t[6] = {0, 0, 0, 0, 0, 0};
         if (li < ni && lj < nj && (!diag || lj < li)) tile_of<T>(A, pos, bi0 + li, bj0 + lj, t);
         for (int k = 0; k < 6; ++k) tD[k][li][lj] = t[k];
     }
     __syncthreads();
     // phase 2: rows (into bead i of tile I), 8 lanes per row
-    const int row = tid >> 3, lane = tid & 7;
+    const int row = tid / LPR, lane = tid % LPR;
     T acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     T eps = 0;
-    for (int lj = lane; lj < TB; lj += 8) {
+    for (int lj = lane; lj < TT; lj += LPR) {
         const T xx = tD[0][row][lj], yy = tD[1][row][lj], zz = tD[2][row][lj];
         const T xy = tD[3][row][lj], xz = tD[4][row][lj], yz = tD[5][row][lj];
         const T* f = sF[1][lj];
@@ -283,16 +284,16 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
         acc[8] += xz * x[0] + yz * x[1] + zz * x[2];
         eps += xx + yy + zz + 2 * (xy + xz + yz);
     }
-    for (int o = 1; o < 8; o <<= 1) {
+    for (int o = 1; o < LPR; o <<= 1) {
         for (int k = 0; k < 9; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
         eps += __shfl_xor_sync(0xffffffffu, eps, o);
     }
     if (lane == 0)
         for (int k = 0; k < 9; ++k) sAcc[row][k] = (double)acc[k];
-    // eps: one value per warp (rows 4w..4w+3), then fixed-order sum
+    // eps: one value per warp (its 32 / LPR rows), then fixed-order sum
     {
         double e = lane == 0 ? (double)eps : 0.0;
-        for (int o = 8; o < 32; o <<= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        for (int o = LPR; o < 32; o <<= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
         if ((tid & 31) == 0) sEps[tid >> 5] = e;
     }
     __syncthreads();
@@ -305,14 +306,14 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
     // column sums below first
     if (!diag) {
         if (lane == 0 && row < ni) {
-            double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.J * g.count + jb.I * TB + row);
+            double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.J * g.count + jb.I * TT + row);
             for (int k = 0; k < 9; ++k) dst[k] = sAcc[row][k];
         }
     }
     // phase 3: columns (into bead j of tile J)
-    const int col = tid >> 3;
+    const int col = tid / LPR;
     for (int k = 0; k < 9; ++k) acc[k] = 0;
-    for (int li = lane; li < TB; li += 8) {
+    for (int li = lane; li < TT; li += LPR) {
         const T xx = tD[0][li][col], yy = tD[1][li][col], zz = tD[2][li][col];
         const T xy = tD[3][li][col], xz = tD[4][li][col], yz = tD[5][li][col];
         const T* f = sF[0][li];
@@ -328,10 +329,10 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
         acc[7] += xy * x[0] + yy * x[1] + yz * x[2];
         acc[8] += xz * x[0] + yz * x[1] + zz * x[2];
     }
-    for (int o = 1; o < 8; o <<= 1)
+    for (int o = 1; o < LPR; o <<= 1)
         for (int k = 0; k < 9; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
     if (lane == 0 && col < nj) {
-        double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.I * g.count + jb.J * TB + col);
+        double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.I * g.count + jb.J * TT + col);
         if (diag) {
             for (int k = 0; k < 9; ++k) dst[k] = (double)acc[k] + sAcc[col][k];
         } else {
@@ -414,24 +415,79 @@ __global__ void k_tea_finish(TensorArgs A, int n, const TeaSeg* __restrict__ seg
 
 int tea_setup(bdb_system* s);
 
+template <int TT>
+static void tea_launch(bdb_system* s, const TensorArgs& A, const TeaSeg* tsegs, bool want_rs)
+{
+    if (s->p.precision == BDB_PREC_FP64)
+        k_tea<double, TT><<<s->n_jobs, 256, tea_smem_bytes<double, TT>(), s->stream>>>(
+            A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+    else
+        k_tea<float, TT><<<s->n_jobs, 256, tea_smem_bytes<float, TT>(), s->stream>>>(
+            A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+}
+
+static void tea_dispatch(bdb_system* s, const TensorArgs& A, const TeaSeg* tsegs, bool want_rs)
+{
+    if (s->tea_tile == 16) tea_launch<16>(s, A, tsegs, want_rs);
+    else tea_launch<32>(s, A, tsegs, want_rs);
+}
+
+// Autotuning of the TEA tile (16 or 32 beads): each candidate's work list
+// is built and its pair kernel timed twice on the system's stream; the
+// faster one is kept. Runs at the first TEA call of a system with
+// autotuning on (which comes before any graph capture).
+static int tea_tune(bdb_system* s, bool want_rs)
+{
+    const int cands[2] = {16, 32};
+    float best_ms = 1e30f;
+    int best = s->tea_tile;
+    cudaEvent_t e0, e1;
+    BDB_CUDA(cudaEventCreate(&e0));
+    BDB_CUDA(cudaEventCreate(&e1));
+    for (int c : cands) {
+        s->tea_tile = c;
+        int rc = tea_setup(s);
+        if (rc) return rc;
+        if (int rc_e = ewald_tables(s)) return rc_e;
+        const TensorArgs A = targs(s);
+        const TeaSeg* tsegs = reinterpret_cast<const TeaSeg*>(s->tea_meta.p);
+        tea_dispatch(s, A, tsegs, want_rs);   // warm-up
+        BDB_CUDA(cudaEventRecord(e0, s->stream));
+        tea_dispatch(s, A, tsegs, want_rs);
+        tea_dispatch(s, A, tsegs, want_rs);
+        BDB_CUDA(cudaEventRecord(e1, s->stream));
+        BDB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BDB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        s->launches += 3;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->tea_tile = best;
+    s->tea_tuned = true;
+    return tea_setup(s);
+}
+
 int tea_run(bdb_system* s, bool want_rs)
 {
-    if (!s->tea_meta.p) {
+    int rc0 = tensor_attrs();
+    if (rc0) return rc0;
+    if (s->autotune && !s->tea_tuned && s->p.hydro && s->n_jobs >= 0) {
+        int rc = tea_tune(s, want_rs);
+        if (rc) return rc;
+    } else if (!s->tea_meta.p) {
         int rc = tea_setup(s);
         if (rc) return rc;
     }
-    int rc0 = tensor_attrs();
-    if (rc0) return rc0;
     if (int rc_e = ewald_tables(s)) return rc_e;
     const TensorArgs A = targs(s);
     TeaSeg* tsegs = reinterpret_cast<TeaSeg*>(s->tea_meta.p);
     if (s->p.hydro && s->n_jobs) {
-        if (s->p.precision == BDB_PREC_FP64)
-            k_tea<double><<<s->n_jobs, 256, tea_smem_bytes<double>(), s->stream>>>(A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p,
-                                                           s->part.p, s->eps_part.p, want_rs);
-        else
-            k_tea<float><<<s->n_jobs, 256, tea_smem_bytes<float>(), s->stream>>>(A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p,
-                                                          s->part.p, s->eps_part.p, want_rs);
+        tea_dispatch(s, A, tsegs, want_rs);
         BDB_CUDA(cudaGetLastError());
         if (want_rs) {
             const int* job_begin = reinterpret_cast<const int*>(tsegs + s->segs.size());
@@ -462,7 +518,7 @@ int tea_setup(bdb_system* s)
         TeaSeg t;
         t.begin = sg.begin;
         t.count = sg.count;
-        t.ntile = (sg.count + TB - 1) / TB;
+        t.ntile = (sg.count + s->tea_tile - 1) / s->tea_tile;
         t.part_begin = (int)part_records;
         part_records += (size_t)t.ntile * sg.count;
         ts.push_back(t);
@@ -492,10 +548,14 @@ static int tensor_attrs()
                                   (int)build_smem_bytes<double>()));
     BDB_CUDA(cudaFuncSetAttribute(k_build<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)build_smem_bytes<float>()));
-    BDB_CUDA(cudaFuncSetAttribute(k_tea<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)tea_smem_bytes<double>()));
-    BDB_CUDA(cudaFuncSetAttribute(k_tea<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)tea_smem_bytes<float>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_tea<double, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tea_smem_bytes<double, 32>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_tea<float, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tea_smem_bytes<float, 32>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_tea<double, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tea_smem_bytes<double, 16>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_tea<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tea_smem_bytes<float, 16>()));
     done = true;
     return BDB_OK;
 }

@@ -40,7 +40,8 @@ EXPORTS = [
     "bdb_version", "bdb_last_error", "bdb_create", "bdb_create_batch", "bdb_destroy", "bdb_set_bonded",
     "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
-    "bdb_compute_r", "bdb_step", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
+    "bdb_compute_r", "bdb_step", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_autotune", "bdb_get_tuning",
+    "bdb_set_tuning", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc",
 ]
 
@@ -97,6 +98,9 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_step.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.bdb_set_dt.argtypes = [C.c_void_p, C.c_double]
     lib.bdb_set_graphs.argtypes = [C.c_void_p, C.c_int]
+    lib.bdb_autotune.argtypes = [C.c_void_p, C.c_int]
+    lib.bdb_get_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.bdb_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.bdb_adjoint.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _ip, _dp, _dp, _dp, _dp]
     lib.bdb_factor_error.argtypes = [C.c_void_p, _dp]
     lib.bdb_profile.argtypes = [C.c_void_p, C.c_int]
@@ -279,6 +283,18 @@ class System:
         self._check(self.lib.bdb_adjoint(self.h, K, checkpoint, len(pairs), pairs.ctypes.data_as(_ip), _p(targets),
                                          C.byref(loss), _p(gx), _p(gp)))
         return loss.value, gx.reshape(self.n, 3), gp
+
+    def autotune(self, enable: bool = True):
+        self._check(self.lib.bdb_autotune(self.h, int(enable)))
+
+    def tuning(self):
+        """(TEA tile edge, stored-matvec warps per SM) in use."""
+        a, b = C.c_int(), C.c_int()
+        self._check(self.lib.bdb_get_tuning(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_tuning(self, tea_tile: int = 0, mv_warps_per_sm: int = 0):
+        self._check(self.lib.bdb_set_tuning(self.h, tea_tile, mv_warps_per_sm))
 
     def factor_error(self) -> float:
         out = C.c_double()

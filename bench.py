@@ -206,6 +206,7 @@ def run_ours(args):
         n3 = 3 * deck.n
         sysm = engine.System(deck, precision=engine.PREC_MIXED, refresh=REFRESH,
                              noise=engine.NOISE_PHILOX, seed=ranks.replica_seed(SEED, rank))
+        sysm.autotune(True)
         for _ in range(args.warmup):
             sysm.step(1)
         sysm.lib.bdb_reset_stats(sysm.h)
@@ -315,6 +316,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (stored D/L 604 MB read every step)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches.value),
+            "autotuned": {"matvec_warps_per_sm": sysm.tuning()[1]},
             "clocks": clk.summary(), "fp64_gpu": fp64, "errors": errors, "replicas": reps, "adjoint": adj, "ewald_suspension": ew,
         }
         if rank == 0:
@@ -364,10 +366,12 @@ def replicas(torch, engine, steps, warmup):
         ds = [decks.read_deck(decks.write_chain_deck(d, f"r{k}", int(n), seed=1000 + k, hydro="geyer"))
               for k, n in enumerate(sizes)]
     b = engine.System(ds, precision=engine.PREC_MIXED, noise=engine.NOISE_PHILOX, seed=SEED)
+    b.autotune(True)
     for _ in range(warmup):
         b.step(1)
     ms = time_steps(torch, b, steps)
     launches = b.launches()
+    tea_tile = b.tuning()[0]
     total = int(sizes.sum())
     b.close()
     g = np.random.default_rng(13).standard_normal(3 * total)
@@ -388,7 +392,7 @@ def replicas(torch, engine, steps, warmup):
     return {"workload": f"{len(ds)} chains, beads uniform in [64,1024] (seeded), sum N={total}, "
                         f"sum N^2={int((sizes.astype(np.int64) ** 2).sum())}, TEA noise, mixed precision, one batch",
             "metric": "bead-steps/s", "value": total * steps / (ms / 1e3), "steps": steps,
-            "ms_per_step": ms / steps, "gpu_launches": launches,
+            "ms_per_step": ms / steps, "gpu_launches": launches, "autotuned_tea_tile": tea_tile,
             "displacement_rel_vs_fp64": {"max": max(errs), "median": float(np.median(errs))}}
 
 
@@ -463,8 +467,10 @@ def ewald_case(torch, engine, steps=3):
     with tempfile.TemporaryDirectory() as d:
         deck = decks.read_deck(decks.write_suspension_deck(d, "susp4096", 4096, seed=8, ewald_r=3))
     s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_PHILOX, seed=SEED)
+    s.autotune(True)
     s.step(1)
     ms = time_steps(torch, s, steps)
+    tea_tile = s.tuning()[0]
     s.close()
     g = np.random.default_rng(6).standard_normal(3 * deck.n)
     sm = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
@@ -484,7 +490,7 @@ def ewald_case(torch, engine, steps=3):
     s64.close()
     return {"workload": "periodic suspension N=4096, phi=0.10, Beenakker Ewald R=3, TEA on the fly, mixed precision",
             "metric": "steps/s", "value": steps / (ms / 1e3), "ms_per_step": ms / steps,
-            "fp64_steps_per_s": 1.0 / t64,
+            "fp64_steps_per_s": 1.0 / t64, "autotuned_tea_tile": tea_tile,
             "displacement_rel_vs_fp64": float(np.linalg.norm(dm - dd) / np.linalg.norm(dd))}
 
 
