@@ -296,14 +296,26 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
     }
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const size_t base = (size_t)P * PW;
-    for (int idx = tid; idx < PW * PW / 4; idx += blockDim.x) {
-        const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
-        const float4 v = *reinterpret_cast<const float4*>(M + (base + r) * npad + base + c);
-        double* s = S + r * LDS + c;
-        s[0] = c <= r ? (double)v.x : 0.0;
-        s[1] = c + 1 <= r ? (double)v.y : 0.0;
-        s[2] = c + 2 <= r ? (double)v.z : 0.0;
-        s[3] = c + 3 <= r ? (double)v.w : 0.0;
+    {
+        // all loads of a thread first, then the stores (one L2 round trip)
+        constexpr int NV = PW * PW / 4 / POTRF_THREADS;   // 8
+        float4 v[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const int idx = tid + POTRF_THREADS * k;
+            const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
+            v[k] = *reinterpret_cast<const float4*>(M + (base + r) * npad + base + c);
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const int idx = tid + POTRF_THREADS * k;
+            const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
+            double* s = S + r * LDS + c;
+            s[0] = c <= r ? (double)v[k].x : 0.0;
+            s[1] = c + 1 <= r ? (double)v[k].y : 0.0;
+            s[2] = c + 2 <= r ? (double)v[k].z : 0.0;
+            s[3] = c + 3 <= r ? (double)v[k].w : 0.0;
+        }
     }
     if (tid == 0) bad = 0;
     __syncthreads();
@@ -450,17 +462,34 @@ __global__ void __launch_bounds__(256) k_trsm128(float* __restrict__ M, int npad
     const size_t base = (size_t)P * PW;
     const size_t row0 = base + PW + (size_t)blockIdx.x * TRSM_ROWS;
     const int nrow = (int)min((size_t)TRSM_ROWS, (size_t)npad - row0);
-    for (int idx = tid; idx < PW * PW / 2; idx += blockDim.x)
-        reinterpret_cast<double2*>(sW)[idx] = reinterpret_cast<const double2*>(Wt)[idx];
-    for (int idx = tid; idx < TRSM_ROWS * PW / 4; idx += blockDim.x) {
-        const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (r < nrow) v = *reinterpret_cast<const float4*>(M + (row0 + r) * npad + base + c);
-        double* a = A + r * TRSM_LDX + c;
-        a[0] = v.x;
-        a[1] = v.y;
-        a[2] = v.z;
-        a[3] = v.w;
+    // staging: all of a thread's loads are issued before its stores, so the
+    // L2 latency is paid once, not once per element
+    {
+        constexpr int NW = PW * PW / 2 / 256, NA = TRSM_ROWS * PW / 4 / 256;   // 32, 8 per thread
+        const double2* src = reinterpret_cast<const double2*>(Wt);
+        double2 w[NW];
+#pragma unroll
+        for (int k = 0; k < NW; ++k) w[k] = __ldg(src + tid + 256 * k);
+        float4 v[NA];
+#pragma unroll
+        for (int k = 0; k < NA; ++k) {
+            const int idx = tid + 256 * k;
+            const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
+            v[k] = r < nrow ? *reinterpret_cast<const float4*>(M + (row0 + r) * npad + base + c)
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < NW; ++k) reinterpret_cast<double2*>(sW)[tid + 256 * k] = w[k];
+#pragma unroll
+        for (int k = 0; k < NA; ++k) {
+            const int idx = tid + 256 * k;
+            const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
+            double* a = A + r * TRSM_LDX + c;
+            a[0] = v[k].x;
+            a[1] = v[k].y;
+            a[2] = v[k].z;
+            a[3] = v[k].w;
+        }
     }
     __syncthreads();
     const int warp = tid >> 5, lane = tid & 31;
