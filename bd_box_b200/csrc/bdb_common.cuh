@@ -146,7 +146,9 @@ struct bdb_system {
     cudaGraphExec_t step_graph = nullptr;
     long long graph_launches = 0;
     long long eager_steps = 0;
-    bool graphs = true;
+    cudaGraphExec_t refresh_graph = nullptr;   // tensor build + factorisation (mixed path)
+    long long refresh_launches = 0, eager_refreshes = 0;
+    bool graphs = true, graph_refresh = true;
 
     // measurement: CUDA-event pairs per phase, kernel launch count
     struct PhaseRec {

@@ -120,20 +120,56 @@ int ensure_matrix(bdb_system* s)
     return BDB_OK;
 }
 
-// D (and its factor) at the current positions
-static int refresh_factor(bdb_system* s)
+static int build_and_factor(bdb_system* s)
 {
-    int rc = ensure_matrix(s);
-    if (rc) return rc;
-    phase_mark(s, P_REFRESH);
     phase_mark(s, P_BUILD);
-    rc = tensor_build(s);
+    int rc = tensor_build(s);
     if (rc) return rc;
     phase_mark(s, P_BUILD);
     phase_mark(s, P_FACTOR);
     rc = factor_run(s);
     if (rc) return rc;
     phase_mark(s, P_FACTOR);
+    return BDB_OK;
+}
+
+// D (and its factor) at the current positions. After one eager refresh
+// (which allocates and encodes everything the kernels use), the mixed path
+// replays the ~400 launches of a refresh -- both streams of the look-ahead
+// factorisation included -- from a captured CUDA graph.
+static int refresh_factor(bdb_system* s)
+{
+    int rc = ensure_matrix(s);
+    if (rc) return rc;
+    phase_mark(s, P_REFRESH);
+    const bool graph = s->graph_refresh && !s->profiling && s->p.precision == BDB_PREC_MIXED && s->eager_refreshes > 0;
+    if (graph) {
+        if (!s->refresh_graph) {
+            const long long before = s->launches;
+            BDB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            rc = build_and_factor(s);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+            if (rc || e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return rc ? rc : cuda_fail(e, "cudaStreamEndCapture");
+            }
+            const cudaError_t ei = cudaGraphInstantiate(&s->refresh_graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) {
+                s->refresh_graph = nullptr;
+                return cuda_fail(ei, "cudaGraphInstantiate");
+            }
+            s->refresh_launches = s->launches - before;
+            s->launches = before;
+        }
+        BDB_CUDA(cudaGraphLaunch(s->refresh_graph, s->stream));
+        s->launches += s->refresh_launches;
+    } else {
+        rc = build_and_factor(s);
+        if (rc) return rc;
+        s->eager_refreshes++;
+    }
     phase_mark(s, P_REFRESH);
     s->factor_valid = true;
     s->steps_since_refresh = 0;
@@ -175,6 +211,8 @@ void drop_graph(bdb_system* s)
 {
     if (s->step_graph) cudaGraphExecDestroy(s->step_graph);
     s->step_graph = nullptr;
+    if (s->refresh_graph) cudaGraphExecDestroy(s->refresh_graph);
+    s->refresh_graph = nullptr;
 }
 
 // step_body captured once as a CUDA graph and replayed (device noise only:
@@ -627,11 +665,13 @@ int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm)
     return BDB_OK;
 }
 
-int bdb_set_graphs(bdb_system* s, int enable)
+int bdb_set_graphs(bdb_system* s, int mode)
 {
     if (!s) return fail(BDB_ERR_ARG, "null system");
-    s->graphs = enable != 0;
-    if (!s->graphs) drop_graph(s);
+    if (mode < 0 || mode > 3) return fail(BDB_ERR_ARG, "graph mode is a mask of 1 (steps) and 2 (refreshes)");
+    s->graphs = (mode & 1) != 0;
+    s->graph_refresh = (mode & 2) != 0;
+    drop_graph(s);
     return BDB_OK;
 }
 

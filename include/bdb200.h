@@ -175,12 +175,14 @@ int bdb_autotune(bdb_system* s, int enable);
 int bdb_get_tuning(bdb_system* s, int* tea_tile, int* mv_warps_per_sm);
 int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm);
 
-/* Device-noise steps (BDB_NOISE_PHILOX, profiling off) replay the steady
- * part of a step -- noise, D.F and the random displacement, the update, the
- * forces -- from a CUDA graph captured on the second step; refreshes of D
- * and its factor run outside it. On by default; 0 turns it off. No
- * reference counterpart. */
-int bdb_set_graphs(bdb_system* s, int enable);
+/* CUDA graphs (no reference counterpart). Mode bit 1: device-noise steps
+ * (BDB_NOISE_PHILOX, profiling off) replay the steady part of a step --
+ * noise, D.F and the random displacement, the update, the forces -- from a
+ * graph captured on the second step. Bit 2: on the mixed path, refreshes of
+ * D and its factor (tensor build and the two-stream factorisation) replay a
+ * graph captured on the second refresh. Default 3 (both); 0 runs
+ * everything eagerly. */
+int bdb_set_graphs(bdb_system* s, int mode);
 
 /* Time step of the following steps (curr_dt, diff_decl.c:68): the variable
  * step of comp_step_ermak halves it on overlap (diff_comp.c:162-165). */

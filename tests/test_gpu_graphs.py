@@ -1,7 +1,8 @@
 """Device-noise steps replay a captured CUDA graph of the steady part of a
-step. Graph and eager execution must give the same bits, across refreshes of
-the stored tensor and across a change of the time step (which rebuilds the
-graph)."""
+step, and mixed-precision refreshes of D and its factor replay a second one.
+Every graph mode must give the eager run's bits, across refreshes of the
+stored tensor and across a change of the time step (which rebuilds the
+graphs)."""
 import numpy as np
 import pytest
 
@@ -18,7 +19,7 @@ from bd_box_b200 import decks, engine  # noqa: E402
 def test_graph_replay_matches_eager(hydro, precision, refresh, deck_dir):
     deck = decks.read_deck(decks.write_chain_deck(deck_dir, f"g_{hydro}{precision}", 160, seed=31, hydro=hydro))
     runs = []
-    for graphs in (1, 0):
+    for graphs in (3, 2, 1, 0):
         s = engine.System(deck, precision=precision, refresh=refresh, noise=engine.NOISE_PHILOX, seed=77)
         s._check(s.lib.bdb_set_graphs(s.h, graphs))
         out = []
@@ -30,9 +31,10 @@ def test_graph_replay_matches_eager(hydro, precision, refresh, deck_dir):
         out.append(s.get_coord())
         runs.append((np.array(out), s.launches()))
         s.close()
-    (a, la), (b, lb) = runs
-    assert np.array_equal(a, b)
-    assert la == lb
+    a, la = runs[-1]
+    for b, lb in runs[:-1]:
+        assert np.array_equal(a, b)
+        assert la == lb
     # the noise changes from step to step (the device counter advances)
     d1 = a[1, :, :3] - a[0, :, :3]
     d2 = a[2, :, :3] - a[1, :, :3]
