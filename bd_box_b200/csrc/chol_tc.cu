@@ -26,8 +26,10 @@
 //             K step, into one of two TMEM accumulators (128 columns each);
 //             tcgen05.commit frees a ring stage / publishes an accumulator;
 //   warps 2-5 epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
-//             lanes 32(w%4)..), C -= acc in global memory (lower triangle
-//             only on diagonal tiles), then hand the accumulator back.
+//             lanes 32(w%4)..), hand the accumulator back, then -acc per
+//             128x32 box into a 2-box shared-memory ring and a TMA
+//             reduce-add into C (lower triangle only on diagonal tiles);
+//             C is never loaded.
 // The epilogue of tile t overlaps the MMAs of tile t+1 and the loads of the
 // tiles after it. Every mbarrier wait is bounded; a time-out sets
 // ST_TIMEOUT and a shared abort flag that stops all roles, and the CTA frees
@@ -45,11 +47,11 @@ namespace bdb {
 static constexpr int PW = 128;                    // super-panel width = tile size
 static constexpr int KC = 32;                     // K columns per TMA box (128 B of FP32)
 static constexpr int NCHUNK = PW / KC;            // 4
-static constexpr int STAGES = 2;
+static constexpr int STAGES = 3;
 static constexpr int BOX_BYTES = PW * KC * 4;     // 16 KB
 static constexpr int STAGE_BYTES = 4 * BOX_BYTES; // A_hi, A_lo, B_hi, B_lo
-static constexpr int C_BYTES = PW * PW * 4;       // one C tile, 4 boxes of 128 rows x 32 columns
-static constexpr int SYRK_SMEM = STAGES * STAGE_BYTES + C_BYTES + 1024;
+static constexpr int C_BOXES = 2;                 // staging ring of 128x32 boxes for the C update
+static constexpr int SYRK_SMEM = STAGES * STAGE_BYTES + C_BOXES * BOX_BYTES + 1024;
 static constexpr uint32_t WAIT_LIMIT = 1u << 22;
 static constexpr int LDS = PW + 1;                // padded FP64 row in shared memory
 
@@ -100,9 +102,10 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, uint32_t src, int x, int y)
+// C[tile] += smem tile (FP32 add in L2, no load of C by the SM)
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, uint32_t src, int x, int y)
 {
-    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+    asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
                      reinterpret_cast<uint64_t>(map)),
                  "r"(x), "r"(y), "r"(src)
                  : "memory");
@@ -110,12 +113,34 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, uint32_t sr
 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// wait until at most C_BOXES-1 of this thread's bulk groups still read
+// shared memory
+__device__ __forceinline__ void bulk_wait_read_ring()
+{
+    static_assert(C_BOXES == 2, "wait_group count below");
+    asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
 
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // barrier 1 among the 128 epilogue threads only
 __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// barrier 1 with an OR over the 128 epilogue threads: all of them see the
+// same answer, so they leave their loop together
+__device__ __forceinline__ bool epi_any(bool x)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, 1, 128, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)x)
+        : "memory");
+    return r != 0;
+}
 
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups
 // 1024 bytes apart (SBO = 64 x 16 B), LBO = 1 (unused for swizzled K-major),
@@ -530,12 +555,12 @@ __global__ void __launch_bounds__(256) k_trsm128(float* __restrict__ M, int npad
 // ------------------------------------------------------- tensor-core update
 
 struct SyrkBars {
-    uint64_t full[STAGES], empty[STAGES], accfull[2], accempty[2], cfull, cempty;
+    uint64_t full[STAGES], empty[STAGES], accfull[2], accempty[2];
 };
 
-// C tile of the output in shared memory: box cc (columns 32cc..32cc+31) holds
-// 128 rows of 128 bytes with the 128-byte swizzle (16-byte chunk j of row r
-// at position j ^ (r mod 8)), as TMA loads and stores it.
+// Staging slot cc of the C update in shared memory: one 128x32 box, 128
+// rows of 128 bytes with the 128-byte swizzle (16-byte chunk j of row r at
+// position j ^ (r mod 8)), the layout the TMA reduce reads.
 __device__ __forceinline__ float4* c_chunk(unsigned char* cbuf, int cc, int r, int j)
 {
     return reinterpret_cast<float4*>(cbuf + cc * BOX_BYTES + r * 128 + ((j ^ (r & 7)) << 4));
@@ -572,8 +597,6 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             mbar_init(smem_u32(&bars.accfull[b]), 1);
             mbar_init(smem_u32(&bars.accempty[b]), 4);
         }
-        mbar_init(smem_u32(&bars.cfull), 1);
-        mbar_init(smem_u32(&bars.cempty), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -605,18 +628,6 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                     tma_load_2d(st + 2 * BOX_BYTES, &map_hi, kc * KC, rb, fb);
                     tma_load_2d(st + 3 * BOX_BYTES, &map_lo, kc * KC, rb, fb);
                 }
-            }
-        } else if (lane == 1) {
-            // TMA producer of the C tile, once the previous one is stored
-            uint32_t tl = 0;
-            for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++tl) {
-                int ti, tj;
-                tile_of_mode(t, mode, ti, tj);
-                const int ra = (t0 + ti) * PW, rb = (t0 + tj) * PW;
-                if (!mbar_wait(smem_u32(&bars.cempty), (tl & 1) ^ 1, &abort_flag)) break;
-                const uint32_t cb = smem_u32(&bars.cfull);
-                mbar_expect_tx(cb, C_BYTES);
-                for (int cc = 0; cc < PW / KC; ++cc) tma_load_2d(cbase + cc * BOX_BYTES, &map_c, rb + cc * KC, ra, cb);
             }
         }
     } else if (warp == 1) {
@@ -654,16 +665,23 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             }
         }
     } else {
-        // epilogue warps 2..5: TMEM lane quarter = warp % 4
+        // epilogue warps 2..5: TMEM lane quarter = warp % 4. C is never
+        // loaded: each 128x32 box of -acc goes to shared memory and a TMA
+        // reduce-add applies it in L2 (C - acc and C + (-acc) are the same
+        // IEEE sum). On diagonal tiles the upper triangle (D, kept intact)
+        // receives -0.0, which leaves every value as it is.
         const int quarter = warp & 3;
         const int rl = 32 * quarter + lane;   // row inside the tile
         uint32_t tl = 0;
-        for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++tl) {
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
             int ti, tj;
             tile_of_mode(t, mode, ti, tj);
+            const bool diag = ti == tj;
+            const int ra = (t0 + ti) * PW, rb = (t0 + tj) * PW;
             const uint32_t b = tl & 1;
-            if (!mbar_wait(smem_u32(&bars.accfull[b]), (tl >> 1) & 1, &abort_flag)) break;
-            if (!mbar_wait(smem_u32(&bars.cfull), tl & 1, &abort_flag)) break;
+            // a time-out or abort seen by any epilogue thread stops all of
+            // them before the next barrier
+            if (epi_any(!mbar_wait(smem_u32(&bars.accfull[b]), (tl >> 1) & 1, &abort_flag))) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
             for (int cc = 0; cc < PW / 32; ++cc) {
@@ -680,32 +698,31 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                       "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (cc == PW / 32 - 1) {
+                    // the accumulator is free once all its columns are read
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&bars.accempty[b]));
+                }
+                // the reduce that last used this ring slot must have read it
+                if (tid == 64) bulk_wait_read_ring();
+                epi_sync();
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    float4* p = c_chunk(cbuf, cc, rl, j);
-                    float4 c4 = *p;
                     const int c = 32 * cc + 4 * j;   // column inside the tile
-                    const bool diag = ti == tj;
-                    if (!diag || c <= rl) c4.x -= __uint_as_float(v[4 * j]);
-                    if (!diag || c + 1 <= rl) c4.y -= __uint_as_float(v[4 * j + 1]);
-                    if (!diag || c + 2 <= rl) c4.z -= __uint_as_float(v[4 * j + 2]);
-                    if (!diag || c + 3 <= rl) c4.w -= __uint_as_float(v[4 * j + 3]);
-                    *p = c4;
+                    float4 d;
+                    d.x = (!diag || c <= rl) ? -__uint_as_float(v[4 * j]) : -0.0f;
+                    d.y = (!diag || c + 1 <= rl) ? -__uint_as_float(v[4 * j + 1]) : -0.0f;
+                    d.z = (!diag || c + 2 <= rl) ? -__uint_as_float(v[4 * j + 2]) : -0.0f;
+                    d.w = (!diag || c + 3 <= rl) ? -__uint_as_float(v[4 * j + 3]) : -0.0f;
+                    *c_chunk(cbuf, cc % C_BOXES, rl, j) = d;
                 }
-            }
-            // the accumulator is free once all its columns are read
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&bars.accempty[b]));
-            // write the tile back with TMA once every epilogue thread is done
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            epi_sync();
-            if (tid == 64) {
-                const int ra = (t0 + ti) * PW, rb = (t0 + tj) * PW;
-                for (int cc = 0; cc < PW / KC; ++cc) tma_store_2d(&map_c, cbase + cc * BOX_BYTES, rb + cc * KC, ra);
-                bulk_commit();
-                bulk_wait_read0();
-                mbar_arrive(smem_u32(&bars.cempty));
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                epi_sync();
+                if (tid == 64) {
+                    tma_reduce_add_2d(&map_c, cbase + (cc % C_BOXES) * BOX_BYTES, rb + cc * KC, ra);
+                    bulk_commit();
+                }
             }
         }
         if (tid == 64) bulk_wait0();
