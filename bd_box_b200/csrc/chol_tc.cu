@@ -209,16 +209,15 @@ __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__flo
 
 // ------------------------------------------------------------ FP64 panel
 
-// 1/sqrt(x) for x > 0 in FP64: a single-precision estimate refined by two
-// Newton-Raphson steps y <- y (3 - x y^2) / 2 (quadratic convergence:
-// ~2^-22 -> ~2^-44 -> full double precision), a shorter dependency chain
-// than a general double-precision reciprocal square root.
+// 1/sqrt(x) for x > 0 in FP64: the single-precision estimate (relative
+// error ~2^-22) refined by one Newton-Raphson step y <- y (3 - x y^2) / 2,
+// which squares the error to ~2^-43: far below the FP32 rounding of the
+// factor that leaves this kernel, with half the dependency chain of a
+// second step.
 __device__ __forceinline__ double rsqrt_nr(double x)
 {
-    double y = (double)rsqrtf((float)x);
-    y = y * (1.5 - 0.5 * x * y * y);
-    y = y * (1.5 - 0.5 * x * y * y);
-    return y;
+    const double y = (double)rsqrtf((float)x);
+    return y * (1.5 - 0.5 * x * y * y);
 }
 
 // Pivot block of 8 columns at (c0, c0) of the shared FP64 block, factored
@@ -290,25 +289,42 @@ __device__ __forceinline__ void solve_row8(const double* S, int c0, int i, const
     }
 }
 
+// FP64 tensor-core MMA (the only FP64 tensor instruction on sm_100a; the
+// tcgen05 kinds have no FP64): D = A B + C for an 8x8 tile, k = 4. Lane l
+// holds A[l/4][l%4], B[l%4][l/4] and C/D[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 static constexpr int POTRF_THREADS = 512;
-static constexpr int POTRF_SMEM = (PW * LDS + 8 * PW + PW) * 8;
+static constexpr int BKS = PW + 8;   // Bk row stride: the 4 rows of a fragment load fall in distinct banks
+static constexpr int POTRF_SMEM = (PW * LDS + 8 * BKS + PW) * 8;
 
 // FP64 factorisation of the 128x128 diagonal block (P, P) and its inverse,
 // right-looking over 16 blocks of 8 columns. In iteration k warp 0 runs the
 // critical path: the next 8 rows of block column k, the update of diagonal
-// block k+1 and its factorisation (one thread, in registers) and inverse.
-// Warps 1-15 meanwhile solve the other rows of block column k, form row
-// block k of W = L^-1, and apply the rank-8 update of block column k to the
-// trailing lower triangle (L) and to the partial sums of W (upper triangle,
-// transposed: S[j][i] accumulates -sum_m L[i][m] W[m][j] until row block
-// i/8 of W is formed). Bk[m][j] stages the update's right-hand operand:
-// W[c0+m][j] for j < c0+8, L[j][c0+m] for j >= c0+8.
+// block k+1 (two DMMAs) and its factorisation (one thread, in registers) and
+// inverse. The 12 worker warps meanwhile solve the other rows of block
+// column k, form row block k of W = L^-1, and apply the rank-8 update of
+// block column k to the trailing lower triangle (L) and to the partial sums
+// of W (upper triangle, transposed: S[j][i] accumulates -sum_m L[i][m]
+// W[m][j] until row block i/8 of W is formed) as 8x8 DMMA tiles, four at a
+// time, spread evenly over the workers. Warps 4, 8 and 12 share warp 0's
+// scheduler (warp w issues on sub-partition w mod 4) and take no FP64 work,
+// so nothing competes with the critical path for its issue slots and FP64
+// pipe. Bk[m][j] stages the update's right-hand operand: W[c0+m][j] for
+// j < c0+8, L[j][c0+m] for j >= c0+8.
+static constexpr int POTRF_WORKERS = POTRF_THREADS / 32 - POTRF_THREADS / 128;   // 12 warps
+
 __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict__ M, int npad, int P,
                                                             double* __restrict__ Wt, unsigned* __restrict__ status)
 {
-    extern __shared__ double S[];   // [PW][LDS], then Bk [8][PW], dinv [PW]
+    extern __shared__ double S[];   // [PW][LDS], then Bk [8][BKS], dinv [PW]
     double* Bk = S + PW * LDS;
-    double* dinv = Bk + 8 * PW;
+    double* dinv = Bk + 8 * BKS;
     __shared__ int bad;
     {
         // the warp roles and barrier counts assume this exact launch shape
@@ -320,6 +336,9 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         }
     }
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int fr = lane >> 2, fq = lane & 3;   // MMA fragment row / column-pair index
+    // worker warps: those off warp 0's sub-partition, numbered 0..11
+    const int wk = (warp & 3) ? warp - 1 - (warp >> 2) : -1;
     const size_t base = (size_t)P * PW;
     {
         // all loads of a thread first, then the stores (one L2 round trip)
@@ -363,21 +382,21 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
                         S[i * LDS + c0 + c] = l[c];
-                        Bk[c * PW + i] = l[c];
+                        Bk[c * BKS + i] = l[c];
                     }
                 }
                 __syncwarp();
                 asm volatile("bar.arrive 2, %0;" ::"r"(POTRF_THREADS) : "memory");
                 // diagonal block k+1 -= L[k+1][k] L[k+1][k]^T (lower triangle)
-                for (int e = lane; e < 36; e += 32) {
-                    int r = 0;
-                    while ((r + 1) * (r + 2) / 2 <= e) ++r;
-                    const int c = e - r * (r + 1) / 2;
-                    const int ri = c0 + 8 + r, ci = c0 + 8 + c;
-                    double acc = 0.0;
+                {
+                    const int d0 = c0 + 8;
+                    double* c = S + (d0 + fr) * LDS + d0 + 2 * fq;
+                    double e0 = c[0], e1 = c[1];
 #pragma unroll
-                    for (int m = 0; m < 8; ++m) acc += S[ri * LDS + c0 + m] * S[ci * LDS + c0 + m];
-                    S[ri * LDS + ci] -= acc;
+                    for (int h = 0; h < 2; ++h)
+                        dmma884(e0, e1, -Bk[(4 * h + fq) * BKS + d0 + fr], Bk[(4 * h + fq) * BKS + d0 + fr]);
+                    if (2 * fq <= fr) c[0] = e0;
+                    if (2 * fq + 1 <= fr) c[1] = e1;
                 }
                 __syncwarp();
                 if (lane == 0 && !pivot8(S, c0 + 8, dinv)) bad = 1;
@@ -385,72 +404,95 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                 inverse8(S, c0 + 8, dinv, lane);
             }
         } else {
-            const int bt = tid - 32;   // 0 .. POTRF_THREADS-33
-            if (bt < PW - c0 - 16) {
-                // rows c0+16.. of block column k
-                const int i = c0 + 16 + bt;
-                double l[8];
-                solve_row8(S, c0, i, dinv, l);
+            if (wk >= 0) {
+                const int bt = 32 * wk + lane;   // 0 .. 383
+                if (bt < PW - c0 - 16) {
+                    // rows c0+16.. of block column k
+                    const int i = c0 + 16 + bt;
+                    double l[8];
+                    solve_row8(S, c0, i, dinv, l);
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    S[i * LDS + c0 + c] = l[c];
-                    Bk[c * PW + i] = l[c];
+                    for (int c = 0; c < 8; ++c) {
+                        S[i * LDS + c0 + c] = l[c];
+                        Bk[c * BKS + i] = l[c];
+                    }
+                } else if (bt >= 128 && bt < 128 + c0) {
+                    // row block k of W: W[c0+m][j] = sum_{c <= m} W_kk[m][c] T[c0+c][j]
+                    const int j = bt - 128;
+                    double t[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) t[c] = S[j * LDS + c0 + c];
+#pragma unroll
+                    for (int m = 0; m < 8; ++m) {
+                        double v = t[m] * dinv[c0 + m];
+#pragma unroll
+                        for (int c = 0; c < m; ++c) v += S[(c0 + c) * LDS + c0 + m] * t[c];
+                        S[j * LDS + c0 + m] = v;
+                        Bk[m * BKS + j] = v;
+                    }
+                } else if (bt >= 256 && bt < 256 + 64) {
+                    // W_kk into the staging rows
+                    const int m = (bt - 256) >> 3, jj = (bt - 256) & 7;
+                    Bk[m * BKS + c0 + jj] = jj < m ? S[(c0 + jj) * LDS + c0 + m] : (jj == m ? dinv[c0 + m] : 0.0);
                 }
-            } else if (bt >= 128 && bt < 128 + c0) {
-                // row block k of W: W[c0+m][j] = sum_{c <= m} W_kk[m][c] T[c0+c][j]
-                const int j = bt - 128;
-                double t[8];
-#pragma unroll
-                for (int c = 0; c < 8; ++c) t[c] = S[j * LDS + c0 + c];
-#pragma unroll
-                for (int m = 0; m < 8; ++m) {
-                    double v = t[m] * dinv[c0 + m];
-#pragma unroll
-                    for (int c = 0; c < m; ++c) v += S[(c0 + c) * LDS + c0 + m] * t[c];
-                    S[j * LDS + c0 + m] = v;
-                    Bk[m * PW + j] = v;
-                }
-            } else if (bt >= 256 && bt < 256 + 64) {
-                // W_kk into the staging rows
-                const int m = (bt - 256) >> 3, jj = (bt - 256) & 7;
-                Bk[m * PW + c0 + jj] = jj < m ? S[(c0 + jj) * LDS + c0 + m] : (jj == m ? dinv[c0 + m] : 0.0);
             }
             if (!last) {
                 asm volatile("bar.sync 2, %0;" ::"r"(POTRF_THREADS) : "memory");
-                // rank-8 update of row group g (rows 8g..8g+7), columns j <= i:
-                // j < c0+8 -> partial sums of W (S[j][i]); j >= c0+8 -> L (S[i][j]);
-                // the diagonal block k+1 is warp 0's
-                const int g = k + warp;   // warps 1..15 -> g = k+1 ..
-                if (g < PW / 8) {
-                    const int i0 = 8 * g;
-                    const int jmax = g == k + 1 ? c0 + 8 : i0 + 8;
-                    double acc[8][4] = {};
+                if (wk >= 0) {
+                    // rank-8 update as 8x8 tiles (row group g, column tile
+                    // n): g = k+1 has the W tiles n <= k only (its diagonal
+                    // block is warp 0's), g > k+1 the tiles n <= g. Tile t of
+                    // this enumeration goes to worker t % 12; a worker takes
+                    // four tiles per pass, loads all their operands, then
+                    // runs the eight DMMAs, then stores.
+                    // n <= k -> partial sums of W (S[j][i]); else L (S[i][j]).
+                    int g = k + 1, n = wk, width = k + 1;
+                    for (;;) {
+                        int tg[4], tn[4];
+                        bool tv[4];
 #pragma unroll
-                    for (int m = 0; m < 8; ++m) {
-                        double b[4];
-#pragma unroll
-                        for (int p = 0; p < 4; ++p) {
-                            const int j = lane + 32 * p;
-                            b[p] = j < jmax ? Bk[m * PW + j] : 0.0;
+                        for (int u = 0; u < 4; ++u) {
+                            while (g < PW / 8 && n >= width) {
+                                n -= width;
+                                ++g;
+                                width = g + 1;
+                            }
+                            tv[u] = g < PW / 8;
+                            tg[u] = tv[u] ? g : k + 1;   // a valid tile to read for an empty slot
+                            tn[u] = tv[u] ? n : 0;
+                            n += POTRF_WORKERS;
                         }
+                        if (!tv[0]) break;
+                        double av[4][2], bv[4][2], e0[4], e1[4];
+                        double* cp[4];
+                        int cs[4];
 #pragma unroll
-                        for (int r = 0; r < 8; ++r) {
-                            const double a = Bk[m * PW + i0 + r];
+                        for (int u = 0; u < 4; ++u) {
+                            const int i = 8 * tg[u] + fr, j = 8 * tn[u] + 2 * fq;
+                            const bool wpart = tn[u] <= k;
+                            cp[u] = wpart ? S + j * LDS + i : S + i * LDS + j;
+                            cs[u] = wpart ? LDS : 1;
+                            e0[u] = cp[u][0];
+                            e1[u] = cp[u][cs[u]];
 #pragma unroll
-                            for (int p = 0; p < 4; ++p) acc[r][p] += a * b[p];
-                        }
-                    }
-#pragma unroll
-                    for (int r = 0; r < 8; ++r) {
-                        const int i = i0 + r;
-#pragma unroll
-                        for (int p = 0; p < 4; ++p) {
-                            const int j = lane + 32 * p;
-                            if (j < jmax && j <= i) {
-                                if (j < c0 + 8) S[j * LDS + i] -= acc[r][p];
-                                else S[i * LDS + j] -= acc[r][p];
+                            for (int h = 0; h < 2; ++h) {
+                                av[u][h] = -Bk[(4 * h + fq) * BKS + 8 * tg[u] + fr];
+                                bv[u][h] = Bk[(4 * h + fq) * BKS + 8 * tn[u] + fr];
                             }
                         }
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) dmma884(e0[u], e1[u], av[u][h], bv[u][h]);
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            if (!tv[u]) continue;
+                            const int i = 8 * tg[u] + fr, j = 8 * tn[u] + 2 * fq;
+                            const bool full = tn[u] < tg[u];   // W tiles and L tiles left of the diagonal
+                            if (full || j <= i) cp[u][0] = e0[u];
+                            if (full || j + 1 <= i) cp[u][cs[u]] = e1[u];
+                        }
+                        if (!tv[3]) break;
                     }
                 }
             }
@@ -458,96 +500,114 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         __syncthreads();
     }
     if (tid == 0 && bad) atomicOr(status, ST_NOT_SPD);
-    // L_PP to M (FP32, lower triangle); Wt[m][c] = W[c][m] (upper triangular,
-    // row-major), the layout the panel solve X = A W^T reads
+    // L_PP to M (FP32, lower triangle)
     for (int idx = tid; idx < PW * PW; idx += blockDim.x) {
         const int r = idx / PW, c = idx % PW;
         if (c <= r) M[(base + r) * npad + base + c] = (float)S[r * LDS + c];
-        Wt[idx] = r < c ? S[r * LDS + c] : (r == c ? dinv[c] : 0.0);
+    }
+    // W^T (upper triangular: W^T[m][c] = W[c][m], nonzero for m <= c) in the
+    // order the panel solve's DMMA B fragments read it: entry
+    // ((s * 16 + n) * 32 + l) = W^T[4s + l%4][8n + l/4] (k-step s, column
+    // tile n, lane l). W[c][m] for m < c sits in S[m][c].
+    for (int f = tid; f < PW * PW; f += blockDim.x) {
+        const int l = f & 31, n = (f >> 5) & 15, st = f >> 9;
+        const int m = 4 * st + (l & 3), c = 8 * n + (l >> 2);
+        Wt[f] = m < c ? S[m * LDS + c] : (m == c ? dinv[c] : 0.0);
     }
 }
 
 // Rows below block P: X L_PP^T = A, i.e. X = A W^T with W = L_PP^-1 from
-// k_potrf128, for a slab of 64 rows per CTA in FP64. Wt = W^T is upper
-// triangular, so X[r][c] = sum_{m <= c} A[r][m] Wt[m][c]: a product with no
-// sequential dependency. Warp w owns rows 8w..8w+7, lane l the columns
-// l + 32p (p = 0..3); column group p only needs m < 32(p+1). Writes the
-// rows to M and their TF32 split to the panel buffers.
-static constexpr int TRSM_ROWS = 64;
-static constexpr int TRSM_LDX = PW + 1;
-static constexpr int TRSM_SMEM = (PW * PW + TRSM_ROWS * TRSM_LDX) * 8;
+// k_potrf128, in FP64 on the DMMA path. Work unit = one row group of 8 rows,
+// owned by one warp: 16 accumulator tiles of 8x8 (the whole 8x128 row
+// block, 32 doubles per lane) over 32 k-steps of 4; W^T is upper
+// triangular, so column tile n only takes k-steps s <= 2n+1 (272 DMMAs per
+// unit instead of 512). The CTA copies W^T once (128 KB, already in
+// fragment order) into shared memory; each warp stages its unit's 8 FP32
+// rows (row stride 132 floats: the A-fragment reads hit 32 distinct banks).
+// The grid is persistent: unit u goes to warp slot u mod (8 grid), slots
+// ordered so that the first 4 grid slots put one warp on every SM
+// sub-partition, the next 4 grid a second one. Writes the rows to M and
+// their TF32 split L = L_hi + L_lo (L_hi: low 13 mantissa bits cleared,
+// exactly TF32; L_lo = L - L_hi) to the panel buffers.
+static constexpr int TRSM_THREADS = 256;
+static constexpr int TRSM_LDA = PW + 4;
+static constexpr int TRSM_SMEM = PW * PW * 8 + (TRSM_THREADS / 32) * 8 * TRSM_LDA * 4;
 
-__global__ void __launch_bounds__(256) k_trsm128(float* __restrict__ M, int npad, int P, const double* __restrict__ Wt,
-                                                 float* __restrict__ Lhi, float* __restrict__ Llo)
+__global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__ M, int npad, int P,
+                                                          const double* __restrict__ Wf, float* __restrict__ Lhi,
+                                                          float* __restrict__ Llo, unsigned* __restrict__ status)
 {
-    extern __shared__ double sh[];
-    double* sW = sh;                              // [PW][PW], Wt
-    double* A = sh + PW * PW;                     // [TRSM_ROWS][TRSM_LDX]
-    const int tid = threadIdx.x;
-    const size_t base = (size_t)P * PW;
-    const size_t row0 = base + PW + (size_t)blockIdx.x * TRSM_ROWS;
-    const int nrow = (int)min((size_t)TRSM_ROWS, (size_t)npad - row0);
-    // staging: all of a thread's loads are issued before its stores, so the
-    // L2 latency is paid once, not once per element
     {
-        constexpr int NW = PW * PW / 2 / 256, NA = TRSM_ROWS * PW / 4 / 256;   // 32, 8 per thread
-        const double2* src = reinterpret_cast<const double2*>(Wt);
-        double2 w[NW];
-#pragma unroll
-        for (int k = 0; k < NW; ++k) w[k] = __ldg(src + tid + 256 * k);
-        float4 v[NA];
-#pragma unroll
-        for (int k = 0; k < NA; ++k) {
-            const int idx = tid + 256 * k;
-            const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
-            v[k] = r < nrow ? *reinterpret_cast<const float4*>(M + (row0 + r) * npad + base + c)
-                            : make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (blockDim.x != TRSM_THREADS || dyn < (uint32_t)TRSM_SMEM) {
+            if (threadIdx.x == 0) atomicOr(status, ST_LAUNCH);
+            return;
         }
+    }
+    extern __shared__ double sh[];
+    double* Bs = sh;                                          // [32 k-steps][16 tiles][32 lanes]
+    float* As = reinterpret_cast<float*>(sh + PW * PW);      // per warp [8][TRSM_LDA]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int fr = lane >> 2, fq = lane & 3;
+    const size_t base = (size_t)P * PW;
+    const size_t row0 = base + PW;
+    const int units = (int)(((size_t)npad - row0) / 8);
+    {
+        // W^T fragments: a plain 128 KB copy, loads batched ahead of stores
+        const double2* src = reinterpret_cast<const double2*>(Wf);
+        double2* dst = reinterpret_cast<double2*>(Bs);
+        constexpr int NW = PW * PW / 2 / TRSM_THREADS;   // 32 per thread
 #pragma unroll
-        for (int k = 0; k < NW; ++k) reinterpret_cast<double2*>(sW)[tid + 256 * k] = w[k];
+        for (int h = 0; h < 2; ++h) {
+            double2 w[NW / 2];
 #pragma unroll
-        for (int k = 0; k < NA; ++k) {
-            const int idx = tid + 256 * k;
-            const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
-            double* a = A + r * TRSM_LDX + c;
-            a[0] = v[k].x;
-            a[1] = v[k].y;
-            a[2] = v[k].z;
-            a[3] = v[k].w;
+            for (int k = 0; k < NW / 2; ++k) w[k] = __ldg(src + tid + TRSM_THREADS * (k + h * NW / 2));
+#pragma unroll
+            for (int k = 0; k < NW / 2; ++k) dst[tid + TRSM_THREADS * (k + h * NW / 2)] = w[k];
         }
     }
     __syncthreads();
-    const int warp = tid >> 5, lane = tid & 31;
-    const int rbase = 8 * warp;
-    double acc[8][4] = {};
+    float* Aw = As + warp * 8 * TRSM_LDA;
+    const int slot = (warp >> 2) * 4 * gridDim.x + blockIdx.x * 4 + (warp & 3);
+    for (int u = slot; u < units; u += TRSM_THREADS / 32 * gridDim.x) {
+        const size_t r0 = row0 + (size_t)8 * u;
+        {
+            // the unit's 8 rows x 128 FP32 columns: 8 float4 per lane
+            float4 v[8];
 #pragma unroll
-    for (int g = 0; g < 4; ++g) {          // m in [32g, 32g + 32): column groups p >= g
-        for (int mm = 0; mm < 32; ++mm) {
-            const int m = 32 * g + mm;
-            double y[4];
-#pragma unroll
-            for (int p = 0; p < 4; ++p) y[p] = p >= g ? sW[m * PW + lane + 32 * p] : 0.0;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const double x = A[(rbase + q) * TRSM_LDX + m];
-#pragma unroll
-                for (int p = 0; p < 4; ++p)
-                    if (p >= g) acc[q][p] += x * y[p];
+            for (int k = 0; k < 8; ++k) {
+                const int idx = lane + 32 * k;   // row idx/32, float4 column idx%32
+                v[k] = *reinterpret_cast<const float4*>(M + (r0 + (idx >> 5)) * npad + base + 4 * (idx & 31));
             }
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int idx = lane + 32 * k;
+                *reinterpret_cast<float4*>(Aw + (idx >> 5) * TRSM_LDA + 4 * (idx & 31)) = v[k];
+            }
+            __syncwarp();
         }
-    }
+        double acc[16][2];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int r = rbase + q;
-        if (r >= nrow) break;
+        for (int n = 0; n < 16; ++n) acc[n][0] = acc[n][1] = 0.0;
+#pragma unroll 2
+        for (int st = 0; st < 32; ++st) {
+            const double a = (double)Aw[fr * TRSM_LDA + 4 * st + fq];
+            const double* b = Bs + st * 16 * 32 + lane;
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            const int c = lane + 32 * p;
-            const float o = (float)acc[q][p];
-            const float h = tf32_hi(o);
-            M[(row0 + r) * npad + base + c] = o;
-            Lhi[(row0 + r) * PW + c] = h;
-            Llo[(row0 + r) * PW + c] = o - h;
+            for (int n = 0; n < 16; ++n)
+                if (2 * n + 1 >= st) dmma884(acc[n][0], acc[n][1], a, b[n * 32]);
+        }
+        const size_t row = r0 + fr;
+#pragma unroll
+        for (int n = 0; n < 16; ++n) {
+            const int c = 8 * n + 2 * fq;
+            const float o0 = (float)acc[n][0], o1 = (float)acc[n][1];
+            const float h0 = tf32_hi(o0), h1 = tf32_hi(o1);
+            *reinterpret_cast<float2*>(M + row * npad + base + c) = make_float2(o0, o1);
+            *reinterpret_cast<float2*>(Lhi + row * PW + c) = make_float2(h0, h1);
+            *reinterpret_cast<float2*>(Llo + row * PW + c) = make_float2(o0 - h0, o1 - h1);
         }
     }
 }
@@ -830,8 +890,10 @@ int factor_mixed_tc(bdb_system* s)
     for (int P = 0; P + 1 < nt; ++P) {
         const int par = P & 1;
         panel_ptrs(s, par, &hi, &lo, &lkk);
-        const int rows_below = s->npad - (P + 1) * PW;
-        k_trsm128<<<(rows_below + TRSM_ROWS - 1) / TRSM_ROWS, 256, TRSM_SMEM, st>>>(s->M32.p, s->npad, P, lkk, hi, lo);
+        const int units = (s->npad - (P + 1) * PW) / 8;
+        const int per_cta = TRSM_THREADS / 32;
+        k_trsm128<<<std::min(s->sm_count, (units + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st>>>(
+            s->M32.p, s->npad, P, lkk, hi, lo, s->status.p);
         const int rem = nt - P - 1;
         // block column P+1 of the trailing matrix
         k_syrk_tc<<<std::min(s->sm_count, rem), 192, SYRK_SMEM, st>>>(maps[2 * par], maps[2 * par + 1], maps[4], P + 1,
