@@ -220,75 +220,6 @@ __device__ __forceinline__ double rsqrt_nr(double x)
     return y * (1.5 - 0.5 * x * y * y);
 }
 
-// Pivot block of 8 columns at (c0, c0) of the shared FP64 block, factored
-// by one thread in registers; also leaves 1/L_jj in dinv[c0..c0+7].
-__device__ __forceinline__ bool pivot8(double* S, int c0, double* dinv)
-{
-    double a[8][8];
-    bool ok = true;
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-        for (int c = 0; c <= r; ++c) a[r][c] = S[(c0 + r) * LDS + c0 + c];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const double piv = a[j][j];
-        if (!(piv > 0.0)) ok = false;
-        const double inv = rsqrt_nr(piv);
-        a[j][j] = piv * inv;
-        dinv[c0 + j] = inv;
-#pragma unroll
-        for (int r = j + 1; r < 8; ++r) a[r][j] *= inv;
-#pragma unroll
-        for (int r = j + 1; r < 8; ++r)
-#pragma unroll
-            for (int c = j + 1; c <= r; ++c) a[r][c] -= a[r][j] * a[c][j];
-    }
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-        for (int c = 0; c <= r; ++c) S[(c0 + r) * LDS + c0 + c] = a[r][c];
-    return ok;
-}
-
-// W_kk = L_kk^-1 for the 8x8 diagonal block at c0 (lanes 0-7, one column
-// each, forward substitution); stored transposed in the strict upper
-// triangle of the block (S[c0+c][c0+i] = W[i][c], c < i), diagonal in dinv.
-__device__ __forceinline__ void inverse8(double* S, int c0, const double* dinv, int lane)
-{
-    if (lane < 8) {
-        const int c = lane;
-        double w[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            double v = i == c ? 1.0 : 0.0;
-#pragma unroll
-            for (int m = 0; m < i; ++m) v -= S[(c0 + i) * LDS + c0 + m] * w[m];
-            w[i] = i >= c ? v * dinv[c0 + i] : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-            if (i > c) S[(c0 + c) * LDS + c0 + i] = w[i];
-    }
-}
-
-// Row i of block column c0 below the diagonal: L[i][c0+c] = sum_{m <= c}
-// A[i][c0+m] W_kk[c][m] (X L_kk^T = A solved with the inverse). Warp 0 and
-// the bulk warps both call this, so a row gets the same bits from either.
-__device__ __forceinline__ void solve_row8(const double* S, int c0, int i, const double* dinv, double* l)
-{
-    double a[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) a[c] = S[i * LDS + c0 + c];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        double v = a[c] * dinv[c0 + c];
-#pragma unroll
-        for (int m = 0; m < c; ++m) v += a[m] * S[(c0 + m) * LDS + c0 + c];
-        l[c] = v;
-    }
-}
-
 // FP64 tensor-core MMA (the only FP64 tensor instruction on sm_100a; the
 // tcgen05 kinds have no FP64): D = A B + C for an 8x8 tile, k = 4. Lane l
 // holds A[l/4][l%4], B[l%4][l/4] and C/D[l/4][2(l%4) + {0,1}].
@@ -299,32 +230,100 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
                  : "d"(a), "d"(b));
 }
 
+// 8x8 FP64 tiles in shared memory are kept in MMA fragment order, two
+// k-steps per lane (one 16-byte load per operand and tile):
+//   A order: entry 2 l + h = T[l/4][4h + l%4]   (A fragments of T, and also
+//            the B fragments of T^T)
+//   B order: entry 2 l + h = T[4h + l%4][l/4]   (B fragments of T)
+__device__ __forceinline__ int apos(int r, int c) { return ((r << 2) + (c & 3)) * 2 + (c >> 2); }
+__device__ __forceinline__ int bpos(int r, int c) { return ((c << 2) + (r & 3)) * 2 + (r >> 2); }
+// tile (g, n), n <= g, of the lower triangle of 16 x 16 tiles
+__device__ __forceinline__ int tix(int g, int n) { return g * (g + 1) / 2 + n; }
+
+// 1/x for x > 0 in FP64: the single-precision hardware estimate refined by
+// one Newton-Raphson step q <- q + q (1 - x q) (error ~2^-46).
+__device__ __forceinline__ double rcp_nr(double x)
+{
+    float e;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"((float)x));
+    const double q = (double)e;
+    return fma(q, fma(-x, q, 1.0), q);
+}
+
+// Factor the 8x8 block in Dg ([8][9], lower triangle) in registers by one
+// thread: L_kk to the lower triangle of Dg, 1/L_jj to rd. The elimination
+// runs on the unscaled Schur complements, a_ik -= (a_ij a_kj) q_j with
+// q_j = 1/a_jj, so the dependency chain from one pivot to the next is one
+// reciprocal and one FMA (the products a_ij a_kj are formed while q_j is
+// computed); the columns are scaled by 1/sqrt(a_jj) at the end.
+__device__ __forceinline__ bool pivot8(double* Dg, double* rd)
+{
+    double a[8][8];
+    bool ok = true;
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c <= r; ++c) a[r][c] = Dg[r * 9 + c];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (!(a[j][j] > 0.0)) ok = false;
+        const double q = rcp_nr(a[j][j]);
+#pragma unroll
+        for (int r = j + 1; r < 8; ++r)
+#pragma unroll
+            for (int c = j + 1; c <= r; ++c) a[r][c] = fma(-(a[r][j] * a[c][j]), q, a[r][c]);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const double r = rsqrt_nr(a[j][j]);
+        rd[j] = r;
+        Dg[j * 9 + j] = a[j][j] * r;
+#pragma unroll
+        for (int i = j + 1; i < 8; ++i) Dg[i * 9 + j] = a[i][j] * r;
+    }
+    return ok;
+}
+
 static constexpr int POTRF_THREADS = 512;
-static constexpr int BKS = PW + 8;   // Bk row stride: the 4 rows of a fragment load fall in distinct banks
-static constexpr int POTRF_SMEM = (PW * LDS + 8 * BKS + PW) * 8;
+static constexpr int NT = PW / 8;                  // 16 row groups of 8 rows
+static constexpr int NTILE = NT * (NT + 1) / 2;    // 136 tiles in the lower triangle
+static constexpr int POTRF_SMEM = (2 * NTILE * 64 + NT * 64 + 80 + 8) * 8;
 
-// FP64 factorisation of the 128x128 diagonal block (P, P) and its inverse,
-// right-looking over 16 blocks of 8 columns. In iteration k warp 0 runs the
-// critical path: the next 8 rows of block column k, the update of diagonal
-// block k+1 (two DMMAs) and its factorisation (one thread, in registers) and
-// inverse. The 12 worker warps meanwhile solve the other rows of block
-// column k, form row block k of W = L^-1, and apply the rank-8 update of
-// block column k to the trailing lower triangle (L) and to the partial sums
-// of W (upper triangle, transposed: S[j][i] accumulates -sum_m L[i][m]
-// W[m][j] until row block i/8 of W is formed) as 8x8 DMMA tiles, four at a
-// time, spread evenly over the workers. Warps 4, 8 and 12 share warp 0's
-// scheduler (warp w issues on sub-partition w mod 4) and take no FP64 work,
-// so nothing competes with the critical path for its issue slots and FP64
-// pipe. Bk[m][j] stages the update's right-hand operand: W[c0+m][j] for
-// j < c0+8, L[j][c0+m] for j >= c0+8.
-static constexpr int POTRF_WORKERS = POTRF_THREADS / 32 - POTRF_THREADS / 128;   // 12 warps
+// row group owned by a warp: warp 0 runs the pivots; warps 4, 8, 12 share
+// its scheduler (warp w issues on sub-partition w mod 4) and own the row
+// groups with the least update work (1, 2, 3); the other 12 warps own 4..15
+__device__ __forceinline__ int row_group_of(int warp)
+{
+    return (warp & 3) ? 4 + warp - 1 - (warp >> 2) : warp >> 2;
+}
 
+// FP64 factorisation L_PP of the 128x128 diagonal block (P, P) and its
+// inverse W = L_PP^-1, right-looking over 16 blocks of 8 columns with the
+// trailing matrix held in registers: the warp owning row group g keeps its
+// tiles (g, n), n <= g, as DMMA accumulators. Iteration k:
+//   warp 0      factors diagonal tile (k, k) (pivot8) and inverts it
+//               (lanes 0-7), publishing W_kk, L_kk in shared memory;
+//   barrier;
+//   owners g>k  solve tile (g, k): L[g][k] = C[g][k] W_kk^T (two DMMAs),
+//               published in A order;
+//   barrier;
+//   owners g>k  update their tiles n = k+1..g: C[g][n] -= L[g][k] L[n][k]^T.
+//               The owner of row group k+1 updates its diagonal tile first
+//               and hands it to warp 0 (named barrier 1), so the next pivot
+//               overlaps the rest of the update.
+// Then each warp h+1 forms block column h of W by forward substitution,
+// W[g][h] = -W_gg sum_{m=h}^{g-1} L[g][m] W[m][h], with W tiles in B order.
+// Finally L_PP goes to M (FP32) and W^T to Wt in the fragment order the
+// panel solve reads: entry ((s * 16 + n) * 32 + l) = W^T[4s + l%4][8n + l/4].
 __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict__ M, int npad, int P,
                                                             double* __restrict__ Wt, unsigned* __restrict__ status)
 {
-    extern __shared__ double S[];   // [PW][LDS], then Bk [8][BKS], dinv [PW]
-    double* Bk = S + PW * LDS;
-    double* dinv = Bk + 8 * BKS;
+    extern __shared__ double sh[];
+    double* Lt = sh;                       // [NTILE][64] A order
+    double* Wtl = Lt + NTILE * 64;         // [NTILE][64] B order
+    double* Wa = Wtl + NTILE * 64;         // [NT][64] W_kk in A order
+    double* Dg = Wa + NT * 64;             // [8][9] diagonal block being factored
+    double* rd = Dg + 80;                  // [8] 1/L_jj of that block
     __shared__ int bad;
     {
         // the warp roles and barrier counts assume this exact launch shape
@@ -336,183 +335,151 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         }
     }
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int fr = lane >> 2, fq = lane & 3;   // MMA fragment row / column-pair index
-    // worker warps: those off warp 0's sub-partition, numbered 0..11
-    const int wk = (warp & 3) ? warp - 1 - (warp >> 2) : -1;
+    const int fr = lane >> 2, fq = lane & 3;
     const size_t base = (size_t)P * PW;
-    {
-        // all loads of a thread first, then the stores (one L2 round trip)
-        constexpr int NV = PW * PW / 4 / POTRF_THREADS;   // 8
-        float4 v[NV];
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            const int idx = tid + POTRF_THREADS * k;
-            const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
-            v[k] = *reinterpret_cast<const float4*>(M + (base + r) * npad + base + c);
-        }
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            const int idx = tid + POTRF_THREADS * k;
-            const int r = idx / (PW / 4), c = 4 * (idx % (PW / 4));
-            double* s = S + r * LDS + c;
-            s[0] = c <= r ? (double)v[k].x : 0.0;
-            s[1] = c + 1 <= r ? (double)v[k].y : 0.0;
-            s[2] = c + 2 <= r ? (double)v[k].z : 0.0;
-            s[3] = c + 3 <= r ? (double)v[k].w : 0.0;
-        }
-    }
+    const int g = row_group_of(warp);
     if (tid == 0) bad = 0;
-    __syncthreads();
     if (warp == 0) {
-        if (lane == 0 && !pivot8(S, 0, dinv)) bad = 1;
-        __syncwarp();
-        inverse8(S, 0, dinv, lane);
-    }
-    __syncthreads();
-    for (int k = 0; k < PW / 8; ++k) {
-        const int c0 = 8 * k;
-        const bool last = k == PW / 8 - 1;
-        if (warp == 0) {
-            if (!last) {
-                // rows c0+8..c0+15 of block column k
-                if (lane < 8) {
-                    const int i = c0 + 8 + lane;
-                    double l[8];
-                    solve_row8(S, c0, i, dinv, l);
+        // ---------------------------------------------------- pivot warp
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        S[i * LDS + c0 + c] = l[c];
-                        Bk[c * BKS + i] = l[c];
-                    }
+        for (int e = 0; e < 2; ++e) {
+            const int c = 2 * fq + e;
+            Dg[fr * 9 + c] = c <= fr ? (double)M[(base + fr) * npad + base + c] : 0.0;
+        }
+        for (int k = 0; k < NT; ++k) {
+            if (k > 0) asm volatile("bar.sync 1, 64;" ::: "memory");   // diagonal tile k from its owner
+            __syncwarp();
+            if (lane == 0 && !pivot8(Dg, rd)) bad = 1;
+            __syncwarp();
+            if (lane < 8) {
+                // column c of W_kk by forward substitution; W_kk and L_kk out
+                const int c = lane;
+                double w[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    double v = i == c ? 1.0 : 0.0;
+#pragma unroll
+                    for (int m = 0; m < i; ++m)
+                        if (m >= c) v -= Dg[i * 9 + m] * w[m];
+                    w[i] = i >= c ? v * rd[i] : 0.0;
                 }
-                __syncwarp();
-                asm volatile("bar.arrive 2, %0;" ::"r"(POTRF_THREADS) : "memory");
-                // diagonal block k+1 -= L[k+1][k] L[k+1][k]^T (lower triangle)
-                {
-                    const int d0 = c0 + 8;
-                    double* c = S + (d0 + fr) * LDS + d0 + 2 * fq;
-                    double e0 = c[0], e1 = c[1];
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
-                        dmma884(e0, e1, -Bk[(4 * h + fq) * BKS + d0 + fr], Bk[(4 * h + fq) * BKS + d0 + fr]);
-                    if (2 * fq <= fr) c[0] = e0;
-                    if (2 * fq + 1 <= fr) c[1] = e1;
-                }
-                __syncwarp();
-                if (lane == 0 && !pivot8(S, c0 + 8, dinv)) bad = 1;
-                __syncwarp();
-                inverse8(S, c0 + 8, dinv, lane);
-            }
-        } else {
-            if (wk >= 0) {
-                const int bt = 32 * wk + lane;   // 0 .. 383
-                if (bt < PW - c0 - 16) {
-                    // rows c0+16.. of block column k
-                    const int i = c0 + 16 + bt;
-                    double l[8];
-                    solve_row8(S, c0, i, dinv, l);
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        S[i * LDS + c0 + c] = l[c];
-                        Bk[c * BKS + i] = l[c];
-                    }
-                } else if (bt >= 128 && bt < 128 + c0) {
-                    // row block k of W: W[c0+m][j] = sum_{c <= m} W_kk[m][c] T[c0+c][j]
-                    const int j = bt - 128;
-                    double t[8];
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) t[c] = S[j * LDS + c0 + c];
-#pragma unroll
-                    for (int m = 0; m < 8; ++m) {
-                        double v = t[m] * dinv[c0 + m];
-#pragma unroll
-                        for (int c = 0; c < m; ++c) v += S[(c0 + c) * LDS + c0 + m] * t[c];
-                        S[j * LDS + c0 + m] = v;
-                        Bk[m * BKS + j] = v;
-                    }
-                } else if (bt >= 256 && bt < 256 + 64) {
-                    // W_kk into the staging rows
-                    const int m = (bt - 256) >> 3, jj = (bt - 256) & 7;
-                    Bk[m * BKS + c0 + jj] = jj < m ? S[(c0 + jj) * LDS + c0 + m] : (jj == m ? dinv[c0 + m] : 0.0);
+                for (int i = 0; i < 8; ++i) {
+                    Wa[k * 64 + apos(i, c)] = w[i];
+                    Wtl[tix(k, k) * 64 + bpos(i, c)] = w[i];
+                    Lt[tix(k, k) * 64 + apos(i, c)] = i >= c ? Dg[i * 9 + c] : 0.0;
                 }
             }
-            if (!last) {
-                asm volatile("bar.sync 2, %0;" ::"r"(POTRF_THREADS) : "memory");
-                if (wk >= 0) {
-                    // rank-8 update as 8x8 tiles (row group g, column tile
-                    // n): g = k+1 has the W tiles n <= k only (its diagonal
-                    // block is warp 0's), g > k+1 the tiles n <= g. Tile t of
-                    // this enumeration goes to worker t % 12; a worker takes
-                    // four tiles per pass, loads all their operands, then
-                    // runs the eight DMMAs, then stores.
-                    // n <= k -> partial sums of W (S[j][i]); else L (S[i][j]).
-                    int g = k + 1, n = wk, width = k + 1;
-                    for (;;) {
-                        int tg[4], tn[4];
-                        bool tv[4];
+            __syncthreads();   // A: W_kk published
+            __syncthreads();   // B: block column k solved
+        }
+    } else {
+        // -------------------------------------------------- tile owners
+        double cacc[NT][2];
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            while (g < PW / 8 && n >= width) {
-                                n -= width;
-                                ++g;
-                                width = g + 1;
-                            }
-                            tv[u] = g < PW / 8;
-                            tg[u] = tv[u] ? g : k + 1;   // a valid tile to read for an empty slot
-                            tn[u] = tv[u] ? n : 0;
-                            n += POTRF_WORKERS;
-                        }
-                        if (!tv[0]) break;
-                        double av[4][2], bv[4][2], e0[4], e1[4];
-                        double* cp[4];
-                        int cs[4];
+        for (int n = 0; n < NT; ++n) {
+            cacc[n][0] = cacc[n][1] = 0.0;
+            if (n <= g) {
+                const float2 v =
+                    *reinterpret_cast<const float2*>(M + (base + 8 * g + fr) * npad + base + 8 * n + 2 * fq);
+                cacc[n][0] = (n < g || 2 * fq <= fr) ? (double)v.x : 0.0;
+                cacc[n][1] = (n < g || 2 * fq + 1 <= fr) ? (double)v.y : 0.0;
+            }
+        }
+        for (int k = 0; k < NT; ++k) {
+            __syncthreads();   // A
+            if (g > k) {
+                // A fragments of C[g][k] (C layout -> A layout by shuffles)
+                double c0 = 0.0, c1 = 0.0;
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int i = 8 * tg[u] + fr, j = 8 * tn[u] + 2 * fq;
-                            const bool wpart = tn[u] <= k;
-                            cp[u] = wpart ? S + j * LDS + i : S + i * LDS + j;
-                            cs[u] = wpart ? LDS : 1;
-                            e0[u] = cp[u][0];
-                            e1[u] = cp[u][cs[u]];
-#pragma unroll
-                            for (int h = 0; h < 2; ++h) {
-                                av[u][h] = -Bk[(4 * h + fq) * BKS + 8 * tg[u] + fr];
-                                bv[u][h] = Bk[(4 * h + fq) * BKS + 8 * tn[u] + fr];
-                            }
-                        }
-#pragma unroll
-                        for (int h = 0; h < 2; ++h)
-#pragma unroll
-                            for (int u = 0; u < 4; ++u) dmma884(e0[u], e1[u], av[u][h], bv[u][h]);
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            if (!tv[u]) continue;
-                            const int i = 8 * tg[u] + fr, j = 8 * tn[u] + 2 * fq;
-                            const bool full = tn[u] < tg[u];   // W tiles and L tiles left of the diagonal
-                            if (full || j <= i) cp[u][0] = e0[u];
-                            if (full || j + 1 <= i) cp[u][cs[u]] = e1[u];
-                        }
-                        if (!tv[3]) break;
+                for (int t = 0; t < NT; ++t)
+                    if (t == k) {
+                        c0 = cacc[t][0];
+                        c1 = cacc[t][1];
                     }
+                double x0 = 0.0, x1 = 0.0;
+                const double2 wb = *reinterpret_cast<const double2*>(Wa + k * 64 + 2 * lane);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int src = (fr << 2) + 2 * h + (fq >> 1);
+                    const double v0 = __shfl_sync(0xffffffffu, c0, src);
+                    const double v1 = __shfl_sync(0xffffffffu, c1, src);
+                    dmma884(x0, x1, (fq & 1) ? v1 : v0, h ? wb.y : wb.x);
+                }
+                Lt[tix(g, k) * 64 + apos(fr, 2 * fq)] = x0;
+                Lt[tix(g, k) * 64 + apos(fr, 2 * fq + 1)] = x1;
+            }
+            __syncthreads();   // B
+            if (g > k) {
+                const double2 av = *reinterpret_cast<const double2*>(Lt + tix(g, k) * 64 + 2 * lane);
+#pragma unroll
+                for (int n = 1; n < NT; ++n) {
+                    if (n > k && n <= g) {
+                        const double2 bv = *reinterpret_cast<const double2*>(Lt + tix(n, k) * 64 + 2 * lane);
+                        dmma884(cacc[n][0], cacc[n][1], -av.x, bv.x);
+                        dmma884(cacc[n][0], cacc[n][1], -av.y, bv.y);
+                    }
+                }
+                if (g == k + 1) {
+                    // hand the finished diagonal tile to the pivot warp
+                    double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+                    for (int t = 0; t < NT; ++t)
+                        if (t == g) {
+                            d0 = cacc[t][0];
+                            d1 = cacc[t][1];
+                        }
+                    Dg[fr * 9 + 2 * fq] = d0;
+                    Dg[fr * 9 + 2 * fq + 1] = d1;
+                    __syncwarp();
+                    asm volatile("bar.arrive 1, 64;" ::: "memory");
                 }
             }
         }
-        __syncthreads();
     }
+    __syncthreads();
+    if (warp > 0) {
+        // block column h of W (warp h+1), tiles in B order
+        const int h = warp - 1;
+        for (int gg = h + 1; gg < NT; ++gg) {
+            double p0 = 0.0, p1 = 0.0, q0 = 0.0, q1 = 0.0;
+            for (int m = h; m < gg; ++m) {
+                const double2 a = *reinterpret_cast<const double2*>(Lt + tix(gg, m) * 64 + 2 * lane);
+                const double2 b = *reinterpret_cast<const double2*>(Wtl + tix(m, h) * 64 + 2 * lane);
+                dmma884(p0, p1, a.x, b.x);
+                dmma884(q0, q1, a.y, b.y);
+            }
+            p0 += q0;
+            p1 += q1;
+            // W[gg][h] = -W_gg (p): A = W_gg, B fragments of p by shuffles
+            const double2 wa = *reinterpret_cast<const double2*>(Wa + gg * 64 + 2 * lane);
+            double z0 = 0.0, z1 = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {
+                const int src = ((4 * kk + fq) << 2) + (fr >> 1);
+                const double v0 = __shfl_sync(0xffffffffu, p0, src);
+                const double v1 = __shfl_sync(0xffffffffu, p1, src);
+                dmma884(z0, z1, kk ? wa.y : wa.x, (fr & 1) ? v1 : v0);
+            }
+            Wtl[tix(gg, h) * 64 + bpos(fr, 2 * fq)] = -z0;
+            Wtl[tix(gg, h) * 64 + bpos(fr, 2 * fq + 1)] = -z1;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
     if (tid == 0 && bad) atomicOr(status, ST_NOT_SPD);
     // L_PP to M (FP32, lower triangle)
-    for (int idx = tid; idx < PW * PW; idx += blockDim.x) {
+#pragma unroll 4
+    for (int idx = tid; idx < PW * PW; idx += POTRF_THREADS) {
         const int r = idx / PW, c = idx % PW;
-        if (c <= r) M[(base + r) * npad + base + c] = (float)S[r * LDS + c];
+        if (c <= r) M[(base + r) * npad + base + c] = (float)Lt[tix(r >> 3, c >> 3) * 64 + apos(r & 7, c & 7)];
     }
-    // W^T (upper triangular: W^T[m][c] = W[c][m], nonzero for m <= c) in the
-    // order the panel solve's DMMA B fragments read it: entry
-    // ((s * 16 + n) * 32 + l) = W^T[4s + l%4][8n + l/4] (k-step s, column
-    // tile n, lane l). W[c][m] for m < c sits in S[m][c].
-    for (int f = tid; f < PW * PW; f += blockDim.x) {
-        const int l = f & 31, n = (f >> 5) & 15, st = f >> 9;
-        const int m = 4 * st + (l & 3), c = 8 * n + (l >> 2);
-        Wt[f] = m < c ? S[m * LDS + c] : (m == c ? dinv[c] : 0.0);
+    // W^T in the panel solve's fragment order: W^T[4s + l%4][8n + l/4] =
+    // W[8n + l/4][4s + l%4], tile (n, s/2), element (l/4, 4(s%2) + l%4)
+#pragma unroll 4
+    for (int f = tid; f < PW * PW; f += POTRF_THREADS) {
+        const int l = f & 31, n = (f >> 5) & 15, s = f >> 9;
+        Wt[f] = (s >> 1) <= n ? Wtl[tix(n, s >> 1) * 64 + bpos(l >> 2, 4 * (s & 1) + (l & 3))] : 0.0;
     }
 }
 
