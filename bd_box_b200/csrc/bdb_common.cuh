@@ -193,8 +193,13 @@ __device__ __forceinline__ double sq3(const double* v)
 
 // kernel entry points used across translation units
 namespace bdb {
-enum Phase { P_STEP, P_REFRESH, P_BUILD, P_FACTOR, P_MATVEC, P_TEA, P_FORCES, P_NOISE, P_UPDATE, P_COUNT };
+enum Phase {
+    P_STEP, P_REFRESH, P_BUILD, P_FACTOR, P_MATVEC, P_TEA, P_FORCES, P_NOISE, P_UPDATE,
+    // kernels of the mixed-precision factorisation, each on its own stream
+    P_POTRF, P_TRSM, P_SYRK_COL, P_SYRK_REST, P_COUNT
+};
 void phase_mark(bdb_system* s, int phase);   // records begin/end events when profiling
+void phase_mark_on(bdb_system* s, int phase, cudaStream_t stream);
 void drop_graph(bdb_system* s);              // forget the captured step
 int forces_setup(bdb_system* s);
 int forces_run(bdb_system* s, bool want_energy, bool want_counts);

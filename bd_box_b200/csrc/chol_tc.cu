@@ -352,16 +352,22 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
             if (lane == 0 && !pivot8(Dg, rd)) bad = 1;
             __syncwarp();
             if (lane < 8) {
-                // column c of W_kk by forward substitution; W_kk and L_kk out
+                // column c of W_kk by forward substitution (w[m] = 0 for
+                // m < c, so every row sums over all m < i); W_kk and L_kk out
                 const int c = lane;
-                double w[8];
+                double lk[8][8], r8[8], w[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    r8[i] = rd[i];
+#pragma unroll
+                    for (int m = 0; m < i; ++m) lk[i][m] = Dg[i * 9 + m];
+                }
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
                     double v = i == c ? 1.0 : 0.0;
 #pragma unroll
-                    for (int m = 0; m < i; ++m)
-                        if (m >= c) v -= Dg[i * 9 + m] * w[m];
-                    w[i] = i >= c ? v * rd[i] : 0.0;
+                    for (int m = 0; m < i; ++m) v = fma(-lk[i][m], w[m], v);
+                    w[i] = i >= c ? v * r8[i] : 0.0;
                 }
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -412,12 +418,25 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
             __syncthreads();   // B
             if (g > k) {
                 const double2 av = *reinterpret_cast<const double2*>(Lt + tix(g, k) * 64 + 2 * lane);
+                // four tiles per batch: their operand loads first (predicated,
+                // no branch), then the MMAs
 #pragma unroll
-                for (int n = 1; n < NT; ++n) {
-                    if (n > k && n <= g) {
-                        const double2 bv = *reinterpret_cast<const double2*>(Lt + tix(n, k) * 64 + 2 * lane);
-                        dmma884(cacc[n][0], cacc[n][1], -av.x, bv.x);
-                        dmma884(cacc[n][0], cacc[n][1], -av.y, bv.y);
+                for (int n0 = 1; n0 < NT; n0 += 4) {
+                    double2 bv[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int n = n0 + u;
+                        const bool act = n < NT && n > k && n <= g;
+                        bv[u] = act ? *reinterpret_cast<const double2*>(Lt + tix(n, k) * 64 + 2 * lane)
+                                    : make_double2(0.0, 0.0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int n = n0 + u;
+                        if (n < NT && n > k && n <= g) {
+                            dmma884(cacc[n][0], cacc[n][1], -av.x, bv[u].x);
+                            dmma884(cacc[n][0], cacc[n][1], -av.y, bv[u].y);
+                        }
                     }
                 }
                 if (g == k + 1) {
@@ -438,19 +457,33 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         }
     }
     __syncthreads();
-    if (warp > 0) {
-        // block column h of W (warp h+1), tiles in B order
-        const int h = warp - 1;
+    // block column h of W per warp; column h costs (15-h)(18-h) DMMAs, and
+    // this assignment (nibble w = column of warp w, 15 = none) gives every
+    // SM sub-partition (warps w = 0..3 mod 4) 392-404 of the 1600
+    const int h = (int)((0xDCEF9BA856742103ull >> (4 * warp)) & 15);
+    if (h < NT - 1) {
+        // tiles in B order
         for (int gg = h + 1; gg < NT; ++gg) {
-            double p0 = 0.0, p1 = 0.0, q0 = 0.0, q1 = 0.0;
-            for (int m = h; m < gg; ++m) {
+            double p0 = 0.0, p1 = 0.0, q0 = 0.0, q1 = 0.0, u0 = 0.0, u1 = 0.0, v0 = 0.0, v1 = 0.0;
+            int m = h;
+            for (; m + 1 < gg; m += 2) {
+                const double2 a = *reinterpret_cast<const double2*>(Lt + tix(gg, m) * 64 + 2 * lane);
+                const double2 b = *reinterpret_cast<const double2*>(Wtl + tix(m, h) * 64 + 2 * lane);
+                const double2 a2 = *reinterpret_cast<const double2*>(Lt + tix(gg, m + 1) * 64 + 2 * lane);
+                const double2 b2 = *reinterpret_cast<const double2*>(Wtl + tix(m + 1, h) * 64 + 2 * lane);
+                dmma884(p0, p1, a.x, b.x);
+                dmma884(q0, q1, a.y, b.y);
+                dmma884(u0, u1, a2.x, b2.x);
+                dmma884(v0, v1, a2.y, b2.y);
+            }
+            if (m < gg) {
                 const double2 a = *reinterpret_cast<const double2*>(Lt + tix(gg, m) * 64 + 2 * lane);
                 const double2 b = *reinterpret_cast<const double2*>(Wtl + tix(m, h) * 64 + 2 * lane);
                 dmma884(p0, p1, a.x, b.x);
                 dmma884(q0, q1, a.y, b.y);
             }
-            p0 += q0;
-            p1 += q1;
+            p0 += q0 + (u0 + v0);
+            p1 += q1 + (u1 + v1);
             // W[gg][h] = -W_gg (p): A = W_gg, B fragments of p by shuffles
             const double2 wa = *reinterpret_cast<const double2*>(Wa + gg * 64 + 2 * lane);
             double z0 = 0.0, z1 = 0.0;
@@ -474,12 +507,14 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         const int r = idx / PW, c = idx % PW;
         if (c <= r) M[(base + r) * npad + base + c] = (float)Lt[tix(r >> 3, c >> 3) * 64 + apos(r & 7, c & 7)];
     }
-    // W^T in the panel solve's fragment order: W^T[4s + l%4][8n + l/4] =
-    // W[8n + l/4][4s + l%4], tile (n, s/2), element (l/4, 4(s%2) + l%4)
+    // W^T for the panel solve, compact: tile (n, t) of W (t <= n) holds the
+    // B fragments of k-steps s = 2t, 2t+1 for column tile n, entry
+    // 64 tix(n, t) + 32 (s - 2t) + l = W^T[4s + l%4][8n + l/4]
+    //                                = W[8n + l/4][4s + l%4]
 #pragma unroll 4
-    for (int f = tid; f < PW * PW; f += POTRF_THREADS) {
-        const int l = f & 31, n = (f >> 5) & 15, s = f >> 9;
-        Wt[f] = (s >> 1) <= n ? Wtl[tix(n, s >> 1) * 64 + bpos(l >> 2, 4 * (s & 1) + (l & 3))] : 0.0;
+    for (int f = tid; f < NTILE * 64; f += POTRF_THREADS) {
+        const int e = f & 63, l = e & 31, s1 = e >> 5;
+        Wt[f] = Wtl[(f & ~63) + bpos(l >> 2, 4 * s1 + (l & 3))];
     }
 }
 
@@ -521,17 +556,28 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__
     const size_t row0 = base + PW;
     const int units = (int)(((size_t)npad - row0) / 8);
     {
-        // W^T fragments: a plain 128 KB copy, loads batched ahead of stores
+        // W^T fragments from the 136 compact tiles of k_potrf128 (tile
+        // (n, t) -> k-steps 2t, 2t+1 of column tile n); entries with
+        // k-step s > 2n+1 are never read. Loads batched ahead of stores.
         const double2* src = reinterpret_cast<const double2*>(Wf);
-        double2* dst = reinterpret_cast<double2*>(Bs);
-        constexpr int NW = PW * PW / 2 / TRSM_THREADS;   // 32 per thread
+        constexpr int NC = NTILE * 32;                              // double2 entries
+        constexpr int PER = (NC + TRSM_THREADS - 1) / TRSM_THREADS;  // 17
+        double2 w[PER];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            double2 w[NW / 2];
+        for (int k = 0; k < PER; ++k) {
+            const int f = tid + TRSM_THREADS * k;
+            if (f < NC) w[k] = __ldg(src + f);
+        }
 #pragma unroll
-            for (int k = 0; k < NW / 2; ++k) w[k] = __ldg(src + tid + TRSM_THREADS * (k + h * NW / 2));
-#pragma unroll
-            for (int k = 0; k < NW / 2; ++k) dst[tid + TRSM_THREADS * (k + h * NW / 2)] = w[k];
+        for (int k = 0; k < PER; ++k) {
+            const int f = tid + TRSM_THREADS * k;
+            if (f < NC) {
+                const int tile = f >> 5, e = 2 * (f & 31);   // entry within the tile (even)
+                int n, t;
+                tri_index(tile, n, t);
+                const int st = 2 * t + (e >> 5), l = e & 31;
+                *reinterpret_cast<double2*>(Bs + (st * 16 + n) * 32 + l) = w[k];
+            }
         }
     }
     __syncthreads();
@@ -558,13 +604,18 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__
         double acc[16][2];
 #pragma unroll
         for (int n = 0; n < 16; ++n) acc[n][0] = acc[n][1] = 0.0;
-#pragma unroll 2
-        for (int st = 0; st < 32; ++st) {
-            const double a = (double)Aw[fr * TRSM_LDA + 4 * st + fq];
-            const double* b = Bs + st * 16 * 32 + lane;
+        // k-steps 2m, 2m+1 reach column tiles n >= m: compile-time bounds,
+        // so the fragment loads are issued ahead of the MMAs (no branches)
 #pragma unroll
-            for (int n = 0; n < 16; ++n)
-                if (2 * n + 1 >= st) dmma884(acc[n][0], acc[n][1], a, b[n * 32]);
+        for (int m = 0; m < 16; ++m) {
+#pragma unroll
+            for (int s2 = 0; s2 < 2; ++s2) {
+                const int st = 2 * m + s2;
+                const double a = (double)Aw[fr * TRSM_LDA + 4 * st + fq];
+                const double* b = Bs + st * 16 * 32 + lane;
+#pragma unroll
+                for (int n = m; n < 16; ++n) dmma884(acc[n][0], acc[n][1], a, b[n * 32]);
+            }
         }
         const size_t row = r0 + fr;
 #pragma unroll
@@ -852,19 +903,25 @@ int factor_mixed_tc(bdb_system* s)
     float *hi, *lo;
     double* lkk;
     panel_ptrs(s, 0, &hi, &lo, &lkk);
+    phase_mark_on(s, P_POTRF, st);
     k_potrf128<<<1, POTRF_THREADS, POTRF_SMEM, st>>>(s->M32.p, s->npad, 0, lkk, s->status.p);
+    phase_mark_on(s, P_POTRF, st);
     s->launches += 1;
     for (int P = 0; P + 1 < nt; ++P) {
         const int par = P & 1;
         panel_ptrs(s, par, &hi, &lo, &lkk);
         const int units = (s->npad - (P + 1) * PW) / 8;
         const int per_cta = TRSM_THREADS / 32;
+        phase_mark_on(s, P_TRSM, st);
         k_trsm128<<<std::min(s->sm_count, (units + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st>>>(
             s->M32.p, s->npad, P, lkk, hi, lo, s->status.p);
+        phase_mark_on(s, P_TRSM, st);
         const int rem = nt - P - 1;
         // block column P+1 of the trailing matrix
+        phase_mark_on(s, P_SYRK_COL, st);
         k_syrk_tc<<<std::min(s->sm_count, rem), 192, SYRK_SMEM, st>>>(maps[2 * par], maps[2 * par + 1], maps[4], P + 1,
                                                                       rem, 1, s->status.p);
+        phase_mark_on(s, P_SYRK_COL, st);
         s->launches += 2;
         // diagonal block P+1 on the side stream, beside the rest of the update
         float *hi2, *lo2;
@@ -872,13 +929,17 @@ int factor_mixed_tc(bdb_system* s)
         panel_ptrs(s, par ^ 1, &hi2, &lo2, &lkk2);
         BDB_CUDA(cudaEventRecord(s->la_ev[0], st));
         BDB_CUDA(cudaStreamWaitEvent(st2, s->la_ev[0], 0));
+        phase_mark_on(s, P_POTRF, st2);
         k_potrf128<<<1, POTRF_THREADS, POTRF_SMEM, st2>>>(s->M32.p, s->npad, P + 1, lkk2, s->status.p);
+        phase_mark_on(s, P_POTRF, st2);
         BDB_CUDA(cudaEventRecord(s->la_ev[1], st2));
         s->launches += 1;
         const int rest = rem * (rem + 1) / 2 - rem;
         if (rest > 0) {
+            phase_mark_on(s, P_SYRK_REST, st);
             k_syrk_tc<<<std::min(s->sm_count - 1, rest), 192, SYRK_SMEM, st>>>(maps[2 * par], maps[2 * par + 1], maps[4],
                                                                            P + 1, rest, 2, s->status.p);
+            phase_mark_on(s, P_SYRK_REST, st);
             s->launches += 1;
         }
         BDB_CUDA(cudaStreamWaitEvent(st, s->la_ev[1], 0));

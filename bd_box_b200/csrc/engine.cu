@@ -71,10 +71,11 @@ template struct DevBuf<long long>;
 template struct DevBuf<Segment>;
 template struct DevBuf<TileJob>;
 
-static const char* kPhaseNames[P_COUNT] = {"step", "refresh", "build", "factor", "matvec",
-                                           "tea", "forces", "noise", "update"};
+static const char* kPhaseNames[P_COUNT] = {"step",   "refresh", "build",    "factor",   "matvec",
+                                           "tea",    "forces",  "noise",    "update",   "potrf",
+                                           "trsm",   "syrk_col", "syrk_rest"};
 
-void phase_mark(bdb_system* s, int ph)
+void phase_mark_on(bdb_system* s, int ph, cudaStream_t stream)
 {
     if (!s->profiling) return;
     auto& r = s->phases[ph];
@@ -83,8 +84,10 @@ void phase_mark(bdb_system* s, int ph)
         if (cudaEventCreate(&e) != cudaSuccess) return;
         r.ev.push_back(e);
     }
-    cudaEventRecord(r.ev[r.used++], s->stream);
+    cudaEventRecord(r.ev[r.used++], stream);
 }
+
+void phase_mark(bdb_system* s, int ph) { phase_mark_on(s, ph, s->stream); }
 
 static int check_status(bdb_system* s, bool* overlap)
 {
@@ -709,6 +712,7 @@ int bdb_phase_stats(bdb_system* s, const char* phase, double* total_ms, long lon
         if (!strcmp(phase, kPhaseNames[k])) ph = k;
     if (ph < 0) return fail(BDB_ERR_ARG, "unknown phase");
     BDB_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->stream2) BDB_CUDA(cudaStreamSynchronize(s->stream2));
     auto& r = s->phases[ph];
     double tot = 0;
     for (size_t k = 0; k + 1 < r.used; k += 2) {

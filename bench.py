@@ -292,6 +292,10 @@ def run_ours(args):
                     "peak_source": f"{src} hbm", "ms_per_launch": mv_avg, "share_of_step_time": share_mv}
         roof["phases_ms_per_call"] = {"factor": fac_avg, "build": bld_ms / max(bld_calls, 1),
                                       "matvec": mv_avg, "forces": frc_ms / max(frc_calls, 1)}
+        # live per-launch time of the factorisation's kernels (profiled pass)
+        roof["factor_kernels_us_per_launch"] = {
+            k: 1e3 * t / max(c, 1) for k, (t, c) in
+            ((k, phase(sysm, k)) for k in ("potrf", "trsm", "syrk_col", "syrk_rest"))}
         reps = None
         if rank == 0 and world == 1 and not args.skip_replicas:
             reps = replicas(torch, engine, max(3, args.steps // 5), 3)
