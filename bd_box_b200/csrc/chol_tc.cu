@@ -287,7 +287,7 @@ __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
 static constexpr int POTRF_THREADS = 512;
 static constexpr int NT = PW / 8;                  // 16 row groups of 8 rows
 static constexpr int NTILE = NT * (NT + 1) / 2;    // 136 tiles in the lower triangle
-static constexpr int POTRF_SMEM = (2 * NTILE * 64 + NT * 64 + 80 + 8) * 8;
+static constexpr int POTRF_SMEM = (2 * NTILE * 64 + NT * 64 + 80 + 8 + 2 * 64) * 8;
 
 // row group owned by a warp: warp 0 runs the pivots; warps 4, 8, 12 share
 // its scheduler (warp w issues on sub-partition w mod 4) and own the row
@@ -307,14 +307,22 @@ __device__ __forceinline__ int row_group_of(int warp)
 //   owners g>k  solve tile (g, k): L[g][k] = C[g][k] W_kk^T (two DMMAs),
 //               published in A order;
 //   barrier;
-//   owners g>k  update their tiles n = k+1..g: C[g][n] -= L[g][k] L[n][k]^T.
-//               The owner of row group k+1 updates its diagonal tile first
-//               and hands it to warp 0 (named barrier 1), so the next pivot
-//               overlaps the rest of the update.
-// Then each warp h+1 forms block column h of W by forward substitution,
+//   warp 0      applies the last update to diagonal tile k+1 itself (two
+//               DMMAs on the copy its owner handed over one iteration
+//               earlier), then goes on to pivot k+1;
+//   owners g>k+1 update their tiles n = k+1..g: C[g][n] -= L[g][k] L[n][k]^T,
+//               and the owner of row group k+2 hands its diagonal tile
+//               (now updated through column k) to warp 0.
+//   The next pivot thus waits for no owner: warp 0's sub-partition carries
+//   no bulk update (its other warps own row groups 1-3), while an owner's
+//   MMAs queue behind those of the three other owners on its own.
+// Then the warps form the block columns of W by forward substitution,
 // W[g][h] = -W_gg sum_{m=h}^{g-1} L[g][m] W[m][h], with W tiles in B order.
-// Finally L_PP goes to M (FP32) and W^T to Wt in the fragment order the
-// panel solve reads: entry ((s * 16 + n) * 32 + l) = W^T[4s + l%4][8n + l/4].
+// Finally L_PP goes to M (FP32, lower triangle) and W^T to Wt in the compact
+// fragment order the panel solve reads: entry 64 tix(n, t) + 32 (s - 2t) + l
+// = W^T[4s + l%4][8n + l/4] for k-steps s = 2t, 2t+1 of column tile n
+// (t <= n). (Storing each tile as soon as it is final measured slower: the
+// stores then compete with the pivot chain.)
 __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict__ M, int npad, int P,
                                                             double* __restrict__ Wt, unsigned* __restrict__ status)
 {
@@ -324,6 +332,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
     double* Wa = Wtl + NTILE * 64;         // [NT][64] W_kk in A order
     double* Dg = Wa + NT * 64;             // [8][9] diagonal block being factored
     double* rd = Dg + 80;                  // [8] 1/L_jj of that block
+    double* Hd = rd + 8;                   // [2][64] diagonal tiles handed to warp 0 (C layout)
     __shared__ int bad;
     {
         // the warp roles and barrier counts assume this exact launch shape
@@ -347,7 +356,6 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
             Dg[fr * 9 + c] = c <= fr ? (double)M[(base + fr) * npad + base + c] : 0.0;
         }
         for (int k = 0; k < NT; ++k) {
-            if (k > 0) asm volatile("bar.sync 1, 64;" ::: "memory");   // diagonal tile k from its owner
             __syncwarp();
             if (lane == 0 && !pivot8(Dg, rd)) bad = 1;
             __syncwarp();
@@ -371,13 +379,24 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                 }
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
+                    const double l = i >= c ? Dg[i * 9 + c] : 0.0;
                     Wa[k * 64 + apos(i, c)] = w[i];
                     Wtl[tix(k, k) * 64 + bpos(i, c)] = w[i];
-                    Lt[tix(k, k) * 64 + apos(i, c)] = i >= c ? Dg[i * 9 + c] : 0.0;
+                    Lt[tix(k, k) * 64 + apos(i, c)] = l;
                 }
             }
             __syncthreads();   // A: W_kk published
             __syncthreads();   // B: block column k solved
+            if (k + 1 < NT) {
+                // diagonal tile k+1 = its owner's copy - L[k+1][k] L[k+1][k]^T
+                const double2 t = *reinterpret_cast<const double2*>(Hd + ((k + 1) & 1) * 64 + 2 * lane);
+                const double2 av = *reinterpret_cast<const double2*>(Lt + tix(k + 1, k) * 64 + 2 * lane);
+                double e0 = t.x, e1 = t.y;
+                dmma884(e0, e1, -av.x, av.x);
+                dmma884(e0, e1, -av.y, av.y);
+                Dg[fr * 9 + 2 * fq] = e0;
+                Dg[fr * 9 + 2 * fq + 1] = e1;
+            }
         }
     } else {
         // -------------------------------------------------- tile owners
@@ -392,6 +411,8 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                 cacc[n][1] = (n < g || 2 * fq + 1 <= fr) ? (double)v.y : 0.0;
             }
         }
+        if (g == 1)   // row group 1's diagonal tile needs only column 0: warp 0's
+            *reinterpret_cast<double2*>(Hd + 64 + 2 * lane) = make_double2(cacc[1][0], cacc[1][1]);
         for (int k = 0; k < NT; ++k) {
             __syncthreads();   // A
             if (g > k) {
@@ -416,7 +437,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                 Lt[tix(g, k) * 64 + apos(fr, 2 * fq + 1)] = x1;
             }
             __syncthreads();   // B
-            if (g > k) {
+            if (g > k + 1) {
                 const double2 av = *reinterpret_cast<const double2*>(Lt + tix(g, k) * 64 + 2 * lane);
                 // four tiles per batch: their operand loads first (predicated,
                 // no branch), then the MMAs
@@ -439,8 +460,9 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                         }
                     }
                 }
-                if (g == k + 1) {
-                    // hand the finished diagonal tile to the pivot warp
+                if (g == k + 2) {
+                    // hand the diagonal tile (updated through column k) to
+                    // warp 0, which applies column k+1 itself
                     double d0 = 0.0, d1 = 0.0;
 #pragma unroll
                     for (int t = 0; t < NT; ++t)
@@ -448,10 +470,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                             d0 = cacc[t][0];
                             d1 = cacc[t][1];
                         }
-                    Dg[fr * 9 + 2 * fq] = d0;
-                    Dg[fr * 9 + 2 * fq + 1] = d1;
-                    __syncwarp();
-                    asm volatile("bar.arrive 1, 64;" ::: "memory");
+                    *reinterpret_cast<double2*>(Hd + (g & 1) * 64 + 2 * lane) = make_double2(d0, d1);
                 }
             }
         }
@@ -507,10 +526,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         const int r = idx / PW, c = idx % PW;
         if (c <= r) M[(base + r) * npad + base + c] = (float)Lt[tix(r >> 3, c >> 3) * 64 + apos(r & 7, c & 7)];
     }
-    // W^T for the panel solve, compact: tile (n, t) of W (t <= n) holds the
-    // B fragments of k-steps s = 2t, 2t+1 for column tile n, entry
-    // 64 tix(n, t) + 32 (s - 2t) + l = W^T[4s + l%4][8n + l/4]
-    //                                = W[8n + l/4][4s + l%4]
+    // W^T, compact tiles, B order -> fragment order
 #pragma unroll 4
     for (int f = tid; f < NTILE * 64; f += POTRF_THREADS) {
         const int e = f & 63, l = e & 31, s1 = e >> 5;
