@@ -563,6 +563,7 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__
             return;
         }
     }
+    asm volatile("griddepcontrol.launch_dependents;");
     extern __shared__ double sh[];
     double* Bs = sh;                                          // [32 k-steps][16 tiles][32 lanes]
     float* As = reinterpret_cast<float*>(sh + PW * PW);      // per warp [8][TRSM_LDA]
@@ -702,6 +703,11 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_sh;
+    // launched as a programmatic dependent of the previous kernel on the
+    // stream: the set-up above overlaps its tail; nothing below may read or
+    // write what it produces before this wait (a no-op for a plain launch)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
 
     if (warp == 0) {
         if (lane == 0) {
@@ -903,6 +909,24 @@ static int tc_setup(bdb_system* s)
     return BDB_OK;
 }
 
+// k_syrk_tc as a programmatic dependent launch: its CTAs may start while the
+// previous kernel on the stream drains and wait in griddepcontrol.wait.
+static cudaError_t launch_syrk(bdb_system* s, int grid, cudaStream_t st, const CUtensorMap& hi, const CUtensorMap& lo,
+                               const CUtensorMap& c, int t0, int ntiles, int mode)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(192);
+    cfg.dynamicSmemBytes = SYRK_SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_syrk_tc, hi, lo, c, t0, ntiles, mode, s->status.p);
+}
+
 // Factorisation with one panel of look-ahead. For panel P the trailing
 // update is split: block column P+1 first (main stream), then the FP64
 // diagonal factorisation of block P+1 runs on the second stream on an SM
@@ -935,8 +959,7 @@ int factor_mixed_tc(bdb_system* s)
         const int rem = nt - P - 1;
         // block column P+1 of the trailing matrix
         phase_mark_on(s, P_SYRK_COL, st);
-        k_syrk_tc<<<std::min(s->sm_count, rem), 192, SYRK_SMEM, st>>>(maps[2 * par], maps[2 * par + 1], maps[4], P + 1,
-                                                                      rem, 1, s->status.p);
+        BDB_CUDA(launch_syrk(s, std::min(s->sm_count, rem), st, maps[2 * par], maps[2 * par + 1], maps[4], P + 1, rem, 1));
         phase_mark_on(s, P_SYRK_COL, st);
         s->launches += 2;
         // diagonal block P+1 on the side stream, beside the rest of the update
@@ -953,8 +976,8 @@ int factor_mixed_tc(bdb_system* s)
         const int rest = rem * (rem + 1) / 2 - rem;
         if (rest > 0) {
             phase_mark_on(s, P_SYRK_REST, st);
-            k_syrk_tc<<<std::min(s->sm_count - 1, rest), 192, SYRK_SMEM, st>>>(maps[2 * par], maps[2 * par + 1], maps[4],
-                                                                           P + 1, rest, 2, s->status.p);
+            BDB_CUDA(launch_syrk(s, std::min(s->sm_count - 1, rest), st, maps[2 * par], maps[2 * par + 1], maps[4], P + 1,
+                                 rest, 2));
             phase_mark_on(s, P_SYRK_REST, st);
             s->launches += 1;
         }
