@@ -287,7 +287,9 @@ __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
 static constexpr int POTRF_THREADS = 512;
 static constexpr int NT = PW / 8;                  // 16 row groups of 8 rows
 static constexpr int NTILE = NT * (NT + 1) / 2;    // 136 tiles in the lower triangle
-static constexpr int POTRF_SMEM = (2 * NTILE * 64 + NT * 64 + 80 + 8 + 2 * 64) * 8;
+static constexpr int POTRF_SMEM = (NTILE * 64 + NT * 64 + 80 + 8 + 2 * 64) * 8;
+// factor hand-off to the panel solve: L_PP tiles then the W_kk, A order
+static constexpr int PANEL_FAC = (NTILE + NT) * 64;
 
 // row group owned by a warp: warp 0 runs the pivots; warps 4, 8, 12 share
 // its scheduler (warp w issues on sub-partition w mod 4) and own the row
@@ -297,8 +299,9 @@ __device__ __forceinline__ int row_group_of(int warp)
     return (warp & 3) ? 4 + warp - 1 - (warp >> 2) : warp >> 2;
 }
 
-// FP64 factorisation L_PP of the 128x128 diagonal block (P, P) and its
-// inverse W = L_PP^-1, right-looking over 16 blocks of 8 columns with the
+// FP64 factorisation L_PP of the 128x128 diagonal block (P, P) and the
+// inverses W_kk of its 8x8 diagonal tiles, right-looking over 16 blocks of 8
+// columns with the
 // trailing matrix held in registers: the warp owning row group g keeps its
 // tiles (g, n), n <= g, as DMMA accumulators. Iteration k:
 //   warp 0      factors diagonal tile (k, k) (pivot8) and inverts it
@@ -316,20 +319,16 @@ __device__ __forceinline__ int row_group_of(int warp)
 //   The next pivot thus waits for no owner: warp 0's sub-partition carries
 //   no bulk update (its other warps own row groups 1-3), while an owner's
 //   MMAs queue behind those of the three other owners on its own.
-// Then the warps form the block columns of W by forward substitution,
-// W[g][h] = -W_gg sum_{m=h}^{g-1} L[g][m] W[m][h], with W tiles in B order.
-// Finally L_PP goes to M (FP32, lower triangle) and W^T to Wt in the compact
-// fragment order the panel solve reads: entry 64 tix(n, t) + 32 (s - 2t) + l
-// = W^T[4s + l%4][8n + l/4] for k-steps s = 2t, 2t+1 of column tile n
-// (t <= n). (Storing each tile as soon as it is final measured slower: the
+// Finally L_PP goes to M (FP32, lower triangle) and, in FP64 for the panel
+// solve, its 136 tiles followed by the 16 W_kk to Wt (A order; PANEL_FAC
+// doubles). (Storing each tile as soon as it is final measured slower: the
 // stores then compete with the pivot chain.)
 __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict__ M, int npad, int P,
                                                             double* __restrict__ Wt, unsigned* __restrict__ status)
 {
     extern __shared__ double sh[];
     double* Lt = sh;                       // [NTILE][64] A order
-    double* Wtl = Lt + NTILE * 64;         // [NTILE][64] B order
-    double* Wa = Wtl + NTILE * 64;         // [NT][64] W_kk in A order
+    double* Wa = Lt + NTILE * 64;          // [NT][64] W_kk in A order
     double* Dg = Wa + NT * 64;             // [8][9] diagonal block being factored
     double* rd = Dg + 80;                  // [8] 1/L_jj of that block
     double* Hd = rd + 8;                   // [2][64] diagonal tiles handed to warp 0 (C layout)
@@ -381,7 +380,6 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                 for (int i = 0; i < 8; ++i) {
                     const double l = i >= c ? Dg[i * 9 + c] : 0.0;
                     Wa[k * 64 + apos(i, c)] = w[i];
-                    Wtl[tix(k, k) * 64 + bpos(i, c)] = w[i];
                     Lt[tix(k, k) * 64 + apos(i, c)] = l;
                 }
             }
@@ -476,49 +474,6 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         }
     }
     __syncthreads();
-    // block column h of W per warp; column h costs (15-h)(18-h) DMMAs, and
-    // this assignment (nibble w = column of warp w, 15 = none) gives every
-    // SM sub-partition (warps w = 0..3 mod 4) 392-404 of the 1600
-    const int h = (int)((0xDCEF9BA856742103ull >> (4 * warp)) & 15);
-    if (h < NT - 1) {
-        // tiles in B order
-        for (int gg = h + 1; gg < NT; ++gg) {
-            double p0 = 0.0, p1 = 0.0, q0 = 0.0, q1 = 0.0, u0 = 0.0, u1 = 0.0, v0 = 0.0, v1 = 0.0;
-            int m = h;
-            for (; m + 1 < gg; m += 2) {
-                const double2 a = *reinterpret_cast<const double2*>(Lt + tix(gg, m) * 64 + 2 * lane);
-                const double2 b = *reinterpret_cast<const double2*>(Wtl + tix(m, h) * 64 + 2 * lane);
-                const double2 a2 = *reinterpret_cast<const double2*>(Lt + tix(gg, m + 1) * 64 + 2 * lane);
-                const double2 b2 = *reinterpret_cast<const double2*>(Wtl + tix(m + 1, h) * 64 + 2 * lane);
-                dmma884(p0, p1, a.x, b.x);
-                dmma884(q0, q1, a.y, b.y);
-                dmma884(u0, u1, a2.x, b2.x);
-                dmma884(v0, v1, a2.y, b2.y);
-            }
-            if (m < gg) {
-                const double2 a = *reinterpret_cast<const double2*>(Lt + tix(gg, m) * 64 + 2 * lane);
-                const double2 b = *reinterpret_cast<const double2*>(Wtl + tix(m, h) * 64 + 2 * lane);
-                dmma884(p0, p1, a.x, b.x);
-                dmma884(q0, q1, a.y, b.y);
-            }
-            p0 += q0 + (u0 + v0);
-            p1 += q1 + (u1 + v1);
-            // W[gg][h] = -W_gg (p): A = W_gg, B fragments of p by shuffles
-            const double2 wa = *reinterpret_cast<const double2*>(Wa + gg * 64 + 2 * lane);
-            double z0 = 0.0, z1 = 0.0;
-#pragma unroll
-            for (int kk = 0; kk < 2; ++kk) {
-                const int src = ((4 * kk + fq) << 2) + (fr >> 1);
-                const double v0 = __shfl_sync(0xffffffffu, p0, src);
-                const double v1 = __shfl_sync(0xffffffffu, p1, src);
-                dmma884(z0, z1, kk ? wa.y : wa.x, (fr & 1) ? v1 : v0);
-            }
-            Wtl[tix(gg, h) * 64 + bpos(fr, 2 * fq)] = -z0;
-            Wtl[tix(gg, h) * 64 + bpos(fr, 2 * fq + 1)] = -z1;
-            __syncwarp();
-        }
-    }
-    __syncthreads();
     if (tid == 0 && bad) atomicOr(status, ST_NOT_SPD);
     // L_PP to M (FP32, lower triangle)
 #pragma unroll 4
@@ -526,33 +481,44 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         const int r = idx / PW, c = idx % PW;
         if (c <= r) M[(base + r) * npad + base + c] = (float)Lt[tix(r >> 3, c >> 3) * 64 + apos(r & 7, c & 7)];
     }
-    // W^T, compact tiles, B order -> fragment order
+    // L_PP tiles and the W_kk (A order, FP64) for the panel solve
+    {
+        const double2* src = reinterpret_cast<const double2*>(Lt);
+        double2* dst = reinterpret_cast<double2*>(Wt);
 #pragma unroll 4
-    for (int f = tid; f < NTILE * 64; f += POTRF_THREADS) {
-        const int e = f & 63, l = e & 31, s1 = e >> 5;
-        Wt[f] = Wtl[(f & ~63) + bpos(l >> 2, 4 * s1 + (l & 3))];
+        for (int f = tid; f < PANEL_FAC / 2; f += POTRF_THREADS) dst[f] = src[f];
     }
 }
 
-// Rows below block P: X L_PP^T = A, i.e. X = A W^T with W = L_PP^-1 from
-// k_potrf128, in FP64 on the DMMA path. Work unit = one row group of 8 rows,
-// owned by one warp: 16 accumulator tiles of 8x8 (the whole 8x128 row
-// block, 32 doubles per lane) over 32 k-steps of 4; W^T is upper
-// triangular, so column tile n only takes k-steps s <= 2n+1 (272 DMMAs per
-// unit instead of 512). The CTA copies W^T once (128 KB, already in
-// fragment order) into shared memory; each warp stages its unit's 8 FP32
-// rows (row stride 132 floats: the A-fragment reads hit 32 distinct banks).
-// The grid is persistent: unit u goes to warp slot u mod (8 grid), slots
-// ordered so that the first 4 grid slots put one warp on every SM
-// sub-partition, the next 4 grid a second one. Writes the rows to M and
-// their TF32 split L = L_hi + L_lo (L_hi: low 13 mantissa bits cleared,
-// exactly TF32; L_lo = L - L_hi) to the panel buffers.
+// Rows below block P: X L_PP^T = A by blocked forward substitution in FP64
+// on the DMMA path, from the tiles of L_PP and the inverses W_kk of its
+// diagonal tiles (k_potrf128). Work unit = one row group of 8 rows, owned by
+// one warp, which keeps the unit's 16 tiles C_n (8x8, 32 doubles per lane)
+// as DMMA accumulators loaded straight from M. For n = 0..15:
+//   X_n = C_n W_nn^T                       (two DMMAs),
+//   C_n' -= X_n L_n'n^T for n' > n         (two DMMAs each),
+// 272 DMMAs per unit; C_n -> A fragments by shuffles. The CTA copies the
+// factor (76 KB) into shared memory once. The grid is persistent: unit u goes
+// to warp slot u mod (8 grid), slots ordered so that the first 4 grid slots
+// put one warp on every SM sub-partition, the next 4 grid a second one.
+// Writes the rows to M and their TF32 split L = L_hi + L_lo (L_hi: low 13
+// mantissa bits cleared, exactly TF32; L_lo = L - L_hi) to the panel
+// buffers.
 static constexpr int TRSM_THREADS = 256;
-static constexpr int TRSM_LDA = PW + 4;
-static constexpr int TRSM_SMEM = PW * PW * 8 + (TRSM_THREADS / 32) * 8 * TRSM_LDA * 4;
+static constexpr int TRSM_SMEM = PANEL_FAC * 8;
+
+// A fragment of k-step h of an 8x8 tile held as C fragments (lane (r, q)
+// holds T[r][2q], T[r][2q+1]; the A fragment is T[r][4h + q])
+__device__ __forceinline__ double c2a(double c0, double c1, int h, int fr, int fq)
+{
+    const int src = (fr << 2) + 2 * h + (fq >> 1);
+    const double v0 = __shfl_sync(0xffffffffu, c0, src);
+    const double v1 = __shfl_sync(0xffffffffu, c1, src);
+    return (fq & 1) ? v1 : v0;
+}
 
 __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__ M, int npad, int P,
-                                                          const double* __restrict__ Wf, float* __restrict__ Lhi,
+                                                          const double* __restrict__ Lf, float* __restrict__ Lhi,
                                                           float* __restrict__ Llo, unsigned* __restrict__ status)
 {
     {
@@ -565,20 +531,19 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__
     }
     asm volatile("griddepcontrol.launch_dependents;");
     extern __shared__ double sh[];
-    double* Bs = sh;                                          // [32 k-steps][16 tiles][32 lanes]
-    float* As = reinterpret_cast<float*>(sh + PW * PW);      // per warp [8][TRSM_LDA]
+    const double2* Ls = reinterpret_cast<const double2*>(sh);               // [NTILE][32] pairs
+    const double2* Ws = reinterpret_cast<const double2*>(sh + NTILE * 64);  // [NT][32] pairs
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int fr = lane >> 2, fq = lane & 3;
     const size_t base = (size_t)P * PW;
     const size_t row0 = base + PW;
     const int units = (int)(((size_t)npad - row0) / 8);
     {
-        // W^T fragments from the 136 compact tiles of k_potrf128 (tile
-        // (n, t) -> k-steps 2t, 2t+1 of column tile n); entries with
-        // k-step s > 2n+1 are never read. Loads batched ahead of stores.
-        const double2* src = reinterpret_cast<const double2*>(Wf);
-        constexpr int NC = NTILE * 32;                              // double2 entries
-        constexpr int PER = (NC + TRSM_THREADS - 1) / TRSM_THREADS;  // 17
+        // the factor: a plain copy, loads batched ahead of stores
+        const double2* src = reinterpret_cast<const double2*>(Lf);
+        double2* dst = reinterpret_cast<double2*>(sh);
+        constexpr int NC = PANEL_FAC / 2;
+        constexpr int PER = (NC + TRSM_THREADS - 1) / TRSM_THREADS;   // 19
         double2 w[PER];
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
@@ -588,61 +553,41 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
             const int f = tid + TRSM_THREADS * k;
-            if (f < NC) {
-                const int tile = f >> 5, e = 2 * (f & 31);   // entry within the tile (even)
-                int n, t;
-                tri_index(tile, n, t);
-                const int st = 2 * t + (e >> 5), l = e & 31;
-                *reinterpret_cast<double2*>(Bs + (st * 16 + n) * 32 + l) = w[k];
-            }
+            if (f < NC) dst[f] = w[k];
         }
     }
     __syncthreads();
-    float* Aw = As + warp * 8 * TRSM_LDA;
     const int slot = (warp >> 2) * 4 * gridDim.x + blockIdx.x * 4 + (warp & 3);
     for (int u = slot; u < units; u += TRSM_THREADS / 32 * gridDim.x) {
-        const size_t r0 = row0 + (size_t)8 * u;
-        {
-            // the unit's 8 rows x 128 FP32 columns: 8 float4 per lane
-            float4 v[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int idx = lane + 32 * k;   // row idx/32, float4 column idx%32
-                v[k] = *reinterpret_cast<const float4*>(M + (r0 + (idx >> 5)) * npad + base + 4 * (idx & 31));
-            }
-            __syncwarp();
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int idx = lane + 32 * k;
-                *reinterpret_cast<float4*>(Aw + (idx >> 5) * TRSM_LDA + 4 * (idx & 31)) = v[k];
-            }
-            __syncwarp();
-        }
-        double acc[16][2];
-#pragma unroll
-        for (int n = 0; n < 16; ++n) acc[n][0] = acc[n][1] = 0.0;
-        // k-steps 2m, 2m+1 reach column tiles n >= m: compile-time bounds,
-        // so the fragment loads are issued ahead of the MMAs (no branches)
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-#pragma unroll
-            for (int s2 = 0; s2 < 2; ++s2) {
-                const int st = 2 * m + s2;
-                const double a = (double)Aw[fr * TRSM_LDA + 4 * st + fq];
-                const double* b = Bs + st * 16 * 32 + lane;
-#pragma unroll
-                for (int n = m; n < 16; ++n) dmma884(acc[n][0], acc[n][1], a, b[n * 32]);
-            }
-        }
-        const size_t row = r0 + fr;
+        const size_t row = row0 + (size_t)8 * u + fr;
+        double c[16][2];
 #pragma unroll
         for (int n = 0; n < 16; ++n) {
-            const int c = 8 * n + 2 * fq;
-            const float o0 = (float)acc[n][0], o1 = (float)acc[n][1];
+            const float2 v = *reinterpret_cast<const float2*>(M + row * npad + base + 8 * n + 2 * fq);
+            c[n][0] = v.x;
+            c[n][1] = v.y;
+        }
+#pragma unroll
+        for (int n = 0; n < 16; ++n) {
+            double x0 = 0.0, x1 = 0.0;
+            const double2 w = Ws[n * 32 + lane];
+            dmma884(x0, x1, c2a(c[n][0], c[n][1], 0, fr, fq), w.x);
+            dmma884(x0, x1, c2a(c[n][0], c[n][1], 1, fr, fq), w.y);
+            const int col = 8 * n + 2 * fq;
+            const float o0 = (float)x0, o1 = (float)x1;
             const float h0 = tf32_hi(o0), h1 = tf32_hi(o1);
-            *reinterpret_cast<float2*>(M + row * npad + base + c) = make_float2(o0, o1);
-            *reinterpret_cast<float2*>(Lhi + row * PW + c) = make_float2(h0, h1);
-            *reinterpret_cast<float2*>(Llo + row * PW + c) = make_float2(o0 - h0, o1 - h1);
+            *reinterpret_cast<float2*>(M + row * npad + base + col) = make_float2(o0, o1);
+            *reinterpret_cast<float2*>(Lhi + row * PW + col) = make_float2(h0, h1);
+            *reinterpret_cast<float2*>(Llo + row * PW + col) = make_float2(o0 - h0, o1 - h1);
+            if (n < 15) {
+                const double xa0 = -c2a(x0, x1, 0, fr, fq), xa1 = -c2a(x0, x1, 1, fr, fq);
+#pragma unroll
+                for (int n2 = n + 1; n2 < 16; ++n2) {
+                    const double2 b = Ls[tix(n2, n) * 32 + lane];
+                    dmma884(c[n2][0], c[n2][1], xa0, b.x);
+                    dmma884(c[n2][0], c[n2][1], xa1, b.y);
+                }
+            }
         }
     }
 }
