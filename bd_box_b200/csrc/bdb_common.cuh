@@ -130,6 +130,13 @@ struct bdb_system {
     int ewald_nk = 0, ewald_nimg = 0;
     bdb::DevBuf<double> M64;                   // stored D (upper) + L (lower), FP64
     bdb::DevBuf<float> M32;                    // same, FP32 (mixed path)
+    // IGT predictor-corrector: the tensor at the predicted positions, the
+    // step's starting positions, the two deterministic displacements and
+    // diag(D) at the start
+    bdb::DevBuf<double> M64b;
+    bdb::DevBuf<float> M32b;
+    bdb::DevBuf<double4> pos_igt;
+    bdb::DevBuf<double> Rf_igt, Rf2_igt, dD_igt;
     bdb::DevBuf<double> panel64;               // Cholesky workspace
     bool factor_valid = false;
     alignas(64) unsigned char tc_map[640];     // CUtensorMaps: TF32 hi / lo panel buffers (x2), FP32 matrix
@@ -201,6 +208,9 @@ enum Phase {
 void phase_mark(bdb_system* s, int phase);   // records begin/end events when profiling
 void phase_mark_on(bdb_system* s, int phase, cudaStream_t stream);
 void drop_graph(bdb_system* s);              // forget the captured step
+int build_and_factor(bdb_system* s);         // tensor build + factorisation into the stored matrix, eagerly
+int forces_phase(bdb_system* s);             // forces at the current positions (profiled phase)
+int check_status(bdb_system* s, bool* overlap);   // read and decode the status word (synchronises)
 int forces_setup(bdb_system* s);
 int forces_run(bdb_system* s, bool want_energy, bool want_counts);
 int bonded_setup(bdb_system* s);

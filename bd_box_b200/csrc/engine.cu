@@ -89,7 +89,7 @@ void phase_mark_on(bdb_system* s, int ph, cudaStream_t stream)
 
 void phase_mark(bdb_system* s, int ph) { phase_mark_on(s, ph, s->stream); }
 
-static int check_status(bdb_system* s, bool* overlap)
+int check_status(bdb_system* s, bool* overlap)
 {
     unsigned st = 0;
     BDB_CUDA(cudaMemcpyAsync(&st, s->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
@@ -123,7 +123,7 @@ int ensure_matrix(bdb_system* s)
     return BDB_OK;
 }
 
-static int build_and_factor(bdb_system* s)
+int build_and_factor(bdb_system* s)
 {
     phase_mark(s, P_BUILD);
     int rc = tensor_build(s);
@@ -179,7 +179,7 @@ static int refresh_factor(bdb_system* s)
     return BDB_OK;
 }
 
-static int forces_phase(bdb_system* s)
+int forces_phase(bdb_system* s)
 {
     phase_mark(s, P_FORCES);
     int rc = forces_run(s, false, false);

@@ -40,7 +40,7 @@ EXPORTS = [
     "bdb_version", "bdb_last_error", "bdb_create", "bdb_create_batch", "bdb_destroy", "bdb_set_bonded",
     "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
-    "bdb_compute_r", "bdb_step", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_autotune", "bdb_get_tuning",
+    "bdb_compute_r", "bdb_step", "bdb_step_igt", "bdb_step_igt_corrector", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_autotune", "bdb_get_tuning",
     "bdb_set_tuning", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc",
 ]
@@ -96,6 +96,8 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_compute_Rf.argtypes = [C.c_void_p, _dp]
     lib.bdb_compute_r.argtypes = [C.c_void_p, _dp, _dp]
     lib.bdb_step.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.bdb_step_igt.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.bdb_step_igt_corrector.argtypes = [C.c_void_p, _dp]
     lib.bdb_set_dt.argtypes = [C.c_void_p, C.c_double]
     lib.bdb_set_graphs.argtypes = [C.c_void_p, C.c_int]
     lib.bdb_autotune.argtypes = [C.c_void_p, C.c_int]
@@ -255,6 +257,20 @@ class System:
     def step(self, K: int = 1, gauss=None) -> int:
         g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
         return self._check(self.lib.bdb_step(self.h, K, _p(g)))
+
+    def step_igt(self, K: int = 1, gauss=None) -> int:
+        """K IGT predictor-corrector steps (bdb_step_igt); gauss: K*2*3N
+        host Gaussians (predictor then corrector per step) in host-noise
+        mode. Returns the overlap flags (1: at the predicted positions, 2:
+        after the step)."""
+        g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
+        return self._check(self.lib.bdb_step_igt(self.h, K, _p(g)))
+
+    def igt_corrector(self, gauss=None) -> int:
+        """The last IGT step's corrector again with fresh Gaussians
+        (bdb_step_igt_corrector); returns 1 on an overlap."""
+        g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
+        return self._check(self.lib.bdb_step_igt_corrector(self.h, _p(g)))
 
     def compute_hydro(self, gauss_attempts=None, move_attempts=None) -> int:
         """One step with comp_step_ermak's retry loop: on an overlap the saved

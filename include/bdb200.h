@@ -162,6 +162,27 @@ int bdb_compute_r(bdb_system* s, const double* gauss, double* Rs);
  * caller's, as in comp_step_ermak) or a negative error. */
 int bdb_step(bdb_system* s, int K, const double* gauss);
 
+/* IGT predictor-corrector steps (comp_step_IGT_const, diff_comp.c:76-107;
+ * compute_hydro_IGT + compute_hydro_IGT_second_phase,
+ * diff_equation.c:288-374) for hydro none or cholesky (one system): a
+ * predictor Ermak-McCammon step to r', forces and D(r') F' there, then
+ * r += (D(r)F + D(r')F') dt/(2 kB T) + L X2 with L the Cholesky factor of
+ * (D(r) + D(r'))/2 and fresh Gaussians; D is rebuilt and factored twice per
+ * step (the refresh interval does not apply). gauss: K*2*3N host Gaussians
+ * (predictor then corrector, per step) when noise == BDB_NOISE_HOST, else
+ * NULL. Returns the OR over the steps of 1 (overlap in the forces at r') and
+ * 2 (overlap after the step), or a negative error; retries are the
+ * caller's. */
+int bdb_step_igt(bdb_system* s, int K, const double* gauss);
+
+/* The corrector of the last IGT step again, from that step's start
+ * positions, with fresh Gaussians (gauss: 3N host Gaussians, or NULL for
+ * Philox) and the same averaged factor and deterministic displacement, then
+ * forces: compute_hydro_IGT_second_phase after an overlap
+ * (comp_step_IGT_const, diff_comp.c:87-96). Returns 1 on an overlap, else 0,
+ * or a negative error. */
+int bdb_step_igt_corrector(bdb_system* s, const double* gauss);
+
 /* Autotuner (no reference counterpart). With autotuning on, the first use
  * of each tunable site times its candidates on the system's stream and
  * keeps the fastest: the TEA tile edge (16 or 32 beads; the matrix-free

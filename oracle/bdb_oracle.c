@@ -900,3 +900,105 @@ int orc_run_steps(orc_system* s, double* coord, double* F, double dt, int K, con
     free(X);
     return rep;
 }
+
+/* K IGT predictor-corrector steps without retries (comp_step_IGT_const,
+ * diff_comp.c:76-107; compute_hydro_IGT and compute_hydro_IGT_second_phase,
+ * diff_equation.c:288-374). Predictor: the Ermak-McCammon step of
+ * compute_hydro_ermak (diff_equation.c:216-286) into r'. Forces F' at r'.
+ * Rf0 = (D(r)F + D(r')F')/2 * dt/kT; the stored tensor is averaged,
+ * D = (D(r) + D(r'))/2, over the off-diagonal 3x3 blocks (the diagonal
+ * blocks do not depend on the positions); corrector: r += Rf0 + L X2 with
+ * L = chol(D) and fresh Gaussians, then forces. gauss: K*2*3N (the
+ * predictor's 3N, then the corrector's, per step). Hydro none or cholesky.
+ * Returns the OR of overlap flags (1: forces at r', 2: forces after the
+ * step), or -1 on a failed Cholesky. */
+int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K, const double* gauss,
+                      double* traj)
+{
+    int n3 = 3 * s->n, step, i, k, rep = 0;
+    double *D = NULL, *Dp = NULL, *L = NULL;
+    double* Rf = (double*)malloc(sizeof(double) * n3);
+    double* Rf2 = (double*)malloc(sizeof(double) * n3);
+    double* Rs = (double*)malloc(sizeof(double) * n3);
+    double* X = (double*)malloc(sizeof(double) * n3);
+    double* Fp = (double*)malloc(sizeof(double) * n3);
+    double* cp = (double*)malloc(sizeof(double) * 4 * s->n);
+    double preDii, preDij;
+    orc_prefactors(s, &preDii, &preDij);
+    if (s->hydro == 1) {
+        D = (double*)malloc(sizeof(double) * (size_t)n3 * n3);
+        Dp = (double*)malloc(sizeof(double) * (size_t)n3 * n3);
+        L = (double*)malloc(sizeof(double) * (size_t)n3 * n3);
+    }
+    for (step = 0; step < K && rep >= 0; ++step) {
+        const double* x1 = gauss + (size_t)step * 2 * n3;
+        const double* x2 = x1 + n3;
+        s->coord = coord;
+        /* predictor */
+        if (s->hydro == 1) {
+            orc_D(s, D);
+            orc_df(s, D, F, dt, Rf);
+            memcpy(L, D, sizeof(double) * (size_t)n3 * n3);
+            if (orc_cholesky(n3, L, n3)) {
+                rep = -1;
+                break;
+            }
+            for (i = 0; i < n3; ++i) X[i] = x1[i] * sqrt(2 * dt);
+            orc_trmv_lower(n3, L, n3, X, Rs);
+        } else {
+            orc_df(s, NULL, F, dt, Rf);
+            for (i = 0; i < n3; ++i) Rs[i] = x1[i] * sqrt(preDii / coord[4 * (i / 3) + 3] * 2 * dt);
+        }
+        for (i = 0; i < s->n; ++i) {
+            for (k = 0; k < 3; ++k) cp[4 * i + k] = Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
+            cp[4 * i + 3] = coord[4 * i + 3];
+            if (s->bc == 1)
+                for (k = 0; k < 3; ++k) cp[4 * i + k] -= s->box[k] * floor(cp[4 * i + k] * s->inv_L[k] + 0.5f);
+        }
+        /* forces and D(r') F' at the predicted positions */
+        s->coord = cp;
+        if (orc_forces(s, Fp, NULL, NULL)) rep |= 1;
+        if (s->hydro == 1) {
+            orc_D(s, Dp);
+            orc_df(s, Dp, Fp, dt, Rf2);
+        } else {
+            orc_df(s, NULL, Fp, dt, Rf2);
+        }
+        s->coord = coord;
+        for (i = 0; i < n3; ++i) Rf[i] = 0.5 * (Rf[i] + Rf2[i]);
+        /* corrector */
+        if (s->hydro == 1) {
+            int a, b;
+            for (a = 0; a < n3; ++a)
+                for (b = 0; b < n3; ++b)
+                    L[(size_t)a * n3 + b] = a / 3 != b / 3 ? (D[(size_t)a * n3 + b] + Dp[(size_t)a * n3 + b]) / 2
+                                                           : D[(size_t)a * n3 + b];
+            if (orc_cholesky(n3, L, n3)) {
+                rep = -1;
+                break;
+            }
+            for (i = 0; i < n3; ++i) X[i] = x2[i] * sqrt(2 * dt);
+            orc_trmv_lower(n3, L, n3, X, Rs);
+        } else {
+            for (i = 0; i < n3; ++i) Rs[i] = x2[i] * sqrt(preDii / coord[4 * (i / 3) + 3] * 2 * dt);
+        }
+        for (i = 0; i < s->n; ++i) {
+            for (k = 0; k < 3; ++k) coord[4 * i + k] += Rf[3 * i + k] + Rs[3 * i + k];
+            if (s->bc == 1)
+                for (k = 0; k < 3; ++k) coord[4 * i + k] -= s->box[k] * floor(coord[4 * i + k] * s->inv_L[k] + 0.5f);
+        }
+        if (orc_forces(s, F, NULL, NULL)) rep |= 2;
+        if (traj) memcpy(traj + (size_t)step * 4 * s->n, coord, sizeof(double) * 4 * s->n);
+    }
+    s->coord = coord;
+    free(D);
+    free(Dp);
+    free(L);
+    free(Rf);
+    free(Rf2);
+    free(Rs);
+    free(X);
+    free(Fp);
+    free(cp);
+    return rep;
+}

@@ -99,6 +99,14 @@ int orc_forces(const orc_system* s, double* F, double* E, long long counts[2]);
 int orc_run_steps(orc_system* s, double* coord, double* F, double dt, int K,
                   const double* gauss, int refresh, double* traj);
 
+/* K IGT predictor-corrector steps (comp_step_IGT_const without retries,
+ * diff_comp.c:76-107; diff_equation.c:288-374). gauss: K*2*3N Gaussians
+ * (predictor, then corrector, per step). Hydro none or cholesky. Returns the
+ * OR of overlap flags (1: forces at the predicted positions, 2: forces
+ * after the step), or -1 on a failed Cholesky. */
+int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K,
+                      const double* gauss, double* traj);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,8 @@ def load():
     lib.orc_forces.restype = C.c_int
     lib.orc_run_steps.argtypes = [P, _dp, _dp, C.c_double, C.c_int, _dp, C.c_int, _dp]
     lib.orc_run_steps.restype = C.c_int
+    lib.orc_run_igt_steps.argtypes = [P, _dp, _dp, C.c_double, C.c_int, _dp, _dp]
+    lib.orc_run_igt_steps.restype = C.c_int
     _LIB = lib
     return lib
 
@@ -176,4 +178,16 @@ class Oracle:
         traj = np.zeros((K, self.deck.n, 4))
         g = np.ascontiguousarray(gauss, dtype=np.float64)
         rep = self.lib.orc_run_steps(C.byref(self.s), _p(self.coord), _p(F), dt, K, _p(g), refresh, _p(traj))
+        return traj, F, rep
+
+    def run_igt_steps(self, K, gauss, dt=None, F=None):
+        """K IGT predictor-corrector steps (orc_run_igt_steps); gauss holds
+        K*2*3N Gaussians, the predictor's then the corrector's per step."""
+        dt = self.deck.prm["dt"] if dt is None else dt
+        if F is None:
+            F, _, _, _ = self.forces()
+        F = np.ascontiguousarray(F, dtype=np.float64).copy()
+        traj = np.zeros((K, self.deck.n, 4))
+        g = np.ascontiguousarray(gauss, dtype=np.float64)
+        rep = self.lib.orc_run_igt_steps(C.byref(self.s), _p(self.coord), _p(F), dt, K, _p(g), _p(traj))
         return traj, F, rep
