@@ -6,7 +6,7 @@ sources) with a shared Gaussian stream. The .npz keeps the deck text, the
 Gaussians and every output, so the tests need neither the reference
 sources nor the harness:
 
-    python tests/golden/make_golden.py      # rewrites tests/golden/*.npz
+    python tests/golden/make_golden.py [case ...]   # rewrites tests/golden/*.npz
 """
 from __future__ import annotations
 
@@ -54,6 +54,12 @@ CASES = {
     "susp24_ewald": lambda d: decks.write_suspension_deck(d, "c", 24, seed=104, ewald_r=2, phi=0.15,
                                                           extra={"geyer_on_the_fly": "no"}),
     "chain24_bonded": lambda d: bonded_chain(d, "c", 24, 105),
+    # IGT predictor-corrector (comp_step_IGT_const): two 3N Gaussian draws
+    # per step, the predictor's then the corrector's
+    "chain24_igt_chol": lambda d: decks.write_chain_deck(d, "c", 24, seed=106, hydro="cholesky",
+                                                         extra={"algorithm": "igt_const"}),
+    "chain20_igt_none": lambda d: decks.write_chain_deck(d, "c", 20, seed=107, hydro="none",
+                                                         extra={"algorithm": "igt_const"}),
 }
 
 STEPS = 3
@@ -72,7 +78,8 @@ def make(name, fn):
         prm = fn(d)
         deck = decks.read_deck(prm)
         n, n3 = deck.n, 3 * deck.n
-        g = np.random.default_rng(zlib.crc32(name.encode())).standard_normal(n3 * STEPS)
+        draws = 2 if deck.prm["algorithm"] >= decks.ALGORITHM["igt_const"] else 1
+        g = np.random.default_rng(zlib.crc32(name.encode())).standard_normal(n3 * STEPS * draws)
         g.tofile(os.path.join(d, "g.bin"))
         res = {"prm": open(prm).read(), "str": open(prm[:-4] + ".str").read(), "gauss": g}
         res["D"] = run(d, prm, "D").reshape(n3, n3)
@@ -90,8 +97,10 @@ def make(name, fn):
 def main():
     if not os.path.exists(HARNESS):
         raise SystemExit("build the reference harness first: make -C oracle ref")
+    only = set(sys.argv[1:])
     for name, fn in CASES.items():
-        make(name, fn)
+        if not only or name in only:
+            make(name, fn)
 
 
 if __name__ == "__main__":

@@ -8,7 +8,7 @@ import golden_cases
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
 
-from bd_box_b200 import engine  # noqa: E402
+from bd_box_b200 import decks, engine  # noqa: E402
 
 
 def rel(a, b):
@@ -35,6 +35,10 @@ def test_engine_matches_reference_outputs(name):
     s2 = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
     K = ref["traj"].shape[0]
     disp = np.abs(ref["traj"][0, :, :3] - deck.coord[:, :3]).max()
+    igt = deck.prm["algorithm"] >= decks.ALGORITHM["igt_const"]
     for k in range(K):
-        s2.step(1, ref["gauss"][k * n3:(k + 1) * n3])
+        if igt:   # comp_step_IGT_const: two draws per step
+            s2.step_igt(1, ref["gauss"][2 * k * n3:2 * (k + 1) * n3])
+        else:
+            s2.step(1, ref["gauss"][k * n3:(k + 1) * n3])
         assert np.abs(s2.get_coord() - ref["traj"][k]).max() <= 1e-9 * disp, k

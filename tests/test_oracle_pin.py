@@ -44,7 +44,10 @@ def test_oracle_matches_golden(name):
         Rs, eps, beta = o.tea(ref["gauss"][:n3], deck.prm["dt"], Dst if deck.prm["hydro"] == 2 and Dst is not None else None)
         assert rel(Rs, ref["tea_Rs"]) < 1e-13
         assert abs(eps - float(ref["tea_eps"])) <= 1e-13 * abs(eps)
-    traj, _, _ = o.run_steps(ref["traj"].shape[0], ref["gauss"])
+    if deck.prm["algorithm"] >= decks.ALGORITHM["igt_const"]:
+        traj, _, _ = pyoracle.Oracle(deck).run_igt_steps(ref["traj"].shape[0], ref["gauss"])
+    else:
+        traj, _, _ = o.run_steps(ref["traj"].shape[0], ref["gauss"])
     disp = np.abs(ref["traj"][0, :, :3] - deck.coord[:, :3]).max()
     assert np.abs(traj - ref["traj"]).max() <= 1e-9 * disp
 
