@@ -137,6 +137,7 @@ struct bdb_system {
     bdb::DevBuf<float> M32b;
     bdb::DevBuf<double4> pos_igt;
     bdb::DevBuf<double> Rf_igt, Rf2_igt, dD_igt;
+    bool igt_ready = false;                    // a predictor awaits its corrector
     bdb::DevBuf<double> panel64;               // Cholesky workspace
     bool factor_valid = false;
     alignas(64) unsigned char tc_map[640];     // CUtensorMaps: TF32 hi / lo panel buffers (x2), FP32 matrix

@@ -122,7 +122,10 @@ static int displacements(bdb_system* s, bool want_rs)
     return rc;
 }
 
-static int igt_step(bdb_system* s, const double* g1, const double* g2, unsigned* flags)
+// predictor, forces at r', D(r') F', and the averaged tensor's factor;
+// with stop_on_overlap the rest is skipped when the forces at r' overlap
+// (compute_hydro_IGT returns 1 there, diff_equation.c:325-329)
+static int igt_predictor(bdb_system* s, const double* g1, bool stop_on_overlap, unsigned* flags)
 {
     int rc;
     const bool chol = s->p.hydro == BDB_HYDRO_CHOLESKY;
@@ -150,6 +153,8 @@ static int igt_step(bdb_system* s, const double* g1, const double* g2, unsigned*
     if ((rc = check_status(s, &ov))) return rc;
     if (ov) *flags |= 1;
     BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
+    s->igt_ready = false;
+    if (ov && stop_on_overlap) return BDB_OK;
     if (chol) {
         swap_matrices(s);
         phase_mark(s, P_BUILD);
@@ -162,8 +167,7 @@ static int igt_step(bdb_system* s, const double* g1, const double* g2, unsigned*
         return rc;
     }
     BDB_CUDA(cudaMemcpyAsync(s->Rf2_igt.p, s->Rf.p, v3, cudaMemcpyDeviceToDevice, s->stream));
-    // corrector: averaged tensor, its factor, fresh noise, from the start positions
-    BDB_CUDA(cudaMemcpyAsync(s->pos.p, s->pos_igt.p, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+    // averaged tensor and its factor
     if (chol) {
         const int nb = (s->n3 + 31) / 32;
         const dim3 grid(nb, nb), block(32, 8);
@@ -178,6 +182,15 @@ static int igt_step(bdb_system* s, const double* g1, const double* g2, unsigned*
         if ((rc = factor_run(s))) return rc;
         phase_mark(s, P_FACTOR);
     }
+    s->igt_ready = true;
+    return BDB_OK;
+}
+
+// corrector: fresh Gaussians, r <- r0 + ((Rf + Rf')/2 + L X2), forces
+static int igt_corrector(bdb_system* s, const double* g2)
+{
+    int rc;
+    BDB_CUDA(cudaMemcpyAsync(s->pos.p, s->pos_igt.p, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
     phase_mark(s, P_NOISE);
     if ((rc = noise_fill(s, g2))) return rc;
     phase_mark(s, P_NOISE);
@@ -197,28 +210,46 @@ static int igt_step(bdb_system* s, const double* g1, const double* g2, unsigned*
 
 using namespace bdb;
 
-extern "C" int bdb_step_igt(bdb_system* s, int K, const double* gauss)
+static int igt_buffers(bdb_system* s)
 {
-    if (!s || K < 0) return fail(BDB_ERR_ARG, "bad arguments");
+    if (s->pos_igt.n < (size_t)s->n && s->pos_igt.alloc(s->n)) return BDB_ERR_NOMEM;
+    for (DevBuf<double>* b : {&s->Rf_igt, &s->Rf2_igt, &s->dD_igt})
+        if (b->n < (size_t)s->n3 && b->alloc(s->n3)) return BDB_ERR_NOMEM;
+    return BDB_OK;
+}
+
+static int igt_checks(bdb_system* s, const double* gauss)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
     if (s->p.noise == BDB_NOISE_HOST && !gauss) return fail(BDB_ERR_ARG, "host noise mode needs Gaussians");
     if (s->p.hydro == BDB_HYDRO_GEYER)
         return fail(BDB_ERR_UNSUPPORTED, "IGT steps need hydro none or cholesky (the averaged tensor is stored)");
     if (s->segs.size() > 1) return fail(BDB_ERR_UNSUPPORTED, "IGT steps take one system");
-    if (s->pos_igt.n < (size_t)s->n && s->pos_igt.alloc(s->n)) return BDB_ERR_NOMEM;
-    for (DevBuf<double>* b : {&s->Rf_igt, &s->Rf2_igt, &s->dD_igt})
-        if (b->n < (size_t)s->n3 && b->alloc(s->n3)) return BDB_ERR_NOMEM;
+    return igt_buffers(s);
+}
+
+static int stage_gauss(bdb_system* s, const double* gauss, size_t count)
+{
+    if (!gauss) return BDB_OK;
+    if (s->gbuf.n < count && s->gbuf.alloc(count)) return BDB_ERR_NOMEM;
+    BDB_CUDA(cudaMemcpyAsync(s->gbuf.p, gauss, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream));
+    return BDB_OK;
+}
+
+extern "C" int bdb_step_igt(bdb_system* s, int K, const double* gauss)
+{
+    if (K < 0) return fail(BDB_ERR_ARG, "bad arguments");
+    int rc0 = igt_checks(s, gauss);
+    if (rc0) return rc0;
     phase_mark(s, P_STEP);
-    if (gauss) {
-        const size_t need = (size_t)K * 2 * s->n3;
-        if (s->gbuf.n < need && s->gbuf.alloc(need)) return BDB_ERR_NOMEM;
-        BDB_CUDA(cudaMemcpyAsync(s->gbuf.p, gauss, sizeof(double) * need, cudaMemcpyHostToDevice, s->stream));
-    }
+    if ((rc0 = stage_gauss(s, gauss, (size_t)K * 2 * s->n3))) return rc0;
     unsigned flags = 0;
     for (int k = 0; k < K; ++k) {
         BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
         const double* g1 = gauss ? s->gbuf.p + (size_t)k * 2 * s->n3 : nullptr;
         const double* g2 = gauss ? g1 + s->n3 : nullptr;
-        int rc = igt_step(s, g1, g2, &flags);
+        int rc = igt_predictor(s, g1, false, &flags);
+        if (!rc) rc = igt_corrector(s, g2);
         if (rc) return rc;
         bool ov = false;
         rc = check_status(s, &ov);
@@ -229,32 +260,32 @@ extern "C" int bdb_step_igt(bdb_system* s, int K, const double* gauss)
     return (int)flags;
 }
 
-// compute_hydro_IGT_second_phase again after an overlap
-// (comp_step_IGT_const, diff_comp.c:87-96): from the step's start positions,
-// fresh Gaussians with the same averaged factor and the same deterministic
-// displacement, then forces
+// compute_hydro_IGT's first part (diff_equation.c:317-368): the predictor
+// from the current positions and forces, the forces at r' and, unless they
+// overlap, D(r') F' and the averaged factor for bdb_step_igt_corrector
+extern "C" int bdb_step_igt_predictor(bdb_system* s, const double* gauss)
+{
+    int rc = igt_checks(s, gauss);
+    if (rc) return rc;
+    if ((rc = stage_gauss(s, gauss, s->n3))) return rc;
+    BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
+    unsigned flags = 0;
+    if ((rc = igt_predictor(s, gauss ? s->gbuf.p : nullptr, true, &flags))) return rc;
+    return flags ? 1 : 0;
+}
+
+// compute_hydro_IGT_second_phase (diff_equation.c:288-315), after
+// bdb_step_igt_predictor or again after an overlap (comp_step_IGT_const,
+// diff_comp.c:87-96): from the step's start positions, fresh Gaussians with
+// the same averaged factor and deterministic displacement, then forces
 extern "C" int bdb_step_igt_corrector(bdb_system* s, const double* gauss)
 {
-    if (!s) return fail(BDB_ERR_ARG, "null system");
-    if (s->p.noise == BDB_NOISE_HOST && !gauss) return fail(BDB_ERR_ARG, "host noise mode needs Gaussians");
-    if (!s->pos_igt.p || s->pos_igt.n < (size_t)s->n)
-        return fail(BDB_ERR_ARG, "no IGT step to repeat the corrector of");
-    if (gauss) {
-        if (s->gbuf.n < (size_t)s->n3 && s->gbuf.alloc(s->n3)) return BDB_ERR_NOMEM;
-        BDB_CUDA(cudaMemcpyAsync(s->gbuf.p, gauss, sizeof(double) * s->n3, cudaMemcpyHostToDevice, s->stream));
-    }
+    int rc = igt_checks(s, gauss);
+    if (rc) return rc;
+    if (!s->igt_ready) return fail(BDB_ERR_ARG, "no IGT predictor to finish");
+    if ((rc = stage_gauss(s, gauss, s->n3))) return rc;
     BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
-    BDB_CUDA(cudaMemcpyAsync(s->pos.p, s->pos_igt.p, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
-    int rc;
-    if ((rc = noise_fill(s, gauss ? s->gbuf.p : nullptr))) return rc;
-    if ((rc = displacements(s, true))) return rc;
-    k_igt_update<<<(s->n + 127) / 128, 128, 0, s->stream>>>(
-        s->n, s->p.bc == 1, make_double3(s->p.box[0], s->p.box[1], s->p.box[2]),
-        make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]), s->pos_igt.p, s->Rf_igt.p, s->Rf2_igt.p, s->Rs.p,
-        s->pos.p);
-    BDB_CUDA(cudaGetLastError());
-    s->launches += 1;
-    if ((rc = forces_phase(s))) return rc;
+    if ((rc = igt_corrector(s, gauss ? s->gbuf.p : nullptr))) return rc;
     bool ov = false;
     if ((rc = check_status(s, &ov))) return rc;
     return ov ? 1 : 0;

@@ -33,7 +33,8 @@
  *
  * Not available in the engine, and reported through the host's
  * unexpected_error (err.c:48-90) like any other fatal input error: IGT
- * algorithms, Newton overlap removal when an overlap actually occurs, the
+ * algorithms with hydro geyer, Newton overlap removal when an overlap
+ * actually occurs, the
  * Smith Ewald tensor, Chebyshev noise, sphere boundaries, external electric
  * fields and velocity-gradient flows.
  */
@@ -143,8 +144,9 @@ static size_t coord_bytes(void) { return sizeof(DOUBLE) * DIMS1 * (size_t)size; 
 
 static void check_supported(void)
 {
-    if (algorithm != DIFF_ALG_ERMAK_CONST && algorithm != DIFF_ALG_ERMAK_VAR && algorithm != DIFF_ALG_ERMAK_NEWTON)
-        UNERR("bdb200: only the Ermak-McCammon algorithms (ermak_const, ermak_var, ermak_newton) are available")
+    if (algorithm == DIFF_ALG_IGT_VAR_REV) UNERR("Unimplemented method: comp_step_rev_IGT")
+    if ((algorithm == DIFF_ALG_IGT_CONST || algorithm == DIFF_ALG_IGT_VAR) && hydro == DIFF_GEYER)
+        UNERR("bdb200: the IGT algorithms need hydro none or cholesky")
     if (hydro != DIFF_NONE && hydro != DIFF_CHOLESKY && hydro != DIFF_GEYER)
         UNERR("bdb200: hydro must be none, cholesky or geyer")
     if (ewald && ewald_method != EWALD_METHOD_BEENAKKER)
@@ -447,10 +449,15 @@ static DOUBLE ermak_step(DOUBLE* _E)
     return algorithm == DIFF_ALG_ERMAK_NEWTON ? dt : curr_dt;
 }
 
+static DOUBLE igt_step(DOUBLE* _E);
+
 void compute_hydro(DOUBLE* _E)
 {
     engine();
-    curr_time += ermak_step(_E);
+    if (algorithm == DIFF_ALG_IGT_CONST || algorithm == DIFF_ALG_IGT_VAR)
+        curr_time += igt_step(_E);
+    else
+        curr_time += ermak_step(_E);
 }
 
 /* the move alone, into coord_out (diff_equation.c:216-286); the engine also
@@ -462,18 +469,64 @@ void compute_hydro_ermak(DOUBLE* coord_out)
     pull_coord(coord_out);
 }
 
-INT compute_hydro_IGT(DOUBLE* _E)
-{
-    (void)_E;
-    UNERR("bdb200: the IGT algorithms are not available")
-    return 1;
-}
+/* ---- IGT predictor-corrector (diff_equation.c:288-374, diff_comp.c:76-144) */
 
+/* the corrector from the step's start positions with fresh Gaussians (the
+ * averaged factor of the predictor is kept); 2 on an overlap */
 INT compute_hydro_IGT_second_phase(DOUBLE* _E)
 {
-    (void)_E;
-    UNERR("bdb200: the IGT algorithms are not available")
-    return 1;
+    int rc;
+    if (g_noise_host) gauss_rand(X, DIMS0 * size);
+    rc = bdb_step_igt_corrector(g_sys, g_noise_host ? X : NULL);
+    if (rc < 0) fatal("bdb_step_igt_corrector", rc);
+    pull_coord(coord);
+    if (_E && !rc) CHK(bdb_compute_forces(g_sys, F[0], _E, NULL));
+    return rc ? 2 : 0;
+}
+
+/* predictor, forces at r' (1 on an overlap there), then the corrector */
+INT compute_hydro_IGT(DOUBLE* _E)
+{
+    int rc;
+    engine();
+    push_coord();
+    set_dt();
+    if (g_noise_host) gauss_rand(X, DIMS0 * size);
+    rc = bdb_step_igt_predictor(g_sys, g_noise_host ? X : NULL);
+    if (rc < 0) fatal("bdb_step_igt_predictor", rc);
+    if (rc) return 1;
+    curr_iter++;
+    return compute_hydro_IGT_second_phase(_E);
+}
+
+/* comp_step_IGT_const and comp_step_IGT_var (diff_comp.c:76-144): after an
+ * overlap in the corrector the constant-step variant repeats only the
+ * corrector; otherwise the step is revoked (the variable-step variant also
+ * halves dt, at most 16 times) and taken again with new Gaussians */
+static DOUBLE igt_step(DOUBLE* _E)
+{
+    INT count = 0;
+    curr_dt = dt;
+    curr_iter++;
+    push_coord();
+    CHK(bdb_save_state(g_sys));
+    for (;;) {
+        INT res = compute_hydro_IGT(_E);
+        if (!res) break;
+        if (algorithm == DIFF_ALG_IGT_CONST && res == 2) {
+            while (compute_hydro_IGT_second_phase(_E)) {
+                ++count;
+                if (count > move_attempts) UNERR("Wrong conformation, can't move")
+            }
+            break;
+        }
+        if (algorithm == DIFF_ALG_IGT_VAR && count < 16) curr_dt /= 2;
+        CHK(bdb_load_state(g_sys));
+        ++count;
+        if (count > move_attempts) UNERR("Wrong conformation, can't move")
+    }
+    pull_coord(coord);
+    return curr_dt;
 }
 
 /* ---- state save/restore (diff_decl.c:219-237) ---------------------------- */

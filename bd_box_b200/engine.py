@@ -40,7 +40,7 @@ EXPORTS = [
     "bdb_version", "bdb_last_error", "bdb_create", "bdb_create_batch", "bdb_destroy", "bdb_set_bonded",
     "bdb_set_coord", "bdb_get_coord", "bdb_save_state", "bdb_load_state",
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
-    "bdb_compute_r", "bdb_step", "bdb_step_igt", "bdb_step_igt_corrector", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_autotune", "bdb_get_tuning",
+    "bdb_compute_r", "bdb_step", "bdb_step_igt", "bdb_step_igt_predictor", "bdb_step_igt_corrector", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_autotune", "bdb_get_tuning",
     "bdb_set_tuning", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc",
 ]
@@ -97,6 +97,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_compute_r.argtypes = [C.c_void_p, _dp, _dp]
     lib.bdb_step.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.bdb_step_igt.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.bdb_step_igt_predictor.argtypes = [C.c_void_p, _dp]
     lib.bdb_step_igt_corrector.argtypes = [C.c_void_p, _dp]
     lib.bdb_set_dt.argtypes = [C.c_void_p, C.c_double]
     lib.bdb_set_graphs.argtypes = [C.c_void_p, C.c_int]
@@ -266,9 +267,16 @@ class System:
         g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
         return self._check(self.lib.bdb_step_igt(self.h, K, _p(g)))
 
+    def igt_predictor(self, gauss=None) -> int:
+        """The predictor half of an IGT step (bdb_step_igt_predictor);
+        returns 1 when the forces at the predicted positions overlap."""
+        g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
+        return self._check(self.lib.bdb_step_igt_predictor(self.h, _p(g)))
+
     def igt_corrector(self, gauss=None) -> int:
-        """The last IGT step's corrector again with fresh Gaussians
-        (bdb_step_igt_corrector); returns 1 on an overlap."""
+        """The corrector of the pending IGT step, or again after an overlap,
+        with fresh Gaussians (bdb_step_igt_corrector); returns 1 on an
+        overlap."""
         g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
         return self._check(self.lib.bdb_step_igt_corrector(self.h, _p(g)))
 

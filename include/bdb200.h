@@ -175,12 +175,17 @@ int bdb_step(bdb_system* s, int K, const double* gauss);
  * caller's. */
 int bdb_step_igt(bdb_system* s, int K, const double* gauss);
 
-/* The corrector of the last IGT step again, from that step's start
- * positions, with fresh Gaussians (gauss: 3N host Gaussians, or NULL for
- * Philox) and the same averaged factor and deterministic displacement, then
- * forces: compute_hydro_IGT_second_phase after an overlap
- * (comp_step_IGT_const, diff_comp.c:87-96). Returns 1 on an overlap, else 0,
- * or a negative error. */
+/* One IGT step in two calls, for callers that retry like
+ * comp_step_IGT_const (diff_comp.c:76-107); gauss: 3N host Gaussians, or
+ * NULL for Philox. bdb_step_igt_predictor is compute_hydro_IGT up to the
+ * corrector (diff_equation.c:317-368): the predictor, forces at r' and,
+ * unless they overlap (return 1), D(r') F' and the factor of the averaged
+ * tensor. bdb_step_igt_corrector is compute_hydro_IGT_second_phase
+ * (:288-315): from the step's start positions, fresh Gaussians with that
+ * factor and deterministic displacement, then forces; it may be called again
+ * after an overlap (return 1). Both return 0 otherwise, or a negative
+ * error. */
+int bdb_step_igt_predictor(bdb_system* s, const double* gauss);
 int bdb_step_igt_corrector(bdb_system* s, const double* gauss);
 
 /* Autotuner (no reference counterpart). With autotuning on, the first use

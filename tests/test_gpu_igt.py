@@ -93,6 +93,15 @@ def test_igt_corrector_retry(igt_decks):
     s = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
     s.step_igt(1, g)
     assert s.igt_corrector(g2) == 0
+    # the same step in two calls, as a retrying caller makes it
+    t = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
+    assert t.igt_predictor(g[:n3]) == 0
+    assert t.igt_corrector(g[n3:]) == 0
+    u = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
+    u.step_igt(1, g)
+    assert np.array_equal(t.get_coord(), u.get_coord())
+    t.close()
+    u.close()
     traj, _, _ = pyoracle.Oracle(deck).run_igt_steps(1, np.concatenate([g[:n3], g2]))
     disp = np.abs(traj[0][:, :3] - deck.coord[:, :3]).max()
     assert np.abs(s.get_coord()[:, :3] - traj[0][:, :3]).max() / disp < 1e-9
