@@ -305,6 +305,9 @@ def run_ours(args):
         ew = None
         if rank == 0 and world == 1 and not args.skip_ewald:
             ew = ewald_case(torch, engine)
+        igt = None
+        if rank == 0 and world == 1 and not args.skip_igt:
+            igt = igt_case(torch, engine, deck)
         cpu = None
         if rank == 0 and world == 1 and not args.skip_cpu:
             cpu = reference_cpu(prm, deck, args.cpu_steps)
@@ -322,6 +325,7 @@ def run_ours(args):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches.value),
             "autotuned": {"matvec_warps_per_sm": sysm.tuning()[1]},
             "clocks": clk.summary(), "fp64_gpu": fp64, "errors": errors, "replicas": reps, "adjoint": adj, "ewald_suspension": ew,
+            "igt": igt,
         }
         if rank == 0:
             print(json.dumps(out), flush=True)
@@ -498,6 +502,40 @@ def ewald_case(torch, engine, steps=3):
             "displacement_rel_vs_fp64": float(np.linalg.norm(dm - dd) / np.linalg.norm(dd))}
 
 
+def igt_case(torch, engine, deck, steps=5):
+    """IGT predictor-corrector (igt_const) on the bench chain: two tensor
+    builds and two Cholesky factorisations per step (D at r, then the
+    average of D(r) and D(r')); steps/s of the mixed and FP64 paths and one
+    step's displacement error of mixed against FP64 with the same noise."""
+    s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_PHILOX, seed=SEED)
+    s.step_igt(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.step_igt(steps)
+    torch.cuda.synchronize()
+    t_mixed = (time.perf_counter() - t0) / steps
+    s.close()
+    n3 = 3 * deck.n
+    g = np.random.default_rng(7).standard_normal(2 * n3)
+    sm = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
+    s64 = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
+    x0 = s64.get_coord()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s64.step_igt(1, g)
+    torch.cuda.synchronize()
+    t64 = time.perf_counter() - t0
+    sm.step_igt(1, g)
+    dd = s64.get_coord()[:, :3] - x0[:, :3]
+    dm = sm.get_coord()[:, :3] - x0[:, :3]
+    sm.close()
+    s64.close()
+    return {"workload": f"chain N={deck.n}, free-space RPY + Cholesky noise, IGT predictor-corrector (igt_const)",
+            "metric": "steps/s", "value": 1.0 / t_mixed, "ms_per_step": 1e3 * t_mixed,
+            "fp64_steps_per_s": 1.0 / t64,
+            "displacement_rel_vs_fp64": float(np.linalg.norm(dm - dd) / np.linalg.norm(dd))}
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -533,6 +571,7 @@ def main():
     ap.add_argument("--skip-replicas", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-ewald", action="store_true")
+    ap.add_argument("--skip-igt", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
