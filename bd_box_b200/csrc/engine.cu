@@ -299,6 +299,8 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     if (p->bc == 1 && (p->box[0] <= 0 || p->box[1] <= 0 || p->box[2] <= 0))
         return fail(BDB_ERR_ARG, "Wrong box size");
     if (p->ewald && (p->ewald_real < 0 || p->ewald_real > 5)) return fail(BDB_ERR_ARG, "ewald_real wrong value, only 0..5");
+    if (p->ewald && p->ewald_method != BDB_EWALD_BEENAKKER && p->ewald_method != BDB_EWALD_SMITH)
+        return fail(BDB_ERR_ARG, "ewald_method must be beenakker or smith");
     if (p->ewald && !(p->box[0] == p->box[1] && p->box[1] == p->box[2]))
         return fail(BDB_ERR_ARG, "In Ewald box must be cube");
     if (p->visc == 0.0 || p->vfactor == 0.0) return fail(BDB_ERR_ARG, "Wrong value for visc/vfactor");

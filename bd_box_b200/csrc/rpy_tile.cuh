@@ -12,6 +12,10 @@
 //    correction on the raw (not minimum-image) separation, alpha = sqrt(pi)/L
 //    (init_tensor, :546-559). Constants that the reference forms from the
 //    float literal M_PIF are formed the same way on the host.
+//  * rpy_smith_tab: diff_tensor_calc_ewald_smith (diff_tensor.c:102-243) with
+//    its self term (:245-263): Oseen (O) and sigma^2 (Q) sums over the
+//    images r/L + m and the reciprocal vectors of the same sphere, in units
+//    of L, alpha = ewald_alpha, preO = 0.75/L, preQ = sigma^2/(2 L^3).
 #pragma once
 
 #include "bdb_common.cuh"
@@ -32,7 +36,15 @@ struct EwaldConst {
     const double4* img = nullptr;
     int nk = 0, nimg = 0;
     float rcut_sq = 0.f;   // mixed precision: real-space images beyond this are dropped
+    // Smith (rpy_smith_tab): rk rows are h, f, g, then the identity, e e^T
+    // and sigma^2 e e^T coefficients (k and -k together), then the six
+    // products e_a e_b (xx, yy, zz, xy, xz, yz)
+    int smith = 0;
+    double s_alpha = 0, s_alpha2 = 0, s_alpha3 = 0;
 };
+
+// 1/sqrt(pi) as the reference's double build spells it (data.h:228)
+#define BDB_M1_SQRTPI 0.5641895835
 
 inline EwaldConst make_ewald(double L, double inv_L, int R)
 {
@@ -54,6 +66,16 @@ inline EwaldConst make_ewald(double L, double inv_L, int R)
     e.six_pif = six;
     e.R = R;
     e.rr_sq = R * R;
+    return e;
+}
+
+inline EwaldConst make_ewald_smith(double L, double inv_L, int R, double alpha)
+{
+    EwaldConst e = make_ewald(L, inv_L, R);
+    e.smith = 1;
+    e.s_alpha = alpha;
+    e.s_alpha2 = alpha * alpha;
+    e.s_alpha3 = alpha * e.s_alpha2;
     return e;
 }
 
@@ -204,6 +226,80 @@ __device__ __forceinline__ void rpy_ewald_tab(const double4& pi, const double4& 
         const double a = ec.alpha, a3 = ec.alpha3;
         const double sc3 = (-6 * a / BDB_SQRTPI + 40 * a3 * aw * aw / (3 * BDB_SQRTPI)) * preDii;
         for (int k = 0; k < 3; ++k) t[k] = preDii / aw + sc3 + t[k];
+        t[3] = t[4] = t[5] = 0;
+    }
+}
+
+// diff_tensor_calc_ewald_smith(i, j) (+ _diag for i == j) from the lattice
+// tables, in FP64 in both precisions.
+__device__ __forceinline__ void rpy_smith_tab(const double4& pi, const double4& pj, bool self, double preDii,
+                                              double preDij, const EwaldConst& ec, double* t)
+{
+    const double sigma_i = pj.w, sigma_j = pi.w;
+    // dist_vec(coord_j, coord_i): v = r_i - r_j, no minimum image
+    const double r0 = pi.x - pj.x, r1 = pi.y - pj.y, r2 = pi.z - pj.z;
+    const double sigma_sq = 0.5 * (sigma_i * sigma_i + sigma_j * sigma_j);
+    const double preO = 0.75 * ec.inv_L;
+    const double preQ = 0.5 * sigma_sq * ec.inv_L * ec.inv_L * ec.inv_L;
+    for (int k = 0; k < 6; ++k) t[k] = 0;
+    const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    const double rr = r0 * r0 + r1 * r1 + r2 * r2;
+    if (!self && rr < (sigma_i + sigma_j) * (sigma_i + sigma_j)) {
+        const double r = sqrt(rr), inv = 1 / r;
+        const double e[3] = {r0 * inv, r1 * inv, r2 * inv};
+        const double sigma = (sigma_i + sigma_j) / 2;
+        const double pre = preDii / sigma;
+        const double part1 = 1 - (9 * r / (32 * sigma));
+        const double pre2 = preDij / r;
+        const double sigm_r = (sigma_i * sigma_i + sigma_j * sigma_j) / rr;
+        const double p1 = 1 + sigm_r / 3;
+        for (int k = 0; k < 3; ++k)
+            t[k] += pre * (part1 + 3 * e[k] * e[k] * r / (32 * sigma)) - pre2 * (p1 + e[k] * e[k] * (1 - sigm_r));
+        for (int k = 3; k < 6; ++k)
+            t[k] += pre * 3 * e[ia[k]] * e[ib[k]] * r / (32 * sigma) - pre2 * e[ia[k]] * e[ib[k]] * (1 - sigm_r);
+    }
+    const double v0 = r0 * ec.inv_L, v1 = r1 * ec.inv_L, v2 = r2 * ec.inv_L;
+    const double a = ec.s_alpha, a2 = ec.s_alpha2, a3 = ec.s_alpha3;
+    double O[6] = {0, 0, 0, 0, 0, 0}, Q[6] = {0, 0, 0, 0, 0, 0};
+    // real space: images v + m (m from the image table, stored as L m)
+    for (int m = 0; m < ec.nimg; ++m) {
+        const double4 off = ec.img[m];
+        const double x = v0 + rint(off.x * ec.inv_L), y = v1 + rint(off.y * ec.inv_L), z = v2 + rint(off.z * ec.inv_L);
+        const double r_sq = x * x + y * y + z * z;
+        if (r_sq == 0.0) continue;
+        const double r = sqrt(r_sq);
+        const double inv_r = 1 / r, inv_r3 = 1 / (r * r_sq);
+        const double e[3] = {x * inv_r, y * inv_r, z * inv_r};
+        const double er = erfc(r * a), ex = exp(-a2 * r_sq);
+        const double so = er * inv_r, so2 = so + 2 * a * BDB_M1_SQRTPI * ex;
+        const double sq = inv_r3 * (er + 2 * a * r * BDB_M1_SQRTPI * ex);
+        const double sq2 = -3 * sq - 4 * a3 * BDB_M1_SQRTPI * ex;
+        for (int k = 0; k < 3; ++k) {
+            O[k] += so + so2 * e[k] * e[k];
+            Q[k] += sq + sq2 * e[k] * e[k];
+        }
+        for (int k = 3; k < 6; ++k) {
+            O[k] += so2 * e[ia[k]] * e[ib[k]];
+            Q[k] += sq2 * e[ia[k]] * e[ib[k]];
+        }
+    }
+    // reciprocal space: one row per pair k, -k
+    double Rc[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < ec.nk; ++k) {
+        const double* q = ec.rk + 12 * k;
+        const double cs = cos(ec.two_pif * (v0 * q[0] + v1 * q[1] + v2 * q[2]));
+        const double ci = q[3] * cs, ce = (q[4] + sigma_sq * q[5]) * cs;
+        for (int c = 0; c < 3; ++c) Rc[c] += ci + ce * q[6 + c];
+        for (int c = 3; c < 6; ++c) Rc[c] += ce * q[6 + c];
+    }
+    for (int k = 0; k < 6; ++k) t[k] += preDii * (preO * O[k] + preQ * Q[k] + Rc[k]);
+    if (self) {
+        const double aw = pi.w, il = ec.inv_L;
+        double sc3 = a * aw * il;
+        sc3 = sc3 * sc3 * sc3 * BDB_M1_SQRTPI / 3;
+        sc3 = 0.75 * il * 1.5 * a * aw * BDB_M1_SQRTPI * il + 0.5 * aw * aw * il * il * il * sc3;
+        sc3 *= preDii;
+        for (int k = 0; k < 3; ++k) t[k] = preDii / aw - sc3 + t[k];
         t[3] = t[4] = t[5] = 0;
     }
 }

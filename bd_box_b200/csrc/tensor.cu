@@ -42,10 +42,26 @@ struct TensorArgs {
 // in the order diff_tensor_calc_ewald_beenakker walks the sphere |m|^2 <= R^2
 // (diff_tensor.c:319-326); the k-only factors of the reciprocal term are
 // evaluated as the device evaluates them per pair.
+static EwaldConst system_ewald(const bdb_system* s)
+{
+    if (s->p.ewald_method == BDB_EWALD_SMITH)
+        return make_ewald_smith(s->p.box[0], s->inv_L[0], s->p.ewald_real,
+                                s->p.ewald_alpha > 0 ? s->p.ewald_alpha : BDB_SQRTPI);
+    return make_ewald(s->p.box[0], s->inv_L[0], s->p.ewald_real);
+}
+
 static int ewald_tables(bdb_system* s)
 {
     if (!s->p.ewald || s->ewald_tab.p) return BDB_OK;
-    const EwaldConst ec = make_ewald(s->p.box[0], s->inv_L[0], s->p.ewald_real);
+    const EwaldConst ec = system_ewald(s);
+    // Smith's k-only factors (diff_tensor.c:206-239 with init_tensor's
+    // M_PI_ALPHA_SQ = -pi_f^2/alpha^2, pi_f^2 formed in float)
+    volatile float pif = BDB_M_PIF;
+    volatile float npif2 = -pif * pif;
+    volatile float four_pif = 4 * pif;
+    const double m_pi_alpha_sq = ec.smith ? (double)npif2 / ec.s_alpha2 : 0.0;
+    const double preO = 0.75 * ec.inv_L;
+    const double qL3 = ec.inv_L * ec.inv_L * ec.inv_L;
     std::vector<double> rk, img;
     const int R = ec.R;
     for (int h = -R; h <= R; ++h) {
@@ -59,6 +75,17 @@ static int ewald_tables(bdb_system* s)
                 const double k_sq = (double)(h * h + f * f + g * g);
                 const double kn = std::sqrt(k_sq), ik = 1 / kn;
                 const double e[3] = {h * ik, f * ik, g * ik};
+                if (ec.smith) {
+                    // Op: A (I + (m k^2 - 1) e e^T), Qp: C e e^T, both times cos;
+                    // k and -k together: 2x
+                    const double ex = std::exp(m_pi_alpha_sq * k_sq);
+                    const double A = 2 * ex / ((double)pif * k_sq);
+                    const double C = (double)four_pif * ex;
+                    rk.insert(rk.end(), {(double)h, (double)f, (double)g, 2 * preO * A,
+                                         2 * preO * A * (-1 + m_pi_alpha_sq * k_sq), 2 * 0.5 * qL3 * C,
+                                         e[0] * e[0], e[1] * e[1], e[2] * e[2], e[0] * e[1], e[0] * e[2], e[1] * e[2]});
+                    continue;
+                }
                 const double k2 = k_sq * ec.four_pif2;
                 double P = 1 + (ec.inv_alpha2 * k2 / 4) * (1 + ec.inv_alpha2 * k2 / 2);
                 P *= ec.six_pif * std::exp(-ec.inv_alpha2 * k2 / 4) / k2;
@@ -85,7 +112,7 @@ static TensorArgs targs(const bdb_system* s)
     a.preDii = s->preDii;
     a.preDij = s->preDij;
     a.ewald = s->p.ewald;
-    a.ec = make_ewald(s->p.box[0], s->inv_L[0], s->p.ewald_real);
+    a.ec = system_ewald(s);
     if (s->p.ewald) {
         a.ec.rk = s->ewald_tab.p;
         a.ec.nk = s->ewald_nk;
@@ -103,7 +130,10 @@ __device__ __forceinline__ void tile_of(const TensorArgs& A, const double4* pos,
     const double4 pi = pos[i], pj = pos[j];
     if (A.ewald) {
         double d[6];
-        rpy_ewald_tab<sizeof(T) == 4>(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
+        if (A.ec.smith)
+            rpy_smith_tab(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
+        else
+            rpy_ewald_tab<sizeof(T) == 4>(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
         for (int k = 0; k < 6; ++k) t[k] = (T)d[k];
     } else if (i == j) {
         const T d = (T)(A.preDii / pi.w);

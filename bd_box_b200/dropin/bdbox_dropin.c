@@ -34,8 +34,7 @@
  * Not available in the engine, and reported through the host's
  * unexpected_error (err.c:48-90) like any other fatal input error: IGT
  * algorithms with hydro geyer, Newton overlap removal when an overlap
- * actually occurs, the
- * Smith Ewald tensor, Chebyshev noise, sphere boundaries, external electric
+ * actually occurs, Chebyshev noise, sphere boundaries, external electric
  * fields and velocity-gradient flows.
  */
 #if HAVE_CONFIG_H
@@ -149,8 +148,6 @@ static void check_supported(void)
         UNERR("bdb200: the IGT algorithms need hydro none or cholesky")
     if (hydro != DIFF_NONE && hydro != DIFF_CHOLESKY && hydro != DIFF_GEYER)
         UNERR("bdb200: hydro must be none, cholesky or geyer")
-    if (ewald && ewald_method != EWALD_METHOD_BEENAKKER)
-        UNERR("bdb200: the Ewald-summed tensor is available with ewald_method beenakker only")
     if (bc == BC_SPHERE) UNERR("bdb200: sphere boundary conditions are not available")
     if (E_ext) UNERR("bdb200: external electric fields are not available")
     if (vel_grad_tensor) UNERR("bdb200: velocity-gradient flows are not available")
@@ -168,6 +165,8 @@ static void make_params(bdb_params* p)
     p->hydro = hydro;
     p->ewald = ewald;
     p->ewald_real = ewald_real;
+    p->ewald_method = ewald_method == EWALD_METHOD_SMITH ? BDB_EWALD_SMITH : BDB_EWALD_BEENAKKER;
+    p->ewald_alpha = ewald_alpha;
     p->T = T;
     p->visc = visc;
     p->vfactor = vfactor;
@@ -365,7 +364,7 @@ void diff_tensor_calc_pos(INT i, INT j, DOUBLE* tD)
 
 void diff_tensor_calc_ewald_beenakker(INT i, INT j, DOUBLE* tD)
 {
-    if (!ewald) UNERR("bdb200: the system is not Ewald-summed")
+    if (!ewald || ewald_method != EWALD_METHOD_BEENAKKER) UNERR("bdb200: the system is not Beenakker-Ewald-summed")
     compute_Dij(i, j, tD);
 }
 
@@ -376,10 +375,8 @@ void diff_tensor_calc_ewald_beenakker_diag(INT i, DOUBLE* tD)
 
 void diff_tensor_calc_ewald_smith(INT i, INT j, DOUBLE* tD)
 {
-    (void)i;
-    (void)j;
-    (void)tD;
-    UNERR("bdb200: the Smith Ewald tensor is not available")
+    if (!ewald || ewald_method != EWALD_METHOD_SMITH) UNERR("bdb200: the system is not Smith-Ewald-summed")
+    compute_Dij(i, j, tD);
 }
 
 void diff_tensor_calc_ewald_smith_diag(INT i, DOUBLE* tD) { diff_tensor_calc_ewald_smith(i, i, tD); }

@@ -63,6 +63,7 @@ class Params(C.Structure):
         ("bond_lj_scale", C.c_double), ("bond_c_scale", C.c_double),
         ("check_overlap", C.c_int), ("nb_list", C.c_int), ("max_force_cutoff", C.c_double),
         ("precision", C.c_int), ("refresh", C.c_int), ("noise", C.c_int), ("seed", C.c_uint64),
+        ("ewald_method", C.c_int), ("ewald_alpha", C.c_double),
     ]
 
 
@@ -136,6 +137,10 @@ def params_from_deck(deck, precision=PREC_FP64, refresh=1, noise=NOISE_PHILOX, s
     P.hydro = p["hydro"]
     P.ewald = deck.ewald
     P.ewald_real = p["ewald_real"]
+    # the deck's ewald_method: 0 smith, 1 beenakker (diff_decl.c); the ABI's
+    # BDB_EWALD_*: 0 beenakker, 1 smith
+    P.ewald_method = 1 if p["ewald_method"] == 0 else 0
+    P.ewald_alpha = p["ewald_alpha"]
     P.T, P.visc, P.vfactor, P.dt = p["T"], p["visc"], p["vfactor"], p["dt"]
     P.elec = p["elec"]
     P.epsilon_c, P.kappa_c, P.gamma_c, P.cutoff_c = p["epsilon_c"], p["kappa_c"], p["gamma_c"], p["cutoff_c"]

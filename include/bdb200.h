@@ -48,6 +48,9 @@ enum { BDB_E_NONE, BDB_E_BOND, BDB_E_ANGLE, BDB_E_ANGLE_COS, BDB_E_DIHE,
 
 /* hydrodynamic methods, DIFF_* (diff_tensor.h:44-52) */
 enum { BDB_HYDRO_NONE = 0, BDB_HYDRO_CHOLESKY = 1, BDB_HYDRO_GEYER = 2 };
+/* Ewald-summed tensor (ewald_method, diff_decl.c): Beenakker
+ * (diff_tensor.c:265-422) or Smith (:102-263) */
+enum { BDB_EWALD_BEENAKKER = 0, BDB_EWALD_SMITH = 1 };
 
 /* arithmetic of the diffusion part of the step */
 enum {
@@ -69,7 +72,7 @@ typedef struct {
     int bc;                   /* 0 none, 1 periodic box (trans.h:43-63) */
     double box[3];            /* xbox, ybox, zbox */
     int hydro;                /* BDB_HYDRO_* */
-    int ewald;                /* 1: Beenakker Ewald tensor (periodic, hydro != none) */
+    int ewald;                /* 1: Ewald-summed tensor (periodic, hydro != none), see ewald_method */
     int ewald_real;           /* lattice radius R (ewald_real == ewald_recip, 0..5) */
     double T, visc, vfactor, dt;
     int elec;                 /* Debye-Hueckel on */
@@ -85,6 +88,8 @@ typedef struct {
     int refresh;              /* rebuild D and its factor every `refresh` steps (>= 1) */
     int noise;                /* BDB_NOISE_* */
     uint64_t seed;            /* Philox key */
+    int ewald_method;         /* BDB_EWALD_* (after the engine choices, so that zeroed structs mean Beenakker) */
+    double ewald_alpha;       /* Smith's splitting parameter in units of 1/L (ewald_alpha; <= 0: sqrt(pi)) */
 } bdb_params;
 
 typedef struct bdb_system bdb_system;

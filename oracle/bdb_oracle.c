@@ -208,6 +208,128 @@ static void tile_beenakker(const orc_system* s, double preDii, double preDij, in
     }
 }
 
+/* 1/sqrt(pi) as the reference's double build spells it (data.h:228) */
+#define M1_SQRTPI_REF 0.5641895835
+
+/* diff_tensor_calc_ewald_smith(i, j) (diff_tensor.c:102-243) with the
+ * constants of init_tensor (diff_tensor.c:546-559): distances in units of
+ * L, alpha = ewald_alpha, preO = 0.75/L, preQ = sigma^2/(2 L^3),
+ * M_PI_ALPHA_SQ = -pi_f^2/alpha^2 (pi_f^2 formed in float) */
+static void tile_smith(const orc_system* s, double preDii, double preDij, int i, int j, double* _tD)
+{
+    const double* coord = s->coord;
+    double sigma_i = coord[4 * j + 3], sigma_j = coord[4 * i + 3];
+    double v[3];
+    const double sigma_sq = 0.5 * (sigma_i * sigma_i + sigma_j * sigma_j);
+    int k, l, f, g, h;
+    double Op[9] = {0}, Qp[9] = {0};
+    const double ewald_alpha = s->ewald_alpha;
+    const double alpha2 = ewald_alpha * ewald_alpha;
+    const double alpha3 = ewald_alpha * alpha2;
+    const float pif2 = -M_PIF * M_PIF;
+    const double m_pi_alpha_sq = pif2 / alpha2;
+    const double preO = 0.75 * s->inv_L[0];
+    const double preQ = 0.5 * sigma_sq * s->inv_L[0] * s->inv_L[0] * s->inv_L[0];
+    const int ewald_rr = s->ewald_real;
+    const int rr_sq = s->ewald_real * s->ewald_real;
+    /* dist_vec(coord_j, coord_i): v = r_i - r_j, no minimum image */
+    v[0] = coord[4 * i] - coord[4 * j];
+    v[1] = coord[4 * i + 1] - coord[4 * j + 1];
+    v[2] = coord[4 * i + 2] - coord[4 * j + 2];
+    if ((v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) < (sigma_i + sigma_j) * (sigma_i + sigma_j) && i != j) {
+        double r_norm, r_sq, e[3];
+        int a, b;
+        ev2(v[0], v[1], v[2], e, &r_norm, &r_sq);
+        {
+            double sigma = (sigma_i + sigma_j) / 2;
+            double pre = preDii / sigma;
+            double part1 = (1 - (9 * r_norm / (32 * sigma)));
+            for (a = 0; a < 3; ++a) {
+                _tD[a + 3 * a] += pre * (part1 + 3 * e[a] * e[a] * r_norm / (32 * sigma));
+                for (b = 0; b < a; ++b) {
+                    double vval = pre * 3 * e[a] * e[b] * r_norm / (32 * sigma);
+                    _tD[b + 3 * a] += vval;
+                    _tD[a + 3 * b] += vval;
+                }
+            }
+        }
+        {
+            double pre = preDij / r_norm;
+            double sigm_r = (sigma_i * sigma_i + sigma_j * sigma_j) / r_sq;
+            double part1 = 1 + sigm_r / 3;
+            for (a = 0; a < 3; ++a) {
+                _tD[a + 3 * a] -= pre * (part1 + e[a] * e[a] * (1 - sigm_r));
+                for (b = 0; b < a; ++b) {
+                    double vval = pre * e[a] * e[b] * (1 - sigm_r);
+                    _tD[b + 3 * a] -= vval;
+                    _tD[a + 3 * b] -= vval;
+                }
+            }
+        }
+    }
+    v[0] *= s->inv_L[0];
+    v[1] *= s->inv_L[1];
+    v[2] *= s->inv_L[2];
+    for (h = -ewald_rr; h <= ewald_rr; ++h) {
+        int next_f = (int)sqrt(rr_sq - h * h);
+        for (f = -next_f; f <= next_f; ++f) {
+            int next_g = (int)sqrt(rr_sq - h * h - f * f);
+            for (g = -next_g; g <= next_g; ++g) {
+                double r_norm, r_sq, e[3], inv_r, inv_r3, sc, sc2;
+                /* real space: O (Oseen) and Q (sigma^2) sums */
+                ev2(v[0] + h, v[1] + f, v[2] + g, e, &r_norm, &r_sq);
+                if (r_norm != 0.0f) {
+                    inv_r = 1 / r_norm;
+                    inv_r3 = 1 / (r_norm * r_sq);
+                    sc = erfc(r_norm * ewald_alpha) * inv_r;
+                    sc2 = 2 * ewald_alpha * M1_SQRTPI_REF * exp(-alpha2 * r_sq);
+                    for (k = 0; k < 3; ++k) {
+                        double sc_ek = e[k] * (sc + sc2);
+                        Op[k * 4] += sc + sc_ek * e[k];
+                        for (l = 0; l < k; ++l) Op[k + l * 3] += e[l] * sc_ek;
+                    }
+                    sc = inv_r3 * (erfc(r_norm * ewald_alpha) +
+                                   2 * ewald_alpha * r_norm * M1_SQRTPI_REF * exp(-alpha2 * r_sq));
+                    sc2 = -4 * alpha3 * M1_SQRTPI_REF * exp(-alpha2 * r_sq);
+                    for (k = 0; k < 3; ++k) {
+                        double sc_ek = (-3 * sc + sc2) * e[k];
+                        Qp[k * 4] += sc + sc_ek * e[k];
+                        for (l = 0; l < k; ++l) Qp[k + l * 3] += e[l] * sc_ek;
+                    }
+                }
+                /* reciprocal space */
+                ev2(h, f, g, e, &r_norm, &r_sq);
+                if (r_norm != 0.0f) {
+                    const double ph = cos(2 * M_PIF * (v[0] * h + v[1] * f + v[2] * g));
+                    sc = 2 * exp(m_pi_alpha_sq * r_sq) / (M_PIF * r_sq);
+                    sc2 = -1 + m_pi_alpha_sq * r_sq;
+                    sc *= ph;
+                    sc2 *= sc;
+                    for (k = 0; k < 3; ++k) {
+                        double sc_ek = sc2 * e[k];
+                        Op[k * 4] += sc + sc_ek * e[k];
+                        for (l = 0; l < k; ++l) Op[k + l * 3] += e[l] * sc_ek;
+                    }
+                    sc = 4 * M_PIF * exp(m_pi_alpha_sq * r_sq);
+                    sc *= ph;
+                    for (k = 0; k < 3; ++k) {
+                        double sc_ek = sc * e[k];
+                        Qp[k * 4] += sc_ek * e[k];
+                        for (l = 0; l < k; ++l) Qp[k + l * 3] += e[l] * sc_ek;
+                    }
+                }
+            }
+        }
+    }
+    for (k = 0; k < 3; ++k) {
+        _tD[k * 4] += preDii * (preO * Op[k * 4] + preQ * Qp[k * 4]);
+        for (l = 0; l < k; ++l) {
+            _tD[k + l * 3] += preDii * (preO * Op[k + l * 3] + preQ * Qp[k + l * 3]);
+            _tD[l + k * 3] += preDii * (preO * Op[k + l * 3] + preQ * Qp[k + l * 3]);
+        }
+    }
+}
+
 void orc_tile(const orc_system* s, int i, int j, double tD[9])
 {
     double preDii, preDij;
@@ -217,6 +339,21 @@ void orc_tile(const orc_system* s, int i, int j, double tD[9])
     if (i == j) {
         if (!s->ewald) {
             tD[0] = tD[4] = tD[8] = preDii / s->coord[4 * i + 3];
+        } else if (s->ewald_method == 0) {
+            /* diff_tensor_calc_ewald_smith_diag (diff_tensor.c:245-263) */
+            double aw = s->coord[4 * i + 3];
+            double il = s->inv_L[0];
+            double sc3;
+            int l;
+            tile_smith(s, preDii, preDij, i, i, tD);
+            sc3 = s->ewald_alpha * aw * il;
+            sc3 = sc3 * sc3 * sc3 * M1_SQRTPI_REF / 3;
+            sc3 = 0.75f * il * 1.5f * s->ewald_alpha * aw * M1_SQRTPI_REF * il + 0.5f * aw * aw * il * il * il * sc3;
+            sc3 *= preDii;
+            for (k = 0; k < 3; ++k) {
+                tD[k * 4] = preDii / aw - sc3 + tD[k * 4];
+                for (l = 0; l < k; ++l) tD[l + 3 * k] = tD[k + 3 * l] = 0;
+            }
         } else {
             /* diff_tensor_calc_ewald_beenakker_diag (diff_tensor.c:404-422) */
             double aw = s->coord[4 * i + 3];
@@ -234,6 +371,8 @@ void orc_tile(const orc_system* s, int i, int j, double tD[9])
         }
     } else if (!s->ewald) {
         tile_free(s, preDii, preDij, i, j, tD);
+    } else if (s->ewald_method == 0) {
+        tile_smith(s, preDii, preDij, i, j, tD);
     } else {
         tile_beenakker(s, preDii, preDij, i, j, tD);
     }

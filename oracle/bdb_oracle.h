@@ -30,8 +30,9 @@ typedef struct {
     int hydro;                  /* 0 none, 1 cholesky, 2 geyer */
     double T, visc, vfactor;
     int ewald;                  /* Ewald-summed tensor (periodic + hydro) */
-    int ewald_method;           /* 1 beenakker (0 smith: not restated) */
+    int ewald_method;           /* 0 smith, 1 beenakker (the reference's EWALD_METHOD_*) */
     int ewald_real;
+    double ewald_alpha;         /* Smith's splitting parameter, in units of 1/L */
     /* non-bonded */
     int elec;
     double epsilon_c, kappa_c, gamma_c, cutoff_c;

@@ -25,7 +25,7 @@ class OrcSystem(C.Structure):
         ("n", C.c_int), ("coord", _dp), ("Q", _dp), ("LJ", _dp),
         ("bc", C.c_int), ("box", C.c_double * 3), ("inv_L", C.c_double * 3),
         ("hydro", C.c_int), ("T", C.c_double), ("visc", C.c_double), ("vfactor", C.c_double),
-        ("ewald", C.c_int), ("ewald_method", C.c_int), ("ewald_real", C.c_int),
+        ("ewald", C.c_int), ("ewald_method", C.c_int), ("ewald_real", C.c_int), ("ewald_alpha", C.c_double),
         ("elec", C.c_int), ("epsilon_c", C.c_double), ("kappa_c", C.c_double),
         ("gamma_c", C.c_double), ("cutoff_c", C.c_double),
         ("alpha_lj", C.c_double), ("cutoff_lj", C.c_double), ("lj_6_term", C.c_int),
@@ -105,6 +105,7 @@ class Oracle:
         s.ewald = deck.ewald
         s.ewald_method = p["ewald_method"]
         s.ewald_real = p["ewald_real"]
+        s.ewald_alpha = p["ewald_alpha"]
         s.elec = p["elec"]
         s.epsilon_c, s.kappa_c, s.gamma_c, s.cutoff_c = p["epsilon_c"], p["kappa_c"], p["gamma_c"], p["cutoff_c"]
         s.alpha_lj, s.cutoff_lj, s.lj_6_term = p["alpha_lj"], p["cutoff_lj"], p["lj_6_term"]

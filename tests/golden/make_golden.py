@@ -54,6 +54,14 @@ CASES = {
     "susp24_ewald": lambda d: decks.write_suspension_deck(d, "c", 24, seed=104, ewald_r=2, phi=0.15,
                                                           extra={"geyer_on_the_fly": "no"}),
     "chain24_bonded": lambda d: bonded_chain(d, "c", 24, 105),
+    # Smith's Ewald sums (diff_tensor.c:102-263): TEA on the stored tensor,
+    # and Cholesky on a dilute suspension (positive definite at R=3)
+    "susp24_smith": lambda d: decks.write_suspension_deck(d, "c", 24, seed=108, ewald_r=2, phi=0.15,
+                                                          extra={"geyer_on_the_fly": "no",
+                                                                 "ewald_method": "smith"}),
+    "susp32_smith_chol": lambda d: decks.write_suspension_deck(d, "c", 32, seed=109, ewald_r=3, phi=0.05,
+                                                               extra={"hydro": "cholesky",
+                                                                      "ewald_method": "smith"}),
     # IGT predictor-corrector (comp_step_IGT_const): two 3N Gaussian draws
     # per step, the predictor's then the corrector's
     "chain24_igt_chol": lambda d: decks.write_chain_deck(d, "c", 24, seed=106, hydro="cholesky",
