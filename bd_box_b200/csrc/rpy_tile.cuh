@@ -41,6 +41,7 @@ struct EwaldConst {
     // products e_a e_b (xx, yy, zz, xy, xz, yz)
     int smith = 0;
     double s_alpha = 0, s_alpha2 = 0, s_alpha3 = 0;
+    float s_rcut_sq = 0.f;   // mixed precision: (4.45/alpha)^2 in units of L^2, erfc(4.45) ~ 3e-10
 };
 
 // 1/sqrt(pi) as the reference's double build spells it (data.h:228)
@@ -76,6 +77,7 @@ inline EwaldConst make_ewald_smith(double L, double inv_L, int R, double alpha)
     e.s_alpha = alpha;
     e.s_alpha2 = alpha * alpha;
     e.s_alpha3 = alpha * e.s_alpha2;
+    e.s_rcut_sq = (float)((4.45 / alpha) * (4.45 / alpha));
     return e;
 }
 
@@ -231,7 +233,12 @@ __device__ __forceinline__ void rpy_ewald_tab(const double4& pi, const double4& 
 }
 
 // diff_tensor_calc_ewald_smith(i, j) (+ _diag for i == j) from the lattice
-// tables, in FP64 in both precisions.
+// tables. The FP64 path keeps every real-space image; with MIXED the
+// real-space images are summed in FP32 (images beyond 4.45/alpha dropped,
+// 2.5 L at the default alpha = sqrt(pi): erfc there is below 3e-10) and the
+// reciprocal phases taken as FP32 cosines of the same argument, both
+// accumulated in FP64.
+template <bool MIXED>
 __device__ __forceinline__ void rpy_smith_tab(const double4& pi, const double4& pj, bool self, double preDii,
                                               double preDij, const EwaldConst& ec, double* t)
 {
@@ -262,7 +269,41 @@ __device__ __forceinline__ void rpy_smith_tab(const double4& pi, const double4& 
     const double a = ec.s_alpha, a2 = ec.s_alpha2, a3 = ec.s_alpha3;
     double O[6] = {0, 0, 0, 0, 0, 0}, Q[6] = {0, 0, 0, 0, 0, 0};
     // real space: images v + m (m from the image table, stored as L m)
-    for (int m = 0; m < ec.nimg; ++m) {
+    if (MIXED) {
+        const float fa = (float)a, fa2 = (float)a2, fa3 = (float)a3, isp = (float)BDB_M1_SQRTPI;
+        const float fx = (float)v0, fy = (float)v1, fz = (float)v2;
+        float o[6] = {0, 0, 0, 0, 0, 0}, qq[6] = {0, 0, 0, 0, 0, 0};
+        for (int m = 0; m < ec.nimg; ++m) {
+            const double4 off = ec.img[m];
+            const float x = fx + (float)rint(off.x * ec.inv_L), y = fy + (float)rint(off.y * ec.inv_L),
+                        z = fz + (float)rint(off.z * ec.inv_L);
+            const float r_sq = x * x + y * y + z * z;
+            if (r_sq == 0.f || r_sq > ec.s_rcut_sq) continue;
+            const float inv_r = rsqrtf(r_sq), r = r_sq * inv_r, inv_r3 = inv_r * inv_r * inv_r;
+            const float e0 = x * inv_r, e1 = y * inv_r, e2 = z * inv_r;
+            const float er = erfcf(r * fa), ex = __expf(-fa2 * r_sq);
+            const float so = er * inv_r, so2 = so + 2.f * fa * isp * ex;
+            const float sq = inv_r3 * (er + 2.f * fa * r * isp * ex);
+            const float sq2 = -3.f * sq - 4.f * fa3 * isp * ex;
+            o[0] += so + so2 * e0 * e0;
+            o[1] += so + so2 * e1 * e1;
+            o[2] += so + so2 * e2 * e2;
+            o[3] += so2 * e0 * e1;
+            o[4] += so2 * e0 * e2;
+            o[5] += so2 * e1 * e2;
+            qq[0] += sq + sq2 * e0 * e0;
+            qq[1] += sq + sq2 * e1 * e1;
+            qq[2] += sq + sq2 * e2 * e2;
+            qq[3] += sq2 * e0 * e1;
+            qq[4] += sq2 * e0 * e2;
+            qq[5] += sq2 * e1 * e2;
+        }
+        for (int k = 0; k < 6; ++k) {
+            O[k] = o[k];
+            Q[k] = qq[k];
+        }
+    }
+    for (int m = 0; !MIXED && m < ec.nimg; ++m) {
         const double4 off = ec.img[m];
         const double x = v0 + rint(off.x * ec.inv_L), y = v1 + rint(off.y * ec.inv_L), z = v2 + rint(off.z * ec.inv_L);
         const double r_sq = x * x + y * y + z * z;
@@ -287,7 +328,9 @@ __device__ __forceinline__ void rpy_smith_tab(const double4& pi, const double4& 
     double Rc[6] = {0, 0, 0, 0, 0, 0};
     for (int k = 0; k < ec.nk; ++k) {
         const double* q = ec.rk + 12 * k;
-        const double cs = cos(ec.two_pif * (v0 * q[0] + v1 * q[1] + v2 * q[2]));
+        const double ph = v0 * q[0] + v1 * q[1] + v2 * q[2];
+        // cos(2 pi_f ph), pi_f the float pi of the reference's constants
+        const double cs = MIXED ? (double)cospif((float)(ph * (ec.two_pif / BDB_PI_D))) : cos(ec.two_pif * ph);
         const double ci = q[3] * cs, ce = (q[4] + sigma_sq * q[5]) * cs;
         for (int c = 0; c < 3; ++c) Rc[c] += ci + ce * q[6 + c];
         for (int c = 3; c < 6; ++c) Rc[c] += ce * q[6 + c];

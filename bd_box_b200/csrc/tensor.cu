@@ -131,7 +131,7 @@ __device__ __forceinline__ void tile_of(const TensorArgs& A, const double4* pos,
     if (A.ewald) {
         double d[6];
         if (A.ec.smith)
-            rpy_smith_tab(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
+            rpy_smith_tab<sizeof(T) == 4>(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
         else
             rpy_ewald_tab<sizeof(T) == 4>(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
         for (int k = 0; k < 6; ++k) t[k] = (T)d[k];

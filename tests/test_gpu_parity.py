@@ -216,3 +216,22 @@ def test_tea_mixed_within_bound(name, request):
     s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
     assert rel(s.compute_Rf(), Rf_o) < 1e-5
     assert rel(s.compute_r(g), Rs_o) < 1e-5
+
+
+def test_smith_mixed_close_to_fp64(deck_dir):
+    """Smith Ewald (diff_tensor.c:102-263) on a periodic suspension with TEA
+    noise: the mixed path (FP64 Smith tiles, FP32 stored/TEA arithmetic)
+    against FP64 on one step with the same noise."""
+    p = decks.write_suspension_deck(deck_dir, "smith_mixed", 200, seed=15, ewald_r=2, phi=0.1,
+                                    extra={"ewald_method": "smith"})
+    deck = decks.read_deck(p)
+    g = gauss(3 * deck.n, 1, seed=16)
+    out = []
+    for prec in (engine.PREC_FP64, engine.PREC_MIXED):
+        s = engine.System(deck, precision=prec, noise=engine.NOISE_HOST)
+        s.step(1, g)
+        out.append(s.get_coord()[:, :3] - deck.coord[:, :3])
+        s.close()
+    box = deck.box[0]
+    d64, dm = [d - box * np.round(d / box) for d in out]
+    assert np.linalg.norm(dm - d64) / np.linalg.norm(d64) < 1e-5
