@@ -142,6 +142,9 @@ struct bdb_system {
     bool factor_valid = false;
     alignas(64) unsigned char tc_map[640];     // CUtensorMaps: TF32 hi / lo panel buffers (x2), FP32 matrix
     bool tc_map_ok = false;
+    alignas(64) unsigned char mv_map[384];     // CUtensorMaps for the stored matvec: FP32 matrix, X, F
+    const void* mv_map_src[3] = {};            // buffers the maps were encoded for
+    int mv_ctas_per_sm = 0;                    // resident CTAs of the TMA matvec kernel per SM
     int sm_count = 148;
     int steps_since_refresh = 0;
 

@@ -41,6 +41,7 @@
 #include <algorithm>
 
 #include "bdb_common.cuh"
+#include "sm100.cuh"
 
 namespace bdb {
 
@@ -52,55 +53,7 @@ static constexpr int BOX_BYTES = PW * KC * 4;     // 16 KB
 static constexpr int STAGE_BYTES = 4 * BOX_BYTES; // A_hi, A_lo, B_hi, B_lo
 static constexpr int C_BOXES = 2;                 // staging ring of 128x32 boxes for the C update
 static constexpr int SYRK_SMEM = STAGES * STAGE_BYTES + C_BOXES * BOX_BYTES + 1024;
-static constexpr uint32_t WAIT_LIMIT = 1u << 22;
 static constexpr int LDS = PW + 1;                // padded FP64 row in shared memory
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-// bounded wait for the phase of the given parity; false on time-out or abort
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort)
-{
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-        if ((it & 1023) == 1023 && *abort) return false;
-    }
-    *abort = 1;
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
 
 // C[tile] += smem tile (FP32 add in L2, no load of C by the SM)
 __device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, uint32_t src, int x, int y)
@@ -783,19 +736,6 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
 }
 
 // ---------------------------------------------------------------- host side
-
-static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        void* p = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
 
 // row-major FP32 [rows][cols] buffer, boxes of 128 rows x 32 columns
 static int make_panel_map(float* buf, int rows, CUtensorMap* map, int cols = PW)

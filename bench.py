@@ -287,8 +287,8 @@ def run_ours(args):
         else:
             bytes_ = 4.0 * n * n
             ach = bytes_ / (mv_avg / 1e3) / 1e9
-            roof = {"kernel": "k_strip_mv (D.F + L.X)", "bound": "hbm", "achieved": ach, "peak": hbm,
-                    "unit": "GB/s", "frac": ach / hbm, "traffic": profile_traffic("strip_mv_n12288"),
+            roof = {"kernel": "k_strip_mv_tma (D.F + L.X)", "bound": "hbm", "achieved": ach, "peak": hbm,
+                    "unit": "GB/s", "frac": ach / hbm, "traffic": profile_traffic("k_strip_mv_tma_n12288"),
                     "peak_source": f"{src} hbm", "ms_per_launch": mv_avg, "share_of_step_time": share_mv}
         roof["phases_ms_per_call"] = {"factor": fac_avg, "build": bld_ms / max(bld_calls, 1),
                                       "matvec": mv_avg, "forces": frc_ms / max(frc_calls, 1)}
@@ -324,7 +324,6 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (stored D/L 604 MB read every step)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches.value),
-            "autotuned": {"matvec_warps_per_sm": sysm.tuning()[1]},
             "clocks": clk.summary(), "fp64_gpu": fp64, "errors": errors, "replicas": reps, "adjoint": adj, "ewald_suspension": ew,
             "smith_suspension": ews,
             "igt": igt,

@@ -196,11 +196,13 @@ int bdb_step_igt_corrector(bdb_system* s, const double* gauss);
 /* Autotuner (no reference counterpart). With autotuning on, the first use
  * of each tunable site times its candidates on the system's stream and
  * keeps the fastest: the TEA tile edge (16 or 32 beads; the matrix-free
- * D.F and TEA noise) and the column segmentation of the stored-matrix
- * product (8, 16 or 32 warps per SM). Different choices sum in different
- * orders, so results can differ at rounding level between tuned runs;
- * bdb_set_tuning pins the values (0 keeps one) and bdb_get_tuning reports
- * them. Off by default (32-bead tiles, 16 warps per SM).
+ * D.F and TEA noise) and the column segmentation of the FP64 stored-matrix
+ * product (8, 16 or 32 warps per SM; the mixed-precision product is a
+ * persistent kernel with one CTA per SM and ignores it). Different choices
+ * sum in different orders, so results can differ at rounding level between
+ * tuned runs; bdb_set_tuning pins the values (0 keeps one) and
+ * bdb_get_tuning reports them. Off by default (32-bead tiles, 16 warps per
+ * SM).
  * Switch it on before the first step. */
 int bdb_autotune(bdb_system* s, int enable);
 int bdb_get_tuning(bdb_system* s, int* tea_tile, int* mv_warps_per_sm);

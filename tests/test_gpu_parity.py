@@ -102,6 +102,28 @@ def test_cholesky_mixed_error(chain_chol):
     assert err <= 1e-5, err
 
 
+@pytest.mark.parametrize("n", [5, 22, 43, 96, 171])
+def test_stored_products_mixed_ragged(n, deck_dir):
+    """The FP32-matrix products (Rf = pre D F from the upper triangle and
+    its transpose, Rs = L X from the lower) at sizes whose 3N cuts the
+    64-row strips and 128-column tiles raggedly: Rf against the same FP32
+    tensor multiplied in FP64 by the oracle (only the summation order
+    differs), Rs against the FP64 factor within the mixed factor's bound."""
+    deck = decks.read_deck(decks.write_chain_deck(deck_dir, f"rag{n}", n, seed=60 + n, hydro="cholesky"))
+    o = pyoracle.Oracle(deck)
+    n3 = 3 * n
+    dt = deck.prm["dt"]
+    s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
+    D32 = s.compute_D()
+    up = np.triu(D32, 1)
+    Dsym = up + up.T + np.diag(np.diag(D32))
+    F, _, _, _ = o.forces()
+    assert rel(s.compute_Rf(), o.df(F, dt, Dsym)) < 1e-11
+    g = gauss(n3, 1, seed=n)
+    L = o.cholesky(o.D())
+    assert rel(s.compute_r(g), L @ (g * np.sqrt(2 * dt))) < 2e-5
+
+
 @pytest.mark.parametrize("name", ["chain_chol", "chain_tea", "chain_none", "susp"])
 def test_df(name, request):
     deck = request.getfixturevalue(name)
