@@ -156,6 +156,11 @@ struct bdb_system {
     // changes (time step, bonded terms)
     cudaGraphExec_t step_graph = nullptr;
     long long graph_launches = 0;
+    // the same for steps with caller Gaussians, for the device copy of them
+    // at the address it captured (the staging buffer's first slot)
+    cudaGraphExec_t step_graph_host = nullptr;
+    const double* step_graph_host_src = nullptr;
+    long long graph_launches_host = 0;
     long long eager_steps = 0;
     cudaGraphExec_t refresh_graph = nullptr;   // tensor build + factorisation (mixed path)
     long long refresh_launches = 0, eager_refreshes = 0;

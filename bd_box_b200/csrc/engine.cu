@@ -214,36 +214,48 @@ void drop_graph(bdb_system* s)
 {
     if (s->step_graph) cudaGraphExecDestroy(s->step_graph);
     s->step_graph = nullptr;
+    if (s->step_graph_host) cudaGraphExecDestroy(s->step_graph_host);
+    s->step_graph_host = nullptr;
+    s->step_graph_host_src = nullptr;
     if (s->refresh_graph) cudaGraphExecDestroy(s->refresh_graph);
     s->refresh_graph = nullptr;
 }
 
-// step_body captured once as a CUDA graph and replayed (device noise only:
-// caller Gaussians change address every step; not while profiling, whose
-// event records would be frozen into the graph)
-static int step_body_graph(bdb_system* s)
+// step_body captured once as a CUDA graph and replayed (not while
+// profiling, whose event records would be frozen into the graph). Device
+// noise has one graph; caller Gaussians have another, which holds the device
+// address of the Gaussians it was captured with and is captured again when a
+// step's Gaussians sit elsewhere (a K-step call walks its staging buffer).
+static int step_body_graph(bdb_system* s, const double* dev_gauss)
 {
-    if (!s->step_graph) {
+    cudaGraphExec_t* exec = dev_gauss ? &s->step_graph_host : &s->step_graph;
+    long long* nl = dev_gauss ? &s->graph_launches_host : &s->graph_launches;
+    if (dev_gauss && *exec && s->step_graph_host_src != dev_gauss) {
+        cudaGraphExecDestroy(*exec);
+        *exec = nullptr;
+    }
+    if (!*exec) {
         const long long before = s->launches;
         BDB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        const int rc = step_body(s, nullptr);
+        const int rc = step_body(s, dev_gauss);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
         if (rc || e != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             return rc ? rc : cuda_fail(e, "cudaStreamEndCapture");
         }
-        const cudaError_t ei = cudaGraphInstantiate(&s->step_graph, g, 0);
+        const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
         cudaGraphDestroy(g);
         if (ei != cudaSuccess) {
-            s->step_graph = nullptr;
+            *exec = nullptr;
             return cuda_fail(ei, "cudaGraphInstantiate");
         }
-        s->graph_launches = s->launches - before;
+        *nl = s->launches - before;
         s->launches = before;
+        if (dev_gauss) s->step_graph_host_src = dev_gauss;
     }
-    BDB_CUDA(cudaGraphLaunch(s->step_graph, s->stream));
-    s->launches += s->graph_launches;
+    BDB_CUDA(cudaGraphLaunch(*exec, s->stream));
+    s->launches += *nl;
     return BDB_OK;
 }
 
@@ -260,7 +272,7 @@ static int one_step(bdb_system* s, const double* dev_gauss)
     }
     // the first step runs eagerly, so that buffers allocated on first use
     // exist (at fixed addresses) before a graph captures them
-    if (s->graphs && !dev_gauss && !s->profiling && s->eager_steps > 0) return step_body_graph(s);
+    if (s->graphs && !s->profiling && s->eager_steps > 0) return step_body_graph(s, dev_gauss);
     s->eager_steps++;
     return step_body(s, dev_gauss);
 }
@@ -626,8 +638,15 @@ int bdb_step(bdb_system* s, int K, const double* gauss)
         BDB_CUDA(cudaMemcpyAsync(s->gbuf.p, gauss, sizeof(double) * need, cudaMemcpyHostToDevice, s->stream));
     }
     BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
+    const bool replay = s->graphs && !s->profiling;
     for (int k = 0; k < K; ++k) {
-        int rc = one_step(s, gauss ? s->gbuf.p + (size_t)k * s->n3 : nullptr);
+        const double* g = gauss ? s->gbuf.p + (size_t)k * s->n3 : nullptr;
+        if (g && k > 0 && replay) {
+            // the step graph reads the first slot (already consumed)
+            BDB_CUDA(cudaMemcpyAsync(s->gbuf.p, g, sizeof(double) * s->n3, cudaMemcpyDeviceToDevice, s->stream));
+            g = s->gbuf.p;
+        }
+        int rc = one_step(s, g);
         if (rc) return rc;
     }
     phase_mark(s, P_STEP);

@@ -39,3 +39,31 @@ def test_graph_replay_matches_eager(hydro, precision, refresh, deck_dir):
     d1 = a[1, :, :3] - a[0, :, :3]
     d2 = a[2, :, :3] - a[1, :, :3]
     assert not np.allclose(d1, d2)
+
+
+@pytest.mark.parametrize("hydro,precision,refresh", [("cholesky", engine.PREC_MIXED, 3),
+                                                     ("geyer", engine.PREC_FP64, 1)])
+def test_host_noise_graph_matches_eager(hydro, precision, refresh, deck_dir):
+    """Steps with caller Gaussians replay their own graph (one-step calls,
+    multi-step calls that stage several steps' Gaussians at once, and a time
+    step change in between) and give the eager run's bits."""
+    deck = decks.read_deck(decks.write_chain_deck(deck_dir, f"gh_{hydro}{precision}", 120, seed=32, hydro=hydro))
+    n3 = 3 * deck.n
+    g = np.random.default_rng(8).standard_normal(12 * n3)
+    runs = []
+    for graphs in (1, 0):
+        s = engine.System(deck, precision=precision, refresh=refresh, noise=engine.NOISE_HOST)
+        s._check(s.lib.bdb_set_graphs(s.h, graphs))
+        out = []
+        for k in range(5):
+            s.step(1, g[k * n3:(k + 1) * n3])
+            out.append(s.get_coord())
+        s.step(3, g[5 * n3:8 * n3])
+        out.append(s.get_coord())
+        s._check(s.lib.bdb_set_dt(s.h, deck.prm["dt"] / 2))
+        s.step(1, g[8 * n3:9 * n3])
+        s.step(3, g[9 * n3:12 * n3])
+        out.append(s.get_coord())
+        runs.append(np.array(out))
+        s.close()
+    assert np.array_equal(runs[0], runs[1])
