@@ -208,10 +208,11 @@ int bdb_autotune(bdb_system* s, int enable);
 int bdb_get_tuning(bdb_system* s, int* tea_tile, int* mv_warps_per_sm);
 int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm);
 
-/* CUDA graphs (no reference counterpart). Mode bit 1: device-noise steps
- * (BDB_NOISE_PHILOX, profiling off) replay the steady part of a step --
- * noise, D.F and the random displacement, the update, the forces -- from a
- * graph captured on the second step. Bit 2: on the mixed path, refreshes of
+/* CUDA graphs (no reference counterpart). Mode bit 1: steps (profiling
+ * off) replay the steady part of a step -- noise, D.F and the random
+ * displacement, the update, the forces -- from a graph captured on the
+ * second step; steps with caller Gaussians use a second graph that reads
+ * them from a fixed device staging slot. Bit 2: on the mixed path, refreshes of
  * D and its factor (tensor build and the two-stream factorisation) replay a
  * graph captured on the second refresh. Default 3 (both); 0 runs
  * everything eagerly. */
