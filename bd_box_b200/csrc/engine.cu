@@ -689,6 +689,28 @@ int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm)
     return BDB_OK;
 }
 
+int bdb_shard_replicas(int nrep, const int* beads, int nshards, int* shard_of)
+{
+    if (nrep < 0 || nshards < 1 || (nrep > 0 && (!beads || !shard_of)))
+        return fail(BDB_ERR_ARG, "bdb_shard_replicas: bad arguments");
+    std::vector<int> order(nrep);
+    for (int k = 0; k < nrep; ++k) {
+        if (beads[k] < 2) return fail(BDB_ERR_ARG, "bdb_shard_replicas: every replica needs at least two beads");
+        order[k] = k;
+    }
+    auto cost = [&](int k) { return (long long)beads[k] * beads[k] + beads[k]; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    std::vector<long long> load(nshards, 0);
+    for (int k : order) {
+        int best = 0;
+        for (int g = 1; g < nshards; ++g)
+            if (load[g] < load[best]) best = g;
+        shard_of[k] = best;
+        load[best] += cost(k);
+    }
+    return BDB_OK;
+}
+
 int bdb_set_graphs(bdb_system* s, int mode)
 {
     if (!s) return fail(BDB_ERR_ARG, "null system");

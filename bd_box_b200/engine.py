@@ -42,7 +42,7 @@ EXPORTS = [
     "bdb_compute_forces", "bdb_compute_D", "bdb_compute_Dij", "bdb_compute_Rf",
     "bdb_compute_r", "bdb_step", "bdb_step_igt", "bdb_step_igt_predictor", "bdb_step_igt_corrector", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_autotune", "bdb_get_tuning",
     "bdb_set_tuning", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
-    "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc",
+    "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc", "bdb_shard_replicas",
 ]
 
 
@@ -115,6 +115,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_stream.restype = C.c_void_p
     lib.bdb_stored_matvec_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.bdb_shard_replicas.argtypes = [C.c_int, _ip, C.c_int, _ip]
     _lib = lib
     return lib
 
@@ -347,6 +348,18 @@ class System:
         out = C.c_longlong()
         self._check(self.lib.bdb_launches(self.h, C.byref(out)))
         return out.value
+
+
+def shard_replicas(beads, nshards: int) -> np.ndarray:
+    """Shard index of every replica (bdb_shard_replicas): N^2 + N cost,
+    longest-processing-time greedy, the same answer on every process."""
+    lib = load_library()
+    b = np.ascontiguousarray(beads, dtype=np.int32)
+    out = np.zeros(b.size, dtype=np.int32)
+    rc = lib.bdb_shard_replicas(b.size, _ip_(b), int(nshards), _ip_(out))
+    if rc:
+        raise BDBError(rc, lib.bdb_last_error().decode())
+    return out
 
 
 def open_deck(prm_path: str, overrides=None, **kw) -> System:

@@ -310,8 +310,10 @@ def run_ours(args):
             k: 1e3 * t / max(c, 1) for k, (t, c) in
             ((k, phase(sysm, k)) for k in ("potrf", "trsm", "syrk_col", "syrk_rest"))}
         reps = None
-        if rank == 0 and world == 1 and not args.skip_replicas:
-            reps = replicas(torch, engine, max(3, args.steps // 5), 3)
+        if not args.skip_replicas:
+            # every rank takes part: with N processes the 256 chains are
+            # sharded over them (bdb_shard_replicas)
+            reps = replicas(torch, engine, max(3, args.steps // 5), 3, dist, rank, world)
         adj = None
         if rank == 0 and world == 1 and not args.skip_adjoint:
             adj = adjoint_case(torch, engine)
@@ -379,47 +381,63 @@ def accuracy(torch, engine, deck):
     return out
 
 
-def replicas(torch, engine, steps, warmup):
+def replicas(torch, engine, steps, warmup, dist=None, rank=0, world=1):
     """Batched-replica workload: 256 independent chains, bead counts uniform
     in [64, 1024] (seeded), chain force field, free-space RPY with TEA noise,
     FP32 tensor with FP64 TEA sums, all in one batch (bdb_create_batch).
-    Aggregate bead-steps/s over `steps` device-noise steps, and the per-replica
-    displacement error of one step against the FP64 batch with the same
-    Gaussians."""
-    from bd_box_b200 import decks
+    Aggregate bead-steps/s over `steps` device-noise steps. With several
+    processes each runs its shard of the chains (bdb_shard_replicas, no
+    collective on the data path) and the time is the slowest rank's
+    (strong scaling: the total work is fixed). On one process, also the
+    per-replica displacement error of one step against the FP64 batch with
+    the same Gaussians."""
+    from bd_box_b200 import decks, ranks
     sizes = decks.replica_sizes()
+    shard = engine.shard_replicas(sizes, world)
+    mine = np.flatnonzero(shard == rank)
     with tempfile.TemporaryDirectory() as d:
-        ds = [decks.read_deck(decks.write_chain_deck(d, f"r{k}", int(n), seed=1000 + k, hydro="geyer"))
-              for k, n in enumerate(sizes)]
-    b = engine.System(ds, precision=engine.PREC_MIXED, noise=engine.NOISE_PHILOX, seed=SEED)
-    b.autotune(True)
-    for _ in range(warmup):
-        b.step(1)
-    ms = time_steps(torch, b, steps)
-    launches = b.launches()
-    tea_tile = b.tuning()[0]
+        ds = [decks.read_deck(decks.write_chain_deck(d, f"r{k}", int(sizes[k]), seed=1000 + int(k), hydro="geyer"))
+              for k in mine]
     total = int(sizes.sum())
-    b.close()
-    g = np.random.default_rng(13).standard_normal(3 * total)
-    bm = engine.System(ds, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
-    b64 = engine.System(ds, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
-    x0 = b64.get_coord()
-    bm.step(1, g)
-    b64.step(1, g)
-    xm, x64 = bm.get_coord(), b64.get_coord()
-    bm.close()
-    b64.close()
-    errs = []
-    for k in range(len(ds)):
-        lo, hi = b64.begins[k], b64.begins[k] + ds[k].n
-        dd = x64[lo:hi, :3] - x0[lo:hi, :3]
-        dm = xm[lo:hi, :3] - x0[lo:hi, :3]
-        errs.append(float(np.linalg.norm(dm - dd) / np.linalg.norm(dd)))
-    return {"workload": f"{len(ds)} chains, beads uniform in [64,1024] (seeded), sum N={total}, "
-                        f"sum N^2={int((sizes.astype(np.int64) ** 2).sum())}, TEA noise, mixed precision, one batch",
-            "metric": "bead-steps/s", "value": total * steps / (ms / 1e3), "steps": steps,
-            "ms_per_step": ms / steps, "gpu_launches": launches, "autotuned_tea_tile": tea_tile,
-            "displacement_rel_vs_fp64": {"max": max(errs), "median": float(np.median(errs))}}
+    ms, launches, tea_tile = 0.0, 0, None
+    if ds:
+        b = engine.System(ds, precision=engine.PREC_MIXED, noise=engine.NOISE_PHILOX,
+                          seed=ranks.replica_seed(SEED, rank))
+        b.autotune(True)
+        for _ in range(warmup):
+            b.step(1)
+        ranks.barrier(dist)
+        ms = time_steps(torch, b, steps)
+        launches = b.launches()
+        tea_tile = b.tuning()[0]
+        b.close()
+    else:
+        ranks.barrier(dist)
+    ms = ranks.max_over_ranks(dist, ms, "cuda")
+    out = {"workload": f"{len(sizes)} chains, beads uniform in [64,1024] (seeded), sum N={total}, "
+                       f"sum N^2={int((sizes.astype(np.int64) ** 2).sum())}, TEA noise, mixed precision, "
+                       + ("one batch" if world == 1 else f"sharded over {world} processes, one batch each"),
+           "metric": "bead-steps/s", "value": total * steps / (ms / 1e3), "steps": steps,
+           "ms_per_step": ms / steps, "gpu_launches": launches, "autotuned_tea_tile": tea_tile,
+           "scaling": "strong", "displacement_rel_vs_fp64": None}
+    if world == 1:
+        g = np.random.default_rng(13).standard_normal(3 * total)
+        bm = engine.System(ds, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
+        b64 = engine.System(ds, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
+        x0 = b64.get_coord()
+        bm.step(1, g)
+        b64.step(1, g)
+        xm, x64 = bm.get_coord(), b64.get_coord()
+        bm.close()
+        b64.close()
+        errs = []
+        for k in range(len(ds)):
+            lo, hi = b64.begins[k], b64.begins[k] + ds[k].n
+            dd = x64[lo:hi, :3] - x0[lo:hi, :3]
+            dm = xm[lo:hi, :3] - x0[lo:hi, :3]
+            errs.append(float(np.linalg.norm(dm - dd) / np.linalg.norm(dd)))
+        out["displacement_rel_vs_fp64"] = {"max": max(errs), "median": float(np.median(errs))}
+    return out
 
 
 def adjoint_case(torch, engine):

@@ -117,6 +117,17 @@ int bdb_destroy(bdb_system* s);   /* free_diff_tensor + free_forces + free_cuda 
 int bdb_create_batch(bdb_system** out, const bdb_params* p, int nseg, const int* counts,
                      const double* coord, const double* Q, const double* LJ);
 
+/* Replicas over processes (one per GPU): shard_of[k] in [0, nshards) for
+ * replica k of beads[k] beads, balancing the per-step cost, taken as N^2
+ * (the tensor tiles, TEA and D.F of a replica) plus N (forces, noise,
+ * update). Longest-processing-time greedy: replicas in decreasing cost
+ * (ties: lower index first) go to the least-loaded shard (ties: lower
+ * shard), so every process computes the same answer without a collective;
+ * the largest load is at most 4/3 of the optimum. Host-only, needs no
+ * device. No reference counterpart: BD_BOX's MPI ranks split the pair
+ * loops of one system (diff_tensor.c:486, calc_func.c:205). */
+int bdb_shard_replicas(int nrep, const int* beads, int nshards, int* shard_of);
+
 /* Bonded terms, BD_BOX's arrays as read by read_str_file (input.c:567-641):
  * bond_pairs int[2B], bond_parms double[3B] (r0, rmax, H) (bond.c:94-111);
  * angle_pairs int[3A], angle_parms double[2A] (phi0 [rad], k) (angle.c:88-100);

@@ -1,9 +1,11 @@
 """The multi-GPU path (independent replicas, one process per GPU) on CPU
 with the gloo backend and world size 2: rendezvous, distinct replica seeds,
-the max-over-ranks of the timed region and a clean shutdown."""
+the max-over-ranks of the timed region, the replica sharder
+(bdb_shard_replicas, host-only) and a clean shutdown."""
 import os
 import socket
 
+import numpy as np
 import pytest
 
 
@@ -22,6 +24,12 @@ def _worker(rank, world, port, out):
     ranks.barrier(dist)
     t = ranks.max_over_ranks(dist, 10.0 + 5.0 * rank)
     seed = ranks.replica_seed(2, r)
+    # every rank shards the same replica list by itself: the answers agree
+    from bd_box_b200 import decks, engine
+    mine = [int(k) for k in np.flatnonzero(engine.shard_replicas(decks.replica_sizes(), w) == r)]
+    gathered = [None] * w
+    dist.all_gather_object(gathered, mine)
+    assert sorted(sum(gathered, [])) == list(range(len(decks.replica_sizes())))
     out.put((r, t, seed))
     ranks.finish(dist)
 
@@ -51,3 +59,34 @@ def test_single_process_needs_no_group():
     assert dist is None and (r, w) == (0, 1)
     assert ranks.max_over_ranks(dist, 3.5) == 3.5
     ranks.finish(dist)
+
+
+def _cost(n):
+    return n.astype(np.int64) ** 2 + n
+
+
+@pytest.mark.parametrize("nshards", [1, 2, 3, 4, 8])
+def test_shard_replicas_balances(nshards):
+    from bd_box_b200 import decks, engine
+    sizes = decks.replica_sizes()
+    sh = engine.shard_replicas(sizes, nshards)
+    assert sh.shape == sizes.shape and sh.min() >= 0 and sh.max() < nshards
+    load = np.bincount(sh, weights=_cost(sizes), minlength=nshards)
+    c = _cost(sizes)
+    # longest-processing-time greedy: within 4/3 of the optimum, which is
+    # at least the mean load and at least the largest replica
+    assert load.max() <= 4 / 3 * max(c.sum() / nshards, c.max()) + 1e-9
+    assert np.array_equal(sh, engine.shard_replicas(sizes, nshards))
+
+
+def test_shard_replicas_small_cases():
+    from bd_box_b200 import engine
+    # decreasing cost to the least-loaded shard, ties to the lower index
+    assert engine.shard_replicas([10, 10, 10, 10], 2).tolist() == [0, 1, 0, 1]
+    assert engine.shard_replicas([100, 3, 3, 3], 2).tolist() == [0, 1, 1, 1]
+    # more shards than replicas: the extra shards stay empty
+    assert engine.shard_replicas([5, 7], 4).tolist() == [1, 0]
+    assert engine.shard_replicas([], 3).size == 0
+    for bad in (([5, 1], 2), ([5, 6], 0)):
+        with pytest.raises(engine.BDBError):
+            engine.shard_replicas(*bad)
