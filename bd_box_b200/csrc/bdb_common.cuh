@@ -43,6 +43,8 @@ enum : unsigned {
 };
 
 // A bead segment: one independent system inside a batch.
+struct FrameRing;   // asynchronous trajectory frames (frames.cu)
+
 struct Segment {
     int begin;     // first bead
     int count;     // beads
@@ -166,6 +168,12 @@ struct bdb_system {
     long long refresh_launches = 0, eager_refreshes = 0;
     bool graphs = true, graph_refresh = true;
 
+    // steps taken (bdb_step, bdb_step_igt), simulated time, and the frame
+    // ring of bdb_frames_start
+    long long step_count = 0;
+    double sim_time = 0;
+    bdb::FrameRing* frames = nullptr;
+
     // measurement: CUDA-event pairs per phase, kernel launch count
     struct PhaseRec {
         std::vector<cudaEvent_t> ev;   // begin/end pairs
@@ -217,6 +225,8 @@ enum Phase {
 void phase_mark(bdb_system* s, int phase);   // records begin/end events when profiling
 void phase_mark_on(bdb_system* s, int phase, cudaStream_t stream);
 void drop_graph(bdb_system* s);              // forget the captured step
+int after_step(bdb_system* s, double dt);     // count a finished step, record a frame when due
+void frames_release(bdb_system* s);           // wait for frame copies in flight, free the ring
 int build_and_factor(bdb_system* s);         // tensor build + factorisation into the stored matrix, eagerly
 int forces_phase(bdb_system* s);             // forces at the current positions (profiled phase)
 int check_status(bdb_system* s, bool* overlap);   // read and decode the status word (synchronises)

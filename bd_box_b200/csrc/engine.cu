@@ -423,6 +423,7 @@ int bdb_destroy(bdb_system* s)
     for (auto e : s->la_ev)
         if (e) cudaEventDestroy(e);
     drop_graph(s);
+    frames_release(s);
     if (s->stream2) cudaStreamDestroy(s->stream2);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -647,6 +648,7 @@ int bdb_step(bdb_system* s, int K, const double* gauss)
             g = s->gbuf.p;
         }
         int rc = one_step(s, g);
+        if (!rc) rc = after_step(s, s->p.dt);
         if (rc) return rc;
     }
     phase_mark(s, P_STEP);

@@ -1,0 +1,182 @@
+// Asynchronous trajectory frames: the positions of every `every`-th step go
+// to a ring of pinned host buffers by cudaMemcpyAsync on the engine's
+// stream, so the step loop (and its graph replays) never waits for output.
+// BD_BOX writes its XYZ/DCD frames from the host copy of coord after each
+// saved step (output.c:64-100, save_output :250-257, called from
+// main_loop.c:97-116); here the host takes finished frames when it likes.
+//
+// A frame whose copy has not finished stays in the ring. When the ring is
+// full, recording a new frame first waits for the oldest one and moves it to
+// a host-side queue, so no frame is ever dropped.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <deque>
+#include <vector>
+
+#include "bdb_common.cuh"
+
+namespace bdb {
+
+struct Frame {
+    long long step;
+    double time;
+    std::vector<double> coord;   // 4n: x, y, z, radius
+};
+
+struct FrameRing {
+    int every = 1, cap = 0;
+    long long start = 0;
+    size_t frame_doubles = 0;
+    double* host = nullptr;      // pinned: cap frames
+    std::vector<cudaEvent_t> ev;
+    std::vector<long long> step;
+    std::vector<double> time;
+    int head = 0, count = 0;     // oldest slot, frames in the ring
+    std::deque<Frame> spill;     // frames moved out of a full ring, oldest first
+};
+
+void frames_release(bdb_system* s)
+{
+    FrameRing* f = s->frames;
+    if (!f) return;
+    for (int k = 0; k < f->count; ++k) cudaEventSynchronize(f->ev[(f->head + k) % f->cap]);
+    for (auto e : f->ev)
+        if (e) cudaEventDestroy(e);
+    if (f->host) cudaFreeHost(f->host);
+    delete f;
+    s->frames = nullptr;
+}
+
+// move the ring's oldest frame to the host-side queue (its copy must be done)
+static int spill_oldest(FrameRing* f)
+{
+    const int slot = f->head;
+    BDB_CUDA(cudaEventSynchronize(f->ev[slot]));
+    Frame fr;
+    fr.step = f->step[slot];
+    fr.time = f->time[slot];
+    fr.coord.assign(f->host + slot * f->frame_doubles, f->host + (slot + 1) * f->frame_doubles);
+    f->spill.push_back(std::move(fr));
+    f->head = (f->head + 1) % f->cap;
+    --f->count;
+    return BDB_OK;
+}
+
+static int record(bdb_system* s)
+{
+    FrameRing* f = s->frames;
+    if (f->count == f->cap) {
+        int rc = spill_oldest(f);
+        if (rc) return rc;
+    }
+    const int slot = (f->head + f->count) % f->cap;
+    BDB_CUDA(cudaMemcpyAsync(f->host + slot * f->frame_doubles, s->pos.p, sizeof(double) * f->frame_doubles,
+                             cudaMemcpyDeviceToHost, s->stream));
+    BDB_CUDA(cudaEventRecord(f->ev[slot], s->stream));
+    f->step[slot] = s->step_count;
+    f->time[slot] = s->sim_time;
+    ++f->count;
+    return BDB_OK;
+}
+
+// after every completed step of bdb_step / bdb_step_igt
+int after_step(bdb_system* s, double dt)
+{
+    ++s->step_count;
+    s->sim_time += dt;
+    FrameRing* f = s->frames;
+    if (!f || (s->step_count - f->start) % f->every) return BDB_OK;
+    return record(s);
+}
+
+}  // namespace bdb
+
+using namespace bdb;
+
+extern "C" {
+
+int bdb_frames_start(bdb_system* s, int every, int capacity)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    if (every < 1 || capacity < 1) return fail(BDB_ERR_ARG, "bdb_frames_start: every and capacity must be >= 1");
+    frames_release(s);
+    FrameRing* f = new FrameRing;
+    s->frames = f;
+    f->every = every;
+    f->cap = capacity;
+    f->start = s->step_count;
+    f->frame_doubles = (size_t)4 * s->n;
+    f->ev.assign(capacity, nullptr);
+    f->step.assign(capacity, 0);
+    f->time.assign(capacity, 0.0);
+    cudaError_t e = cudaMallocHost(&f->host, sizeof(double) * f->frame_doubles * capacity);
+    for (int k = 0; k < capacity && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&f->ev[k], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        frames_release(s);
+        return cuda_fail(e, "bdb_frames_start");
+    }
+    // the starting state is the first frame (main_loop.c:93-97 saves step 0)
+    return record(s);
+}
+
+int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* times, double* coord, int* nframes)
+{
+    if (!s || !nframes || max_frames < 0) return fail(BDB_ERR_ARG, "bad arguments");
+    *nframes = 0;
+    FrameRing* f = s->frames;
+    if (!f) return fail(BDB_ERR_ARG, "bdb_frames_take: frames were not started");
+    if (max_frames > 0 && (!steps || !times || !coord)) return fail(BDB_ERR_ARG, "null output array");
+    // finished frames, oldest first: the queue, then the ring up to the
+    // first copy still in flight
+    const size_t fd = f->frame_doubles;
+    int n = 0;
+    while (n < max_frames && !f->spill.empty()) {
+        Frame& fr = f->spill.front();
+        steps[n] = fr.step;
+        times[n] = fr.time;
+        std::memcpy(coord + n * fd, fr.coord.data(), sizeof(double) * fd);
+        f->spill.pop_front();
+        ++n;
+    }
+    while (n < max_frames && f->count > 0) {
+        const int slot = f->head;
+        const cudaError_t q = cudaEventQuery(f->ev[slot]);
+        if (q == cudaErrorNotReady) break;
+        if (q != cudaSuccess) return cuda_fail(q, "bdb_frames_take");
+        steps[n] = f->step[slot];
+        times[n] = f->time[slot];
+        std::memcpy(coord + n * fd, f->host + slot * fd, sizeof(double) * fd);
+        f->head = (f->head + 1) % f->cap;
+        --f->count;
+        ++n;
+    }
+    *nframes = n;
+    return BDB_OK;
+}
+
+int bdb_frames_pending(bdb_system* s, int* nframes)
+{
+    if (!s || !nframes) return fail(BDB_ERR_ARG, "bad arguments");
+    FrameRing* f = s->frames;
+    *nframes = f ? (int)f->spill.size() + f->count : 0;
+    return BDB_OK;
+}
+
+int bdb_frames_flush(bdb_system* s)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    FrameRing* f = s->frames;
+    if (!f) return BDB_OK;
+    for (int k = 0; k < f->count; ++k) BDB_CUDA(cudaEventSynchronize(f->ev[(f->head + k) % f->cap]));
+    return BDB_OK;
+}
+
+int bdb_frames_stop(bdb_system* s)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    frames_release(s);
+    return BDB_OK;
+}
+
+}  // extern "C"

@@ -250,6 +250,7 @@ extern "C" int bdb_step_igt(bdb_system* s, int K, const double* gauss)
         const double* g2 = gauss ? g1 + s->n3 : nullptr;
         int rc = igt_predictor(s, g1, false, &flags);
         if (!rc) rc = igt_corrector(s, g2);
+        if (!rc) rc = after_step(s, s->p.dt);
         if (rc) return rc;
         bool ov = false;
         rc = check_status(s, &ov);

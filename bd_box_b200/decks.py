@@ -119,6 +119,7 @@ class Deck:
     dihe_parms: np.ndarray     # (Dh, 2) -k*delta, m
     dihe_angle_pairs: np.ndarray
     dihe_angle_parms: np.ndarray  # (Dh, 2) k, theta0 [rad]
+    names: list = field(default_factory=list)   # bead names of the sub lines (output.c writes them)
     box: np.ndarray = field(default_factory=lambda: np.zeros(4))
     inv_L: np.ndarray = field(default_factory=lambda: np.zeros(4))
     ewald: int = 0
@@ -166,7 +167,7 @@ def read_str(path: str):
             if tag == "sub":
                 if len(tok) != 11:
                     raise ValueError("Wrong line in sub")
-                subs.append((int(tok[2]), [float(v) for v in tok[3:11]]))
+                subs.append((int(tok[2]), [float(v) for v in tok[3:11]], tok[1]))
             elif tag == "bond":
                 bonds.append(([int(v) for v in tok[1:3]], [float(v) for v in tok[3:6]]))
             elif tag == "angle":
@@ -220,7 +221,7 @@ def read_deck(prm_path: str, overrides: dict | None = None) -> Deck:
     deck = Deck(prm=prm, coord=coord, Q=Q, LJ=LJ, masses=masses, ids=ids,
                 bond_pairs=bp, bond_parms=bv, angle_pairs=ap, angle_parms=av,
                 angle_cos_pairs=acp, angle_cos_parms=acv, dihe_pairs=dp, dihe_parms=dv,
-                dihe_angle_pairs=dap, dihe_angle_parms=dav)
+                dihe_angle_pairs=dap, dihe_angle_parms=dav, names=[s[2] for s in subs])
     _apply_options(deck)
     _center_coords(deck)
     _to_box(deck)

@@ -43,6 +43,7 @@ EXPORTS = [
     "bdb_compute_r", "bdb_step", "bdb_step_igt", "bdb_step_igt_predictor", "bdb_step_igt_corrector", "bdb_set_graphs", "bdb_set_dt", "bdb_adjoint", "bdb_autotune", "bdb_get_tuning",
     "bdb_set_tuning", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc", "bdb_shard_replicas",
+    "bdb_frames_start", "bdb_frames_take", "bdb_frames_pending", "bdb_frames_flush", "bdb_frames_stop",
 ]
 
 
@@ -116,6 +117,11 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_stored_matvec_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.bdb_shard_replicas.argtypes = [C.c_int, _ip, C.c_int, _ip]
+    lib.bdb_frames_start.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.bdb_frames_take.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), _dp, _dp, _ip]
+    lib.bdb_frames_pending.argtypes = [C.c_void_p, _ip]
+    lib.bdb_frames_flush.argtypes = [C.c_void_p]
+    lib.bdb_frames_stop.argtypes = [C.c_void_p]
     _lib = lib
     return lib
 
@@ -343,6 +349,33 @@ class System:
 
     def reset_stats(self):
         self._check(self.lib.bdb_reset_stats(self.h))
+
+    # asynchronous trajectory frames (bdb_frames_*)
+    def frames_start(self, every: int = 1, capacity: int = 16):
+        self._check(self.lib.bdb_frames_start(self.h, int(every), int(capacity)))
+
+    def frames_pending(self) -> int:
+        out = C.c_int()
+        self._check(self.lib.bdb_frames_pending(self.h, C.byref(out)))
+        return out.value
+
+    def frames_take(self, max_frames: int | None = None, flush: bool = False):
+        """(steps, times, coords (k, N, 4)) of the finished frames, oldest
+        first; with flush, after waiting for every copy in flight."""
+        if flush:
+            self._check(self.lib.bdb_frames_flush(self.h))
+        m = self.frames_pending() if max_frames is None else int(max_frames)
+        steps = np.zeros(max(m, 1), dtype=np.int64)
+        times = np.zeros(max(m, 1))
+        coord = np.zeros((max(m, 1), self.n, 4))
+        got = C.c_int()
+        self._check(self.lib.bdb_frames_take(self.h, m, steps.ctypes.data_as(C.POINTER(C.c_longlong)), _p(times),
+                                             _p(coord), C.byref(got)))
+        k = got.value
+        return steps[:k], times[:k], coord[:k]
+
+    def frames_stop(self):
+        self._check(self.lib.bdb_frames_stop(self.h))
 
     def launches(self) -> int:
         out = C.c_longlong()

@@ -117,6 +117,27 @@ int bdb_destroy(bdb_system* s);   /* free_diff_tensor + free_forces + free_cuda 
 int bdb_create_batch(bdb_system** out, const bdb_params* p, int nseg, const int* counts,
                      const double* coord, const double* Q, const double* LJ);
 
+/* Asynchronous trajectory frames (no reference counterpart; BD_BOX writes
+ * XYZ/DCD frames from the host coord after each saved step, output.c:64-100
+ * and save_output :250-257, which needs the positions on the host every
+ * such step). bdb_frames_start records the current state as a frame, then
+ * the state after every `every`-th step of bdb_step / bdb_step_igt, by an
+ * asynchronous copy into a ring of `capacity` pinned host frames: no step
+ * waits for output. bdb_frames_take hands over up to max_frames finished
+ * frames, oldest first, without blocking: steps[i] (steps since the system
+ * was created), times[i] (simulated time, the sum of dt), coord[4N * i ..]
+ * (x, y, z, radius per bead, BD_BOX's coord layout); *nframes is how many.
+ * When the ring is full, recording the next frame waits for the oldest one
+ * and keeps it on the host, so frames are never dropped. bdb_frames_pending
+ * counts frames not yet taken, finished or not; bdb_frames_flush waits for
+ * every copy in flight; bdb_frames_stop (and bdb_destroy) free the ring,
+ * discarding frames not taken. Starting again discards the old ring. */
+int bdb_frames_start(bdb_system* s, int every, int capacity);
+int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* times, double* coord, int* nframes);
+int bdb_frames_pending(bdb_system* s, int* nframes);
+int bdb_frames_flush(bdb_system* s);
+int bdb_frames_stop(bdb_system* s);
+
 /* Replicas over processes (one per GPU): shard_of[k] in [0, nshards) for
  * replica k of beads[k] beads, balancing the per-step cost, taken as N^2
  * (the tensor tiles, TEA and D.F of a replica) plus N (forces, noise,

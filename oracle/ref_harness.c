@@ -29,6 +29,13 @@
  *           are rebuilt only every R steps, by calling the reference's own
  *           compute_D, my_dpotrf, my_dtrmv, dsymv_ and compute_forces.
  *
+ *   output K
+ *           K steps as main_loop.c:89-116 runs them, with BD_BOX's own output
+ *           code writing the files the deck names (init_save, save_output,
+ *           free_save; output.c:250-311): xyz_filename / dcd_filename with
+ *           their save_*_freq. OUT gets the 4N coordinates at the start and
+ *           after each step.
+ *
  * The Gaussian stream comes from BDB_GAUSS_FILE (oracle/ref_rand_file.c).
  */
 #if HAVE_CONFIG_H
@@ -46,6 +53,7 @@
 #include "input.h"
 #include "main_loop.h"
 #include "math_help.h"
+#include "output.h"
 #include "myblas.h"
 #include "rand_move.h"
 #include "trans.h"
@@ -271,6 +279,21 @@ int main(int argc, char** argv)
                 put(f, coord, (size_t)DIMS1 * size);
             }
         }
+    } else if (strcmp(mode, "output") == 0) {
+        int K = argc > argi && argv[argi][0] != '-' ? atoi(argv[argi++]) : 1;
+        if (compute_forces(NULL, 0.0)) fprintf(stderr, "harness: overlap at start (ignored)\n");
+        init_save();
+        step = 0;
+        save_output();
+        put(f, coord, (size_t)DIMS1 * size);
+        for (step = 1; step <= K; ++step) {
+            save_curr_coord();
+            save_curr_forces();
+            compute_hydro(NULL);
+            save_output();
+            put(f, coord, (size_t)DIMS1 * size);
+        }
+        free_save();
     } else {
         fprintf(stderr, "harness: unknown mode %s\n", mode);
         return 1;
