@@ -8,6 +8,11 @@
 // A frame whose copy has not finished stays in the ring. When the ring is
 // full, recording a new frame first waits for the oldest one and moves it to
 // a host-side queue, so no frame is ever dropped.
+//
+// With energies on, a saved step also runs the energy variant of the force
+// pass at the new positions (the forces it writes are the ones the step
+// already has) and copies E[0..BDB_E_LAST] with the frame: BD_BOX forms E
+// only on the steps it writes to the energy file (main_loop.c:102, 112).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -18,17 +23,22 @@
 
 namespace bdb {
 
+static constexpr int NE = BDB_E_LAST + 1;   // energies per frame
+
 struct Frame {
     long long step;
     double time;
     std::vector<double> coord;   // 4n: x, y, z, radius
+    std::vector<double> E;       // NE, or empty without energies
 };
 
 struct FrameRing {
     int every = 1, cap = 0;
+    bool energy = false;
     long long start = 0;
     size_t frame_doubles = 0;
     double* host = nullptr;      // pinned: cap frames
+    double* host_e = nullptr;    // pinned: cap x NE energies (with energies on)
     std::vector<cudaEvent_t> ev;
     std::vector<long long> step;
     std::vector<double> time;
@@ -44,6 +54,7 @@ void frames_release(bdb_system* s)
     for (auto e : f->ev)
         if (e) cudaEventDestroy(e);
     if (f->host) cudaFreeHost(f->host);
+    if (f->host_e) cudaFreeHost(f->host_e);
     delete f;
     s->frames = nullptr;
 }
@@ -57,6 +68,7 @@ static int spill_oldest(FrameRing* f)
     fr.step = f->step[slot];
     fr.time = f->time[slot];
     fr.coord.assign(f->host + slot * f->frame_doubles, f->host + (slot + 1) * f->frame_doubles);
+    if (f->energy) fr.E.assign(f->host_e + slot * NE, f->host_e + (slot + 1) * NE);
     f->spill.push_back(std::move(fr));
     f->head = (f->head + 1) % f->cap;
     --f->count;
@@ -73,6 +85,13 @@ static int record(bdb_system* s)
     const int slot = (f->head + f->count) % f->cap;
     BDB_CUDA(cudaMemcpyAsync(f->host + slot * f->frame_doubles, s->pos.p, sizeof(double) * f->frame_doubles,
                              cudaMemcpyDeviceToHost, s->stream));
+    if (f->energy) {
+        int rc = forces_run(s, true, false);
+        if (rc) return rc;
+        s->have_forces = true;
+        BDB_CUDA(cudaMemcpyAsync(f->host_e + slot * NE, s->scal.p + 16, sizeof(double) * NE, cudaMemcpyDeviceToHost,
+                                 s->stream));
+    }
     BDB_CUDA(cudaEventRecord(f->ev[slot], s->stream));
     f->step[slot] = s->step_count;
     f->time[slot] = s->sim_time;
@@ -96,7 +115,7 @@ using namespace bdb;
 
 extern "C" {
 
-int bdb_frames_start(bdb_system* s, int every, int capacity)
+int bdb_frames_start(bdb_system* s, int every, int capacity, int with_energy)
 {
     if (!s) return fail(BDB_ERR_ARG, "null system");
     if (every < 1 || capacity < 1) return fail(BDB_ERR_ARG, "bdb_frames_start: every and capacity must be >= 1");
@@ -105,12 +124,14 @@ int bdb_frames_start(bdb_system* s, int every, int capacity)
     s->frames = f;
     f->every = every;
     f->cap = capacity;
+    f->energy = with_energy != 0;
     f->start = s->step_count;
     f->frame_doubles = (size_t)4 * s->n;
     f->ev.assign(capacity, nullptr);
     f->step.assign(capacity, 0);
     f->time.assign(capacity, 0.0);
     cudaError_t e = cudaMallocHost(&f->host, sizeof(double) * f->frame_doubles * capacity);
+    if (e == cudaSuccess && f->energy) e = cudaMallocHost(&f->host_e, sizeof(double) * NE * capacity);
     for (int k = 0; k < capacity && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&f->ev[k], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         frames_release(s);
@@ -120,13 +141,15 @@ int bdb_frames_start(bdb_system* s, int every, int capacity)
     return record(s);
 }
 
-int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* times, double* coord, int* nframes)
+int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* times, double* coord, double* energies,
+                    int* nframes)
 {
     if (!s || !nframes || max_frames < 0) return fail(BDB_ERR_ARG, "bad arguments");
     *nframes = 0;
     FrameRing* f = s->frames;
     if (!f) return fail(BDB_ERR_ARG, "bdb_frames_take: frames were not started");
     if (max_frames > 0 && (!steps || !times || !coord)) return fail(BDB_ERR_ARG, "null output array");
+    const bool want_e = f->energy && energies;
     // finished frames, oldest first: the queue, then the ring up to the
     // first copy still in flight
     const size_t fd = f->frame_doubles;
@@ -136,6 +159,7 @@ int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* tim
         steps[n] = fr.step;
         times[n] = fr.time;
         std::memcpy(coord + n * fd, fr.coord.data(), sizeof(double) * fd);
+        if (want_e) std::memcpy(energies + n * NE, fr.E.data(), sizeof(double) * NE);
         f->spill.pop_front();
         ++n;
     }
@@ -147,6 +171,7 @@ int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* tim
         steps[n] = f->step[slot];
         times[n] = f->time[slot];
         std::memcpy(coord + n * fd, f->host + slot * fd, sizeof(double) * fd);
+        if (want_e) std::memcpy(energies + n * NE, f->host_e + slot * NE, sizeof(double) * NE);
         f->head = (f->head + 1) % f->cap;
         --f->count;
         ++n;

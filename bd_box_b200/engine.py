@@ -117,8 +117,8 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_stored_matvec_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.bdb_shard_replicas.argtypes = [C.c_int, _ip, C.c_int, _ip]
-    lib.bdb_frames_start.argtypes = [C.c_void_p, C.c_int, C.c_int]
-    lib.bdb_frames_take.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), _dp, _dp, _ip]
+    lib.bdb_frames_start.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+    lib.bdb_frames_take.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), _dp, _dp, _dp, _ip]
     lib.bdb_frames_pending.argtypes = [C.c_void_p, _ip]
     lib.bdb_frames_flush.argtypes = [C.c_void_p]
     lib.bdb_frames_stop.argtypes = [C.c_void_p]
@@ -351,8 +351,9 @@ class System:
         self._check(self.lib.bdb_reset_stats(self.h))
 
     # asynchronous trajectory frames (bdb_frames_*)
-    def frames_start(self, every: int = 1, capacity: int = 16):
-        self._check(self.lib.bdb_frames_start(self.h, int(every), int(capacity)))
+    def frames_start(self, every: int = 1, capacity: int = 16, energy: bool = False):
+        self._frames_energy = bool(energy)
+        self._check(self.lib.bdb_frames_start(self.h, int(every), int(capacity), int(bool(energy))))
 
     def frames_pending(self) -> int:
         out = C.c_int()
@@ -360,19 +361,21 @@ class System:
         return out.value
 
     def frames_take(self, max_frames: int | None = None, flush: bool = False):
-        """(steps, times, coords (k, N, 4)) of the finished frames, oldest
-        first; with flush, after waiting for every copy in flight."""
+        """(steps, times, coords (k, N, 4), energies (k, 9) or None) of the
+        finished frames, oldest first; with flush, after waiting for every
+        copy in flight."""
         if flush:
             self._check(self.lib.bdb_frames_flush(self.h))
         m = self.frames_pending() if max_frames is None else int(max_frames)
         steps = np.zeros(max(m, 1), dtype=np.int64)
         times = np.zeros(max(m, 1))
         coord = np.zeros((max(m, 1), self.n, 4))
+        energy = np.zeros((max(m, 1), 9)) if getattr(self, "_frames_energy", False) else None
         got = C.c_int()
         self._check(self.lib.bdb_frames_take(self.h, m, steps.ctypes.data_as(C.POINTER(C.c_longlong)), _p(times),
-                                             _p(coord), C.byref(got)))
+                                             _p(coord), _p(energy), C.byref(got)))
         k = got.value
-        return steps[:k], times[:k], coord[:k]
+        return steps[:k], times[:k], coord[:k], None if energy is None else energy[:k]
 
     def frames_stop(self):
         self._check(self.lib.bdb_frames_stop(self.h))

@@ -6,7 +6,9 @@ System.frames_take (bdb_frames_*), byte for byte as BD_BOX writes them:
   all numbers with C's "%f";
 * DCD (init_dcd, output.c:97-141, and save_dcd :77-95): a CHARMM-style
   header whose frame count is bdsteps / save_dcd_freq, then per frame the
-  x, y and z blocks as float32, each between two 4-byte block sizes.
+  x, y and z blocks as float32, each between two 4-byte block sizes;
+* energies (init_enr :152-156, save_energy :143-150): a header line, then
+  per frame the time, the sum of the terms and the terms, "%15f" and "%15g".
 
 The bytes are pinned against BD_BOX's own output.c by
 tests/test_output_format.py.
@@ -65,6 +67,33 @@ class DCDWriter:
         for k in range(3):
             out += size + c[:, k].astype("<f4").tobytes() + size
         self.f.write(out)
+        self.f.flush()
+
+    def close(self):
+        self.f.close()
+
+
+# ENERGY_TYPE indices (data.h:278-289)
+E_BOND, E_ANGLE, E_ANGLE_COS, E_DIHE, E_DIHE_ANGLE, E_LJ, E_COULOMB = 1, 2, 3, 4, 5, 6, 7
+
+
+class ENRWriter:
+    """init_enr + save_energy. The columns are BD_BOX's, labels included
+    (its DIHE column holds the dihedral-angle term and DIHE_COS the cosine
+    dihedral term)."""
+
+    def __init__(self, path: str):
+        self.f = open(path, "w")
+        self.f.write("#%14s%15s %15s %15s %15s %15s %15s %15s %15s\n" %
+                     ("TIME", "ALL", "BOND", "ANG", "ANG_COS", "DIHE", "DIHE_COS", "LJ", "COULOMB"))
+        self.f.flush()
+
+    def write(self, time: float, E):
+        E = [float(v) for v in E]
+        total = E[E_BOND] + E[E_ANGLE] + E[E_ANGLE_COS] + E[E_DIHE_ANGLE] + E[E_DIHE] + E[E_LJ] + E[E_COULOMB]
+        self.f.write("%15f%15f %15g %15g %15g %15g %15g %15g %15g\n" %
+                     (time, total, E[E_BOND], E[E_ANGLE], E[E_ANGLE_COS], E[E_DIHE_ANGLE], E[E_DIHE], E[E_LJ],
+                      E[E_COULOMB]))
         self.f.flush()
 
     def close(self):

@@ -123,17 +123,22 @@ int bdb_create_batch(bdb_system** out, const bdb_params* p, int nseg, const int*
  * such step). bdb_frames_start records the current state as a frame, then
  * the state after every `every`-th step of bdb_step / bdb_step_igt, by an
  * asynchronous copy into a ring of `capacity` pinned host frames: no step
- * waits for output. bdb_frames_take hands over up to max_frames finished
- * frames, oldest first, without blocking: steps[i] (steps since the system
- * was created), times[i] (simulated time, the sum of dt), coord[4N * i ..]
- * (x, y, z, radius per bead, BD_BOX's coord layout); *nframes is how many.
+ * waits for output. With with_energy, each frame also carries the energies
+ * at its positions (a force pass with energies on each saved step, as BD_BOX
+ * forms E only on the steps it writes, main_loop.c:102-112).
+ * bdb_frames_take hands over up to max_frames finished frames, oldest
+ * first, without blocking: steps[i] (steps since the system was created),
+ * times[i] (simulated time, the sum of dt), coord[4N * i ..] (x, y, z,
+ * radius per bead, BD_BOX's coord layout), energies[(BDB_E_LAST + 1) * i ..]
+ * (may be NULL; ignored without with_energy); *nframes is how many.
  * When the ring is full, recording the next frame waits for the oldest one
  * and keeps it on the host, so frames are never dropped. bdb_frames_pending
  * counts frames not yet taken, finished or not; bdb_frames_flush waits for
  * every copy in flight; bdb_frames_stop (and bdb_destroy) free the ring,
  * discarding frames not taken. Starting again discards the old ring. */
-int bdb_frames_start(bdb_system* s, int every, int capacity);
-int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* times, double* coord, int* nframes);
+int bdb_frames_start(bdb_system* s, int every, int capacity, int with_energy);
+int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* times, double* coord,
+                    double* energies, int* nframes);
 int bdb_frames_pending(bdb_system* s, int* nframes);
 int bdb_frames_flush(bdb_system* s);
 int bdb_frames_stop(bdb_system* s);

@@ -32,9 +32,11 @@
  *   output K
  *           K steps as main_loop.c:89-116 runs them, with BD_BOX's own output
  *           code writing the files the deck names (init_save, save_output,
- *           free_save; output.c:250-311): xyz_filename / dcd_filename with
- *           their save_*_freq. OUT gets the 4N coordinates at the start and
- *           after each step.
+ *           free_save; output.c:250-311): xyz_filename / dcd_filename /
+ *           enr_filename with their save_*_freq, the energies formed on the
+ *           steps the energy file is written (main_loop.c:89, 102, 112). OUT
+ *           gets, at the start and after each step, the 4N coordinates and
+ *           E[0..ENERGY_LAST] (current on the written steps only).
  *
  * The Gaussian stream comes from BDB_GAUSS_FILE (oracle/ref_rand_file.c).
  */
@@ -281,17 +283,20 @@ int main(int argc, char** argv)
         }
     } else if (strcmp(mode, "output") == 0) {
         int K = argc > argi && argv[argi][0] != '-' ? atoi(argv[argi++]) : 1;
-        if (compute_forces(NULL, 0.0)) fprintf(stderr, "harness: overlap at start (ignored)\n");
         init_save();
         step = 0;
+        if (compute_forces(enr_file ? E : NULL, 0.0)) fprintf(stderr, "harness: overlap at start (ignored)\n");
         save_output();
         put(f, coord, (size_t)DIMS1 * size);
+        put(f, E, ENERGY_LAST + 1);
         for (step = 1; step <= K; ++step) {
+            const int comp_E = enr_file && (step % save_enr_freq) == 0;
             save_curr_coord();
             save_curr_forces();
-            compute_hydro(NULL);
+            compute_hydro(comp_E ? E : NULL);
             save_output();
             put(f, coord, (size_t)DIMS1 * size);
+            put(f, E, ENERGY_LAST + 1);
         }
         free_save();
     } else {

@@ -38,7 +38,8 @@ def test_frames_match_trajectory(chain):
         s.step(1)
     s.step(5)                                     # steps 11..15 in one call
     assert s.frames_pending() == 6
-    steps, times, coords = s.frames_take(flush=True)
+    steps, times, coords, energies = s.frames_take(flush=True)
+    assert energies is None
     assert steps.tolist() == [0, 3, 6, 9, 12, 15]
     t = 0.0
     acc = [0.0]
@@ -82,7 +83,29 @@ def test_frames_igt(chain):
     s = engine.System(chain, **kw)
     s.frames_start(every=2, capacity=4)
     s.step_igt(4)
-    steps, _, coords = s.frames_take(flush=True)
+    steps, _, coords, _ = s.frames_take(flush=True)
     assert steps.tolist() == [0, 2, 4]
     assert np.array_equal(coords[1], ref[1]) and np.array_equal(coords[2], ref[3])
+    s.close()
+
+
+def test_frames_with_energies(chain):
+    """Energy frames: E of each saved state equals bdb_compute_forces' E at
+    that state, and the extra energy pass leaves the trajectory unchanged."""
+    kw = dict(precision=engine.PREC_MIXED, refresh=3, noise=engine.NOISE_PHILOX, seed=9)
+    r = engine.System(chain, **kw)
+    ref_x, ref_e = [r.get_coord()], [r.compute_forces()[1]]
+    for _ in range(6):
+        r.step(1)
+        ref_x.append(r.get_coord())
+        ref_e.append(r.compute_forces()[1])
+    r.close()
+    s = engine.System(chain, **kw)
+    s.frames_start(every=2, capacity=2, energy=True)
+    s.step(6)
+    steps, _, coords, energies = s.frames_take(flush=True)
+    assert steps.tolist() == [0, 2, 4, 6]
+    for k, c, e in zip(steps, coords, energies):
+        assert np.array_equal(c, ref_x[k]) and np.array_equal(e, ref_e[k]), k
+    assert np.all(energies[:, [6, 7]] != 0)
     s.close()
