@@ -445,6 +445,8 @@ extern "C" int bdb_adjoint(bdb_system* s, int K, int checkpoint, int npairs, con
         s->p.noise != BDB_NOISE_PHILOX || s->p.bc != 0 || s->segs.size() != 1)
         return fail(BDB_ERR_UNSUPPORTED,
                     "the adjoint needs one free-space system, hydro cholesky, FP64, refresh 1 and device noise");
+    if (s->p.e_ext && s->p.e_type != 0)
+        return fail(BDB_ERR_UNSUPPORTED, "the adjoint takes a constant (DC) external field only");
     if (s->n_angle || s->n_angle_cos || s->n_dihe || s->n_dihe_angle)
         return fail(BDB_ERR_UNSUPPORTED, "the adjoint covers bonds, LJ and Debye-Hueckel terms only");
     for (int p = 0; p < 2 * npairs; ++p)

@@ -232,6 +232,7 @@ int forces_phase(bdb_system* s);             // forces at the current positions 
 int check_status(bdb_system* s, bool* overlap);   // read and decode the status word (synchronises)
 int forces_setup(bdb_system* s);
 int forces_run(bdb_system* s, bool want_energy, bool want_counts);
+int set_force_time(bdb_system* s, double t);   // time of the next force evaluations (time-dependent field only)
 int bonded_setup(bdb_system* s);
 int tensor_build(bdb_system* s);       // stored D into M64/M32 + dD
 int tensor_tile_host(bdb_system* s, int i, int j, double* tD);

@@ -262,7 +262,9 @@ static int step_body_graph(bdb_system* s, const double* dev_gauss)
 static int one_step(bdb_system* s, const double* dev_gauss)
 {
     int rc;
-    if (!s->have_forces && (rc = forces_phase(s))) return rc;
+    if (!s->have_forces) {
+        if ((rc = set_force_time(s, s->sim_time)) || (rc = forces_phase(s))) return rc;
+    }
     if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
         if (!s->factor_valid || s->steps_since_refresh >= std::max(1, s->p.refresh)) {
             rc = refresh_factor(s);
@@ -270,6 +272,8 @@ static int one_step(bdb_system* s, const double* dev_gauss)
         }
         s->steps_since_refresh++;
     }
+    // the forces after the step act at the step's end time (diff_comp.c:161)
+    if ((rc = set_force_time(s, s->sim_time + s->p.dt))) return rc;
     // the first step runs eagerly, so that buffers allocated on first use
     // exist (at fixed addresses) before a graph captures them
     if (s->graphs && !s->profiling && s->eager_steps > 0) return step_body_graph(s, dev_gauss);
@@ -308,8 +312,20 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
         return fail(BDB_ERR_UNSUPPORTED, "batched segments need hydro none or geyer (the stored tensor holds one system)");
     if (p->n <= 1) return fail(BDB_ERR_ARG, "need at least two beads");
     if (p->hydro < 0 || p->hydro > 2) return fail(BDB_ERR_ARG, "hydro must be none, cholesky or geyer");
+    if (p->bc < 0 || p->bc > 2) return fail(BDB_ERR_ARG, "bc must be none, periodic or sphere");
     if (p->bc == 1 && (p->box[0] <= 0 || p->box[1] <= 0 || p->box[2] <= 0))
         return fail(BDB_ERR_ARG, "Wrong box size");
+    if (p->bc == 2) {
+        // iscorrect (trans.c:130-145): every bead inside the sphere
+        const double sr = p->sphere_radius * p->sphere_radius;
+        for (int i = 0; i < p->n; ++i) {
+            const double* c = coord + 4 * i;
+            if (c[0] * c[0] + c[1] * c[1] + c[2] * c[2] > sr) return fail(BDB_ERR_ARG, "Wrong correction");
+        }
+    }
+    if (p->e_ext && (p->e_type < 0 || p->e_type > 2 || p->e_dir1 < 0 || p->e_dir1 > 2 || p->e_dir2 < 0 || p->e_dir2 > 2))
+        return fail(BDB_ERR_ARG, "E_type must be DC, AC or RF and E_dir1/E_dir2 x, y or z");
+    if (p->sboundary && p->sboundary_n < 0) return fail(BDB_ERR_ARG, "sboundary_n must be >= 0");
     if (p->ewald && (p->ewald_real < 0 || p->ewald_real > 5)) return fail(BDB_ERR_ARG, "ewald_real wrong value, only 0..5");
     if (p->ewald && p->ewald_method != BDB_EWALD_BEENAKKER && p->ewald_method != BDB_EWALD_SMITH)
         return fail(BDB_ERR_ARG, "ewald_method must be beenakker or smith");
@@ -517,7 +533,8 @@ int bdb_compute_forces(bdb_system* s, double* F, double* E, long long* counts)
 {
     if (!s) return fail(BDB_ERR_ARG, "null system");
     BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
-    int rc = forces_run(s, E != nullptr, counts != nullptr);
+    int rc = set_force_time(s, s->sim_time);
+    if (!rc) rc = forces_run(s, E != nullptr, counts != nullptr);
     if (rc) return rc;
     if (F) BDB_CUDA(cudaMemcpyAsync(F, s->F.p, sizeof(double) * s->n3, cudaMemcpyDeviceToHost, s->stream));
     if (E) BDB_CUDA(cudaMemcpyAsync(E, s->scal.p + 16, sizeof(double) * (BDB_E_LAST + 1), cudaMemcpyDeviceToHost,
@@ -593,7 +610,7 @@ int bdb_compute_Rf(bdb_system* s, double* Rf)
 {
     if (!s || !Rf) return fail(BDB_ERR_ARG, "null argument");
     int rc;
-    if (!s->have_forces && (rc = forces_run(s, false, false))) return rc;
+    if (!s->have_forces && ((rc = set_force_time(s, s->sim_time)) || (rc = forces_run(s, false, false)))) return rc;
     if (s->p.hydro == BDB_HYDRO_CHOLESKY) {
         if (!s->factor_valid && (rc = refresh_factor(s))) return rc;
         rc = stored_matvec(s, false);
@@ -610,7 +627,7 @@ int bdb_compute_r(bdb_system* s, const double* gauss, double* Rs)
     if (!s || !Rs) return fail(BDB_ERR_ARG, "null argument");
     int rc;
     BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
-    if (!s->have_forces && (rc = forces_run(s, false, false))) return rc;
+    if (!s->have_forces && ((rc = set_force_time(s, s->sim_time)) || (rc = forces_run(s, false, false)))) return rc;
     double* dg = nullptr;
     if (gauss) {
         dg = s->work.p;
@@ -710,6 +727,20 @@ int bdb_shard_replicas(int nrep, const int* beads, int nshards, int* shard_of)
         shard_of[k] = best;
         load[best] += cost(k);
     }
+    return BDB_OK;
+}
+
+int bdb_set_time(bdb_system* s, double t)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    s->sim_time = t;
+    return BDB_OK;
+}
+
+int bdb_get_time(bdb_system* s, double* t)
+{
+    if (!s || !t) return fail(BDB_ERR_ARG, "null argument");
+    *t = s->sim_time;
     return BDB_OK;
 }
 

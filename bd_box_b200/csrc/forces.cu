@@ -728,6 +728,79 @@ __global__ void k_bonded_gather(int n, const int* __restrict__ slot_ptr, const i
     F[3 * i + 2] = f[2];
 }
 
+// External forces per bead, after the bonded terms (bonded_inter,
+// pre_func.c:135-158): the electric field on charged beads
+// (electro_ext_force, electro_ext.c:38-51; DC, AC = cos(w t) on dir1, RF =
+// cos on dir1 and sin on dir2, at the force time t) and the bounding-sphere
+// force (sboundary_ext, sboundary.c:36-73: -A x / (r R^n) beyond the cutoff
+// radius, R = sphere_radius - r; a bead within 1e-6 of the wall flags a
+// retry). No energy term, as in BD_BOX. The force time is a device scalar
+// so that replayed graphs see the current step's time.
+struct ExtArgs {
+    int e_ext, e_type, dir1, dir2;
+    double e_factor, e_magn, e_freq;
+    int sbound, sb_n;
+    double sb_A, sb_cut, sphere_R;
+};
+
+__global__ void k_external(int n, ExtArgs a, const double4* __restrict__ pos, const double* __restrict__ Q,
+                           const double* __restrict__ t_force, double* __restrict__ F, unsigned* __restrict__ status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double f[3] = {F[3 * i], F[3 * i + 1], F[3 * i + 2]};
+    bool bad = false;
+    const double q = Q[i];
+    if (a.e_ext && q != 0.0) {
+        const double base = q * a.e_factor * a.e_magn;
+        if (a.e_type == 0) {
+            f[a.dir1] += base;
+        } else {
+            const double wt = a.e_freq * *t_force;
+            f[a.dir1] += base * cos(wt);
+            if (a.e_type == 2) f[a.dir2] += base * sin(wt);
+        }
+        bad = isnan(f[a.dir1]) || isinf(f[a.dir1]) || (a.e_type == 2 && (isnan(f[a.dir2]) || isinf(f[a.dir2])));
+    }
+    if (a.sbound) {
+        const double4 p = pos[i];
+        const double r = sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
+        if (r >= a.sb_cut) {
+            const double R = a.sphere_R - r;
+            if (R >= 0.000001) {
+                // 1 / (r R^n) by binary powers of 1/R, as sboundary_ext forms it
+                double inr = 1.0 / r, inR = 1.0 / R;
+                for (int b = 1; b <= a.sb_n; b *= 2) {
+                    if (a.sb_n & b) inr *= inR;
+                    inR *= inR;
+                }
+                f[0] -= a.sb_A * p.x * inr;
+                f[1] -= a.sb_A * p.y * inr;
+                f[2] -= a.sb_A * p.z * inr;
+            } else {
+                bad = true;
+            }
+        }
+    }
+    F[3 * i] = f[0];
+    F[3 * i + 1] = f[1];
+    F[3 * i + 2] = f[2];
+    if (bad) atomicOr(status, ST_OVERLAP);
+}
+
+__global__ void k_set_time(double* t_force, double t) { *t_force = t; }
+
+static bool has_external(const bdb_system* s) { return s->p.e_ext || (s->p.sboundary && s->p.bc == 2); }
+
+int set_force_time(bdb_system* s, double t)
+{
+    if (!(s->p.e_ext && s->p.e_type != 0)) return BDB_OK;   // only AC and RF depend on time
+    k_set_time<<<1, 1, 0, s->stream>>>(s->scal.p + 8, t);
+    BDB_CUDA(cudaGetLastError());
+    s->launches += 1;
+    return BDB_OK;
+}
+
 // Energies: E[1..5] from the bonded terms (sums per type), E[6], E[7] from
 // the non-bonded block partials. One CTA, fixed order.
 struct TermRanges {
@@ -918,6 +991,24 @@ int forces_run(bdb_system* s, bool want_energy, bool want_counts)
         BDB_CUDA(cudaMemsetAsync(Fb, 0, sizeof(double) * 3 * s->n, st));
     }
     BDB_CUDA(cudaGetLastError());
+    if (has_external(s)) {
+        ExtArgs a;
+        a.e_ext = s->p.e_ext;
+        a.e_type = s->p.e_type;
+        a.dir1 = s->p.e_dir1;
+        a.dir2 = s->p.e_dir2;
+        a.e_factor = s->p.e_factor;
+        a.e_magn = s->p.e_magn;
+        a.e_freq = s->p.e_freq;
+        a.sbound = s->p.sboundary && s->p.bc == 2;
+        a.sb_n = s->p.sboundary_n;
+        a.sb_A = s->p.sboundary_A;
+        a.sb_cut = s->p.sboundary_cutoff;
+        a.sphere_R = s->p.sphere_radius;
+        k_external<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, a, s->pos.p, s->Q.p, s->scal.p + 8, Fb, s->status.p);
+        BDB_CUDA(cudaGetLastError());
+        s->launches += 1;
+    }
     const int nblk = (s->n * 32 + NB_THREADS - 1) / NB_THREADS;
     k_nonbonded<<<nblk, NB_THREADS, 0, st>>>(make_fp(s), s->n, s->pos.p, s->Q.p, s->LJ.p, s->d_bead_seg.p,
                                              s->d_segs.p, s->cell_range.p, s->cell_off.p, s->sorted_idx.p, s->grid.p,

@@ -130,7 +130,9 @@ static int igt_predictor(bdb_system* s, const double* g1, bool stop_on_overlap, 
     int rc;
     const bool chol = s->p.hydro == BDB_HYDRO_CHOLESKY;
     const size_t v3 = sizeof(double) * s->n3;
-    if (!s->have_forces && (rc = forces_phase(s))) return rc;
+    if (!s->have_forces && ((rc = set_force_time(s, s->sim_time)) || (rc = forces_phase(s)))) return rc;
+    // both force passes of the step act at its end time (diff_equation.c:314, 327)
+    if ((rc = set_force_time(s, s->sim_time + s->p.dt))) return rc;
     // predictor
     if (chol) {
         if ((rc = ensure_matrix(s)) || (rc = ensure_matrix_b(s))) return rc;

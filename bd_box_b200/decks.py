@@ -55,7 +55,8 @@ def _F(x: float) -> float:
 
 # key -> (type, default), defaults from the MAKE_STR_IN declarations
 # (diff_decl.c:65-82, calc_func.c:51-53, LJ.c:31-33, electro.c:30-34,
-#  input.c:60-89, trans.c:33-34, bucket.c:40, rand_move.c:40, main_loop.c:45)
+#  input.c:60-89, trans.c:33-35, bucket.c:40, rand_move.c:40, main_loop.c:45,
+#  electro_ext.c:30-36, sboundary.c:31-34)
 PRM_KEYS = {
     "out_filename": ("STR", None), "dt": ("DOUBLE", 0.0), "visc": ("DOUBLE", 0.01),
     "vfactor": ("DOUBLE", 14.4), "T": ("DOUBLE", _F(298.15)), "epsilon_c": ("DOUBLE", _F(78.54)),
@@ -67,7 +68,7 @@ PRM_KEYS = {
     "hydro": ("HYDRO", 0), "algorithm": ("ALGORITHM", 2), "str_filename": ("STR", None),
     "xyz_filename": ("STR", None), "dcd_filename": ("STR", None), "enr_filename": ("STR", None),
     "rst_filename": ("STR", None), "pqr_filename": ("STR", None), "rand_seed": ("INT", 12345),
-    "E_ext": ("YESNO", 0), "E_magn": ("DOUBLE", 0.0), "E_type": ("STR", "DC"),
+    "E_ext": ("YESNO", 0), "E_magn": ("DOUBLE", 1.0), "E_type": ("STR", "DC"),
     "E_freq": ("DOUBLE", 0.0), "E_dir1": ("STR", "x"), "E_dir2": ("STR", "y"),
     "E_factor": ("DOUBLE", 1.0), "bc": ("BC", 1), "sphere_radius": ("DOUBLE", 0.0),
     "bond_lj_scale": ("DOUBLE", 1.0), "bond_c_scale": ("DOUBLE", 1.0), "restart": ("STR", None),
@@ -76,7 +77,7 @@ PRM_KEYS = {
     "ewald_method": ("EWALD", 0), "MPI_nprow": ("INT", 0), "MPI_npcol": ("INT", 0),
     "MPI_block": ("INT", 0), "cuda_devices": ("STR", None), "e_collision": ("DOUBLE", 1.0),
     "single_point": ("STR", None), "nb_list": ("NB", 0), "sboundary": ("YESNO", 0),
-    "sboundary_A": ("DOUBLE", 0.0), "sboundary_n": ("INT", 0), "sboundary_cutoff": ("DOUBLE", 0.0),
+    "sboundary_A": ("DOUBLE", 1.0), "sboundary_n": ("INT", 2), "sboundary_cutoff": ("DOUBLE", 0.0),
     "check_overlap": ("YESNO", 1), "geyer_on_the_fly": ("YESNO", 1), "cuda_block": ("INT", 0),
 }
 _ENUMS = {"HYDRO": HYDRO, "ALGORITHM": ALGORITHM, "BC": BC, "NB": NB_LIST, "EWALD": EWALD_METHOD}
@@ -268,6 +269,11 @@ def _center_coords(d: Deck) -> None:
             raise ValueError("Particles don't fit in the box")
     # same summation order as the C loop: coord += (0 - g)
     d.coord[:, :3] += (0.0 - g)[None, :]
+    if d.prm["bc"] == BC["sphere"]:
+        # iscorrect (trans.c:130-145): every bead inside the sphere
+        sq = d.coord[:, 0] * d.coord[:, 0] + d.coord[:, 1] * d.coord[:, 1] + d.coord[:, 2] * d.coord[:, 2]
+        if np.any(sq > d.prm["sphere_radius"] * d.prm["sphere_radius"]):
+            raise ValueError("Wrong correction")
 
 
 def _to_box(d: Deck) -> None:

@@ -148,8 +148,6 @@ static void check_supported(void)
         UNERR("bdb200: the IGT algorithms need hydro none or cholesky")
     if (hydro != DIFF_NONE && hydro != DIFF_CHOLESKY && hydro != DIFF_GEYER)
         UNERR("bdb200: hydro must be none, cholesky or geyer")
-    if (bc == BC_SPHERE) UNERR("bdb200: sphere boundary conditions are not available")
-    if (E_ext) UNERR("bdb200: external electric fields are not available")
     if (vel_grad_tensor) UNERR("bdb200: velocity-gradient flows are not available")
 }
 
@@ -158,7 +156,7 @@ static void make_params(bdb_params* p)
     const char* r = getenv("BDB_REFRESH");
     memset(p, 0, sizeof *p);
     p->n = size;
-    p->bc = bc == BC_BOX ? 1 : 0;
+    p->bc = bc == BC_BOX ? 1 : (bc == BC_SPHERE ? 2 : 0);
     p->box[0] = box[0];
     p->box[1] = box[1];
     p->box[2] = box[2];
@@ -184,6 +182,19 @@ static void make_params(bdb_params* p)
     p->check_overlap = check_overlap;
     p->nb_list = nb_list;
     p->max_force_cutoff = max_force_cutoff;
+    /* external forces (pre_func.c:135-158) */
+    p->e_ext = E_ext;
+    p->e_type = E_type;
+    p->e_dir1 = E_dir1 - 'x';
+    p->e_dir2 = E_dir2 - 'x';
+    p->e_factor = E_factor;
+    p->e_magn = E_magn;
+    p->e_freq = E_freq;
+    p->sboundary = sboundary;
+    p->sboundary_n = sboundary_n;
+    p->sboundary_A = sboundary_A;
+    p->sboundary_cutoff = sboundary_cutoff;
+    p->sphere_radius = sphere_radius;
     p->precision = env_choice("BDB_PRECISION", "fp64", "mixed", 0) ? BDB_PREC_MIXED : BDB_PREC_FP64;
     p->refresh = r && atoi(r) > 0 ? atoi(r) : 1;
     p->noise = g_noise_host ? BDB_NOISE_HOST : BDB_NOISE_PHILOX;
@@ -259,8 +270,8 @@ void free_forces(void)
 INT compute_forces(DOUBLE* _E, DOUBLE t)
 {
     int rc;
-    (void)t;
     push_coord();
+    CHK(bdb_set_time(g_sys, t));   /* the time-dependent field acts at t */
     rc = bdb_compute_forces(g_sys, F[0], _E, NULL);
     if (rc < 0) fatal("bdb_compute_forces", rc);
     return rc;
@@ -417,6 +428,7 @@ static int attempt(void)
 {
     int rc;
     set_dt();
+    CHK(bdb_set_time(g_sys, curr_time));   /* BD_BOX's clock; a retried step starts from it again */
     if (g_noise_host) gauss_rand(X, DIMS0 * size);
     rc = bdb_step(g_sys, 1, g_noise_host ? X : NULL);
     if (rc < 0) fatal("bdb_step", rc);
@@ -488,6 +500,7 @@ INT compute_hydro_IGT(DOUBLE* _E)
     engine();
     push_coord();
     set_dt();
+    CHK(bdb_set_time(g_sys, curr_time));
     if (g_noise_host) gauss_rand(X, DIMS0 * size);
     rc = bdb_step_igt_predictor(g_sys, g_noise_host ? X : NULL);
     if (rc < 0) fatal("bdb_step_igt_predictor", rc);

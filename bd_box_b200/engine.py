@@ -44,6 +44,7 @@ EXPORTS = [
     "bdb_set_tuning", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc", "bdb_shard_replicas",
     "bdb_frames_start", "bdb_frames_take", "bdb_frames_pending", "bdb_frames_flush", "bdb_frames_stop",
+    "bdb_set_time", "bdb_get_time",
 ]
 
 
@@ -65,6 +66,10 @@ class Params(C.Structure):
         ("check_overlap", C.c_int), ("nb_list", C.c_int), ("max_force_cutoff", C.c_double),
         ("precision", C.c_int), ("refresh", C.c_int), ("noise", C.c_int), ("seed", C.c_uint64),
         ("ewald_method", C.c_int), ("ewald_alpha", C.c_double),
+        ("e_ext", C.c_int), ("e_type", C.c_int), ("e_dir1", C.c_int), ("e_dir2", C.c_int),
+        ("e_factor", C.c_double), ("e_magn", C.c_double), ("e_freq", C.c_double),
+        ("sboundary", C.c_int), ("sboundary_n", C.c_int), ("sboundary_A", C.c_double),
+        ("sboundary_cutoff", C.c_double), ("sphere_radius", C.c_double),
     ]
 
 
@@ -121,6 +126,8 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_frames_take.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), _dp, _dp, _dp, _ip]
     lib.bdb_frames_pending.argtypes = [C.c_void_p, _ip]
     lib.bdb_frames_flush.argtypes = [C.c_void_p]
+    lib.bdb_set_time.argtypes = [C.c_void_p, C.c_double]
+    lib.bdb_get_time.argtypes = [C.c_void_p, _dp]
     lib.bdb_frames_stop.argtypes = [C.c_void_p]
     _lib = lib
     return lib
@@ -138,7 +145,7 @@ def params_from_deck(deck, precision=PREC_FP64, refresh=1, noise=NOISE_PHILOX, s
     p = deck.prm
     P = Params()
     P.n = deck.n
-    P.bc = 1 if p["bc"] == 1 else 0
+    P.bc = p["bc"]
     for k in range(3):
         P.box[k] = deck.box[k]
     P.hydro = p["hydro"]
@@ -160,6 +167,13 @@ def params_from_deck(deck, precision=PREC_FP64, refresh=1, noise=NOISE_PHILOX, s
     P.refresh = refresh
     P.noise = noise
     P.seed = p["rand_seed"] if seed is None else seed
+    P.e_ext = p["E_ext"]
+    P.e_type = {"DC": 0, "AC": 1, "RF": 2}[p["E_type"]]
+    P.e_dir1, P.e_dir2 = "xyz".index(p["E_dir1"][0]), "xyz".index(p["E_dir2"][0])
+    P.e_factor, P.e_magn, P.e_freq = p["E_factor"], p["E_magn"], p["E_freq"]
+    P.sboundary, P.sboundary_n = p["sboundary"], p["sboundary_n"]
+    P.sboundary_A, P.sboundary_cutoff = p["sboundary_A"], p["sboundary_cutoff"]
+    P.sphere_radius = p["sphere_radius"]
     return P
 
 
@@ -349,6 +363,14 @@ class System:
 
     def reset_stats(self):
         self._check(self.lib.bdb_reset_stats(self.h))
+
+    def set_time(self, t: float):
+        self._check(self.lib.bdb_set_time(self.h, float(t)))
+
+    def get_time(self) -> float:
+        out = C.c_double()
+        self._check(self.lib.bdb_get_time(self.h, C.byref(out)))
+        return out.value
 
     # asynchronous trajectory frames (bdb_frames_*)
     def frames_start(self, every: int = 1, capacity: int = 16, energy: bool = False):

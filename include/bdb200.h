@@ -69,7 +69,7 @@ enum {
  * float rounding of DOUBLE keys, input.c:1010-1013) plus engine choices. */
 typedef struct {
     int n;                    /* beads */
-    int bc;                   /* 0 none, 1 periodic box (trans.h:43-63) */
+    int bc;                   /* 0 none, 1 periodic box, 2 sphere (trans.h:43-63) */
     double box[3];            /* xbox, ybox, zbox */
     int hydro;                /* BDB_HYDRO_* */
     int ewald;                /* 1: Ewald-summed tensor (periodic, hydro != none), see ewald_method */
@@ -90,6 +90,16 @@ typedef struct {
     uint64_t seed;            /* Philox key */
     int ewald_method;         /* BDB_EWALD_* (after the engine choices, so that zeroed structs mean Beenakker) */
     double ewald_alpha;       /* Smith's splitting parameter in units of 1/L (ewald_alpha; <= 0: sqrt(pi)) */
+    /* external forces, added per bead after the bonded terms (bonded_inter,
+     * pre_func.c:135-158); zeroed structs switch them off */
+    int e_ext;                /* E_ext: field on charged beads (electro_ext_force, electro_ext.c:38-51) */
+    int e_type;               /* E_type: 0 DC, 1 AC (cos), 2 RF (cos on e_dir1, sin on e_dir2) */
+    int e_dir1, e_dir2;       /* E_dir1, E_dir2: 0 x, 1 y, 2 z */
+    double e_factor, e_magn, e_freq;   /* E_factor, E_magn, E_freq */
+    int sboundary;            /* bounding-sphere force, bc 2 only (sboundary_ext, sboundary.c:36-73) */
+    int sboundary_n;          /* sboundary_n >= 0 */
+    double sboundary_A, sboundary_cutoff;
+    double sphere_radius;     /* bc 2: the reflective sphere around the origin (trans.c:35) */
 } bdb_params;
 
 typedef struct bdb_system bdb_system;
@@ -142,6 +152,13 @@ int bdb_frames_take(bdb_system* s, int max_frames, long long* steps, double* tim
 int bdb_frames_pending(bdb_system* s, int* nframes);
 int bdb_frames_flush(bdb_system* s);
 int bdb_frames_stop(bdb_system* s);
+
+/* Simulated time of the current state (curr_time, main_loop.c:47): the
+ * time-dependent field (E_type AC, RF) acts at curr_time + dt on the forces
+ * after a step (diff_comp.c:161). Steps advance it by dt; a host that keeps
+ * its own clock (a restart, BD_BOX's curr_time) sets it here. */
+int bdb_set_time(bdb_system* s, double t);
+int bdb_get_time(bdb_system* s, double* t);
 
 /* Replicas over processes (one per GPU): shard_of[k] in [0, nshards) for
  * replica k of beads[k] beads, balancing the per-step cost, taken as N^2

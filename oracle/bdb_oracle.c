@@ -952,6 +952,47 @@ static int dihe_angle_calc(const orc_system* s, int pos, double* F, double* E)
     return r || bad(k_theta) || (E ? bad(E[ORC_E_DIHE_ANGLE]) : 0);
 }
 
+/* electro_ext_force (electro_ext.c:38-51): Q * E_factor * E_magn on E_dir1,
+ * times cos(E_freq t) for AC and RF, plus the sin part on E_dir2 for RF */
+static int electro_ext_force(const orc_system* s, double Q, double* F)
+{
+    int pos = s->e_dir1, pos2 = 0;
+    switch (s->e_type) {
+        case 0: F[pos] += Q * s->e_factor * s->e_magn; break;
+        case 1: F[pos] += Q * s->e_factor * s->e_magn * cos(s->e_freq * s->t); break;
+        case 2:
+            pos2 = s->e_dir2;
+            F[pos] += Q * s->e_factor * s->e_magn * cos(s->e_freq * s->t);
+            F[pos2] += Q * s->e_factor * s->e_magn * sin(s->e_freq * s->t);
+            break;
+    }
+    return isnan(F[pos]) || isinf(F[pos]) || (s->e_type == 2 && (isnan(F[pos2]) || isinf(F[pos2])));
+}
+
+/* sboundary_ext (sboundary.c:36-73): -A x / (r R^n), R = sphere_radius - r,
+ * beyond the cutoff radius; 1 (retry) within 1e-6 of the wall */
+static int sboundary_ext(const orc_system* s, const double* c, double* F)
+{
+    double r = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    if (r >= s->sboundary_cutoff) {
+        double R = s->sphere_radius - r;
+        if (R >= 0.000001) {
+            double inr = 1.0f / r, inR = 1.0f / R;
+            int i;
+            for (i = 1; i <= s->sboundary_n; i *= 2) {
+                if (s->sboundary_n & i) inr *= inR;
+                inR *= inR;
+            }
+            F[0] -= s->sboundary_A * c[0] * inr;
+            F[1] -= s->sboundary_A * c[1] * inr;
+            F[2] -= s->sboundary_A * c[2] * inr;
+            return 0;
+        }
+        return 1;
+    }
+    return 0;
+}
+
 int orc_forces(const orc_system* s, double* F, double* E, long long counts[2])
 {
     int i, j, rep = 0, r;
@@ -968,6 +1009,11 @@ int orc_forces(const orc_system* s, double* F, double* E, long long counts[2])
     }
     for (i = 0; i < s->n_dihe; ++i) rep |= dihe_calc(s, i, F, E);
     for (i = 0; i < s->n_dihe_angle; ++i) rep |= dihe_angle_calc(s, i, F, E);
+    if (s->e_ext)
+        for (i = 0; i < s->n; ++i)
+            if (s->Q[i] != 0.0) rep |= electro_ext_force(s, s->Q[i], F + 3 * i);
+    if (s->sboundary && s->bc == 2)
+        for (i = 0; i < s->n; ++i) rep |= sboundary_ext(s, s->coord + 4 * i, F + 3 * i);
     /* brute_force_val (calc_func.c:188-228) */
     if (s->elec || s->alpha_lj != 0.0) {
         for (i = 0; i < s->n; ++i)
@@ -1029,6 +1075,8 @@ int orc_run_steps(orc_system* s, double* coord, double* F, double dt, int K, con
                 for (k = 0; k < 3; ++k)
                     coord[4 * i + k] -= s->box[k] * floor(coord[4 * i + k] * s->inv_L[k] + 0.5f);
         }
+        /* forces at curr_time + curr_dt, then curr_time += dt (diff_comp.c:161, 216) */
+        s->t = s->t + dt;
         rep |= orc_forces(s, F, NULL, NULL);
         if (traj) memcpy(traj + (size_t)step * 4 * s->n, coord, sizeof(double) * 4 * s->n);
     }
@@ -1094,7 +1142,10 @@ int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K,
             if (s->bc == 1)
                 for (k = 0; k < 3; ++k) cp[4 * i + k] -= s->box[k] * floor(cp[4 * i + k] * s->inv_L[k] + 0.5f);
         }
-        /* forces and D(r') F' at the predicted positions */
+        /* forces and D(r') F' at the predicted positions, at curr_time +
+         * curr_dt like the forces after the step (diff_equation.c:314, 327) */
+        const double t0 = s->t;
+        s->t = t0 + dt;
         s->coord = cp;
         if (orc_forces(s, Fp, NULL, NULL)) rep |= 1;
         if (s->hydro == 1) {

@@ -46,6 +46,13 @@ typedef struct {
     int n_angle_cos;   const int* angle_cos_pairs;  const double* angle_cos_parms;  /* (cos phi0, k) */
     int n_dihe;        const int* dihe_pairs;       const double* dihe_parms;       /* (-k delta, m) */
     int n_dihe_angle;  const int* dihe_angle_pairs; const double* dihe_angle_parms; /* (k, theta0) */
+    /* external forces (pre_func.c:135-158): electro_ext_force
+     * (electro_ext.c:38-51) and sboundary_ext (sboundary.c:36-73, bc 2) */
+    int e_ext, e_type, e_dir1, e_dir2;   /* E_type 0 DC, 1 AC, 2 RF; dirs 0..2 */
+    double e_factor, e_magn, e_freq;
+    int sboundary, sboundary_n;
+    double sboundary_A, sboundary_cutoff, sphere_radius;
+    double t;                   /* time of the state: forces act at t (curr_time + curr_dt after a step) */
 } orc_system;
 
 /* ENERGY_TYPE indices (data.h:278-289); energy arrays hold 9 doubles. */
@@ -92,7 +99,8 @@ void orc_tea(const orc_system* s, const double* D, const double* gauss, double d
 int orc_forces(const orc_system* s, double* F, double* E, long long counts[2]);
 
 /* K Ermak-McCammon steps (compute_hydro_ermak, diff_equation.c:216-286, and
- * comp_step_ermak, diff_comp.c:152-179) from coord (updated in place).
+ * comp_step_ermak, diff_comp.c:152-179) from coord (updated in place); s->t
+ * is the starting time and advances by dt per step (diff_comp.c:216).
  * gauss: K*3N Gaussians. refresh: rebuild D and its factor every `refresh`
  * steps (1 = every step, the reference schedule). F: 3N forces at the start
  * (updated). traj (nullable): 4N coords after each step. Returns the OR of

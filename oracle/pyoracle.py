@@ -35,6 +35,11 @@ class OrcSystem(C.Structure):
         ("n_angle_cos", C.c_int), ("angle_cos_pairs", _ip), ("angle_cos_parms", _dp),
         ("n_dihe", C.c_int), ("dihe_pairs", _ip), ("dihe_parms", _dp),
         ("n_dihe_angle", C.c_int), ("dihe_angle_pairs", _ip), ("dihe_angle_parms", _dp),
+        ("e_ext", C.c_int), ("e_type", C.c_int), ("e_dir1", C.c_int), ("e_dir2", C.c_int),
+        ("e_factor", C.c_double), ("e_magn", C.c_double), ("e_freq", C.c_double),
+        ("sboundary", C.c_int), ("sboundary_n", C.c_int),
+        ("sboundary_A", C.c_double), ("sboundary_cutoff", C.c_double), ("sphere_radius", C.c_double),
+        ("t", C.c_double),
     ]
 
 
@@ -96,7 +101,15 @@ class Oracle:
         s.coord = _p(self.coord)
         s.Q = _p(arr(deck.Q, np.float64))
         s.LJ = _p(arr(deck.LJ, np.float64))
-        s.bc = 1 if p["bc"] == 1 else 0
+        s.bc = p["bc"]
+        s.e_ext = p["E_ext"]
+        s.e_type = {"DC": 0, "AC": 1, "RF": 2}[p["E_type"]]
+        s.e_dir1, s.e_dir2 = "xyz".index(p["E_dir1"][0]), "xyz".index(p["E_dir2"][0])
+        s.e_factor, s.e_magn, s.e_freq = p["E_factor"], p["E_magn"], p["E_freq"]
+        s.sboundary, s.sboundary_n = p["sboundary"], p["sboundary_n"]
+        s.sboundary_A, s.sboundary_cutoff = p["sboundary_A"], p["sboundary_cutoff"]
+        s.sphere_radius = p["sphere_radius"]
+        s.t = 0.0
         for k in range(3):
             s.box[k] = deck.box[k]
             s.inv_L[k] = deck.inv_L[k]

@@ -125,3 +125,33 @@ def test_stock_main_program_matches_cpu_build(case, tmp_path):
     assert np.abs(xc - xb).max() <= 2e-6          # xyz prints 6 decimals
     assert ec.size == eb.size and ec.size > 0
     assert np.allclose(eb, ec, rtol=1e-5, atol=2e-6)
+
+
+@pytest.mark.parametrize("name", ["rf", "sphere"])
+def test_dropin_external_forces_match_cpu_build(name, tmp_path):
+    """Electric field and bounding sphere through the drop-in: BD_BOX's own
+    compute_forces / compute_hydro callers (harness modes) on the drop-in
+    against the same harness on the CPU build."""
+    need(HARNESS)
+    cpu = os.path.join(REF, "ref_harness")
+    need(cpu)
+    from test_oracle_pin import ext_deck
+    p = ext_deck(tmp_path, name)
+    os.replace(p, os.path.join(tmp_path, "c.prm"))
+    deck = decks.read_deck(os.path.join(tmp_path, "c.prm"))
+    n3 = 3 * deck.n
+    np.random.default_rng(6).standard_normal(8 * n3).tofile(tmp_path / "g.bin")
+    d = str(tmp_path)
+    e = dict(os.environ, BDB_GAUSS_FILE=os.path.join(d, "g.bin"), OMP_NUM_THREADS="1")
+    ref = {}
+    for mode, args in (("forces", []), ("steps", ["3"])):
+        r = subprocess.run([cpu, "c.prm", mode, os.path.join(d, "ref.bin"), *args], cwd=d, env=e,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        ref[mode] = np.fromfile(os.path.join(d, "ref.bin"))
+    f = run(d, "forces")
+    assert rel(f[:n3], ref["forces"][:n3]) < 1e-12 and f[n3 + 9] == ref["forces"][n3 + 9]
+    traj = run(d, "steps", "3").reshape(3, deck.n, 4)
+    traj_ref = ref["steps"].reshape(3, deck.n, 4)
+    disp = np.abs(traj_ref[0, :, :3] - deck.coord[:, :3]).max()
+    assert np.abs(traj - traj_ref).max() <= 1e-9 * disp

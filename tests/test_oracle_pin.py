@@ -84,3 +84,49 @@ def test_oracle_detects_a_planted_error():
     deck, ref = golden_cases.load("chain32_chol")
     deck.coord[3, 3] *= 1.0001   # perturb one hydrodynamic radius
     assert rel(pyoracle.Oracle(deck).D(), ref["D"]) > 1e-8
+
+
+EXT_DECKS = {
+    # time-dependent RF field on the charges (cos on x, sin on z)
+    "rf": dict(E_ext="yes", E_type="RF", E_freq=3.0, E_magn=0.7, E_factor=1.3, E_dir1="x", E_dir2="z"),
+    # AC field on y without hydrodynamic interactions
+    "ac": dict(E_ext="yes", E_type="AC", E_freq=5.0, E_magn=0.4, E_dir1="y"),
+    # bounding sphere: bc sphere with the wall force on beads beyond 6 A
+    "sphere": dict(bc="sphere", sphere_radius=40.0, sboundary="yes", sboundary_A=50.0, sboundary_n=2,
+                   sboundary_cutoff=6.0),
+}
+
+
+def ext_deck(tmp_path, name, n=24, hydro="geyer"):
+    extra = dict(EXT_DECKS[name])
+    return decks.write_chain_deck(str(tmp_path), name, n, seed=91, hydro=hydro if name != "ac" else "none",
+                                  extra=extra)
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("name", sorted(EXT_DECKS))
+def test_oracle_external_forces_match_reference(tmp_path, name):
+    """Electric field (DC/AC/RF at the step's force time) and bounding-sphere
+    forces: the oracle's forces at the start and three steps against BD_BOX's
+    own compute_forces / compute_hydro run by the harness."""
+    p = ext_deck(tmp_path, name)
+    deck = decks.read_deck(p)
+    n3 = 3 * deck.n
+    g = np.random.default_rng(2).standard_normal(4 * n3)
+    g.tofile(tmp_path / "g.bin")
+    env = dict(os.environ, BDB_GAUSS_FILE=str(tmp_path / "g.bin"), OMP_NUM_THREADS="1")
+    prm = os.path.basename(p)
+    subprocess.run([HARNESS, prm, "forces", "f.bin"], cwd=tmp_path, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = np.fromfile(tmp_path / "f.bin")
+    F, E, rep, _ = pyoracle.Oracle(deck).forces()
+    assert rel(F, ref[:n3]) < 1e-13 and rep == int(ref[n3 + 9])
+    subprocess.run([HARNESS, prm, "steps", "s.bin", "3"], cwd=tmp_path, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    traj_ref = np.fromfile(tmp_path / "s.bin").reshape(3, deck.n, 4)
+    traj, _, _ = pyoracle.Oracle(deck).run_steps(3, g)
+    assert np.abs(traj - traj_ref).max() < 1e-11
+    # the external term is not negligible: without it the trajectory differs
+    off = decks.read_deck(p, overrides={"E_ext": "no", "sboundary": "no"})
+    traj_off, _, _ = pyoracle.Oracle(off).run_steps(3, g)
+    assert np.abs(traj_off - traj_ref).max() > 1e-6
