@@ -173,6 +173,15 @@ struct bdb_system {
     long long step_count = 0;
     double sim_time = 0;
     bdb::FrameRing* frames = nullptr;
+    long long saved_step_count = 0;            // bdb_save_state's copy
+    double saved_sim_time = 0;
+
+    // elastic-collision recovery (newton.cu): velocities, masses, pair list,
+    // scan scalars, and the previous scan's list size (BD_BOX keeps it global)
+    bdb::DevBuf<double> nw_vel, nw_mass;
+    bdb::DevBuf<int> nw_pairs;
+    bdb::DevBuf<unsigned long long> nw_scal;
+    int nw_prev_ints = 0;
 
     // measurement: CUDA-event pairs per phase, kernel launch count
     struct PhaseRec {
@@ -227,6 +236,8 @@ void phase_mark_on(bdb_system* s, int phase, cudaStream_t stream);
 void drop_graph(bdb_system* s);              // forget the captured step
 int after_step(bdb_system* s, double dt);     // count a finished step, record a frame when due
 void frames_release(bdb_system* s);           // wait for frame copies in flight, free the ring
+void frames_rewind(bdb_system* s, long long step);   // drop frames of steps after `step`
+int frames_redo_current(bdb_system* s);       // record the current step's frame again
 int build_and_factor(bdb_system* s);         // tensor build + factorisation into the stored matrix, eagerly
 int forces_phase(bdb_system* s);             // forces at the current positions (profiled phase)
 int check_status(bdb_system* s, bool* overlap);   // read and decode the status word (synchronises)

@@ -516,6 +516,8 @@ int bdb_save_state(bdb_system* s)
     if (!s) return fail(BDB_ERR_ARG, "null system");
     BDB_CUDA(cudaMemcpyAsync(s->pos_save.p, s->pos.p, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
     BDB_CUDA(cudaMemcpyAsync(s->F_save.p, s->F.p, sizeof(double) * s->n3, cudaMemcpyDeviceToDevice, s->stream));
+    s->saved_step_count = s->step_count;
+    s->saved_sim_time = s->sim_time;
     return BDB_OK;
 }
 
@@ -526,6 +528,9 @@ int bdb_load_state(bdb_system* s)
     BDB_CUDA(cudaMemcpyAsync(s->F.p, s->F_save.p, sizeof(double) * s->n3, cudaMemcpyDeviceToDevice, s->stream));
     BDB_CUDA(cudaMemsetAsync(s->cells_built.p, 0, sizeof(int) * s->segs.size(), s->stream));
     s->have_forces = true;
+    s->step_count = s->saved_step_count;
+    s->sim_time = s->saved_sim_time;
+    frames_rewind(s, s->step_count);
     return BDB_OK;
 }
 

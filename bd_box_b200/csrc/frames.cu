@@ -99,6 +99,28 @@ static int record(bdb_system* s)
     return BDB_OK;
 }
 
+// drop the frames of steps after `step` (a step taken back by
+// bdb_load_state); their copies may still be in flight, which is harmless:
+// the next copy into a freed slot is ordered after them on the same stream
+void frames_rewind(bdb_system* s, long long step)
+{
+    FrameRing* f = s->frames;
+    if (!f) return;
+    while (f->count > 0 && f->step[(f->head + f->count - 1) % f->cap] > step) --f->count;
+    if (f->count == 0)
+        while (!f->spill.empty() && f->spill.back().step > step) f->spill.pop_back();
+}
+
+// the current step's frame again, after its positions changed (the
+// elastic-collision recovery of an accepted step)
+int frames_redo_current(bdb_system* s)
+{
+    FrameRing* f = s->frames;
+    if (!f || (s->step_count - f->start) % f->every) return BDB_OK;
+    frames_rewind(s, s->step_count - 1);
+    return record(s);
+}
+
 // after every completed step of bdb_step / bdb_step_igt
 int after_step(bdb_system* s, double dt)
 {

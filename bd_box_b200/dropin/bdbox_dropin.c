@@ -435,19 +435,27 @@ static int attempt(void)
     return rc;
 }
 
-/* comp_step_ermak (diff_comp.c:152-179) and, for decks whose moves never
- * overlap, comp_step_ermak_newton (:181-210), which then takes the same path */
+/* comp_step_ermak (diff_comp.c:152-179) and comp_step_ermak_newton
+ * (:181-210): an overlapping move is redone by elastic collisions
+ * (bdb_newton_resolve) and reverted to try new Gaussians if that fails */
 static DOUBLE ermak_step(DOUBLE* _E)
 {
     INT count = 0;
+    int rounds = 0;
     curr_dt = dt;
     curr_iter++;
     push_coord();
     CHK(bdb_save_state(g_sys));
     for (;;) {
         if (!attempt()) break;
-        if (algorithm == DIFF_ALG_ERMAK_NEWTON)
-            UNERR("bdb200: overlap removal by elastic collisions (ermak_newton) is not available")
+        if (algorithm == DIFF_ALG_ERMAK_NEWTON) {
+            int rc = bdb_newton_resolve(g_sys, e_collision, masses, move_attempts, &rounds);
+            if (rc < 0) fatal("bdb_newton_resolve", rc);
+            if (rc == 0) break;
+            CHK(bdb_load_state(g_sys));
+            if (bc != BC_SPHERE) warning("Revert move in none sphere case", __FILE__, __LINE__);
+            continue;
+        }
         if (algorithm == DIFF_ALG_ERMAK_VAR && count < 16) curr_dt /= 2;
         CHK(bdb_load_state(g_sys));
         ++count;

@@ -44,7 +44,7 @@ EXPORTS = [
     "bdb_set_tuning", "bdb_factor_error", "bdb_profile", "bdb_phase_stats",
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc", "bdb_shard_replicas",
     "bdb_frames_start", "bdb_frames_take", "bdb_frames_pending", "bdb_frames_flush", "bdb_frames_stop",
-    "bdb_set_time", "bdb_get_time",
+    "bdb_set_time", "bdb_get_time", "bdb_newton_resolve",
 ]
 
 
@@ -127,6 +127,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_frames_pending.argtypes = [C.c_void_p, _ip]
     lib.bdb_frames_flush.argtypes = [C.c_void_p]
     lib.bdb_set_time.argtypes = [C.c_void_p, C.c_double]
+    lib.bdb_newton_resolve.argtypes = [C.c_void_p, C.c_double, _dp, C.c_int, _ip]
     lib.bdb_get_time.argtypes = [C.c_void_p, _dp]
     lib.bdb_frames_stop.argtypes = [C.c_void_p]
     _lib = lib
@@ -363,6 +364,42 @@ class System:
 
     def reset_stats(self):
         self._check(self.lib.bdb_reset_stats(self.h))
+
+    def save_state(self):
+        self._check(self.lib.bdb_save_state(self.h))
+
+    def load_state(self):
+        self._check(self.lib.bdb_load_state(self.h))
+
+    def step_newton(self, K: int, gauss_attempts, masses=None, e_collision=None, move_attempts=None):
+        """K ermak_newton steps as comp_step_ermak_newton runs them
+        (diff_comp.c:181-210): a move that overlaps is redone by elastic
+        collisions (bdb_newton_resolve) and, if that still overlaps, reverted
+        to try the next Gaussians. gauss_attempts: host Gaussians, 3N per
+        attempt, or None for device noise. Returns (attempts used, collision
+        rounds)."""
+        p = self.deck.prm
+        m = np.ascontiguousarray(self.deck.masses if masses is None else masses, dtype=np.float64)
+        e = p["e_collision"] if e_collision is None else e_collision
+        ma = p["move_attempts"] if move_attempts is None else move_attempts
+        g = None if gauss_attempts is None else np.ascontiguousarray(gauss_attempts, dtype=np.float64)
+        used, rounds = 0, 0
+        for _ in range(K):
+            count = C.c_int(0)
+            self.save_state()
+            while True:
+                gk = None if g is None else g[used * self.n3:(used + 1) * self.n3]
+                if gk is not None and gk.size < self.n3:
+                    raise BDBError(-1, "out of Gaussians")
+                used += 1
+                if self.step(1, gk) == 0:
+                    break
+                rc = self._check(self.lib.bdb_newton_resolve(self.h, e, _p(m), ma, C.byref(count)))
+                if rc == 0:
+                    break
+                self.load_state()
+            rounds += count.value
+        return used, rounds
 
     def set_time(self, t: float):
         self._check(self.lib.bdb_set_time(self.h, float(t)))

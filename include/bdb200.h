@@ -153,6 +153,21 @@ int bdb_frames_pending(bdb_system* s, int* nframes);
 int bdb_frames_flush(bdb_system* s);
 int bdb_frames_stop(bdb_system* s);
 
+/* Elastic-collision overlap removal (algorithm ermak_newton): the recovery
+ * of comp_step_ermak_newton (diff_comp.c:181-210) after a step whose move
+ * overlapped, with the step's start saved by bdb_save_state. Velocities
+ * v = (r - r_start) / dt and r = r_start (newton_init_vel, newton.c:202-213),
+ * then ballistic moves to just before the earliest contact of approaching
+ * pairs and elastic collisions of the pairs that reach it (restitution
+ * e_collision, bead masses[N]), until dt has elapsed (newton_moves and
+ * comp_time, newton.c:57-200); then the forces at the result. *count
+ * accumulates the collision rounds of the step (BD_BOX's count); more than
+ * move_attempts fails ("Ermak Newton error"). Returns 0 when the result is
+ * free of overlaps, 1 when not (the caller restores the start with
+ * bdb_load_state and tries new Gaussians, as BD_BOX does), < 0 on error.
+ * bdb_save_state / bdb_load_state also keep the step count and the time. */
+int bdb_newton_resolve(bdb_system* s, double e_collision, const double* masses, int move_attempts, int* count);
+
 /* Simulated time of the current state (curr_time, main_loop.c:47): the
  * time-dependent field (E_type AC, RF) acts at curr_time + dt on the forces
  * after a step (diff_comp.c:161). Steps advance it by dt; a host that keeps

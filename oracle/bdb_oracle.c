@@ -4,6 +4,7 @@
  * has no FMA) so the operation order below gives the reference's doubles. */
 #include "bdb_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1191,4 +1192,215 @@ int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K,
     free(Fp);
     free(cp);
     return rep;
+}
+
+/* ---- elastic-collision overlap removal (ermak_newton) ------------------ */
+
+#define ORC_NEWTON_EPSILON 0.000001 /* data.h:217 (double build) */
+#define ORC_NEWTON_OFFSET 0.0001    /* data.h:218 */
+
+/* comp_time (newton.c:57-138), one thread: the earliest time at which an
+ * approaching pair (i < j) comes within LJ[2i] + LJ[2j] + NEWTON_OFFSET, and
+ * the pairs that reach it, in (i, j) order. The list-size check reads the
+ * pair count of the previous call (*npairs on entry), as the reference's
+ * global size_pairs. Returns the time (DBL_MAX if no pair approaches). */
+static double newton_comp_time(const orc_system* s, const double* coord, const double* vel, int* pairs, int* npairs)
+{
+    const int prev = *npairs;
+    int cnt = 0, i, j;
+    double tmin = DBL_MAX;
+    for (i = 0; i < s->n; ++i)
+        for (j = i + 1; j < s->n; ++j) {
+            double r[3], v[3], rv, l;
+            dist_vec(s, coord + 4 * j, coord + 4 * i, r);
+            l = s->LJ[2 * j] + s->LJ[2 * i] + ORC_NEWTON_OFFSET;
+            v[0] = vel[3 * i] - vel[3 * j];
+            v[1] = vel[3 * i + 1] - vel[3 * j + 1];
+            v[2] = vel[3 * i + 2] - vel[3 * j + 2];
+            rv = r[0] * v[0] + r[1] * v[1] + r[2] * v[2];
+            if (rv < 0) {
+                double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+                double delta = rv * rv - vv * ((r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) - l * l);
+                if (delta > 0) {
+                    double t2, inv_vv = 1 / vv;
+                    delta = sqrt(delta);
+                    t2 = -(rv + delta) * inv_vv;
+                    if (t2 < 0) t2 = 0;
+                    if (t2 <= tmin) {
+                        cnt = (t2 < tmin) ? 0 : cnt;
+                        if (prev + 1 < 2 * s->n) {
+                            pairs[cnt] = i;
+                            pairs[cnt + 1] = j;
+                            cnt += 2;
+                        }
+                        tmin = t2;
+                    }
+                }
+            }
+        }
+    *npairs = cnt;
+    return tmin;
+}
+
+/* newton_moves (newton.c:140-200): ballistic moves with velocities vel to
+ * just before the earliest contact, elastic collisions of the pairs that
+ * reach it (restitution e_collision, masses), until dt has elapsed.
+ * Returns 1 if a move leaves the sphere (bc 2, iscorrect), 0 otherwise, -2
+ * when *count exceeds move_attempts ("Ermak Newton error"). */
+static int newton_moves(const orc_system* s, double* coord, double* vel, const double* masses, double e_collision,
+                        double dt, int move_attempts, int* count, int* pairs, int* npairs)
+{
+    double elapsed = 0.0;
+    int ret = 0, i, j;
+    while (elapsed < dt - 2 * ORC_NEWTON_EPSILON) {
+        double next;
+        ret = 0;
+        next = newton_comp_time(s, coord, vel, pairs, npairs);
+        if (next < 0 || next > dt - elapsed) next = dt - elapsed;
+        next = (next > ORC_NEWTON_EPSILON) ? next - ORC_NEWTON_EPSILON : 0;
+        elapsed += next;
+        if (next > 0.0) {
+            for (j = 0; j < s->n; ++j) {
+                int k;
+                for (k = 0; k < 3; ++k) coord[4 * j + k] += vel[3 * j + k] * next;
+                if (s->bc == 1)
+                    for (k = 0; k < 3; ++k) coord[4 * j + k] -= s->box[k] * floor(coord[4 * j + k] * s->inv_L[k] + 0.5f);
+            }
+            if (s->bc == 2) {
+                /* iscorrect (trans.c:130-145) */
+                double sr = s->sphere_radius * s->sphere_radius;
+                for (j = 0; j < s->n && !ret; ++j) {
+                    const double* c = coord + 4 * j;
+                    ret = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] > sr;
+                }
+            }
+        }
+        if (ret) break;
+        for (i = 0; i < *npairs / 2; ++i) {
+            int p1 = pairs[2 * i], p2 = pairs[2 * i + 1], k;
+            double e[3], v[3], ev, rr, inv, m1 = masses[p1], m2 = masses[p2];
+            /* get_v2_norms(p2, p1) (math_help.c:40-55) */
+            dist_vec(s, coord + 4 * p2, coord + 4 * p1, e);
+            rr = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+            inv = 1 / rr;
+            e[0] *= inv;
+            e[1] *= inv;
+            e[2] *= inv;
+            for (k = 0; k < 3; ++k) v[k] = vel[3 * p1 + k] - vel[3 * p2 + k];
+            ev = e[0] * v[0] + e[1] * v[1] + e[2] * v[2];
+            ev *= (1 + e_collision) / (m1 + m2);
+            for (k = 0; k < 3; ++k) vel[3 * p1 + k] -= m2 * ev * e[k];
+            for (k = 0; k < 3; ++k) vel[3 * p2 + k] += m1 * ev * e[k];
+        }
+        ++(*count);
+        if (*count > move_attempts) return -2;
+    }
+    return ret;
+}
+
+/* one Ermak-McCammon move from coord with forces F (compute_hydro_ermak,
+ * diff_equation.c:216-286; the tensor and its factor at coord, refresh 1) */
+static int ermak_move(orc_system* s, double* coord, const double* F, double dt, const double* xi, double* D,
+                      double* L, double* Rf, double* Rs, double* X, double preDii)
+{
+    int n3 = 3 * s->n, i, k;
+    s->coord = coord;
+    if (s->hydro == 1) {
+        orc_D(s, D);
+        memcpy(L, D, sizeof(double) * (size_t)n3 * n3);
+        if (orc_cholesky(n3, L, n3)) return -1;
+        orc_df(s, D, F, dt, Rf);
+        for (i = 0; i < n3; ++i) X[i] = xi[i] * sqrt(2 * dt);
+        orc_trmv_lower(n3, L, n3, X, Rs);
+    } else if (s->hydro == 2) {
+        orc_df(s, NULL, F, dt, Rf);
+        orc_tea(s, NULL, xi, dt, Rs, NULL, NULL);
+    } else {
+        orc_df(s, NULL, F, dt, Rf);
+        for (i = 0; i < n3; ++i) Rs[i] = xi[i] * sqrt(preDii / coord[4 * (i / 3) + 3] * 2 * dt);
+    }
+    for (i = 0; i < s->n; ++i) {
+        for (k = 0; k < 3; ++k) coord[4 * i + k] = Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
+        if (s->bc == 1)
+            for (k = 0; k < 3; ++k) coord[4 * i + k] -= s->box[k] * floor(coord[4 * i + k] * s->inv_L[k] + 0.5f);
+    }
+    return 0;
+}
+
+int orc_run_newton_steps(orc_system* s, double* coord, double* F, double dt, int K, const double* gauss,
+                         int n_gauss, const double* masses, double e_collision, int move_attempts, double* traj,
+                         int* used, int* rounds)
+{
+    int n3 = 3 * s->n, step, rc = 0, g = 0, count_total = 0;
+    double *D = NULL, *L = NULL, preDii, preDij;
+    double* Rf = (double*)malloc(sizeof(double) * n3);
+    double* Rs = (double*)malloc(sizeof(double) * n3);
+    double* X = (double*)malloc(sizeof(double) * n3);
+    double* vel = (double*)malloc(sizeof(double) * n3);
+    double* save = (double*)malloc(sizeof(double) * 4 * s->n);
+    double* Fsave = (double*)malloc(sizeof(double) * n3);
+    int* pairs = (int*)malloc(sizeof(int) * 2 * s->n);
+    int npairs = 0;   /* the reference's global size_pairs */
+    orc_prefactors(s, &preDii, &preDij);
+    if (s->hydro == 1) {
+        D = (double*)malloc(sizeof(double) * (size_t)n3 * n3);
+        L = (double*)malloc(sizeof(double) * (size_t)n3 * n3);
+    }
+    for (step = 0; step < K && rc >= 0; ++step) {
+        /* comp_step_ermak_newton (diff_comp.c:181-210) */
+        const double t0 = s->t;
+        int count = 0, ret = 1, i;
+        memcpy(save, coord, sizeof(double) * 4 * s->n);
+        memcpy(Fsave, F, sizeof(double) * n3);
+        while (ret) {
+            if (g >= n_gauss) {
+                rc = -3;
+                break;
+            }
+            if (ermak_move(s, coord, F, dt, gauss + (size_t)g * n3, D, L, Rf, Rs, X, preDii)) {
+                rc = -1;
+                break;
+            }
+            ++g;
+            s->t = t0 + dt;
+            ret = orc_forces(s, F, NULL, NULL);
+            if (ret) {
+                /* newton_init_vel (newton.c:202-213), load_coord, newton_moves */
+                double inv_t = 1.0 / dt;
+                for (i = 0; i < s->n; ++i) {
+                    dist_vec(s, save + 4 * i, coord + 4 * i, vel + 3 * i);
+                    vel[3 * i] *= inv_t;
+                    vel[3 * i + 1] *= inv_t;
+                    vel[3 * i + 2] *= inv_t;
+                }
+                memcpy(coord, save, sizeof(double) * 4 * s->n);
+                ret = newton_moves(s, coord, vel, masses, e_collision, dt, move_attempts, &count, pairs, &npairs);
+                if (ret == -2) {
+                    rc = -2;
+                    break;
+                }
+                ret = ret || orc_forces(s, F, NULL, NULL);
+                if (ret) {
+                    memcpy(coord, save, sizeof(double) * 4 * s->n);
+                    memcpy(F, Fsave, sizeof(double) * n3);
+                    s->t = t0;
+                }
+            }
+        }
+        count_total += count;
+        if (traj) memcpy(traj + (size_t)step * 4 * s->n, coord, sizeof(double) * 4 * s->n);
+    }
+    s->coord = coord;
+    if (used) *used = g;
+    if (rounds) *rounds = count_total;
+    free(D);
+    free(L);
+    free(Rf);
+    free(Rs);
+    free(X);
+    free(vel);
+    free(save);
+    free(Fsave);
+    free(pairs);
+    return rc;
 }

@@ -116,6 +116,17 @@ int orc_run_steps(orc_system* s, double* coord, double* F, double dt, int K,
 int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K,
                       const double* gauss, double* traj);
 
+/* K steps of comp_step_ermak_newton (diff_comp.c:181-210): a move that
+ * overlaps is redone as ballistic moves with elastic collisions
+ * (newton_init_vel, newton_moves, comp_time; newton.c), and reverted to try
+ * new Gaussians if the result still overlaps. gauss: n_gauss blocks of 3N,
+ * one per attempt; *used: blocks consumed; *rounds: collision rounds.
+ * masses: N bead masses. Returns 0, -1 (failed Cholesky), -2 (more rounds
+ * than move_attempts: "Ermak Newton error") or -3 (out of Gaussians). */
+int orc_run_newton_steps(orc_system* s, double* coord, double* F, double dt, int K, const double* gauss,
+                         int n_gauss, const double* masses, double e_collision, int move_attempts, double* traj,
+                         int* used, int* rounds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,9 @@ def load():
     lib.orc_run_steps.restype = C.c_int
     lib.orc_run_igt_steps.argtypes = [P, _dp, _dp, C.c_double, C.c_int, _dp, _dp]
     lib.orc_run_igt_steps.restype = C.c_int
+    lib.orc_run_newton_steps.argtypes = [P, _dp, _dp, C.c_double, C.c_int, _dp, C.c_int, _dp, C.c_double, C.c_int,
+                                         _dp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.orc_run_newton_steps.restype = C.c_int
     _LIB = lib
     return lib
 
@@ -193,6 +196,25 @@ class Oracle:
         g = np.ascontiguousarray(gauss, dtype=np.float64)
         rep = self.lib.orc_run_steps(C.byref(self.s), _p(self.coord), _p(F), dt, K, _p(g), refresh, _p(traj))
         return traj, F, rep
+
+    def run_newton_steps(self, K, gauss, masses=None, e_collision=None, move_attempts=None, dt=None, F=None):
+        """K ermak_newton steps (orc_run_newton_steps); gauss holds 3N
+        Gaussians per attempt. Returns (traj, F, rc, blocks used, collision
+        rounds)."""
+        p = self.deck.prm
+        dt = p["dt"] if dt is None else dt
+        if F is None:
+            F, _, _, _ = self.forces()
+        F = np.ascontiguousarray(F, dtype=np.float64).copy()
+        m = np.ascontiguousarray(self.deck.masses if masses is None else masses, dtype=np.float64)
+        traj = np.zeros((K, self.deck.n, 4))
+        g = np.ascontiguousarray(gauss, dtype=np.float64)
+        used, rounds = C.c_int(), C.c_int()
+        rc = self.lib.orc_run_newton_steps(C.byref(self.s), _p(self.coord), _p(F), dt, K, _p(g), g.size // self.n3,
+                                           _p(m), p["e_collision"] if e_collision is None else e_collision,
+                                           p["move_attempts"] if move_attempts is None else move_attempts,
+                                           _p(traj), C.byref(used), C.byref(rounds))
+        return traj, F, rc, used.value, rounds.value
 
     def run_igt_steps(self, K, gauss, dt=None, F=None):
         """K IGT predictor-corrector steps (orc_run_igt_steps); gauss holds

@@ -155,3 +155,28 @@ def test_dropin_external_forces_match_cpu_build(name, tmp_path):
     traj_ref = ref["steps"].reshape(3, deck.n, 4)
     disp = np.abs(traj_ref[0, :, :3] - deck.coord[:, :3]).max()
     assert np.abs(traj - traj_ref).max() <= 1e-9 * disp
+
+
+@pytest.mark.parametrize("hydro", ["none", "geyer"])
+def test_dropin_newton_matches_cpu_build(hydro, tmp_path):
+    """ermak_newton through the drop-in (bdb_newton_resolve in the retry
+    loop of comp_step_ermak_newton) against the CPU build: the same
+    trajectory from the same Gaussian stream."""
+    need(HARNESS)
+    cpu = os.path.join(REF, "ref_harness")
+    need(cpu)
+    from test_oracle_pin import newton_deck
+    p = newton_deck(tmp_path, hydro)
+    os.replace(p, os.path.join(tmp_path, "c.prm"))
+    deck = decks.read_deck(os.path.join(tmp_path, "c.prm"))
+    n3 = 3 * deck.n
+    np.random.default_rng(4).standard_normal(40 * n3).tofile(tmp_path / "g.bin")
+    d = str(tmp_path)
+    e = dict(os.environ, BDB_GAUSS_FILE=os.path.join(d, "g.bin"), OMP_NUM_THREADS="1")
+    r = subprocess.run([cpu, "c.prm", "steps", os.path.join(d, "ref.bin"), "4"], cwd=d, env=e,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    traj_ref = np.fromfile(os.path.join(d, "ref.bin")).reshape(4, deck.n, 4)
+    traj = run(d, "steps", "4").reshape(4, deck.n, 4)
+    disp = np.abs(traj_ref[0, :, :3] - deck.coord[:, :3]).max()
+    assert np.abs(traj - traj_ref).max() <= 1e-9 * disp

@@ -130,3 +130,81 @@ def test_oracle_external_forces_match_reference(tmp_path, name):
     off = decks.read_deck(p, overrides={"E_ext": "no", "sboundary": "no"})
     traj_off, _, _ = pyoracle.Oracle(off).run_steps(3, g)
     assert np.abs(traj_off - traj_ref).max() > 1e-6
+
+
+def newton_deck(tmp_path, hydro="none"):
+    """A dense periodic suspension whose large moves overlap: ermak_newton
+    resolves them by elastic collisions. (TEA with the stored tensor: BD_BOX's
+    on-the-fly Ewald TEA differs, see test_reference_on_the_fly_ewald_tea.)"""
+    return decks.write_suspension_deck(str(tmp_path), f"nw_{hydro}", 40, seed=5, phi=0.3, dt=0.2,
+                                       extra=dict(algorithm="ermak_newton", check_overlap="yes", hydro=hydro,
+                                                  geyer_on_the_fly="no"))
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("hydro", ["none", "geyer"])
+def test_oracle_newton_matches_reference(tmp_path, hydro):
+    """comp_step_ermak_newton with elastic collisions (newton.c): the
+    oracle's steps against BD_BOX's own run by the harness, with the same
+    Gaussian stream (one block per attempt)."""
+    p = newton_deck(tmp_path, hydro)
+    deck = decks.read_deck(p)
+    n3 = 3 * deck.n
+    g = np.random.default_rng(4).standard_normal(40 * n3)
+    g.tofile(tmp_path / "g.bin")
+    env = dict(os.environ, BDB_GAUSS_FILE=str(tmp_path / "g.bin"), OMP_NUM_THREADS="1")
+    subprocess.run([HARNESS, os.path.basename(p), "steps", "s.bin", "4"], cwd=tmp_path, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = np.fromfile(tmp_path / "s.bin").reshape(4, deck.n, 4)
+    traj, _, rc, used, rounds = pyoracle.Oracle(deck).run_newton_steps(4, g)
+    assert rc == 0 and used >= 4 and rounds > 4      # collisions happened
+    assert np.abs(traj - ref).max() < 1e-10
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("method", ["beenakker", "smith"])
+def test_reference_on_the_fly_ewald_tea(tmp_path, method):
+    """A documented difference. BD_BOX's on-the-fly TEA (diff_rand.c:100-136)
+    zeroes the tile once per bead i and calls compute_Dij(i, k) for k < i;
+    the Ewald tile functions add into their output (diff_tensor.c:265-422
+    and :102-263 use +=), so bead pair (i, k) gets the sum of the tiles
+    (i, 0..k). Its epsilon is exactly that of the accumulated tiles, and
+    differs from its own stored-tensor TEA (geyer_on_the_fly no), which the
+    oracle and this library compute for both settings."""
+    p = decks.write_suspension_deck(str(tmp_path), "tt", 24, seed=5, phi=0.1, dt=0.005,
+                                    extra=dict(geyer_on_the_fly="yes", ewald_method=method))
+    deck = decks.read_deck(p)
+    n, n3 = deck.n, 3 * deck.n
+    g = np.random.default_rng(4).standard_normal(n3)
+    g.tofile(tmp_path / "g.bin")
+    env = dict(os.environ, BDB_GAUSS_FILE=str(tmp_path / "g.bin"), OMP_NUM_THREADS="1")
+
+    def ref_tea(prm):
+        subprocess.run([HARNESS, prm, "tea", "t.bin"], cwd=tmp_path, env=env, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        return np.fromfile(tmp_path / "t.bin")
+
+    o = pyoracle.Oracle(deck)
+    acc = plain = 0.0
+    for i in range(n):
+        A = np.zeros((3, 3))
+        for k in range(i):
+            T = o.tile(i, k)
+            A = A + T
+            acc += A.sum()
+            plain += T.sum()
+    norm = 2.0 / n3 / (n3 - 1)
+    eps_fly = ref_tea("tt.prm")[-1]
+    assert abs(eps_fly - acc * norm) <= 1e-12 * abs(eps_fly)
+    assert abs(eps_fly - plain * norm) > 0.1 * abs(eps_fly)
+    # the stored-tensor TEA of BD_BOX is the oracle's (for both settings)
+    stored = decks.read_deck(p, overrides={"geyer_on_the_fly": "no"})
+    with open(tmp_path / "tt.prm") as f:
+        text = f.read().replace("geyer_on_the_fly yes", "geyer_on_the_fly no")
+    (tmp_path / "ts.prm").write_text(text)
+    t = ref_tea("ts.prm")
+    Rs, eps, _ = pyoracle.Oracle(stored).tea(g, deck.prm["dt"], pyoracle.Oracle(stored).D())
+    assert abs(eps - t[-1]) <= 1e-12 * abs(eps)
+    assert rel(Rs, t[:n3]) < 1e-12
+    Rs_fly, eps2, _ = pyoracle.Oracle(deck).tea(g, deck.prm["dt"])
+    assert abs(eps2 - eps) <= 1e-12 * abs(eps) and rel(Rs_fly, Rs) < 1e-12
