@@ -15,6 +15,7 @@
 // only on the steps it writes to the energy file (main_loop.c:102, 112).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstring>
 #include <deque>
 #include <vector>
@@ -223,6 +224,81 @@ int bdb_frames_stop(bdb_system* s)
 {
     if (!s) return fail(BDB_ERR_ARG, "null system");
     frames_release(s);
+    return BDB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Checkpoints: the state a resumed run needs, as a flat host image.
+
+namespace bdb {
+
+struct CheckpointHeader {
+    uint64_t magic;              // "BDBCKPT1"
+    int64_t n;
+    int64_t step_count;
+    double sim_time;
+    int64_t steps_since_refresh;
+    uint64_t philox_stream;
+    double dt;
+};
+
+static constexpr uint64_t CKPT_MAGIC = 0x3154504b43424442ull;   // "BDBCKPT1" little-endian
+
+}  // namespace bdb
+
+extern "C" {
+
+size_t bdb_checkpoint_size(bdb_system* s)
+{
+    return s ? sizeof(CheckpointHeader) + sizeof(double4) * (size_t)s->n : 0;
+}
+
+int bdb_checkpoint_save(bdb_system* s, void* buf, size_t bytes)
+{
+    if (!s || !buf) return fail(BDB_ERR_ARG, "null argument");
+    if (bytes < bdb_checkpoint_size(s)) return fail(BDB_ERR_ARG, "checkpoint buffer too small");
+    CheckpointHeader h;
+    h.magic = CKPT_MAGIC;
+    h.n = s->n;
+    h.step_count = s->step_count;
+    h.sim_time = s->sim_time;
+    h.steps_since_refresh = s->steps_since_refresh;
+    h.dt = s->p.dt;
+    unsigned long long stream = 0;
+    BDB_CUDA(cudaMemcpyAsync(&stream, s->ctr.p, sizeof stream, cudaMemcpyDeviceToHost, s->stream));
+    unsigned char* out = static_cast<unsigned char*>(buf);
+    BDB_CUDA(cudaMemcpyAsync(out + sizeof h, s->pos.p, sizeof(double4) * s->n, cudaMemcpyDeviceToHost, s->stream));
+    BDB_CUDA(cudaStreamSynchronize(s->stream));
+    h.philox_stream = stream;
+    std::memcpy(out, &h, sizeof h);
+    return BDB_OK;
+}
+
+int bdb_checkpoint_load(bdb_system* s, const void* buf, size_t bytes)
+{
+    if (!s || !buf) return fail(BDB_ERR_ARG, "null argument");
+    CheckpointHeader h;
+    if (bytes < sizeof h) return fail(BDB_ERR_ARG, "checkpoint image too small");
+    std::memcpy(&h, buf, sizeof h);
+    if (h.magic != CKPT_MAGIC) return fail(BDB_ERR_ARG, "not a checkpoint image");
+    if (h.n != s->n || bytes < bdb_checkpoint_size(s)) return fail(BDB_ERR_ARG, "checkpoint of another bead count");
+    const unsigned char* in = static_cast<const unsigned char*>(buf);
+    BDB_CUDA(cudaMemcpyAsync(s->pos.p, in + sizeof h, sizeof(double4) * s->n, cudaMemcpyHostToDevice, s->stream));
+    const unsigned long long ctr[2] = {h.philox_stream, 0ull};
+    BDB_CUDA(cudaMemcpyAsync(s->ctr.p, ctr, sizeof ctr, cudaMemcpyHostToDevice, s->stream));
+    BDB_CUDA(cudaMemsetAsync(s->cells_built.p, 0, sizeof(int) * s->segs.size(), s->stream));
+    BDB_CUDA(cudaStreamSynchronize(s->stream));   // ctr is a stack array
+    s->step_count = h.step_count;
+    s->sim_time = h.sim_time;
+    s->steps_since_refresh = (int)h.steps_since_refresh;
+    if (s->p.dt != h.dt) {
+        s->p.dt = h.dt;
+        drop_graph(s);
+    }
+    s->have_forces = false;     // recomputed at the next step
+    s->factor_valid = false;    // the stored tensor and its factor are rebuilt at the next step
     return BDB_OK;
 }
 

@@ -45,6 +45,7 @@ EXPORTS = [
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc", "bdb_shard_replicas",
     "bdb_frames_start", "bdb_frames_take", "bdb_frames_pending", "bdb_frames_flush", "bdb_frames_stop",
     "bdb_set_time", "bdb_get_time", "bdb_newton_resolve",
+    "bdb_checkpoint_size", "bdb_checkpoint_save", "bdb_checkpoint_load",
 ]
 
 
@@ -128,6 +129,10 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_frames_flush.argtypes = [C.c_void_p]
     lib.bdb_set_time.argtypes = [C.c_void_p, C.c_double]
     lib.bdb_newton_resolve.argtypes = [C.c_void_p, C.c_double, _dp, C.c_int, _ip]
+    lib.bdb_checkpoint_size.argtypes = [C.c_void_p]
+    lib.bdb_checkpoint_size.restype = C.c_size_t
+    lib.bdb_checkpoint_save.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.bdb_checkpoint_load.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.bdb_get_time.argtypes = [C.c_void_p, _dp]
     lib.bdb_frames_stop.argtypes = [C.c_void_p]
     _lib = lib
@@ -400,6 +405,17 @@ class System:
                 self.load_state()
             rounds += count.value
         return used, rounds
+
+    def checkpoint(self) -> bytes:
+        """The resume image (bdb_checkpoint_save)."""
+        buf = C.create_string_buffer(self.lib.bdb_checkpoint_size(self.h))
+        self._check(self.lib.bdb_checkpoint_save(self.h, buf, len(buf)))
+        return buf.raw
+
+    def restore(self, image: bytes):
+        """Resume from an image of a system with the same parameters."""
+        buf = C.create_string_buffer(bytes(image), len(image))
+        self._check(self.lib.bdb_checkpoint_load(self.h, buf, len(image)))
 
     def set_time(self, t: float):
         self._check(self.lib.bdb_set_time(self.h, float(t)))

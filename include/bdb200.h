@@ -168,6 +168,19 @@ int bdb_frames_stop(bdb_system* s);
  * bdb_save_state / bdb_load_state also keep the step count and the time. */
 int bdb_newton_resolve(bdb_system* s, double e_collision, const double* masses, int move_attempts, int* count);
 
+/* Checkpoints for resume (no reference counterpart; BD_BOX's restart files,
+ * restart.c:315-486, hold its globals, coordinates and RNG state). The
+ * image holds the positions, the Philox stream index, the step count, the
+ * time, dt and the refresh phase; bdb_checkpoint_size gives its bytes.
+ * bdb_checkpoint_load restores it into a system created with the same
+ * parameters and bead count. Forces are recomputed and a stored tensor and
+ * its factor are rebuilt at the next step, so a resumed run repeats the
+ * uninterrupted one (to round-off: the cell lists are rebuilt) when the
+ * image was taken at the end of a refresh interval or with refresh 1. */
+size_t bdb_checkpoint_size(bdb_system* s);
+int bdb_checkpoint_save(bdb_system* s, void* buf, size_t bytes);
+int bdb_checkpoint_load(bdb_system* s, const void* buf, size_t bytes);
+
 /* Simulated time of the current state (curr_time, main_loop.c:47): the
  * time-dependent field (E_type AC, RF) acts at curr_time + dt on the forces
  * after a step (diff_comp.c:161). Steps advance it by dt; a host that keeps
