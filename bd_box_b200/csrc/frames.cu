@@ -1,3 +1,6 @@
+// Run state out of the device: asynchronous trajectory frames, and (at the
+// end of this file) checkpoint images for resume.
+//
 // Asynchronous trajectory frames: the positions of every `every`-th step go
 // to a ring of pinned host buffers by cudaMemcpyAsync on the engine's
 // stream, so the step loop (and its graph replays) never waits for output.
