@@ -53,7 +53,6 @@ static constexpr int BOX_BYTES = PW * KC * 4;     // 16 KB
 static constexpr int STAGE_BYTES = 4 * BOX_BYTES; // A_hi, A_lo, B_hi, B_lo
 static constexpr int C_BOXES = 2;                 // staging ring of 128x32 boxes for the C update
 static constexpr int SYRK_SMEM = STAGES * STAGE_BYTES + C_BOXES * BOX_BYTES + 1024;
-static constexpr int LDS = PW + 1;                // padded FP64 row in shared memory
 
 // C[tile] += smem tile (FP32 add in L2, no load of C by the SM)
 __device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, uint32_t src, int x, int y)
