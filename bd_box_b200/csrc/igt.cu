@@ -223,6 +223,7 @@ static int igt_buffers(bdb_system* s)
 static int igt_checks(bdb_system* s, const double* gauss)
 {
     if (!s) return fail(BDB_ERR_ARG, "null system");
+    if (s->p.flow && s->p.bc != 2) return fail(BDB_ERR_UNSUPPORTED, "IGT steps in a flowing solvent are not available");
     if (s->p.noise == BDB_NOISE_HOST && !gauss) return fail(BDB_ERR_ARG, "host noise mode needs Gaussians");
     if (s->p.hydro == BDB_HYDRO_GEYER)
         return fail(BDB_ERR_UNSUPPORTED, "IGT steps need hydro none or cholesky (the averaged tensor is stored)");

@@ -110,16 +110,31 @@ int noise_fill(bdb_system* s, const double* dev_gauss)
     return BDB_OK;
 }
 
-// coord_out = Rf + Rs + coord; trans_to_box (diff_equation.c:254-264)
-__global__ void k_update(int n, int periodic, double3 box, double3 inv_L, const double* __restrict__ Rf,
+// Flowing solvent (vel_grad_tensor, diff_decl.c:72): the displacement
+// dt G r of the flow at the step's start, G row-major
+struct Flow {
+    int on;
+    double dt, G[9];
+};
+
+// coord_out = Rf + Rs + coord (+ dt G coord in a flow); trans_to_box
+// (diff_equation.c:254-283)
+__global__ void k_update(int n, int periodic, double3 box, double3 inv_L, Flow fl, const double* __restrict__ Rf,
                          const double* __restrict__ Rs, double4* __restrict__ pos)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 p = pos[i];
+    const double x = p.x, y = p.y, z = p.z;
     p.x = add(add(Rf[3 * i], Rs[3 * i]), p.x);
     p.y = add(add(Rf[3 * i + 1], Rs[3 * i + 1]), p.y);
     p.z = add(add(Rf[3 * i + 2], Rs[3 * i + 2]), p.z);
+    if (fl.on) {
+        const double* G = fl.G;
+        p.x = add(p.x, mul(fl.dt, add(add(mul(G[0], x), mul(G[1], y)), mul(G[2], z))));
+        p.y = add(p.y, mul(fl.dt, add(add(mul(G[3], x), mul(G[4], y)), mul(G[5], z))));
+        p.z = add(p.z, mul(fl.dt, add(add(mul(G[6], x), mul(G[7], y)), mul(G[8], z))));
+    }
     if (periodic) {
         p.x = sub(p.x, mul(box.x, floor(add(mul(p.x, inv_L.x), 0.5))));
         p.y = sub(p.y, mul(box.y, floor(add(mul(p.y, inv_L.y), 0.5))));
@@ -130,9 +145,13 @@ __global__ void k_update(int n, int periodic, double3 box, double3 inv_L, const 
 
 int update_positions(bdb_system* s)
 {
+    Flow fl;
+    fl.on = s->p.flow && s->p.bc != 2;   // a sphere turns the flow off (input.c:462-468)
+    fl.dt = s->p.dt;
+    for (int k = 0; k < 9; ++k) fl.G[k] = s->p.vel_grad[k];
     k_update<<<(s->n + 127) / 128, 128, 0, s->stream>>>(
         s->n, s->p.bc == 1, make_double3(s->p.box[0], s->p.box[1], s->p.box[2]),
-        make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]), s->Rf.p, s->Rs.p, s->pos.p);
+        make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]), fl, s->Rf.p, s->Rs.p, s->pos.p);
     s->launches += 1;
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;

@@ -156,6 +156,19 @@ def read_prm(path: str, overrides: dict | None = None) -> dict:
     return prm
 
 
+def vel_grad(prm: dict):
+    """The velocity-gradient tensor G (9 doubles, row-major) of a deck, or
+    None: vel_grad_tensor is read as nine doubles (input.c:1110-1124, no
+    float rounding)."""
+    v = prm.get("vel_grad_tensor")
+    if v is None:
+        return None
+    vals = [float(t) for t in str(v).split()]
+    if len(vals) != 9:
+        raise ValueError("vel_grad_tensor needs 9 values")
+    return vals
+
+
 def read_str(path: str):
     subs, bonds, angles, angles_cos, dihes, dihe_angles = [], [], [], [], [], []
     with open(path) as f:

@@ -148,7 +148,8 @@ static void check_supported(void)
         UNERR("bdb200: the IGT algorithms need hydro none or cholesky")
     if (hydro != DIFF_NONE && hydro != DIFF_CHOLESKY && hydro != DIFF_GEYER)
         UNERR("bdb200: hydro must be none, cholesky or geyer")
-    if (vel_grad_tensor) UNERR("bdb200: velocity-gradient flows are not available")
+    if (vel_grad_tensor && (algorithm == DIFF_ALG_IGT_CONST || algorithm == DIFF_ALG_IGT_VAR))
+        UNERR("bdb200: IGT steps in a flowing solvent are not available")
 }
 
 static void make_params(bdb_params* p)
@@ -195,6 +196,10 @@ static void make_params(bdb_params* p)
     p->sboundary_A = sboundary_A;
     p->sboundary_cutoff = sboundary_cutoff;
     p->sphere_radius = sphere_radius;
+    /* flowing solvent (diff_decl.c:72); input.c:462-468 already dropped it for bc sphere */
+    p->flow = vel_grad_tensor != NULL;
+    if (vel_grad_tensor)
+        for (int k = 0; k < 9; ++k) p->vel_grad[k] = vel_grad_tensor[k];
     p->precision = env_choice("BDB_PRECISION", "fp64", "mixed", 0) ? BDB_PREC_MIXED : BDB_PREC_FP64;
     p->refresh = r && atoi(r) > 0 ? atoi(r) : 1;
     p->noise = g_noise_host ? BDB_NOISE_HOST : BDB_NOISE_PHILOX;

@@ -71,6 +71,7 @@ class Params(C.Structure):
         ("e_factor", C.c_double), ("e_magn", C.c_double), ("e_freq", C.c_double),
         ("sboundary", C.c_int), ("sboundary_n", C.c_int), ("sboundary_A", C.c_double),
         ("sboundary_cutoff", C.c_double), ("sphere_radius", C.c_double),
+        ("flow", C.c_int), ("vel_grad", C.c_double * 9),
     ]
 
 
@@ -180,6 +181,11 @@ def params_from_deck(deck, precision=PREC_FP64, refresh=1, noise=NOISE_PHILOX, s
     P.sboundary, P.sboundary_n = p["sboundary"], p["sboundary_n"]
     P.sboundary_A, P.sboundary_cutoff = p["sboundary_A"], p["sboundary_cutoff"]
     P.sphere_radius = p["sphere_radius"]
+    G = _decks.vel_grad(p)
+    if G is not None:
+        P.flow = 1
+        for k in range(9):
+            P.vel_grad[k] = G[k]
     return P
 
 

@@ -1068,10 +1068,18 @@ int orc_run_steps(orc_system* s, double* coord, double* F, double dt, int K, con
             orc_df(s, NULL, F, dt, Rf);
             for (i = 0; i < n3; ++i) Rs[i] = xi[i] * sqrt(preDii / coord[4 * (i / 3) + 3] * 2 * dt);
         }
-        /* diff_equation.c:254-264 */
+        /* diff_equation.c:254-283 */
         for (i = 0; i < s->n; ++i) {
             int k;
-            for (k = 0; k < 3; ++k) coord[4 * i + k] = Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
+            double tmp[3] = {0, 0, 0};
+            if (s->flow) {
+                const double* G = s->vel_grad;
+                const double* c = coord + 4 * i;
+                for (k = 0; k < 3; ++k) tmp[k] = dt * (G[3 * k] * c[0] + G[3 * k + 1] * c[1] + G[3 * k + 2] * c[2]);
+            }
+            for (k = 0; k < 3; ++k)
+                coord[4 * i + k] = s->flow ? Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k] + tmp[k]
+                                           : Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
             if (s->bc == 1)
                 for (k = 0; k < 3; ++k)
                     coord[4 * i + k] -= s->box[k] * floor(coord[4 * i + k] * s->inv_L[k] + 0.5f);
@@ -1320,7 +1328,15 @@ static int ermak_move(orc_system* s, double* coord, const double* F, double dt, 
         for (i = 0; i < n3; ++i) Rs[i] = xi[i] * sqrt(preDii / coord[4 * (i / 3) + 3] * 2 * dt);
     }
     for (i = 0; i < s->n; ++i) {
-        for (k = 0; k < 3; ++k) coord[4 * i + k] = Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
+        double tmp[3] = {0, 0, 0};
+        if (s->flow) {
+            const double* G = s->vel_grad;
+            const double* c = coord + 4 * i;
+            for (k = 0; k < 3; ++k) tmp[k] = dt * (G[3 * k] * c[0] + G[3 * k + 1] * c[1] + G[3 * k + 2] * c[2]);
+        }
+        for (k = 0; k < 3; ++k)
+            coord[4 * i + k] = s->flow ? Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k] + tmp[k]
+                                       : Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
         if (s->bc == 1)
             for (k = 0; k < 3; ++k) coord[4 * i + k] -= s->box[k] * floor(coord[4 * i + k] * s->inv_L[k] + 0.5f);
     }

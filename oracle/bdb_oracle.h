@@ -53,6 +53,8 @@ typedef struct {
     int sboundary, sboundary_n;
     double sboundary_A, sboundary_cutoff, sphere_radius;
     double t;                   /* time of the state: forces act at t (curr_time + curr_dt after a step) */
+    int flow;                   /* vel_grad_tensor set (diff_equation.c:265-283), Ermak steps */
+    double vel_grad[9];         /* G, row-major */
 } orc_system;
 
 /* ENERGY_TYPE indices (data.h:278-289); energy arrays hold 9 doubles. */

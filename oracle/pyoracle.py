@@ -40,6 +40,7 @@ class OrcSystem(C.Structure):
         ("sboundary", C.c_int), ("sboundary_n", C.c_int),
         ("sboundary_A", C.c_double), ("sboundary_cutoff", C.c_double), ("sphere_radius", C.c_double),
         ("t", C.c_double),
+        ("flow", C.c_int), ("vel_grad", C.c_double * 9),
     ]
 
 
@@ -113,6 +114,11 @@ class Oracle:
         s.sboundary_A, s.sboundary_cutoff = p["sboundary_A"], p["sboundary_cutoff"]
         s.sphere_radius = p["sphere_radius"]
         s.t = 0.0
+        G = None if p.get("vel_grad_tensor") is None else [float(v) for v in str(p["vel_grad_tensor"]).split()]
+        if G is not None and p["bc"] != 2:
+            s.flow = 1
+            for k in range(9):
+                s.vel_grad[k] = G[k]
         for k in range(3):
             s.box[k] = deck.box[k]
             s.inv_L[k] = deck.inv_L[k]

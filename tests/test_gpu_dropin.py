@@ -180,3 +180,25 @@ def test_dropin_newton_matches_cpu_build(hydro, tmp_path):
     traj = run(d, "steps", "4").reshape(4, deck.n, 4)
     disp = np.abs(traj_ref[0, :, :3] - deck.coord[:, :3]).max()
     assert np.abs(traj - traj_ref).max() <= 1e-9 * disp
+
+
+def test_dropin_shear_flow_matches_cpu_build(tmp_path):
+    """A flowing solvent (vel_grad_tensor) through the drop-in against the
+    CPU build: three Ermak steps from the same Gaussian stream."""
+    need(HARNESS)
+    cpu = os.path.join(REF, "ref_harness")
+    need(cpu)
+    p = decks.write_chain_deck(str(tmp_path), "fl", 30, seed=23, hydro="cholesky",
+                               extra={"vel_grad_tensor": "0 0.75 0 0 0 0 0.1 0 0"})
+    os.replace(p, os.path.join(tmp_path, "c.prm"))
+    deck = decks.read_deck(os.path.join(tmp_path, "c.prm"))
+    np.random.default_rng(3).standard_normal(9 * deck.n).tofile(tmp_path / "g.bin")
+    d = str(tmp_path)
+    e = dict(os.environ, BDB_GAUSS_FILE=os.path.join(d, "g.bin"), OMP_NUM_THREADS="1")
+    r = subprocess.run([cpu, "c.prm", "steps", os.path.join(d, "ref.bin"), "3"], cwd=d, env=e,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    traj_ref = np.fromfile(os.path.join(d, "ref.bin")).reshape(3, deck.n, 4)
+    traj = run(d, "steps", "3").reshape(3, deck.n, 4)
+    disp = np.abs(traj_ref[0, :, :3] - deck.coord[:, :3]).max()
+    assert np.abs(traj - traj_ref).max() <= 1e-9 * disp

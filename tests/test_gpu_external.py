@@ -75,3 +75,26 @@ def test_rf_field_igt_and_set_time(tmp_path):
         assert err < 1e-9, (k, err)
         prev = traj[k]
     s.close()
+
+
+@pytest.mark.parametrize("hydro", ["none", "cholesky"])
+def test_shear_flow_steps(tmp_path, hydro):
+    """A flowing solvent (vel_grad_tensor): Ermak steps with dt G r against
+    the oracle (pinned to BD_BOX); IGT steps refuse it."""
+    p = decks.write_chain_deck(str(tmp_path), "fl", 30, seed=23, hydro=hydro,
+                               extra={"vel_grad_tensor": "0 0.75 0 0 0 0 0.1 0 0"})
+    deck = decks.read_deck(p)
+    K, n3 = 3, 3 * deck.n
+    g = np.random.default_rng(3).standard_normal(K * n3)
+    traj, _, _ = pyoracle.Oracle(deck).run_steps(K, g)
+    s = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
+    prev = deck.coord
+    for k in range(K):
+        s.step(1, g[k * n3:(k + 1) * n3])
+        x = s.get_coord()
+        err = np.abs(x[:, :3] - traj[k][:, :3]).max() / np.abs(traj[k][:, :3] - prev[:, :3]).max()
+        assert err < 1e-9, (k, err)
+        prev = traj[k]
+    with pytest.raises(engine.BDBError):
+        s.step_igt(1, np.zeros(2 * n3))
+    s.close()

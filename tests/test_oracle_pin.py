@@ -208,3 +208,26 @@ def test_reference_on_the_fly_ewald_tea(tmp_path, method):
     assert rel(Rs, t[:n3]) < 1e-12
     Rs_fly, eps2, _ = pyoracle.Oracle(deck).tea(g, deck.prm["dt"])
     assert abs(eps2 - eps) <= 1e-12 * abs(eps) and rel(Rs_fly, Rs) < 1e-12
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("hydro", ["none", "cholesky"])
+def test_oracle_shear_flow_matches_reference(tmp_path, hydro):
+    """A flowing solvent (vel_grad_tensor): each Ermak step adds dt G r
+    (diff_equation.c:265-283). Three steps of simple shear against BD_BOX's
+    own run."""
+    p = decks.write_chain_deck(str(tmp_path), "fl", 30, seed=23, hydro=hydro,
+                               extra={"vel_grad_tensor": "0 0.75 0 0 0 0 0.1 0 0"})
+    deck = decks.read_deck(p)
+    n3 = 3 * deck.n
+    g = np.random.default_rng(3).standard_normal(3 * n3)
+    g.tofile(tmp_path / "g.bin")
+    env = dict(os.environ, BDB_GAUSS_FILE=str(tmp_path / "g.bin"), OMP_NUM_THREADS="1")
+    subprocess.run([HARNESS, "fl.prm", "steps", "s.bin", "3"], cwd=tmp_path, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = np.fromfile(tmp_path / "s.bin").reshape(3, deck.n, 4)
+    traj, _, _ = pyoracle.Oracle(deck).run_steps(3, g)
+    assert np.abs(traj - ref).max() < 1e-11
+    still = decks.read_deck(p, overrides={"vel_grad_tensor": "0 0 0 0 0 0 0 0 0"})
+    traj0, _, _ = pyoracle.Oracle(still).run_steps(3, g)
+    assert np.abs(traj0 - ref).max() > 1e-3
