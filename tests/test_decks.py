@@ -57,3 +57,27 @@ def test_replica_sizes_are_seeded():
 def test_reads_reference_examples(ex):
     d = decks.read_deck(os.path.join(REF_EXAMPLES, ex))
     assert d.n > 0 and d.coord.shape == (d.n, 4)
+
+
+def test_external_force_and_flow_keys(tmp_path):
+    """The external-field, sphere and flow keys: BD_BOX's defaults
+    (electro_ext.c:30-36, sboundary.c:31-34), their ABI mapping, the sphere
+    check of trans.c iscorrect, and nine doubles for vel_grad_tensor."""
+    from bd_box_b200 import engine
+    p = decks.write_chain_deck(str(tmp_path), "k", 12, seed=2, hydro="none")
+    d = decks.read_deck(p)
+    assert (d.prm["E_magn"], d.prm["sboundary_A"], d.prm["sboundary_n"], d.prm["E_factor"]) == (1.0, 1.0, 2, 1.0)
+    P = engine.params_from_deck(d)
+    assert (P.e_ext, P.sboundary, P.flow) == (0, 0, 0)
+    d = decks.read_deck(p, overrides={"E_ext": "yes", "E_type": "RF", "E_dir1": "z", "E_dir2": "x",
+                                      "vel_grad_tensor": "0 1.5 0 0 0 0 0 0 0.25"})
+    P = engine.params_from_deck(d)
+    # YESNO keys keep BD_BOX's value[0] - 'n' (11 for yes), which is all that is tested
+    assert bool(P.e_ext) and (P.e_type, P.e_dir1, P.e_dir2) == (2, 2, 0)
+    assert P.flow == 1 and list(P.vel_grad) == [0, 1.5, 0, 0, 0, 0, 0, 0, 0.25]
+    with pytest.raises(ValueError):
+        decks.vel_grad({"vel_grad_tensor": "1 2 3"})
+    with pytest.raises(ValueError):       # beads outside the sphere (iscorrect)
+        decks.read_deck(p, overrides={"bc": "sphere", "sphere_radius": 1.0})
+    d = decks.read_deck(p, overrides={"bc": "sphere", "sphere_radius": 500.0})
+    assert engine.params_from_deck(d).bc == 2
