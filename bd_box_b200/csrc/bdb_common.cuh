@@ -139,6 +139,7 @@ struct bdb_system {
     bdb::DevBuf<float> M32b;
     bdb::DevBuf<double4> pos_igt;
     bdb::DevBuf<double> Rf_igt, Rf2_igt, dD_igt;
+    bdb::DevBuf<double> fs_igt;                // the predictor's flow displacement (flowing solvent)
     bool igt_ready = false;                    // a predictor awaits its corrector
     bdb::DevBuf<double> panel64;               // Cholesky workspace
     bool factor_valid = false;
@@ -251,7 +252,7 @@ int factor_run(bdb_system* s);         // Cholesky of the stored D in place
 int stored_matvec(bdb_system* s, bool want_rs);   // Rf = D.F (upper), Rs = L.X (lower)
 int tea_run(bdb_system* s, bool want_rs);         // matrix-free D.F (+ TEA noise)
 int noise_fill(bdb_system* s, const double* host_gauss);   // X = unit Gaussians
-int update_positions(bdb_system* s);  // pos += Rf + Rs, periodic wrap
+int update_positions(bdb_system* s, double* fs = nullptr);  // pos += Rf + Rs, periodic wrap
 int diag_noise(bdb_system* s);        // hydro none: Rs = X sqrt(2 dt D_ii)
 int factor_error(bdb_system* s, double* rel);
 int ensure_matrix(bdb_system* s);    // allocate the stored matrix (identity padding)

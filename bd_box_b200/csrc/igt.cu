@@ -55,7 +55,7 @@ __global__ void k_igt_average(int n3, int npad, T* __restrict__ M, const T* __re
 // with Rf0 = (Rf + Rs)/2 from :333-336)
 __global__ void k_igt_update(int n, int periodic, double3 box, double3 inv_L, const double4* __restrict__ pos0,
                              const double* __restrict__ Rf1, const double* __restrict__ Rf2,
-                             const double* __restrict__ Rs, double4* __restrict__ pos)
+                             const double* __restrict__ Rs, const double* __restrict__ fs, double4* __restrict__ pos)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -63,9 +63,17 @@ __global__ void k_igt_update(int n, int periodic, double3 box, double3 inv_L, co
     const double d0 = mul(0.5, add(Rf1[3 * i], Rf2[3 * i]));
     const double d1 = mul(0.5, add(Rf1[3 * i + 1], Rf2[3 * i + 1]));
     const double d2 = mul(0.5, add(Rf1[3 * i + 2], Rf2[3 * i + 2]));
-    p.x = add(p.x, add(d0, Rs[3 * i]));
-    p.y = add(p.y, add(d1, Rs[3 * i + 1]));
-    p.z = add(p.z, add(d2, Rs[3 * i + 2]));
+    if (fs) {
+        // in a flowing solvent, half the predictor's flow displacement too
+        // (diff_equation.c:303-311)
+        p.x = add(p.x, add(add(d0, Rs[3 * i]), mul(0.5, fs[3 * i])));
+        p.y = add(p.y, add(add(d1, Rs[3 * i + 1]), mul(0.5, fs[3 * i + 1])));
+        p.z = add(p.z, add(add(d2, Rs[3 * i + 2]), mul(0.5, fs[3 * i + 2])));
+    } else {
+        p.x = add(p.x, add(d0, Rs[3 * i]));
+        p.y = add(p.y, add(d1, Rs[3 * i + 1]));
+        p.z = add(p.z, add(d2, Rs[3 * i + 2]));
+    }
     if (periodic) {
         p.x = sub(p.x, mul(box.x, floor(add(mul(p.x, inv_L.x), 0.5))));
         p.y = sub(p.y, mul(box.y, floor(add(mul(p.y, inv_L.y), 0.5))));
@@ -147,7 +155,7 @@ static int igt_predictor(bdb_system* s, const double* g1, bool stop_on_overlap, 
     BDB_CUDA(cudaMemcpyAsync(s->pos_igt.p, s->pos.p, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice, s->stream));
     BDB_CUDA(cudaMemcpyAsync(s->Rf_igt.p, s->Rf.p, v3, cudaMemcpyDeviceToDevice, s->stream));
     phase_mark(s, P_UPDATE);
-    if ((rc = update_positions(s))) return rc;
+    if ((rc = update_positions(s, s->fs_igt.p))) return rc;
     phase_mark(s, P_UPDATE);
     // forces and D(r') F' at the predicted positions
     if ((rc = forces_phase(s))) return rc;
@@ -201,7 +209,7 @@ static int igt_corrector(bdb_system* s, const double* g2)
     k_igt_update<<<(s->n + 127) / 128, 128, 0, s->stream>>>(
         s->n, s->p.bc == 1, make_double3(s->p.box[0], s->p.box[1], s->p.box[2]),
         make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]), s->pos_igt.p, s->Rf_igt.p, s->Rf2_igt.p, s->Rs.p,
-        s->pos.p);
+        (s->p.flow && s->p.bc != 2) ? s->fs_igt.p : nullptr, s->pos.p);
     BDB_CUDA(cudaGetLastError());
     s->launches += 1;
     phase_mark(s, P_UPDATE);
@@ -215,7 +223,7 @@ using namespace bdb;
 static int igt_buffers(bdb_system* s)
 {
     if (s->pos_igt.n < (size_t)s->n && s->pos_igt.alloc(s->n)) return BDB_ERR_NOMEM;
-    for (DevBuf<double>* b : {&s->Rf_igt, &s->Rf2_igt, &s->dD_igt})
+    for (DevBuf<double>* b : {&s->Rf_igt, &s->Rf2_igt, &s->dD_igt, &s->fs_igt})
         if (b->n < (size_t)s->n3 && b->alloc(s->n3)) return BDB_ERR_NOMEM;
     return BDB_OK;
 }
@@ -223,7 +231,6 @@ static int igt_buffers(bdb_system* s)
 static int igt_checks(bdb_system* s, const double* gauss)
 {
     if (!s) return fail(BDB_ERR_ARG, "null system");
-    if (s->p.flow && s->p.bc != 2) return fail(BDB_ERR_UNSUPPORTED, "IGT steps in a flowing solvent are not available");
     if (s->p.noise == BDB_NOISE_HOST && !gauss) return fail(BDB_ERR_ARG, "host noise mode needs Gaussians");
     if (s->p.hydro == BDB_HYDRO_GEYER)
         return fail(BDB_ERR_UNSUPPORTED, "IGT steps need hydro none or cholesky (the averaged tensor is stored)");

@@ -120,7 +120,7 @@ struct Flow {
 // coord_out = Rf + Rs + coord (+ dt G coord in a flow); trans_to_box
 // (diff_equation.c:254-283)
 __global__ void k_update(int n, int periodic, double3 box, double3 inv_L, Flow fl, const double* __restrict__ Rf,
-                         const double* __restrict__ Rs, double4* __restrict__ pos)
+                         const double* __restrict__ Rs, double4* __restrict__ pos, double* __restrict__ fs)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -131,9 +131,19 @@ __global__ void k_update(int n, int periodic, double3 box, double3 inv_L, Flow f
     p.z = add(add(Rf[3 * i + 2], Rs[3 * i + 2]), p.z);
     if (fl.on) {
         const double* G = fl.G;
-        p.x = add(p.x, mul(fl.dt, add(add(mul(G[0], x), mul(G[1], y)), mul(G[2], z))));
-        p.y = add(p.y, mul(fl.dt, add(add(mul(G[3], x), mul(G[4], y)), mul(G[5], z))));
-        p.z = add(p.z, mul(fl.dt, add(add(mul(G[6], x), mul(G[7], y)), mul(G[8], z))));
+        const double t0 = mul(fl.dt, add(add(mul(G[0], x), mul(G[1], y)), mul(G[2], z)));
+        const double t1 = mul(fl.dt, add(add(mul(G[3], x), mul(G[4], y)), mul(G[5], z)));
+        const double t2 = mul(fl.dt, add(add(mul(G[6], x), mul(G[7], y)), mul(G[8], z)));
+        p.x = add(p.x, t0);
+        p.y = add(p.y, t1);
+        p.z = add(p.z, t2);
+        if (fs) {
+            // the flow displacement of an IGT predictor, FS = tmp + dt G r'
+            // at the unwrapped predicted position (diff_equation.c:275-277)
+            fs[3 * i] = add(t0, mul(fl.dt, add(add(mul(G[0], p.x), mul(G[1], p.y)), mul(G[2], p.z))));
+            fs[3 * i + 1] = add(t1, mul(fl.dt, add(add(mul(G[3], p.x), mul(G[4], p.y)), mul(G[5], p.z))));
+            fs[3 * i + 2] = add(t2, mul(fl.dt, add(add(mul(G[6], p.x), mul(G[7], p.y)), mul(G[8], p.z))));
+        }
     }
     if (periodic) {
         p.x = sub(p.x, mul(box.x, floor(add(mul(p.x, inv_L.x), 0.5))));
@@ -143,7 +153,7 @@ __global__ void k_update(int n, int periodic, double3 box, double3 inv_L, Flow f
     pos[i] = p;
 }
 
-int update_positions(bdb_system* s)
+int update_positions(bdb_system* s, double* fs)
 {
     Flow fl;
     fl.on = s->p.flow && s->p.bc != 2;   // a sphere turns the flow off (input.c:462-468)
@@ -151,7 +161,7 @@ int update_positions(bdb_system* s)
     for (int k = 0; k < 9; ++k) fl.G[k] = s->p.vel_grad[k];
     k_update<<<(s->n + 127) / 128, 128, 0, s->stream>>>(
         s->n, s->p.bc == 1, make_double3(s->p.box[0], s->p.box[1], s->p.box[2]),
-        make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]), fl, s->Rf.p, s->Rs.p, s->pos.p);
+        make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]), fl, s->Rf.p, s->Rs.p, s->pos.p, fl.on ? fs : nullptr);
     s->launches += 1;
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;

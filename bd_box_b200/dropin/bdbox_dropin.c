@@ -148,8 +148,6 @@ static void check_supported(void)
         UNERR("bdb200: the IGT algorithms need hydro none or cholesky")
     if (hydro != DIFF_NONE && hydro != DIFF_CHOLESKY && hydro != DIFF_GEYER)
         UNERR("bdb200: hydro must be none, cholesky or geyer")
-    if (vel_grad_tensor && (algorithm == DIFF_ALG_IGT_CONST || algorithm == DIFF_ALG_IGT_VAR))
-        UNERR("bdb200: IGT steps in a flowing solvent are not available")
 }
 
 static void make_params(bdb_params* p)

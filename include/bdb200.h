@@ -101,9 +101,9 @@ typedef struct {
     double sboundary_A, sboundary_cutoff;
     double sphere_radius;     /* bc 2: the reflective sphere around the origin (trans.c:35) */
     /* flowing solvent (vel_grad_tensor, diff_decl.c:72): each Ermak step adds
-     * dt G r, r the bead's start position (diff_equation.c:265-283); off
-     * with bc 2, as BD_BOX turns it off there (input.c:462-468); the IGT
-     * steps refuse it */
+     * dt G r, r the bead's start position (diff_equation.c:265-283); an IGT
+     * corrector adds half the predictor's flow displacement (:303-311); off
+     * with bc 2, as BD_BOX turns it off there (input.c:462-468) */
     int flow;
     double vel_grad[9];       /* G, row-major */
 } bdb_params;

@@ -1119,6 +1119,7 @@ int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K,
     double* X = (double*)malloc(sizeof(double) * n3);
     double* Fp = (double*)malloc(sizeof(double) * n3);
     double* cp = (double*)malloc(sizeof(double) * 4 * s->n);
+    double* FS = (double*)calloc(n3, sizeof(double));
     double preDii, preDij;
     orc_prefactors(s, &preDii, &preDij);
     if (s->hydro == 1) {
@@ -1146,7 +1147,19 @@ int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K,
             for (i = 0; i < n3; ++i) Rs[i] = x1[i] * sqrt(preDii / coord[4 * (i / 3) + 3] * 2 * dt);
         }
         for (i = 0; i < s->n; ++i) {
-            for (k = 0; k < 3; ++k) cp[4 * i + k] = Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
+            if (s->flow) {
+                /* diff_equation.c:265-283: tmp = dt G r, FS = tmp + dt G r' */
+                const double* G = s->vel_grad;
+                const double* c = coord + 4 * i;
+                double tmp[3];
+                for (k = 0; k < 3; ++k) tmp[k] = dt * (G[3 * k] * c[0] + G[3 * k + 1] * c[1] + G[3 * k + 2] * c[2]);
+                for (k = 0; k < 3; ++k) cp[4 * i + k] = Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k] + tmp[k];
+                for (k = 0; k < 3; ++k)
+                    FS[3 * i + k] = tmp[k] + dt * (G[3 * k] * cp[4 * i] + G[3 * k + 1] * cp[4 * i + 1] +
+                                                   G[3 * k + 2] * cp[4 * i + 2]);
+            } else {
+                for (k = 0; k < 3; ++k) cp[4 * i + k] = Rf[3 * i + k] + Rs[3 * i + k] + coord[4 * i + k];
+            }
             cp[4 * i + 3] = coord[4 * i + 3];
             if (s->bc == 1)
                 for (k = 0; k < 3; ++k) cp[4 * i + k] -= s->box[k] * floor(cp[4 * i + k] * s->inv_L[k] + 0.5f);
@@ -1182,7 +1195,9 @@ int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K,
             for (i = 0; i < n3; ++i) Rs[i] = x2[i] * sqrt(preDii / coord[4 * (i / 3) + 3] * 2 * dt);
         }
         for (i = 0; i < s->n; ++i) {
-            for (k = 0; k < 3; ++k) coord[4 * i + k] += Rf[3 * i + k] + Rs[3 * i + k];
+            for (k = 0; k < 3; ++k)
+                coord[4 * i + k] += s->flow ? Rf[3 * i + k] + Rs[3 * i + k] + 0.5 * FS[3 * i + k]
+                                            : Rf[3 * i + k] + Rs[3 * i + k];
             if (s->bc == 1)
                 for (k = 0; k < 3; ++k) coord[4 * i + k] -= s->box[k] * floor(coord[4 * i + k] * s->inv_L[k] + 0.5f);
         }
@@ -1199,6 +1214,7 @@ int orc_run_igt_steps(orc_system* s, double* coord, double* F, double dt, int K,
     free(X);
     free(Fp);
     free(cp);
+    free(FS);
     return rep;
 }
 

@@ -79,8 +79,8 @@ def test_rf_field_igt_and_set_time(tmp_path):
 
 @pytest.mark.parametrize("hydro", ["none", "cholesky"])
 def test_shear_flow_steps(tmp_path, hydro):
-    """A flowing solvent (vel_grad_tensor): Ermak steps with dt G r against
-    the oracle (pinned to BD_BOX); IGT steps refuse it."""
+    """A flowing solvent (vel_grad_tensor): Ermak and IGT steps against the
+    oracle (pinned to BD_BOX)."""
     p = decks.write_chain_deck(str(tmp_path), "fl", 30, seed=23, hydro=hydro,
                                extra={"vel_grad_tensor": "0 0.75 0 0 0 0 0.1 0 0"})
     deck = decks.read_deck(p)
@@ -95,6 +95,19 @@ def test_shear_flow_steps(tmp_path, hydro):
         err = np.abs(x[:, :3] - traj[k][:, :3]).max() / np.abs(traj[k][:, :3] - prev[:, :3]).max()
         assert err < 1e-9, (k, err)
         prev = traj[k]
-    with pytest.raises(engine.BDBError):
-        s.step_igt(1, np.zeros(2 * n3))
+    s.close()
+    # IGT in the flow: the corrector adds half the predictor's flow displacement
+    pi = decks.write_chain_deck(str(tmp_path), "fi", 30, seed=24, hydro=hydro,
+                                extra={"vel_grad_tensor": "0 0.75 0 0 0 0 0.1 0 0", "algorithm": "igt_const"})
+    deck = decks.read_deck(pi)
+    g = np.random.default_rng(5).standard_normal(2 * K * n3)
+    traj, _, _ = pyoracle.Oracle(deck).run_igt_steps(K, g)
+    s = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
+    prev = deck.coord
+    for k in range(K):
+        s.step_igt(1, g[2 * k * n3:2 * (k + 1) * n3])
+        x = s.get_coord()
+        err = np.abs(x[:, :3] - traj[k][:, :3]).max() / np.abs(traj[k][:, :3] - prev[:, :3]).max()
+        assert err < 1e-9, ("igt", k, err)
+        prev = traj[k]
     s.close()

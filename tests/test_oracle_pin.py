@@ -231,3 +231,22 @@ def test_oracle_shear_flow_matches_reference(tmp_path, hydro):
     still = decks.read_deck(p, overrides={"vel_grad_tensor": "0 0 0 0 0 0 0 0 0"})
     traj0, _, _ = pyoracle.Oracle(still).run_steps(3, g)
     assert np.abs(traj0 - ref).max() > 1e-3
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("hydro", ["none", "cholesky"])
+def test_oracle_igt_in_flow_matches_reference(tmp_path, hydro):
+    """IGT predictor-corrector in a flowing solvent: the corrector adds half
+    the predictor's flow displacement FS (diff_equation.c:275-311)."""
+    p = decks.write_chain_deck(str(tmp_path), "fi", 30, seed=24, hydro=hydro,
+                               extra={"vel_grad_tensor": "0 0.75 0 0 0 0 0.1 0 0", "algorithm": "igt_const"})
+    deck = decks.read_deck(p)
+    n3 = 3 * deck.n
+    g = np.random.default_rng(5).standard_normal(6 * n3)
+    g.tofile(tmp_path / "g.bin")
+    env = dict(os.environ, BDB_GAUSS_FILE=str(tmp_path / "g.bin"), OMP_NUM_THREADS="1")
+    subprocess.run([HARNESS, "fi.prm", "steps", "s.bin", "3"], cwd=tmp_path, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = np.fromfile(tmp_path / "s.bin").reshape(3, deck.n, 4)
+    traj, _, rep = pyoracle.Oracle(deck).run_igt_steps(3, g)
+    assert rep == 0 and np.abs(traj - ref).max() < 1e-11
