@@ -250,3 +250,26 @@ def test_oracle_igt_in_flow_matches_reference(tmp_path, hydro):
     ref = np.fromfile(tmp_path / "s.bin").reshape(3, deck.n, 4)
     traj, _, rep = pyoracle.Oracle(deck).run_igt_steps(3, g)
     assert rep == 0 and np.abs(traj - ref).max() < 1e-11
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
+def test_oracle_newton_in_sphere_matches_reference(tmp_path):
+    """ermak_newton inside a reflective sphere with the wall force (bc
+    sphere, sboundary): the collision moves check that every bead stays in
+    the sphere (iscorrect) and the wall pushes beads back; 4 steps against
+    BD_BOX's own run."""
+    p = decks.write_suspension_deck(str(tmp_path), "sp", 40, seed=5, phi=0.3, dt=0.2,
+                                    extra=dict(algorithm="ermak_newton", check_overlap="yes", hydro="none",
+                                               bc="sphere", sphere_radius=7.5, sboundary="yes", sboundary_A=5.0,
+                                               sboundary_n=2, sboundary_cutoff=3.0))
+    deck = decks.read_deck(p)
+    n3 = 3 * deck.n
+    g = np.random.default_rng(4).standard_normal(60 * n3)
+    g.tofile(tmp_path / "g.bin")
+    env = dict(os.environ, BDB_GAUSS_FILE=str(tmp_path / "g.bin"), OMP_NUM_THREADS="1")
+    subprocess.run([HARNESS, "sp.prm", "steps", "s.bin", "4"], cwd=tmp_path, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = np.fromfile(tmp_path / "s.bin").reshape(4, deck.n, 4)
+    traj, _, rc, used, rounds = pyoracle.Oracle(deck).run_newton_steps(4, g)
+    assert rc == 0 and rounds > 4
+    assert np.abs(traj - ref).max() < 1e-10
