@@ -273,3 +273,21 @@ def test_oracle_newton_in_sphere_matches_reference(tmp_path):
     traj, _, rc, used, rounds = pyoracle.Oracle(deck).run_newton_steps(4, g)
     assert rc == 0 and rounds > 4
     assert np.abs(traj - ref).max() < 1e-10
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
+def test_oracle_igt_with_time_dependent_field_matches_reference(tmp_path):
+    """IGT steps under an RF field: both force passes of a step act at
+    curr_time + curr_dt (diff_equation.c:314, 327)."""
+    extra = dict(EXT_DECKS["rf"], algorithm="igt_const")
+    p = decks.write_chain_deck(str(tmp_path), "rfi", 24, seed=91, hydro="cholesky", extra=extra)
+    deck = decks.read_deck(p)
+    n3 = 3 * deck.n
+    g = np.random.default_rng(8).standard_normal(6 * n3)
+    g.tofile(tmp_path / "g.bin")
+    env = dict(os.environ, BDB_GAUSS_FILE=str(tmp_path / "g.bin"), OMP_NUM_THREADS="1")
+    subprocess.run([HARNESS, "rfi.prm", "steps", "s.bin", "3"], cwd=tmp_path, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = np.fromfile(tmp_path / "s.bin").reshape(3, deck.n, 4)
+    traj, _, rep = pyoracle.Oracle(deck).run_igt_steps(3, g)
+    assert rep == 0 and np.abs(traj - ref).max() < 1e-11
