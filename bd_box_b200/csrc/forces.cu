@@ -138,21 +138,27 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
                     H[k] = fmax(H[k], red[3 + k][w]);
                 }
             }
-            // grow the cell until the grid fits the segment's cell table
-            const long long cap = cell_off[2 * blockIdx.x + 1];
+            // grow the cell until the grid fits the segment's cell table. The
+            // cell count is formed in double so that a far-flung bead cannot
+            // overflow it; a non-finite extent (an infinite coordinate) would
+            // never fit, so such a segment takes the brute-force path, where
+            // the non-finite distances raise the overlap flag.
+            const double cap = (double)cell_off[2 * blockIdx.x + 1];
+            bool finite = true;
+            for (int k = 0; k < 3; ++k) finite = finite && isfinite(H[k] - L[k]) && H[k] >= L[k];
             double c = cell;
-            for (;;) {
-                long long tot = 1;
-                for (int k = 0; k < 3; ++k) tot *= (long long)floor((H[k] - L[k]) / c) + 1;
+            while (finite) {
+                double tot = 1;
+                for (int k = 0; k < 3; ++k) tot *= floor((H[k] - L[k]) / c) + 1;
                 if (tot <= cap) break;
                 c *= 1.25;
             }
             for (int k = 0; k < 3; ++k) {
                 g_origin[k] = L[k];
-                g_n[k] = (int)floor((H[k] - L[k]) / c) + 1;
+                g_n[k] = finite ? (int)floor((H[k] - L[k]) / c) + 1 : 1;
             }
             grid[blockIdx.x] = make_double4(L[0], L[1], L[2], c);
-            dims[blockIdx.x] = make_int4(g_n[0], g_n[1], g_n[2], 0);
+            dims[blockIdx.x] = make_int4(g_n[0], g_n[1], g_n[2], finite ? 0 : 1);
         }
     } else if (tid == 0) {
         int nn[3];
@@ -192,7 +198,7 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
             for (int k = 0; k < 3; ++k) {
                 double w = periodic ? (&gr.x)[k] : gr.w;
                 int ci = (int)floor((x[k] - g_origin[k]) / w);
-                if (periodic) ci = ci < 0 ? 0 : (ci >= g_n[k] ? g_n[k] - 1 : ci);
+                ci = ci < 0 ? 0 : (ci >= g_n[k] ? g_n[k] - 1 : ci);   // NaN coordinates stay in the table
                 c[k] = ci;
             }
             unsigned long long cl = ((unsigned long long)c[2] * g_n[1] + c[1]) * g_n[0] + c[0];
@@ -439,59 +445,101 @@ struct BondedArgs {
 
 __device__ __forceinline__ bool bad(double v) { return isnan(v) || isinf(v); }
 
-__device__ void v2n(const BondedArgs& A, const double4* pos, int p1, int p2, double* e, double& r, double& r_sq)
+// ---- vector algebra of the bonded terms ----------------------------------
+struct V3 {
+    double x, y, z;
+};
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b)
 {
-    dist_vec(pos[p1], pos[p2], A.periodic, A.box, A.inv_L, e);
-    r_sq = sq3(e);
-    r = sqrt(r_sq);
-    double inv = 1 / r;
-    e[0] *= inv;
-    e[1] *= inv;
-    e[2] *= inv;
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ bool bad(V3 v) { return bad(v.x) || bad(v.y) || bad(v.z); }
+// clamp into [-1, 1] by comparisons, so that a NaN stays NaN and reaches the
+// overlap flag (fmin/fmax would drop it)
+__device__ __forceinline__ double clamp_unit(double c) { return c <= -1.0 ? -1.0 : (c >= 1.0 ? 1.0 : c); }
+
+// r_to - r_from, with the minimum image when periodic (trans_dist_vec,
+// trans.c:111-121, evaluated exactly)
+__device__ __forceinline__ V3 separation(const BondedArgs& A, const double4* pos, int from, int to)
+{
+    double v[3];
+    dist_vec(pos[from], pos[to], A.periodic, A.box, A.inv_L, v);
+    return {v[0], v[1], v[2]};
 }
 
-__device__ void v3n(const BondedArgs& A, const double4* pos, int p1, int p2, int p3, double* e1, double* e2)
+// The two unit bond vectors of a bond angle at its apex j: u along r_i - r_j
+// and w along r_k - r_j, and cos(theta) = u.w clamped to [-1, 1].
+struct AngleFrame {
+    V3 u, w;
+    double c;
+};
+__device__ __forceinline__ AngleFrame angle_frame(const BondedArgs& A, const double4* pos, int i, int j, int k)
 {
-    dist_vec(pos[p1], pos[p2], A.periodic, A.box, A.inv_L, e1);
-    dist_vec(pos[p3], pos[p2], A.periodic, A.box, A.inv_L, e2);
-    double n1 = 1.0 / sqrt(sq3(e1)), n2 = 1.0 / sqrt(sq3(e2));
-    for (int k = 0; k < 3; ++k) {
-        e1[k] *= n1;
-        e2[k] *= n2;
+    AngleFrame f;
+    const V3 a = separation(A, pos, j, i), b = separation(A, pos, j, k);
+    f.u = (1.0 / sqrt(dot(a, a))) * a;
+    f.w = (1.0 / sqrt(dot(b, b))) * b;
+    f.c = clamp_unit(dot(f.u, f.w));
+    return f;
+}
+
+// Dihedral geometry of the bond vectors b1 = r_j - r_i, b2 = r_k - r_j,
+// b3 = r_l - r_k with the IUPAC sign: n1 = b1 x b2, n2 = b2 x b3,
+// cos phi = n1.n2 / |n1||n2|, sin phi = |b2| b1.n2 / |n1||n2|, and the
+// gradient of phi with respect to the four positions in the form of
+// Blondel and Karplus (J. Comput. Chem. 17, 1132 (1996)):
+//   d phi/d r_i = -|b2| n1 / |n1|^2,   d phi/d r_l = |b2| n2 / |n2|^2,
+//   d phi/d r_j = (b3.b2/|b2|^2) d phi/d r_l - (1 + b1.b2/|b2|^2) d phi/d r_i,
+//   d phi/d r_k = -(the other three),
+// which has no 1/sin phi or 1/cos phi branch. h1, h2: the distances of r_i
+// and r_l from the axis through r_j and r_k (|n1|/|b2|, |n2|/|b2|).
+struct DiheFrame {
+    double c, s, h1, h2;
+    V3 g[4];
+};
+__device__ __forceinline__ DiheFrame dihedral_frame(V3 b1, V3 b2, V3 b3)
+{
+    DiheFrame f;
+    const V3 n1 = cross(b1, b2), n2 = cross(b2, b3);
+    const double q1 = dot(n1, n1), q2 = dot(n2, n2), bb = dot(b2, b2);
+    const double lb = sqrt(bb), inv_n = 1.0 / sqrt(q1 * q2);
+    f.c = dot(n1, n2) * inv_n;
+    f.s = lb * dot(b1, n2) * inv_n;
+    f.h1 = sqrt(q1) / lb;
+    f.h2 = sqrt(q2) / lb;
+    f.g[0] = (-lb / q1) * n1;
+    f.g[3] = (lb / q2) * n2;
+    f.g[1] = (dot(b3, b2) / bb) * f.g[3] - (1.0 + dot(b1, b2) / bb) * f.g[0];
+    f.g[2] = -(f.g[0] + f.g[1] + f.g[3]);
+    return f;
+}
+
+// Chebyshev polynomial T_m(c) = cos(m theta) for c = cos(theta) and its
+// derivative T_m'(c) = m U_{m-1}(c), by the three-term recurrences. BD_BOX
+// tabulates m = 1..6 and takes T = 1, T' = 0 for any other m
+// (get_m_cos / get_delta_cos, dihe.c:146-184).
+__device__ __forceinline__ void chebyshev(int m, double c, double& T, double& dT)
+{
+    if (m < 1 || m > 6) {
+        T = 1.0;
+        dT = 0.0;
+        return;
     }
-}
-
-__device__ __forceinline__ double dcos_m(int m, double c)
-{
-    switch (m) {
-    case 1: return 1;
-    case 2: return 4 * c;
-    case 3: return 12 * c * c - 3;
-    case 4: return c * (32 * c * c - 16);
-    case 5: return c * c * (80 * c * c - 60) + 5;
-    case 6: return c * (192 * c * c * (c * c - 1) + 36);
-    default: return 0;
+    double t_prev = 1.0, t = c, u_prev = 0.0, u = 1.0;   // T_0, T_1; U_-1, U_0
+    for (int k = 1; k < m; ++k) {
+        const double tn = 2.0 * c * t - t_prev, un = 2.0 * c * u - u_prev;
+        t_prev = t;
+        t = tn;
+        u_prev = u;
+        u = un;
     }
-}
-
-__device__ __forceinline__ double cos_m(int m, double c)
-{
-    switch (m) {
-    case 1: return c;
-    case 2: return 2 * c * c - 1;
-    case 3: return 4 * c * c * c - 3 * c;
-    case 4: return 8 * c * c * (c * c - 1) + 1;
-    case 5: return c * (c * c * (16 * c * c - 20) + 5);
-    case 6: return c * c * (c * c * (32 * c * c - 48) + 18) - 1;
-    default: return 1;
-    }
-}
-
-__device__ __forceinline__ void cross3(const double* a, const double* b, double* o)
-{
-    o[0] = a[1] * b[2] - a[2] * b[1];
-    o[1] = a[2] * b[0] - a[0] * b[2];
-    o[2] = a[0] * b[1] - a[1] * b[0];
+    T = t;
+    dT = m * u;
 }
 
 // Term t writes its members' forces into contrib[slot0 + 3*member ...]; slot
@@ -504,209 +552,135 @@ __global__ void k_bonded(BondedArgs A, const double4* __restrict__ pos, double* 
     int slot = 0;
     unsigned st = 0;
     if (t < A.n_bond) {
-        // bond.c:43-85
+        // FENE-type bond (bond.c:43-85): force H (r0 - r) / (1 - r^2/rmax^2)
+        // along the bond, pushing the beads apart when positive; energy
+        // -H/2 [rmax^2 ln((rmax^2 - r^2)/(rmax^2 - r0^2))
+        //       + r0 rmax ln((rmax + r)(rmax - r0) / ((rmax - r)(rmax + r0)))].
+        // r >= rmax is BD_BOX's fatal over-stretch: flagged, no force.
         const int a = A.bond_pairs[2 * t], b = A.bond_pairs[2 * t + 1];
         const double r0 = A.bond_parms[3 * t], rmax = A.bond_parms[3 * t + 1], H = A.bond_parms[3 * t + 2];
-        double e[3], r, r_sq;
-        v2n(A, pos, a, b, e, r, r_sq);
-        double Ff = 0, en = 0;
+        const V3 d = separation(A, pos, a, b);
+        const double r2 = dot(d, d), r = sqrt(r2);
+        const V3 e = (1 / r) * d;                 // unit vector from a to b
+        double push = 0, en = 0;
         if (r < rmax) {
-            en = -0.5 * H * (rmax * rmax * log((rmax * rmax - r_sq) / (rmax * rmax - r0 * r0)) +
+            const double m2 = rmax * rmax;
+            en = -0.5 * H * (m2 * log((m2 - r2) / (m2 - r0 * r0)) +
                              r0 * rmax * log((rmax + r) * (rmax - r0) / ((rmax - r) * (rmax + r0))));
-            double dist_rmax = 1 - r_sq / (rmax * rmax);
-            Ff = H * (r0 - r) / dist_rmax;
+            push = H * (r0 - r) / (1 - r2 / m2);
         } else {
             st |= ST_BOND;
         }
         slot = 2 * t;
         double* c = contrib + 3 * slot;
-        for (int k = 0; k < 3; ++k) {
-            c[k] = -Ff * e[k];
-            c[3 + k] = Ff * e[k];
+        const V3 fb = push * e;
+        c[0] = -fb.x;
+        c[1] = -fb.y;
+        c[2] = -fb.z;
+        c[3] = fb.x;
+        c[4] = fb.y;
+        c[5] = fb.z;
+        energy[t] = en;
+        if (bad(push) || bad(e) || bad(en)) st |= ST_OVERLAP;
+    } else if (t - A.n_bond < A.n_angle + A.n_angle_cos) {
+        // Bond angles at apex j: harmonic in theta (angle.c:38-86) or in
+        // cos theta (angle_cos.c:36-81). BD_BOX's force on an end bead is
+        // the derivative of the energy with respect to its UNIT bond vector:
+        // g times the component of the other bond's unit vector normal to
+        // its own (|w - c u| = sin theta); the 1/|bond| of d theta/d r is
+        // absent in BD_BOX and is left out here too. The apex takes minus
+        // the sum. A harmonic angle within 1e-6 of 0 or pi in cos theta
+        // contributes nothing, energy included.
+        const int ta = t - A.n_bond;
+        const bool harm = ta < A.n_angle;
+        const int tt = harm ? ta : ta - A.n_angle;
+        const int* q = (harm ? A.angle_pairs : A.angle_cos_pairs) + 3 * tt;
+        const double2 prm = reinterpret_cast<const double2*>(harm ? A.angle_parms : A.angle_cos_parms)[tt];
+        const AngleFrame fr = angle_frame(A, pos, q[0], q[1], q[2]);
+        double g = 0.0, en = 0.0;
+        if (harm) {
+            if (!(fr.c >= 1.0 - 0.000001 || fr.c <= -1.0 + 0.000001)) {   // NaN passes on
+                const double d = acos(fr.c) - prm.x;            // theta - theta0
+                en = 0.5 * prm.y * d * d;
+                g = prm.y * d / sqrt(1.0 - fr.c * fr.c);
+            }
+        } else {
+            const double d = fr.c - prm.x;                      // cos theta - cos theta0
+            en = 0.5 * prm.y * d * d;
+            g = -prm.y * d;
+        }
+        const V3 fi = g * (fr.w - fr.c * fr.u), fk = g * (fr.u - fr.c * fr.w);
+        slot = 2 * A.n_bond + 3 * ta;
+        double* c = contrib + 3 * slot;
+        const V3 f3[3] = {fi, -(fi + fk), fk};
+        for (int m = 0; m < 3; ++m) {
+            c[3 * m] = f3[m].x;
+            c[3 * m + 1] = f3[m].y;
+            c[3 * m + 2] = f3[m].z;
         }
         energy[t] = en;
-        if (bad(Ff) || bad(e[0]) || bad(e[1]) || bad(e[2]) || bad(en)) st |= ST_OVERLAP;
-    } else if ((t -= A.n_bond) < A.n_angle) {
-        // angle.c:38-86
-        const int* q = A.angle_pairs + 3 * t;
-        const double phi0 = A.angle_parms[2 * t];
-        double kphi = A.angle_parms[2 * t + 1];
-        double e1[3], e2[3], Fi[3] = {0, 0, 0}, Fk[3] = {0, 0, 0}, en = 0;
-        v3n(A, pos, q[0], q[1], q[2], e1, e2);
-        double cphi = e1[0] * e2[0] + e1[1] * e2[1] + e1[2] * e2[2];
-        cphi = cphi <= -1.0 ? -1.0 : (cphi >= 1.0 ? 1.0 : cphi);
-        if (!(cphi >= 1 - 0.000001 || cphi <= -1 + 0.000001)) {
-            double phi = acos(cphi);
-            kphi *= (phi - phi0);
-            en = 0.5 * kphi * (phi - phi0);
-            kphi /= sqrt(1 - cphi * cphi);
-            for (int k = 0; k < 3; ++k) {
-                Fi[k] = -kphi * (e2[k] - e1[k] * cphi);
-                Fk[k] = -kphi * (e1[k] - e2[k] * cphi);
-            }
-        }
-        slot = 2 * A.n_bond + 3 * t;
-        double* c = contrib + 3 * slot;
-        for (int k = 0; k < 3; ++k) {
-            c[k] = Fi[k];
-            c[3 + k] = -Fi[k] - Fk[k];
-            c[6 + k] = Fk[k];
-        }
-        energy[A.n_bond + t] = en;
-        for (int k = 0; k < 3; ++k)
-            if (bad(Fi[k]) || bad(Fk[k])) st |= ST_OVERLAP;
-        if (bad(en)) st |= ST_OVERLAP;
-    } else if ((t -= A.n_angle) < A.n_angle_cos) {
-        // angle_cos.c:36-81
-        const int* q = A.angle_cos_pairs + 3 * t;
-        const double phi0 = A.angle_cos_parms[2 * t];
-        double kphi = A.angle_cos_parms[2 * t + 1];
-        double e1[3], e2[3], Fi[3], Fk[3];
-        v3n(A, pos, q[0], q[1], q[2], e1, e2);
-        double cphi = e1[0] * e2[0] + e1[1] * e2[1] + e1[2] * e2[2];
-        cphi = cphi <= -1.0 ? -1.0 : (cphi >= 1.0 ? 1.0 : cphi);
-        kphi *= (cphi - phi0);
-        double en = 0.5 * kphi * (cphi - phi0);
-        for (int k = 0; k < 3; ++k) {
-            Fi[k] = kphi * (e2[k] - e1[k] * cphi);
-            Fk[k] = kphi * (e1[k] - e2[k] * cphi);
-        }
-        slot = 2 * A.n_bond + 3 * A.n_angle + 3 * t;
-        double* c = contrib + 3 * slot;
-        for (int k = 0; k < 3; ++k) {
-            c[k] = Fi[k];
-            c[3 + k] = -Fi[k] - Fk[k];
-            c[6 + k] = Fk[k];
-        }
-        energy[A.n_bond + A.n_angle + t] = en;
-        for (int k = 0; k < 3; ++k)
-            if (bad(Fi[k]) || bad(Fk[k])) st |= ST_OVERLAP;
-        if (bad(en)) st |= ST_OVERLAP;
-    } else if ((t -= A.n_angle_cos) < A.n_dihe) {
-        // dihe.c:42-144
+        if (bad(fi) || bad(fk) || bad(en)) st |= ST_OVERLAP;
+    } else if ((t -= A.n_bond + A.n_angle + A.n_angle_cos) < A.n_dihe) {
+        // Cosine dihedral E = |p| (1 + |p| cos(m phi)), p = -k delta
+        // (dihe.c:42-144, parameters as add_dihe stores them, dihe.c:186-203),
+        // bond vectors with the minimum image. Its force is
+        // p T_m'(cos phi) grad(cos phi) = -p sin(phi) T_m'(cos phi) grad(phi).
+        // Nothing (energy included) when r_i or r_l lies within 1e-6 of the
+        // j-k axis.
         const int* q = A.dihe_pairs + 4 * t;
-        const double mkcd = A.dihe_parms[2 * t];
-        const int m = (int)A.dihe_parms[2 * t + 1];
-        double rkj[3], rij[3], rkl[3], rim[3], rln[3];
-        double Fi[3] = {0, 0, 0}, Fj[3] = {0, 0, 0}, Fk[3] = {0, 0, 0}, Fl[3] = {0, 0, 0}, en = 0;
-        dist_vec(pos[q[2]], pos[q[1]], A.periodic, A.box, A.inv_L, rkj);
-        const double nkjsq = rkj[0] * rkj[0] + rkj[1] * rkj[1] + rkj[2] * rkj[2];
-        dist_vec(pos[q[0]], pos[q[1]], A.periodic, A.box, A.inv_L, rij);
-        dist_vec(pos[q[2]], pos[q[3]], A.periodic, A.box, A.inv_L, rkl);
-        const double sijkj = (rij[0] * rkj[0] + rij[1] * rkj[1] + rij[2] * rkj[2]) / nkjsq;
-        const double sklkj = (rkl[0] * rkj[0] + rkl[1] * rkj[1] + rkl[2] * rkj[2]) / nkjsq;
-        for (int k = 0; k < 3; ++k) {
-            rim[k] = -rij[k] + sijkj * rkj[k];
-            rln[k] = rkl[k] - sklkj * rkj[k];
-        }
-        const double nim = sqrt(rim[0] * rim[0] + rim[1] * rim[1] + rim[2] * rim[2]);
-        const double nln = sqrt(rln[0] * rln[0] + rln[1] * rln[1] + rln[2] * rln[2]);
-        if (!(fabs(nim) < 0.000001) && !(fabs(nln) < 0.000001)) {
-            const double inv_nrim = 1.0 / nim, inv_nrln = 1.0 / nln;
-            double ct = (rim[0] * rln[0] + rim[1] * rln[1] + rim[2] * rln[2]) * inv_nrln * inv_nrim;
-            ct = ct < -1 ? -1 : (ct > 1 ? 1 : ct);
-            en = fabs(mkcd) * (1 + fabs(mkcd) * cos_m(m, ct));
-            const double dc = dcos_m(m, ct);
-            double tmp = mkcd * dc * inv_nrim;
-            for (int k = 0; k < 3; ++k) Fi[k] = tmp * (rln[k] * inv_nrln - rim[k] * inv_nrim * ct);
-            tmp = mkcd * dc * inv_nrln;
-            for (int k = 0; k < 3; ++k) Fl[k] = tmp * (rim[k] * inv_nrim - rln[k] * inv_nrln * ct);
-            for (int k = 0; k < 3; ++k) Fj[k] = (sijkj - 1) * Fi[k] - sklkj * Fl[k];
-            for (int k = 0; k < 3; ++k) Fk[k] = -Fi[k] - Fj[k] - Fl[k];
+        const double2 prm = reinterpret_cast<const double2*>(A.dihe_parms)[t];
+        const DiheFrame fr = dihedral_frame(separation(A, pos, q[0], q[1]), separation(A, pos, q[1], q[2]),
+                                            separation(A, pos, q[2], q[3]));
+        double en = 0.0, g = 0.0;
+        const bool live = !(fr.h1 < 0.000001) && !(fr.h2 < 0.000001);   // NaN passes on
+        if (live) {
+            double T, dT;
+            chebyshev((int)prm.y, clamp_unit(fr.c), T, dT);
+            en = fabs(prm.x) * (1.0 + fabs(prm.x) * T);
+            g = -prm.x * fr.s * dT;
         }
         slot = 2 * A.n_bond + 3 * A.n_angle + 3 * A.n_angle_cos + 4 * t;
         double* c = contrib + 3 * slot;
-        for (int k = 0; k < 3; ++k) {
-            c[k] = Fi[k];
-            c[3 + k] = Fj[k];
-            c[6 + k] = Fk[k];
-            c[9 + k] = Fl[k];
+        for (int m = 0; m < 4; ++m) {
+            const V3 f = live ? g * fr.g[m] : V3{0.0, 0.0, 0.0};
+            c[3 * m] = f.x;
+            c[3 * m + 1] = f.y;
+            c[3 * m + 2] = f.z;
+            if (bad(f)) st |= ST_OVERLAP;
         }
         energy[A.n_bond + A.n_angle + A.n_angle_cos + t] = en;
-        for (int k = 0; k < 3; ++k)
-            if (bad(Fi[k]) || bad(Fj[k]) || bad(Fk[k]) || bad(Fl[k])) st |= ST_OVERLAP;
         if (bad(en)) st |= ST_OVERLAP;
     } else if ((t -= A.n_dihe) < A.n_dihe_angle) {
-        // dihe_angle.c:43-255 (no periodic images: measureAndCalcGradDihedral
-        // takes raw coordinate differences)
+        // Harmonic dihedral E = k/2 (phi - phi0)^2 (dihe_angle.c:43-99),
+        // phi with BD_BOX's sign (minus the IUPAC angle) and the difference
+        // wrapped into [-pi, pi] with the float pi; bond vectors WITHOUT the
+        // periodic image, as BD_BOX takes raw differences here. Force
+        // -k (phi - phi0) grad(phi_BD_BOX) = k (phi - phi0) grad(phi_IUPAC);
+        // a collinear triple makes the gradient non-finite, which flags a
+        // retry.
         const int* q = A.dihe_angle_pairs + 4 * t;
-        double kt = A.dihe_angle_parms[2 * t];
-        const double t0 = A.dihe_angle_parms[2 * t + 1];
-        const double4 P1 = pos[q[0]], P2 = pos[q[1]], P3 = pos[q[2]], P4 = pos[q[3]];
-        double r12[3] = {P2.x - P1.x, P2.y - P1.y, P2.z - P1.z};
-        double r23[3] = {P3.x - P2.x, P3.y - P2.y, P3.z - P2.z};
-        double r34[3] = {P4.x - P3.x, P4.y - P3.y, P4.z - P3.z};
-        double Av[3], Bv[3], Cv[3], f1[3], f2[3], f3[3];
-        cross3(r12, r23, Av);
-        cross3(r23, r34, Bv);
-        cross3(r23, Av, Cv);
-        const double rA = 1.0 / sqrt(Av[0] * Av[0] + Av[1] * Av[1] + Av[2] * Av[2]);
-        const double rB = 1.0 / sqrt(Bv[0] * Bv[0] + Bv[1] * Bv[1] + Bv[2] * Bv[2]);
-        const double rC = 1.0 / sqrt(Cv[0] * Cv[0] + Cv[1] * Cv[1] + Cv[2] * Cv[2]);
-        double cp = (Av[0] * Bv[0] + Av[1] * Bv[1] + Av[2] * Bv[2]) * (rA * rB);
-        double sp = (Cv[0] * Bv[0] + Cv[1] * Bv[1] + Cv[2] * Bv[2]) * (rC * rB);
-        cp = cp < -1 ? -1 : (cp > 1 ? 1 : cp);
-        sp = sp < -1 ? -1 : (sp > 1 ? 1 : sp);
-        const double phi = -atan2(sp, cp);
-        for (int k = 0; k < 3; ++k) Bv[k] *= rB;
-        if (fabs(sp) > 0.1) {
-            double dA[3], dB[3];
-            for (int k = 0; k < 3; ++k) Av[k] *= rA;
-            for (int k = 0; k < 3; ++k) {
-                dA[k] = rA * (cp * Av[k] - Bv[k]);
-                dB[k] = rB * (cp * Bv[k] - Av[k]);
-            }
-            const double K1 = 1.0 / sp;
-            f1[0] = K1 * (r23[1] * dA[2] - r23[2] * dA[1]);
-            f1[1] = K1 * (r23[2] * dA[0] - r23[0] * dA[2]);
-            f1[2] = K1 * (r23[0] * dA[1] - r23[1] * dA[0]);
-            f3[0] = K1 * (r23[2] * dB[1] - r23[1] * dB[2]);
-            f3[1] = K1 * (r23[0] * dB[2] - r23[2] * dB[0]);
-            f3[2] = K1 * (r23[1] * dB[0] - r23[0] * dB[1]);
-            f2[0] = K1 * (r12[2] * dA[1] - r12[1] * dA[2] + r34[1] * dB[2] - r34[2] * dB[1]);
-            f2[1] = K1 * (r12[0] * dA[2] - r12[2] * dA[0] + r34[2] * dB[0] - r34[0] * dB[2]);
-            f2[2] = K1 * (r12[1] * dA[0] - r12[0] * dA[1] + r34[0] * dB[1] - r34[1] * dB[0]);
-        } else {
-            double dC[3], dB[3];
-            for (int k = 0; k < 3; ++k) Cv[k] *= rC;
-            for (int k = 0; k < 3; ++k) {
-                dC[k] = rC * (sp * Cv[k] - Bv[k]);
-                dB[k] = rB * (sp * Bv[k] - Cv[k]);
-            }
-            const double K1 = -1.0 / cp;
-            f1[0] = K1 * ((r23[1] * r23[1] + r23[2] * r23[2]) * dC[0] - r23[0] * r23[1] * dC[1] - r23[0] * r23[2] * dC[2]);
-            f1[1] = K1 * ((r23[2] * r23[2] + r23[0] * r23[0]) * dC[1] - r23[1] * r23[2] * dC[2] - r23[1] * r23[0] * dC[0]);
-            f1[2] = K1 * ((r23[0] * r23[0] + r23[1] * r23[1]) * dC[2] - r23[2] * r23[0] * dC[0] - r23[2] * r23[1] * dC[1]);
-            cross3(dB, r23, f3);
-            for (int k = 0; k < 3; ++k) f3[k] *= K1;
-            f2[0] = K1 * (-(r23[1] * r12[1] + r23[2] * r12[2]) * dC[0] + (2.0 * r23[0] * r12[1] - r12[0] * r23[1]) * dC[1] +
-                          (2.0 * r23[0] * r12[2] - r12[0] * r23[2]) * dC[2] + dB[2] * r34[1] - dB[1] * r34[2]);
-            f2[1] = K1 * (-(r23[2] * r12[2] + r23[0] * r12[0]) * dC[1] + (2.0 * r23[1] * r12[2] - r12[1] * r23[2]) * dC[2] +
-                          (2.0 * r23[1] * r12[0] - r12[1] * r23[0]) * dC[0] + dB[0] * r34[2] - dB[2] * r34[0]);
-            f2[2] = K1 * (-(r23[0] * r12[0] + r23[1] * r12[1]) * dC[2] + (2.0 * r23[2] * r12[0] - r12[2] * r23[0]) * dC[0] +
-                          (2.0 * r23[2] * r12[1] - r12[2] * r23[1]) * dC[1] + dB[1] * r34[0] - dB[0] * r34[1]);
-        }
-        double g[12];
-        for (int k = 0; k < 3; ++k) {
-            g[k] = f1[k];
-            g[3 + k] = f2[k] - f1[k];
-            g[6 + k] = f3[k] - f2[k];
-            g[9 + k] = -f3[k];
-        }
-        double tmp = phi - t0;
+        const double2 prm = reinterpret_cast<const double2*>(A.dihe_angle_parms)[t];
+        const double4 P0 = pos[q[0]], P1 = pos[q[1]], P2 = pos[q[2]], P3 = pos[q[3]];
+        const DiheFrame fr = dihedral_frame({P1.x - P0.x, P1.y - P0.y, P1.z - P0.z},
+                                            {P2.x - P1.x, P2.y - P1.y, P2.z - P1.z},
+                                            {P3.x - P2.x, P3.y - P2.y, P3.z - P2.z});
         const double pif = (double)BDB_M_PIF;
-        if (tmp < -pif) tmp += 2 * pif;
-        if (tmp > pif) tmp -= 2 * pif;
-        kt *= -tmp;
-        const double en = -(0.5 * kt * tmp);
+        double d = -atan2(fr.s, fr.c) - prm.y;
+        if (d < -pif) d += 2 * pif;
+        if (d > pif) d -= 2 * pif;
+        const double g = prm.x * d;
+        const double en = 0.5 * g * d;
         slot = 2 * A.n_bond + 3 * A.n_angle + 3 * A.n_angle_cos + 4 * A.n_dihe + 4 * t;
         double* c = contrib + 3 * slot;
-        for (int k = 0; k < 12; ++k) {
-            c[k] = kt * g[k];
-            if (bad(g[k])) st |= ST_OVERLAP;
+        for (int m = 0; m < 4; ++m) {
+            const V3 f = g * fr.g[m];
+            c[3 * m] = f.x;
+            c[3 * m + 1] = f.y;
+            c[3 * m + 2] = f.z;
+            if (bad(fr.g[m])) st |= ST_OVERLAP;
         }
         energy[A.n_bond + A.n_angle + A.n_angle_cos + A.n_dihe + t] = en;
-        if (bad(kt) || bad(en)) st |= ST_OVERLAP;
+        if (bad(g) || bad(en)) st |= ST_OVERLAP;
     }
     if (st) atomicOr(status, st);
 }

@@ -39,6 +39,14 @@
  *           E[0..ENERGY_LAST] (current on the written steps only).
  *
  * The Gaussian stream comes from BDB_GAUSS_FILE (oracle/ref_rand_file.c).
+ *
+ * BDB_EXTRA_DIHE, if set, names a text file of cosine dihedrals, one per
+ * line: "i j k l k_theta m delta" with 0-based bead positions. They are added
+ * through BD_BOX's own add_dihe (potentials/dihe.c:186-204) after the .str
+ * file is read, because BD_BOX's .str parser rejects the cosine dihedral
+ * line (input.c:621-628: parse_doubles(temp, 2) is followed by a check that
+ * no third column exists). The deck must hold no other cosine dihedral, so
+ * that add_dihe starts from an empty array.
  */
 #if HAVE_CONFIG_H
 #include <config.h>
@@ -63,6 +71,7 @@
 #include "potentials/bucket.h"
 #include "potentials/bond.h"
 #include "potentials/calc_func.h"
+#include "potentials/dihe.h"
 #include "potentials/electro.h"
 #include "potentials/LJ.h"
 
@@ -230,6 +239,25 @@ int main(int argc, char** argv)
     apply_options(0);
     init_rand(rand_seed);
     read_str_file();
+    if (getenv("BDB_EXTRA_DIHE")) {
+        FILE* df = fopen(getenv("BDB_EXTRA_DIHE"), "r");
+        int q[4];
+        double kt, m, delta;
+        if (!df || dihe_size) {
+            fprintf(stderr, "harness: cannot add cosine dihedrals\n");
+            return 2;
+        }
+        while (fscanf(df, "%d %d %d %d %lf %lf %lf", q, q + 1, q + 2, q + 3, &kt, &m, &delta) == 7) {
+            if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[3] < 0 || q[0] >= size || q[1] >= size || q[2] >= size ||
+                q[3] >= size) {
+                fprintf(stderr, "harness: dihedral bead out of range\n");
+                return 2;
+            }
+            add_dihe(q[0], q[1], q[2], q[3], kt, m, delta);
+        }
+        fclose(df);
+        end_dihe();
+    }
     init_diff_tensor();
     init_forces();
     for (i = 0; i < DIMS1 * size; i += DIMS1) trans_to_box(coord + i);

@@ -70,12 +70,32 @@ CASES = {
                                                          extra={"algorithm": "igt_const"}),
 }
 
+def cos_dihedrals(n, seed):
+    """Cosine dihedrals on every run of four consecutive beads, rows
+    (i, j, k, l, k_theta, m, delta): multiplicities 1..7 in turn (7 takes
+    BD_BOX's fall-back, cos(m theta) = 1 with no force, dihe.c:146-184),
+    delta = +-1, k_theta in [1, 3]."""
+    rng = np.random.default_rng(seed)
+    return np.array([[i, i + 1, i + 2, i + 3, 1 + 2 * rng.random(), 1 + i % 7, 1.0 if i % 2 else -1.0]
+                     for i in range(n - 3)])
+
+
+# Cases whose cosine dihedrals are added through the harness (BDB_EXTRA_DIHE),
+# because BD_BOX's .str parser cannot read them.
+EXTRA_DIHE = {
+    "chain24_cosdihe": lambda n: cos_dihedrals(n, 110),
+}
+CASES["chain24_cosdihe"] = lambda d: decks.write_chain_deck(d, "c", 24, seed=110, hydro="cholesky")
+
 STEPS = 3
 
 
 def run(d, prm, mode, *args):
     out = os.path.join(d, "out.bin")
     env = dict(os.environ, BDB_GAUSS_FILE=os.path.join(d, "g.bin"), OMP_NUM_THREADS="1")
+    extra = os.path.join(d, "cos_dihe.txt")
+    if os.path.exists(extra):
+        env["BDB_EXTRA_DIHE"] = extra
     subprocess.run([HARNESS, os.path.basename(prm), mode, out, *args], cwd=d, env=env, check=True,
                    stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     return np.fromfile(out)
@@ -90,6 +110,12 @@ def make(name, fn):
         g = np.random.default_rng(zlib.crc32(name.encode())).standard_normal(n3 * STEPS * draws)
         g.tofile(os.path.join(d, "g.bin"))
         res = {"prm": open(prm).read(), "str": open(prm[:-4] + ".str").read(), "gauss": g}
+        if name in EXTRA_DIHE:
+            rows = EXTRA_DIHE[name](n)
+            with open(os.path.join(d, "cos_dihe.txt"), "w") as f:
+                for r in rows:
+                    f.write("%d %d %d %d %.17g %.17g %.17g\n" % tuple(r))
+            res["cos_dihe"] = rows
         res["D"] = run(d, prm, "D").reshape(n3, n3)
         f = run(d, prm, "forces")
         res["F"], res["E"], res["rep"], res["counts"] = f[:n3], f[n3:n3 + 9], f[n3 + 9], f[n3 + 10:n3 + 14]

@@ -22,4 +22,11 @@ def load(name):
     with open(os.path.join(d, "c.str"), "w") as f:
         f.write(str(z["str"]))
     deck = decks.read_deck(os.path.join(d, "c.prm"))
+    if "cos_dihe" in z.files:
+        # cosine dihedrals added through BD_BOX's add_dihe (its .str parser
+        # cannot read them): rows (i, j, k, l, k_theta, m, delta), stored as
+        # add_dihe stores them, (-k_theta delta, m)
+        rows = z["cos_dihe"]
+        deck.dihe_pairs = rows[:, :4].astype(np.int32)
+        deck.dihe_parms = np.stack([-rows[:, 4] * rows[:, 6], rows[:, 5]], axis=1)
     return deck, {k: z[k] for k in z.files if k not in ("prm", "str")}
