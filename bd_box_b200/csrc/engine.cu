@@ -500,6 +500,7 @@ int bdb_set_coord(bdb_system* s, const double* coord)
     BDB_CUDA(cudaMemsetAsync(s->cells_built.p, 0, sizeof(int) * s->segs.size(), s->stream));
     s->have_forces = false;
     s->factor_valid = false;
+    s->igt_ready = false;   // a pending IGT predictor belongs to the old positions
     return BDB_OK;
 }
 
@@ -530,6 +531,7 @@ int bdb_load_state(bdb_system* s)
     s->have_forces = true;
     s->step_count = s->saved_step_count;
     s->sim_time = s->saved_sim_time;
+    s->igt_ready = false;   // a pending IGT predictor belongs to the discarded move
     frames_rewind(s, s->step_count);
     return BDB_OK;
 }

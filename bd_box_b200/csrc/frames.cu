@@ -302,6 +302,7 @@ int bdb_checkpoint_load(bdb_system* s, const void* buf, size_t bytes)
     }
     s->have_forces = false;     // recomputed at the next step
     s->factor_valid = false;    // the stored tensor and its factor are rebuilt at the next step
+    s->igt_ready = false;       // a pending IGT predictor belongs to the replaced state
     return BDB_OK;
 }
 

@@ -16,7 +16,10 @@
 // Products are accumulated in FP64.
 #include <cuda_runtime.h>
 
+#include <cudaTypedefs.h>
+
 #include <algorithm>
+#include <mutex>
 #include <string>
 
 #include "bdb_common.cuh"
@@ -670,8 +673,64 @@ static constexpr size_t NOALLOC_SCRATCH =
 // every device that loads the library, kept until the process exits.
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH];
 
+// Set-up of the entry point, per device: the device address of the array
+// (the host-side symbol is only a stand-in for it) and the SM count. A
+// module's device variables can move when the device's context is destroyed
+// and created again (cudaDeviceReset), so each entry remembers the context it
+// was made in and is made again in a new one. The mutex orders first calls
+// from several host threads.
 static constexpr int NOALLOC_MAX_DEVICES = 64;
-static double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+struct NoallocSlot {
+    bool set = false;
+    unsigned long long ctx_id = 0;
+    double* scratch = nullptr;
+    int sms = 0;
+};
+static NoallocSlot g_noalloc_slot[NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mu;
+
+// ID of the calling thread's current context, 0 if it has none yet
+static unsigned long long current_context_id()
+{
+    static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    if (!get_cur || !get_id) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+        if (!get_cur || !get_id) return 0;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+static int noalloc_setup(int dev, double** scratch, int* sms)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoallocSlot& sl = g_noalloc_slot[dev];
+    unsigned long long id = current_context_id();
+    if (!sl.set || id == 0 || sl.ctx_id != id) {
+        void* p = nullptr;
+        BDB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));   // creates the context if there is none
+        int m = 0;
+        BDB_CUDA(cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev));
+        if (id == 0) id = current_context_id();
+        sl.set = id != 0;   // without a context ID, look the address up on every call
+        sl.ctx_id = id;
+        sl.scratch = static_cast<double*>(p);
+        sl.sms = std::max(1, m);
+    }
+    *scratch = sl.scratch;
+    *sms = sl.sms;
+    return BDB_OK;
+}
 
 }  // namespace bdb
 
@@ -690,21 +749,26 @@ extern "C" int bdb_stored_matvec_noalloc(const float* M, int n3, int ld, const d
     int dev = 0;
     BDB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(BDB_ERR_ARG, "device index out of range");
-    if (!g_noalloc_ptr[dev]) {
-        // set-up, once per device with that device current: the host-side
-        // symbol is only a stand-in, the kernels need its device address
-        void* p = nullptr;
-        BDB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = static_cast<double*>(p);
-    }
+    // set-up, once per device (again in a new context), with the device
+    // current: the kernels need the array's device address
+    double* scratch = nullptr;
+    int sms = 0;
+    int rc = noalloc_setup(dev, &scratch, &sms);
+    if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int nstrip = (n3 + STRIP - 1) / STRIP;
-    int nseg = std::min(NOALLOC_MAX_SEG, std::max(1, (148 * 16 + nstrip - 1) / nstrip));
-    const int seg_cols = ((n3 + nseg - 1) / nseg + 127) / 128 * 128;
-    nseg = (n3 + seg_cols - 1) / seg_cols;
+    // the segmentation of the system path (16 warps per SM), with no more
+    // column segments than the row partials' share of the array holds
+    int nseg, seg_cols;
+    mv_split(n3, 16, sms, &nseg, &seg_cols);
+    const int max_seg = (int)((NOALLOC_SCRATCH - (size_t)nstrip * n3) / (2 * (size_t)n3));
+    if (nseg > max_seg) {
+        seg_cols = ((n3 + max_seg - 1) / max_seg + 127) / 128 * 128;
+        nseg = (n3 + seg_cols - 1) / seg_cols;
+    }
     // every partial that k_mv_finish reads is written first by k_strip_mv,
     // so nothing in the scratch has to start at zero
-    double* rowp = g_noalloc_ptr[dev];
+    double* rowp = scratch;
     double* colp = rowp + (size_t)nseg * n3 * 2;
     const int blocks = (nstrip * nseg + WARPS - 1) / WARPS;
     k_strip_mv<float><<<blocks, 32 * WARPS, 0, st>>>(M, n3, ld, nseg, seg_cols, F, X, rowp, colp);

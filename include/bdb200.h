@@ -359,8 +359,10 @@ void* bdb_stream(bdb_system* s);
  * library's device memory (2.5 MB on every device that loads the library,
  * held until the process exits), so 3N is limited to 3072 (1024 beads) and
  * larger sizes are rejected with BDB_ERR_ARG. The first call on a device
- * looks up that array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture. All calls share the array: calls
+ * looks up that array's device address (cudaGetSymbolAddress) and the SM
+ * count, and looks them up again after the device's context has been
+ * destroyed and created anew (cudaDeviceReset); make that first call before
+ * any stream capture. All calls share the array: calls
  * whose work overlaps on the GPU (different streams, or different host
  * threads) race and must be serialised by the caller. `stream` is a
  * cudaStream_t or NULL for the default stream. */

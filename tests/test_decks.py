@@ -7,7 +7,24 @@ import pytest
 
 from bd_box_b200 import decks
 
-REF_EXAMPLES = "/root/reference/examples"
+
+
+def _reference_examples():
+    """BD_BOX's example decks: $BDB_REFERENCE/examples, else next to the
+    sources the oracle's reference build was compiled from (recorded by
+    `make -C oracle ref` in oracle/_ref/reference_src)."""
+    root = os.environ.get("BDB_REFERENCE")
+    if root:
+        return os.path.join(root, "examples")
+    rec = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "reference_src")
+    if os.path.exists(rec):
+        with open(rec) as f:
+            return os.path.join(os.path.dirname(f.read().strip()), "examples")
+    return ""
+
+
+REF_EXAMPLES = _reference_examples()
 
 
 def test_double_keys_are_float_rounded(tmp_path):

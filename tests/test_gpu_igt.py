@@ -126,3 +126,30 @@ def test_igt_rejects_tea(tmp_path):
     with pytest.raises(engine.BDBError):
         s.step_igt(1)
     s.close()
+
+
+@pytest.mark.parametrize("restore", ["load_state", "set_coord", "checkpoint"])
+def test_corrector_refused_after_a_restore(restore, igt_decks):
+    """A predictor's corrector must not run after the state it belongs to
+    was replaced: it would copy the predictor's start positions over the
+    restored ones. Every restore cancels the pending predictor."""
+    deck = igt_decks["chol"]
+    n3 = 3 * deck.n
+    g = gauss(n3, 1, seed=44)
+    s = engine.System(deck, precision=engine.PREC_FP64, noise=engine.NOISE_HOST)
+    s.save_state()
+    image = s.checkpoint()
+    assert s.igt_predictor(g[:n3]) == 0
+    if restore == "load_state":
+        s.load_state()
+    elif restore == "set_coord":
+        s.set_coord(deck.coord)
+    else:
+        s.restore(image)
+    with pytest.raises(engine.BDBError) as e:
+        s.igt_corrector(g[n3:])
+    assert e.value.code == -1
+    # a new predictor re-arms the corrector
+    assert s.igt_predictor(g[:n3]) == 0
+    assert s.igt_corrector(g[n3:]) == 0
+    s.close()

@@ -28,9 +28,13 @@ def rel(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
-def test_noalloc_matches_existing_entry_points(tmp_path):
+# (beads, extra row padding): a small case; 3N = 3072, where the partial sums
+# fill the fixed array exactly; and 3N = 603, not a multiple of 4, whose edge
+# tiles take the scalar loads, with rows padded past the next multiple of 4
+@pytest.mark.parametrize("beads,pad", [(200, 0), (1024, 0), (201, 64)])
+def test_noalloc_matches_existing_entry_points(tmp_path, beads, pad):
     import torch
-    deck = decks.read_deck(decks.write_chain_deck(str(tmp_path), "na", 200, seed=41, hydro="cholesky"))
+    deck = decks.read_deck(decks.write_chain_deck(str(tmp_path), "na", beads, seed=41, hydro="cholesky"))
     n3 = 3 * deck.n
     dt, T = deck.prm["dt"], deck.prm["T"]
     g = np.random.default_rng(3).standard_normal(n3)
@@ -44,7 +48,7 @@ def test_noalloc_matches_existing_entry_points(tmp_path):
 
     # caller-owned buffers: M holds D above the diagonal and L on/below it
     L = np.linalg.cholesky(D)
-    ld = (n3 + 3) // 4 * 4
+    ld = (n3 + 3) // 4 * 4 + pad
     Mh = np.zeros((n3, ld), dtype=np.float32)
     Mh[:, :n3] = np.triu(D, 1) + L
     dev = torch.device("cuda")
