@@ -75,7 +75,7 @@ struct bdb_system {
     int npad = 0;    // stored-matrix dimension (3n rounded up to the tile)
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;            // look-ahead panel factorisation
-    cudaEvent_t la_ev[2] = {nullptr, nullptr};
+    cudaEvent_t la_ev[3] = {nullptr, nullptr, nullptr};
     double inv_L[3] = {0, 0, 0};
     double preDii = 0, preDij = 0;
 
@@ -127,7 +127,8 @@ struct bdb_system {
     int n_jobs = 0;
     int tea_tile = 32;                         // TEA tile edge (16 or 32 beads)
     int mv_warps = 16;                         // stored matvec: target warps per SM
-    bool autotune = false, tea_tuned = false, mv_tuned = false;
+    int chain_sms = 16;                        // mixed Cholesky: SMs the bulk updates leave to the panel chain
+    bool autotune = false, tea_tuned = false, mv_tuned = false, factor_tuned = false;
     bdb::DevBuf<double> ewald_tab;             // Ewald lattice tables (rpy_tile.cuh EwaldConst)
     int ewald_nk = 0, ewald_nimg = 0;
     bdb::DevBuf<double> M64;                   // stored D (upper) + L (lower), FP64
@@ -143,7 +144,7 @@ struct bdb_system {
     bool igt_ready = false;                    // a predictor awaits its corrector
     bdb::DevBuf<double> panel64;               // Cholesky workspace
     bool factor_valid = false;
-    alignas(64) unsigned char tc_map[640];     // CUtensorMaps: TF32 hi / lo panel buffers (x2), FP32 matrix
+    alignas(64) unsigned char tc_map[1024];    // CUtensorMaps: TF32 hi / lo panel buffers (x3), FP32 matrix
     bool tc_map_ok = false;
     alignas(64) unsigned char mv_map[384];     // CUtensorMaps for the stored matvec: FP32 matrix, X, F
     const void* mv_map_src[3] = {};            // buffers the maps were encoded for

@@ -141,18 +141,18 @@ __device__ __forceinline__ void tri_index(int idx, int& ti, int& tj)
 }
 
 // tile t of a launch -> (ti, tj) relative to the first trailing block:
-// mode 0 all tiles of the lower triangle, 1 only block column 0,
-// 2 all but block column 0
+// mode 0 all tiles of the lower triangle, 1 only block column 0, 2 only
+// block column 1, 3 block columns 2 and beyond
 __device__ __forceinline__ void tile_of_mode(int t, int mode, int& ti, int& tj)
 {
-    if (mode == 1) {
-        ti = t;
-        tj = 0;
+    if (mode == 1 || mode == 2) {
+        tj = mode - 1;
+        ti = t + tj;
     } else {
         tri_index(t, ti, tj);
-        if (mode == 2) {
-            ++ti;
-            ++tj;
+        if (mode == 3) {
+            ti += 2;
+            tj += 2;
         }
     }
 }
@@ -192,22 +192,23 @@ __device__ __forceinline__ int bpos(int r, int c) { return ((c << 2) + (r & 3)) 
 // tile (g, n), n <= g, of the lower triangle of 16 x 16 tiles
 __device__ __forceinline__ int tix(int g, int n) { return g * (g + 1) / 2 + n; }
 
-// 1/x for x > 0 in FP64: the single-precision hardware estimate refined by
-// one Newton-Raphson step q <- q + q (1 - x q) (error ~2^-46).
+// 1/x for x > 0 in FP64: the hardware's FP64 reciprocal estimate (no
+// conversions on the pivot chain) refined by one Newton-Raphson step
+// q <- q + q (1 - x q), which squares its relative error.
 __device__ __forceinline__ double rcp_nr(double x)
 {
-    float e;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"((float)x));
-    const double q = (double)e;
+    double q;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(q) : "d"(x));
     return fma(q, fma(-x, q, 1.0), q);
 }
 
 // Factor the 8x8 block in Dg ([8][9], lower triangle) in registers by one
 // thread: L_kk to the lower triangle of Dg, 1/L_jj to rd. The elimination
-// runs on the unscaled Schur complements, a_ik -= (a_ij a_kj) q_j with
-// q_j = 1/a_jj, so the dependency chain from one pivot to the next is one
-// reciprocal and one FMA (the products a_ij a_kj are formed while q_j is
-// computed); the columns are scaled by 1/sqrt(a_jj) at the end.
+// runs on the unscaled Schur complements with q_j = 1/a_jj: the next pivot
+// a_{j+1,j+1} -= a_{j+1,j}^2 q_j first (the square is formed while q_j is
+// computed, so one reciprocal and one FMA separate two pivots), then the
+// other entries as a_ic -= a_ij (a_cj q_j), one FMA each after the 7-j
+// scaled column entries. The columns are scaled by 1/sqrt(a_jj) at the end.
 __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
 {
     double a[8][8];
@@ -220,10 +221,15 @@ __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
     for (int j = 0; j < 8; ++j) {
         if (!(a[j][j] > 0.0)) ok = false;
         const double q = rcp_nr(a[j][j]);
+        if (j + 1 < 8) a[j + 1][j + 1] = fma(-(a[j + 1][j] * a[j + 1][j]), q, a[j + 1][j + 1]);
+        double t[8];
+#pragma unroll
+        for (int c = j + 1; c < 8; ++c) t[c] = a[c][j] * q;
 #pragma unroll
         for (int r = j + 1; r < 8; ++r)
 #pragma unroll
-            for (int c = j + 1; c <= r; ++c) a[r][c] = fma(-(a[r][j] * a[c][j]), q, a[r][c]);
+            for (int c = j + 1; c <= r; ++c)
+                if (r != j + 1) a[r][c] = fma(-a[r][j], t[c], a[r][c]);
     }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -239,42 +245,87 @@ __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
 static constexpr int POTRF_THREADS = 512;
 static constexpr int NT = PW / 8;                  // 16 row groups of 8 rows
 static constexpr int NTILE = NT * (NT + 1) / 2;    // 136 tiles in the lower triangle
-static constexpr int POTRF_SMEM = (NTILE * 64 + NT * 64 + 80 + 8 + 2 * 64) * 8;
+// Lt tiles, W_kk, the 8x8 block being factored [8][9], 1/L_jj, and one
+// hand-over slot of two tiles per step
+static constexpr int POTRF_SMEM = (NTILE * 64 + NT * 64 + 80 + 8 + NT * 128) * 8;
 // factor hand-off to the panel solve: L_PP tiles then the W_kk, A order
 static constexpr int PANEL_FAC = (NTILE + NT) * 64;
 
 // row group owned by a warp: warp 0 runs the pivots; warps 4, 8, 12 share
 // its scheduler (warp w issues on sub-partition w mod 4) and own the row
-// groups with the least update work (1, 2, 3); the other 12 warps own 4..15
+// groups with the least work (1, 2, 3); the other 12 warps own 4..15
 __device__ __forceinline__ int row_group_of(int warp)
 {
     return (warp & 3) ? 4 + warp - 1 - (warp >> 2) : warp >> 2;
 }
 
+// per-step mbarriers of k_potrf128, each completing exactly once
+struct PotrfBars {
+    uint64_t w[NT];      // W_kk and L_kk published by the pivot warp (32 arrivals)
+    uint64_t lcol[NT];   // every tile of block column k solved (32 per solving warp)
+    uint64_t hand[NT];   // row group k+2's last two tiles and L[k+2][k] handed over (32 arrivals)
+};
+
+// all 32 lanes wait; false on a time-out or an abort seen by this lane
+__device__ __forceinline__ bool bar_wait0(uint64_t* b, volatile int* abort_flag)
+{
+    return mbar_wait(smem_u32(b), 0, abort_flag);
+}
+
+// A solved off-diagonal tile X (C fragments x0, x1 of lane (fr, fq)) of
+// L_PP, tile index t = tix(g, n): to the shared tiles (A order), to the FP64
+// hand-off for the panel solve (the same order) and, as FP32, to M
+__device__ __forceinline__ void put_tile(double* Lt, double* Wt, float* M, size_t row0, size_t col0, int npad, int t,
+                                         int fr, int fq, double x0, double x1)
+{
+    const int p0 = t * 64 + apos(fr, 2 * fq), p1 = t * 64 + apos(fr, 2 * fq + 1);
+    Lt[p0] = x0;
+    Lt[p1] = x1;
+    Wt[p0] = x0;
+    Wt[p1] = x1;
+    *reinterpret_cast<float2*>(M + (row0 + fr) * npad + col0 + 2 * fq) = make_float2((float)x0, (float)x1);
+}
+
+// X = C W^T for an 8x8 tile C held as C fragments (c0, c1) and W in A order
+// (pairs at 2 lane): two DMMAs, the A fragments of C by shuffles
+__device__ __forceinline__ void solve_tile(double c0, double c1, const double* Wk, int lane, int fr, int fq,
+                                           double& x0, double& x1)
+{
+    x0 = 0.0;
+    x1 = 0.0;
+    const double2 wb = *reinterpret_cast<const double2*>(Wk + 2 * lane);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int src = (fr << 2) + 2 * h + (fq >> 1);
+        const double v0 = __shfl_sync(0xffffffffu, c0, src);
+        const double v1 = __shfl_sync(0xffffffffu, c1, src);
+        dmma884(x0, x1, (fq & 1) ? v1 : v0, h ? wb.y : wb.x);
+    }
+}
+
 // FP64 factorisation L_PP of the 128x128 diagonal block (P, P) and the
 // inverses W_kk of its 8x8 diagonal tiles, right-looking over 16 blocks of 8
-// columns with the
-// trailing matrix held in registers: the warp owning row group g keeps its
-// tiles (g, n), n <= g, as DMMA accumulators. Iteration k:
-//   warp 0      factors diagonal tile (k, k) (pivot8) and inverts it
-//               (lanes 0-7), publishing W_kk, L_kk in shared memory;
-//   barrier;
-//   owners g>k  solve tile (g, k): L[g][k] = C[g][k] W_kk^T (two DMMAs),
-//               published in A order;
-//   barrier;
-//   warp 0      applies the last update to diagonal tile k+1 itself (two
-//               DMMAs on the copy its owner handed over one iteration
-//               earlier), then goes on to pivot k+1;
-//   owners g>k+1 update their tiles n = k+1..g: C[g][n] -= L[g][k] L[n][k]^T,
-//               and the owner of row group k+2 hands its diagonal tile
-//               (now updated through column k) to warp 0.
-//   The next pivot thus waits for no owner: warp 0's sub-partition carries
-//   no bulk update (its other warps own row groups 1-3), while an owner's
-//   MMAs queue behind those of the three other owners on its own.
-// Finally L_PP goes to M (FP32, lower triangle) and, in FP64 for the panel
-// solve, its 136 tiles followed by the 16 W_kk to Wt (A order; PANEL_FAC
-// doubles). (Storing each tile as soon as it is final measured slower: the
-// stores then compete with the pivot chain.)
+// columns with the trailing matrix in registers: the warp owning row group g
+// keeps its tiles (g, n), n <= g, as DMMA accumulators. No CTA-wide barrier
+// orders the steps; per-step mbarriers carry exactly what each warp needs:
+//   pivot warp, step k: factor tile (k, k) (pivot8, one thread) and invert
+//     it (lanes 0-7) -> publish W_kk; take row group k+1's last two tiles
+//     (k+1, k) and (k+1, k+1), handed over through column k-2 together with
+//     L[k+1][k-1], and apply column k-1 to them; solve L[k+1][k] = C[k+1][k]
+//     W_kk^T -> publish; update tile (k+1, k+1) with it and go on to pivot
+//     k+1;
+//   owner g, step k < g-1: solve L[g][k] = C[g][k] W_kk^T -> publish; for
+//     k < g-2 update tiles n = k+1..g with column k once all of block column
+//     k is solved and step k's hand-over is made; at k = g-2 hand the tiles
+//     (g, g-1), (g, g) over instead and retire.
+// So the pivot chain waits only for one solve of row group k+2, made while
+// the pivot warp factors and inverts the next block, and the bulk updates
+// of a step start after that hand-over, so that they do not stand in front
+// of it on the FP64 pipes (four warps share each). Each solved tile goes to M (FP32) and
+// to the FP64 hand-off Wt for the panel solve (A order: the 136 L_PP tiles,
+// then the 16 W_kk; PANEL_FAC doubles) as soon as it is final, so nothing
+// is left to store at the end. Every wait is bounded: a time-out sets
+// ST_TIMEOUT and every warp runs out to the final barrier.
 __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict__ M, int npad, int P,
                                                             double* __restrict__ Wt, unsigned* __restrict__ status)
 {
@@ -283,8 +334,10 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
     double* Wa = Lt + NTILE * 64;          // [NT][64] W_kk in A order
     double* Dg = Wa + NT * 64;             // [8][9] diagonal block being factored
     double* rd = Dg + 80;                  // [8] 1/L_jj of that block
-    double* Hd = rd + 8;                   // [2][64] diagonal tiles handed to warp 0 (C layout)
+    double* Hd = rd + 8;                   // [NT][2][64] hand-over slots (C layout)
+    __shared__ PotrfBars bars;
     __shared__ int bad;
+    __shared__ volatile int abort_flag;
     {
         // the warp roles and barrier counts assume this exact launch shape
         uint32_t dyn;
@@ -298,54 +351,136 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
     const int fr = lane >> 2, fq = lane & 3;
     const size_t base = (size_t)P * PW;
     const int g = row_group_of(warp);
-    if (tid == 0) bad = 0;
+    if (tid < NT) {
+        mbar_init(smem_u32(&bars.w[tid]), 32);
+        // solvers of block column k: the pivot warp (row group k+1) and the
+        // owners of row groups k+2..15
+        mbar_init(smem_u32(&bars.lcol[tid]), 32 * (tid < NT - 1 ? NT - 1 - tid : 1));
+        mbar_init(smem_u32(&bars.hand[tid]), 32);
+    }
+    if (tid == 0) {
+        bad = 0;
+        abort_flag = 0;
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncthreads();
+    // launched as a programmatic dependent of the update of this block
+    // column: the set-up above overlaps its tail, M is read only after it
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
     if (warp == 0) {
         // ---------------------------------------------------- pivot warp
+        // tile (0, 0) to Dg; tiles (1, 0) and (1, 1) (nothing updates them
+        // before step 0) as C fragments
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const int c = 2 * fq + e;
             Dg[fr * 9 + c] = c <= fr ? (double)M[(base + fr) * npad + base + c] : 0.0;
+        }
+        double t1[2], t2[2];
+        {
+            const float2 a = *reinterpret_cast<const float2*>(M + (base + 8 + fr) * npad + base + 2 * fq);
+            const float2 b = *reinterpret_cast<const float2*>(M + (base + 8 + fr) * npad + base + 8 + 2 * fq);
+            t1[0] = a.x;
+            t1[1] = a.y;
+            t2[0] = 2 * fq <= fr ? (double)b.x : 0.0;
+            t2[1] = 2 * fq + 1 <= fr ? (double)b.y : 0.0;
         }
         for (int k = 0; k < NT; ++k) {
             __syncwarp();
             if (lane == 0 && !pivot8(Dg, rd)) bad = 1;
             __syncwarp();
             if (lane < 8) {
-                // column c of W_kk by forward substitution (w[m] = 0 for
-                // m < c, so every row sums over all m < i); W_kk and L_kk out
+                // column c of W_kk = L_kk^-1 by right-looking forward
+                // substitution: w_m = acc_m / L_mm, then acc_i -= L_im w_m for
+                // i > m, so only w_m -> acc_m+1 -> w_m+1 is sequential; L_kk
+                // and 1/L_jj are read first
                 const int c = lane;
-                double lk[8][8], r8[8], w[8];
+                double lk[8][8], r8[8], acc[8], w[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
                     r8[i] = rd[i];
 #pragma unroll
-                    for (int m = 0; m < i; ++m) lk[i][m] = Dg[i * 9 + m];
+                    for (int m = 0; m <= i; ++m) lk[i][m] = Dg[i * 9 + m];
+                }
+#pragma unroll
+                for (int i = 0; i < 8; ++i) acc[i] = i == c ? 1.0 : 0.0;
+#pragma unroll
+                for (int m = 0; m < 8; ++m) {
+                    w[m] = m >= c ? acc[m] * r8[m] : 0.0;
+#pragma unroll
+                    for (int i = m + 1; i < 8; ++i) acc[i] = fma(-lk[i][m], w[m], acc[i]);
                 }
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    double v = i == c ? 1.0 : 0.0;
+                    double l = 0.0;
 #pragma unroll
-                    for (int m = 0; m < i; ++m) v = fma(-lk[i][m], w[m], v);
-                    w[i] = i >= c ? v * r8[i] : 0.0;
-                }
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const double l = i >= c ? Dg[i * 9 + c] : 0.0;
-                    Wa[k * 64 + apos(i, c)] = w[i];
-                    Lt[tix(k, k) * 64 + apos(i, c)] = l;
+                    for (int cc = 0; cc <= i; ++cc)
+                        if (cc == c) l = lk[i][cc];
+                    const int pa = apos(i, c);
+                    Wa[k * 64 + pa] = w[i];
+                    Lt[tix(k, k) * 64 + pa] = l;
                 }
             }
-            __syncthreads();   // A: W_kk published
-            __syncthreads();   // B: block column k solved
-            if (k + 1 < NT) {
-                // diagonal tile k+1 = its owner's copy - L[k+1][k] L[k+1][k]^T
-                const double2 t = *reinterpret_cast<const double2*>(Hd + ((k + 1) & 1) * 64 + 2 * lane);
-                const double2 av = *reinterpret_cast<const double2*>(Lt + tix(k + 1, k) * 64 + 2 * lane);
-                double e0 = t.x, e1 = t.y;
-                dmma884(e0, e1, -av.x, av.x);
-                dmma884(e0, e1, -av.y, av.y);
-                Dg[fr * 9 + 2 * fq] = e0;
-                Dg[fr * 9 + 2 * fq + 1] = e1;
+            mbar_arrive(smem_u32(&bars.w[k]));   // release: this lane's writes
+            if (k + 1 == NT) break;
+            __syncwarp();
+            if (k > 0) {
+                // tiles (k+1, k) and (k+1, k+1) through column k-2 and
+                // L[k+1][k-1] from their owner; column k-1 applied here
+                if (!bar_wait0(&bars.hand[k - 1], &abort_flag)) break;
+                const double2 a = *reinterpret_cast<const double2*>(Hd + (size_t)(k - 1) * 128 + 2 * lane);
+                const double2 b = *reinterpret_cast<const double2*>(Hd + (size_t)(k - 1) * 128 + 64 + 2 * lane);
+                const double2 u = *reinterpret_cast<const double2*>(Lt + tix(k + 1, k - 1) * 64 + 2 * lane);
+                const double2 v = *reinterpret_cast<const double2*>(Lt + tix(k, k - 1) * 64 + 2 * lane);
+                t1[0] = a.x;
+                t1[1] = a.y;
+                t2[0] = b.x;
+                t2[1] = b.y;
+                dmma884(t1[0], t1[1], -u.x, v.x);
+                dmma884(t1[0], t1[1], -u.y, v.y);
+                dmma884(t2[0], t2[1], -u.x, u.x);
+                dmma884(t2[0], t2[1], -u.y, u.y);
+            }
+            // L[k+1][k] = C[k+1][k] W_kk^T
+            double x0, x1;
+            solve_tile(t1[0], t1[1], Wa + k * 64, lane, fr, fq, x0, x1);
+            Lt[tix(k + 1, k) * 64 + apos(fr, 2 * fq)] = x0;
+            Lt[tix(k + 1, k) * 64 + apos(fr, 2 * fq + 1)] = x1;
+            __syncwarp();
+            mbar_arrive(smem_u32(&bars.lcol[k]));
+            // tile (k+1, k+1) -= L[k+1][k] L[k+1][k]^T: the next pivot block
+            const double2 av = *reinterpret_cast<const double2*>(Lt + tix(k + 1, k) * 64 + 2 * lane);
+            double e0 = t2[0], e1 = t2[1];
+            dmma884(e0, e1, -av.x, av.x);
+            dmma884(e0, e1, -av.y, av.y);
+            Dg[fr * 9 + 2 * fq] = e0;
+            Dg[fr * 9 + 2 * fq + 1] = e1;
+        }
+    } else if (g == 1) {
+        // ------------------------------------------------------ store warp
+        // (row group 1 needs no owner: the pivot warp takes its tiles). It
+        // copies the pivot warp's results to global memory off the pivot
+        // chain: L_kk and W_kk once published, L[k+1][k] once block column k
+        // is solved; FP64 in A order to Wt, L as FP32 to M
+        for (int k = 0; k < NT; ++k) {
+            if (!bar_wait0(&bars.w[k], &abort_flag)) break;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int p = 2 * lane + h, r = p >> 3, c = ((p & 1) << 2) | ((p & 7) >> 1);
+                const double l = Lt[tix(k, k) * 64 + p];
+                Wt[tix(k, k) * 64 + p] = l;
+                Wt[(NTILE + k) * 64 + p] = Wa[k * 64 + p];
+                if (c <= r) M[(base + 8 * k + r) * npad + base + 8 * k + c] = (float)l;
+            }
+            if (k + 1 == NT) break;
+            if (!bar_wait0(&bars.lcol[k], &abort_flag)) break;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int p = 2 * lane + h, r = p >> 3, c = ((p & 1) << 2) | ((p & 7) >> 1);
+                const double l = Lt[tix(k + 1, k) * 64 + p];
+                Wt[tix(k + 1, k) * 64 + p] = l;
+                M[(base + 8 * (k + 1) + r) * npad + base + 8 * k + c] = (float)l;
             }
         }
     } else {
@@ -361,84 +496,70 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                 cacc[n][1] = (n < g || 2 * fq + 1 <= fr) ? (double)v.y : 0.0;
             }
         }
-        if (g == 1)   // row group 1's diagonal tile needs only column 0: warp 0's
-            *reinterpret_cast<double2*>(Hd + 64 + 2 * lane) = make_double2(cacc[1][0], cacc[1][1]);
-        for (int k = 0; k < NT; ++k) {
-            __syncthreads();   // A
-            if (g > k) {
-                // A fragments of C[g][k] (C layout -> A layout by shuffles)
-                double c0 = 0.0, c1 = 0.0;
+        for (int k = 0; k + 1 < g; ++k) {
+            if (!bar_wait0(&bars.w[k], &abort_flag)) break;
+            // L[g][k] = C[g][k] W_kk^T
+            double c0 = 0.0, c1 = 0.0;
 #pragma unroll
-                for (int t = 0; t < NT; ++t)
-                    if (t == k) {
-                        c0 = cacc[t][0];
-                        c1 = cacc[t][1];
-                    }
-                double x0 = 0.0, x1 = 0.0;
-                const double2 wb = *reinterpret_cast<const double2*>(Wa + k * 64 + 2 * lane);
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int src = (fr << 2) + 2 * h + (fq >> 1);
-                    const double v0 = __shfl_sync(0xffffffffu, c0, src);
-                    const double v1 = __shfl_sync(0xffffffffu, c1, src);
-                    dmma884(x0, x1, (fq & 1) ? v1 : v0, h ? wb.y : wb.x);
+            for (int t = 0; t < NT; ++t)
+                if (t == k) {
+                    c0 = cacc[t][0];
+                    c1 = cacc[t][1];
                 }
-                Lt[tix(g, k) * 64 + apos(fr, 2 * fq)] = x0;
-                Lt[tix(g, k) * 64 + apos(fr, 2 * fq + 1)] = x1;
+            double x0, x1;
+            solve_tile(c0, c1, Wa + k * 64, lane, fr, fq, x0, x1);
+            put_tile(Lt, Wt, M, base + 8 * g, base + 8 * k, npad, tix(g, k), fr, fq, x0, x1);
+            if (k + 2 == g) {
+                // the last two tiles, (g, g-1) and (g, g), through column
+                // k-1, for the pivot warp
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    if (t == g - 1)
+                        *reinterpret_cast<double2*>(Hd + (size_t)k * 128 + 2 * lane) =
+                            make_double2(cacc[t][0], cacc[t][1]);
+                    if (t == g)
+                        *reinterpret_cast<double2*>(Hd + (size_t)k * 128 + 64 + 2 * lane) =
+                            make_double2(cacc[t][0], cacc[t][1]);
+                }
+                __syncwarp();
+                mbar_arrive(smem_u32(&bars.lcol[k]));
+                mbar_arrive(smem_u32(&bars.hand[k]));
+                break;
             }
-            __syncthreads();   // B
-            if (g > k + 1) {
-                const double2 av = *reinterpret_cast<const double2*>(Lt + tix(g, k) * 64 + 2 * lane);
-                // four tiles per batch: their operand loads first (predicated,
-                // no branch), then the MMAs
+            __syncwarp();
+            mbar_arrive(smem_u32(&bars.lcol[k]));
+            const double2 av = *reinterpret_cast<const double2*>(Lt + tix(g, k) * 64 + 2 * lane);
+            // the bulk updates of step k wait for its hand-over, so that the
+            // solve on the pivot chain does not queue behind them
+            if (!bar_wait0(&bars.hand[k], &abort_flag) || !bar_wait0(&bars.lcol[k], &abort_flag)) break;
+            // C[g][n] -= L[g][k] L[n][k]^T for n = k+1..g, four tiles per
+            // batch: their operand loads first (predicated, no branch), then
+            // the MMAs
 #pragma unroll
-                for (int n0 = 1; n0 < NT; n0 += 4) {
-                    double2 bv[4];
+            for (int n0 = 1; n0 < NT; n0 += 4) {
+                double2 bv[4];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int n = n0 + u;
-                        const bool act = n < NT && n > k && n <= g;
-                        bv[u] = act ? *reinterpret_cast<const double2*>(Lt + tix(n, k) * 64 + 2 * lane)
-                                    : make_double2(0.0, 0.0);
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int n = n0 + u;
-                        if (n < NT && n > k && n <= g) {
-                            dmma884(cacc[n][0], cacc[n][1], -av.x, bv[u].x);
-                            dmma884(cacc[n][0], cacc[n][1], -av.y, bv[u].y);
-                        }
-                    }
+                for (int u = 0; u < 4; ++u) {
+                    const int n = n0 + u;
+                    const bool act = n < NT && n > k && n <= g;
+                    bv[u] = act ? *reinterpret_cast<const double2*>(Lt + tix(n, k) * 64 + 2 * lane)
+                                : make_double2(0.0, 0.0);
                 }
-                if (g == k + 2) {
-                    // hand the diagonal tile (updated through column k) to
-                    // warp 0, which applies column k+1 itself
-                    double d0 = 0.0, d1 = 0.0;
 #pragma unroll
-                    for (int t = 0; t < NT; ++t)
-                        if (t == g) {
-                            d0 = cacc[t][0];
-                            d1 = cacc[t][1];
-                        }
-                    *reinterpret_cast<double2*>(Hd + (g & 1) * 64 + 2 * lane) = make_double2(d0, d1);
+                for (int u = 0; u < 4; ++u) {
+                    const int n = n0 + u;
+                    if (n < NT && n > k && n <= g) {
+                        dmma884(cacc[n][0], cacc[n][1], -av.x, bv[u].x);
+                        dmma884(cacc[n][0], cacc[n][1], -av.y, bv[u].y);
+                    }
                 }
             }
         }
     }
     __syncthreads();
-    if (tid == 0 && bad) atomicOr(status, ST_NOT_SPD);
-    // L_PP to M (FP32, lower triangle)
-#pragma unroll 4
-    for (int idx = tid; idx < PW * PW; idx += POTRF_THREADS) {
-        const int r = idx / PW, c = idx % PW;
-        if (c <= r) M[(base + r) * npad + base + c] = (float)Lt[tix(r >> 3, c >> 3) * 64 + apos(r & 7, c & 7)];
-    }
-    // L_PP tiles and the W_kk (A order, FP64) for the panel solve
-    {
-        const double2* src = reinterpret_cast<const double2*>(Lt);
-        double2* dst = reinterpret_cast<double2*>(Wt);
-#pragma unroll 4
-        for (int f = tid; f < PANEL_FAC / 2; f += POTRF_THREADS) dst[f] = src[f];
+    if (tid == 0) {
+        if (bad) atomicOr(status, ST_NOT_SPD);
+        if (abort_flag) atomicOr(status, ST_TIMEOUT);
     }
 }
 
@@ -753,34 +874,40 @@ static int make_panel_map(float* buf, int rows, CUtensorMap* map, int cols = PW)
     return BDB_OK;
 }
 
-// scratch layout in panel64: two panel buffers (hi, lo: FP32 [npad][128]
-// each), then two FP64 128x128 blocks L_PP^T, for even and odd panels
-static void panel_ptrs(bdb_system* s, int par, float** hi, float** lo, double** lkk)
+// scratch layout in panel64: three panel buffer sets (hi, lo: FP32
+// [npad][128] each), then three FP64 128x128 hand-offs of L_PP / W_kk; panel
+// P uses set P mod 3, so a panel's update may still read its set while the
+// next two panels are solved
+static constexpr int PANEL_SETS = 3;
+
+static void panel_ptrs(bdb_system* s, int set, float** hi, float** lo, double** lkk)
 {
     const size_t pan = (size_t)s->npad * PW;
     float* base = reinterpret_cast<float*>(s->panel64.p);
-    *hi = base + (size_t)par * 2 * pan;
+    *hi = base + (size_t)set * 2 * pan;
     *lo = *hi + pan;
-    *lkk = reinterpret_cast<double*>(base + 4 * pan) + (size_t)par * PW * PW;
+    *lkk = reinterpret_cast<double*>(base + (size_t)PANEL_SETS * 2 * pan) + (size_t)set * PANEL_FAC;
 }
 
 static int tc_setup(bdb_system* s)
 {
     if (s->tc_map_ok) return BDB_OK;
     const size_t pan = (size_t)s->npad * PW;
-    if (s->panel64.alloc(2 * pan + 2 * PW * PW + 64)) return BDB_ERR_NOMEM;
+    // floats of the panel sets are counted as half a double each
+    if (s->panel64.alloc((size_t)PANEL_SETS * pan + (size_t)PANEL_SETS * PANEL_FAC + 64)) return BDB_ERR_NOMEM;
     BDB_CUDA(cudaMemset(s->panel64.p, 0, s->panel64.n * sizeof(double)));
-    CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(s->tc_map);   // hi0, lo0, hi1, lo1, M
-    for (int par = 0; par < 2; ++par) {
+    static_assert(sizeof(CUtensorMap) * (2 * PANEL_SETS + 1) <= sizeof(bdb_system::tc_map), "tensor-map storage");
+    CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(s->tc_map);   // hi0, lo0, hi1, lo1, hi2, lo2, M
+    for (int set = 0; set < PANEL_SETS; ++set) {
         float *hi, *lo;
         double* lkk;
-        panel_ptrs(s, par, &hi, &lo, &lkk);
-        int rc = make_panel_map(hi, s->npad, &maps[2 * par]);
+        panel_ptrs(s, set, &hi, &lo, &lkk);
+        int rc = make_panel_map(hi, s->npad, &maps[2 * set]);
         if (rc) return rc;
-        rc = make_panel_map(lo, s->npad, &maps[2 * par + 1]);
+        rc = make_panel_map(lo, s->npad, &maps[2 * set + 1]);
         if (rc) return rc;
     }
-    int rc = make_panel_map(s->M32.p, s->npad, &maps[4], s->npad);
+    int rc = make_panel_map(s->M32.p, s->npad, &maps[2 * PANEL_SETS], s->npad);
     if (rc) return rc;
     BDB_CUDA(cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_potrf128, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM));
@@ -811,62 +938,98 @@ static cudaError_t launch_syrk(bdb_system* s, int grid, cudaStream_t st, const C
     return cudaLaunchKernelEx(&cfg, k_syrk_tc, hi, lo, c, t0, ntiles, mode, s->status.p);
 }
 
-// Factorisation with one panel of look-ahead. For panel P the trailing
-// update is split: block column P+1 first (main stream), then the FP64
-// diagonal factorisation of block P+1 runs on the second stream on an SM
-// that the persistent update of the remaining tiles leaves free; the panel
-// solve of P+1 follows once both are done. Panel buffers alternate between
-// even and odd panels so the two never share one.
+// k_potrf128 the same way, behind the update of its block column
+static cudaError_t launch_potrf(bdb_system* s, cudaStream_t st, int P, double* lkk)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(POTRF_THREADS);
+    cfg.dynamicSmemBytes = POTRF_SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_potrf128, s->M32.p, s->npad, P, lkk, s->status.p);
+}
+
+// Factorisation with two panels of look-ahead on two streams. Panel P's
+// trailing update is split three ways: A (block column P+1), B (block
+// column P+2) and C (block columns P+3 and beyond).
+//   chain stream:  panel solve P -> A(P) -> diagonal block P+1 -> ...
+//   bulk stream:   B(P) -> C(P) -> B(P+1) -> C(P+1) -> ...
+// The bulk stream starts B(P) once panel P is solved; the chain stream
+// waits for B(P-1) before the panel solve P, since A(P) updates block
+// column P+1 after B(P-1) did. So C(P) runs beside the next two steps of
+// the chain, and every tile still receives its updates in panel order
+// (the same sums, so the same bits, as with no look-ahead).
 int factor_mixed_tc(bdb_system* s)
 {
     int rc = tc_setup(s);
     if (rc) return rc;
     const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(s->tc_map);
+    const CUtensorMap& mapc = maps[2 * PANEL_SETS];
     const int nt = s->npad / PW;
     cudaStream_t st = s->stream, st2 = s->stream2;
+    cudaEvent_t ev_solved = s->la_ev[0], ev_b = s->la_ev[1], ev_end = s->la_ev[2];
+    // the persistent bulk updates leave s->chain_sms SMs to the chain
+    // kernels running beside them (tuned: engine.cu factor_tune)
+    const int bulk_sms = std::max(1, s->sm_count - std::min(std::max(s->chain_sms, 0), s->sm_count - 1));
     float *hi, *lo;
     double* lkk;
     panel_ptrs(s, 0, &hi, &lo, &lkk);
     phase_mark_on(s, P_POTRF, st);
-    k_potrf128<<<1, POTRF_THREADS, POTRF_SMEM, st>>>(s->M32.p, s->npad, 0, lkk, s->status.p);
+    BDB_CUDA(launch_potrf(s, st, 0, lkk));
     phase_mark_on(s, P_POTRF, st);
     s->launches += 1;
+    // the bulk stream starts after everything before the factorisation
+    BDB_CUDA(cudaEventRecord(ev_solved, st));
+    BDB_CUDA(cudaStreamWaitEvent(st2, ev_solved, 0));
     for (int P = 0; P + 1 < nt; ++P) {
-        const int par = P & 1;
-        panel_ptrs(s, par, &hi, &lo, &lkk);
+        const int set = P % PANEL_SETS;
+        panel_ptrs(s, set, &hi, &lo, &lkk);
+        const int rem = nt - P - 1;   // trailing block columns
+        if (P > 0) BDB_CUDA(cudaStreamWaitEvent(st, ev_b, 0));   // B(P-1)
         const int units = (s->npad - (P + 1) * PW) / 8;
         const int per_cta = TRSM_THREADS / 32;
         phase_mark_on(s, P_TRSM, st);
         k_trsm128<<<std::min(s->sm_count, (units + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st>>>(
             s->M32.p, s->npad, P, lkk, hi, lo, s->status.p);
         phase_mark_on(s, P_TRSM, st);
-        const int rem = nt - P - 1;
-        // block column P+1 of the trailing matrix
-        phase_mark_on(s, P_SYRK_COL, st);
-        BDB_CUDA(launch_syrk(s, std::min(s->sm_count, rem), st, maps[2 * par], maps[2 * par + 1], maps[4], P + 1, rem, 1));
-        phase_mark_on(s, P_SYRK_COL, st);
-        s->launches += 2;
-        // diagonal block P+1 on the side stream, beside the rest of the update
-        float *hi2, *lo2;
-        double* lkk2;
-        panel_ptrs(s, par ^ 1, &hi2, &lo2, &lkk2);
-        BDB_CUDA(cudaEventRecord(s->la_ev[0], st));
-        BDB_CUDA(cudaStreamWaitEvent(st2, s->la_ev[0], 0));
-        phase_mark_on(s, P_POTRF, st2);
-        k_potrf128<<<1, POTRF_THREADS, POTRF_SMEM, st2>>>(s->M32.p, s->npad, P + 1, lkk2, s->status.p);
-        phase_mark_on(s, P_POTRF, st2);
-        BDB_CUDA(cudaEventRecord(s->la_ev[1], st2));
-        s->launches += 1;
-        const int rest = rem * (rem + 1) / 2 - rem;
-        if (rest > 0) {
-            phase_mark_on(s, P_SYRK_REST, st);
-            BDB_CUDA(launch_syrk(s, std::min(s->sm_count - 1, rest), st, maps[2 * par], maps[2 * par + 1], maps[4], P + 1,
-                                 rest, 2));
-            phase_mark_on(s, P_SYRK_REST, st);
+        BDB_CUDA(cudaGetLastError());
+        BDB_CUDA(cudaEventRecord(ev_solved, st));
+        // bulk: B(P) and C(P)
+        BDB_CUDA(cudaStreamWaitEvent(st2, ev_solved, 0));
+        phase_mark_on(s, P_SYRK_REST, st2);
+        if (rem >= 2) {
+            BDB_CUDA(launch_syrk(s, std::min(bulk_sms, rem - 1), st2, maps[2 * set], maps[2 * set + 1], mapc, P + 1,
+                                 rem - 1, 2));
             s->launches += 1;
         }
-        BDB_CUDA(cudaStreamWaitEvent(st, s->la_ev[1], 0));
+        BDB_CUDA(cudaEventRecord(ev_b, st2));
+        if (rem >= 3) {
+            const int ntc = (rem - 2) * (rem - 1) / 2;
+            BDB_CUDA(launch_syrk(s, std::min(bulk_sms, ntc), st2, maps[2 * set], maps[2 * set + 1], mapc, P + 1, ntc,
+                                 3));
+            s->launches += 1;
+        }
+        phase_mark_on(s, P_SYRK_REST, st2);
+        // chain: A(P), then the diagonal block P+1
+        phase_mark_on(s, P_SYRK_COL, st);
+        BDB_CUDA(launch_syrk(s, std::min(s->sm_count, rem), st, maps[2 * set], maps[2 * set + 1], mapc, P + 1, rem, 1));
+        phase_mark_on(s, P_SYRK_COL, st);
+        double *lkk1;
+        float *hi1, *lo1;
+        panel_ptrs(s, (P + 1) % PANEL_SETS, &hi1, &lo1, &lkk1);
+        phase_mark_on(s, P_POTRF, st);
+        BDB_CUDA(launch_potrf(s, st, P + 1, lkk1));
+        phase_mark_on(s, P_POTRF, st);
+        s->launches += 3;
     }
+    // join the bulk stream
+    BDB_CUDA(cudaEventRecord(ev_end, st2));
+    BDB_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;
 }

@@ -136,6 +136,42 @@ int build_and_factor(bdb_system* s)
     return BDB_OK;
 }
 
+// Autotuning of the mixed Cholesky's split of the GPU between its panel
+// chain and its bulk updates (chol_tc.cu): each candidate reserve is timed on
+// one factorisation of a freshly built D; the last one leaves the factor of
+// the current positions in place.
+static int factor_tune(bdb_system* s)
+{
+    const int cands[4] = {8, 16, 32, 48};
+    float best_ms = 1e30f;
+    int best = s->chain_sms;
+    cudaEvent_t e0, e1;
+    BDB_CUDA(cudaEventCreate(&e0));
+    BDB_CUDA(cudaEventCreate(&e1));
+    int rc = BDB_OK;
+    for (int c : cands) {
+        s->chain_sms = c;
+        if ((rc = tensor_build(s))) break;
+        if (cudaEventRecord(e0, s->stream) != cudaSuccess) { rc = cuda_fail(cudaGetLastError(), "cudaEventRecord"); break; }
+        if ((rc = factor_run(s))) break;
+        if (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = cuda_fail(cudaGetLastError(), "factor timing");
+            break;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->chain_sms = best;
+    s->factor_tuned = true;
+    return rc;
+}
+
 // D (and its factor) at the current positions. After one eager refresh
 // (which allocates and encodes everything the kernels use), the mixed path
 // replays the ~400 launches of a refresh -- both streams of the look-ahead
@@ -169,7 +205,11 @@ static int refresh_factor(bdb_system* s)
         BDB_CUDA(cudaGraphLaunch(s->refresh_graph, s->stream));
         s->launches += s->refresh_launches;
     } else {
-        rc = build_and_factor(s);
+        if (s->autotune && !s->factor_tuned && s->p.precision == BDB_PREC_MIXED) {
+            rc = factor_tune(s);
+        } else {
+            rc = build_and_factor(s);
+        }
         if (rc) return rc;
         s->eager_refreshes++;
     }
@@ -364,7 +404,8 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->la_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->la_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&s->la_ev[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->la_ev[2], cudaEventDisableTiming) != cudaSuccess) {
         bdb_destroy(s);
         return fail(BDB_ERR_CUDA, "stream/event creation failed");
     }
@@ -682,6 +723,18 @@ int bdb_step(bdb_system* s, int K, const double* gauss)
     return ov ? 1 : 0;
 }
 
+int bdb_refresh(bdb_system* s, int count)
+{
+    if (!s || count < 0) return fail(BDB_ERR_ARG, "bad arguments");
+    if (s->p.hydro != BDB_HYDRO_CHOLESKY) return fail(BDB_ERR_UNSUPPORTED, "no stored tensor: hydro is not cholesky");
+    BDB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream));
+    for (int k = 0; k < count; ++k) {
+        const int rc = refresh_factor(s);
+        if (rc) return rc;
+    }
+    return check_status(s, nullptr);
+}
+
 int bdb_autotune(bdb_system* s, int enable)
 {
     if (!s) return fail(BDB_ERR_ARG, "null system");
@@ -712,6 +765,25 @@ int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm)
         drop_graph(s);
     }
     s->tea_tuned = s->mv_tuned = true;   // pinned values are not re-tuned
+    return BDB_OK;
+}
+
+int bdb_get_factor_tuning(bdb_system* s, int* chain_sms)
+{
+    if (!s || !chain_sms) return fail(BDB_ERR_ARG, "null argument");
+    *chain_sms = s->chain_sms;
+    return BDB_OK;
+}
+
+int bdb_set_factor_tuning(bdb_system* s, int chain_sms)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    if (chain_sms < 0 || chain_sms > 4096) return fail(BDB_ERR_ARG, "chain SMs out of range");
+    if (chain_sms && chain_sms != s->chain_sms) {
+        s->chain_sms = chain_sms;
+        drop_graph(s);
+    }
+    s->factor_tuned = true;   // a pinned value is not re-tuned
     return BDB_OK;
 }
 

@@ -45,7 +45,8 @@ EXPORTS = [
     "bdb_reset_stats", "bdb_launches", "bdb_stream", "bdb_stored_matvec_noalloc", "bdb_shard_replicas",
     "bdb_frames_start", "bdb_frames_take", "bdb_frames_pending", "bdb_frames_flush", "bdb_frames_stop",
     "bdb_set_time", "bdb_get_time", "bdb_newton_resolve",
-    "bdb_checkpoint_size", "bdb_checkpoint_save", "bdb_checkpoint_load",
+    "bdb_checkpoint_size", "bdb_checkpoint_save", "bdb_checkpoint_load", "bdb_refresh",
+    "bdb_get_factor_tuning", "bdb_set_factor_tuning",
 ]
 
 
@@ -106,6 +107,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_compute_r.argtypes = [C.c_void_p, _dp, _dp]
     lib.bdb_step.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.bdb_step_igt.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.bdb_refresh.argtypes = [C.c_void_p, C.c_int]
     lib.bdb_step_igt_predictor.argtypes = [C.c_void_p, _dp]
     lib.bdb_step_igt_corrector.argtypes = [C.c_void_p, _dp]
     lib.bdb_set_dt.argtypes = [C.c_void_p, C.c_double]
@@ -113,6 +115,8 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_autotune.argtypes = [C.c_void_p, C.c_int]
     lib.bdb_get_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.bdb_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.bdb_get_factor_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    lib.bdb_set_factor_tuning.argtypes = [C.c_void_p, C.c_int]
     lib.bdb_adjoint.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _ip, _dp, _dp, _dp, _dp]
     lib.bdb_factor_error.argtypes = [C.c_void_p, _dp]
     lib.bdb_profile.argtypes = [C.c_void_p, C.c_int]
@@ -297,6 +301,11 @@ class System:
         g = None if gauss is None else np.ascontiguousarray(gauss, dtype=np.float64)
         return self._check(self.lib.bdb_step(self.h, K, _p(g)))
 
+    def refresh(self, count: int = 1):
+        """Rebuild the stored tensor and its Cholesky factor `count` times
+        at the current positions (bdb_refresh)."""
+        self._check(self.lib.bdb_refresh(self.h, int(count)))
+
     def step_igt(self, K: int = 1, gauss=None) -> int:
         """K IGT predictor-corrector steps (bdb_step_igt); gauss: K*2*3N
         host Gaussians (predictor then corrector per step) in host-noise
@@ -357,6 +366,15 @@ class System:
 
     def set_tuning(self, tea_tile: int = 0, mv_warps_per_sm: int = 0):
         self._check(self.lib.bdb_set_tuning(self.h, tea_tile, mv_warps_per_sm))
+
+    def factor_tuning(self) -> int:
+        """SMs the mixed Cholesky's bulk updates leave to its panel chain."""
+        a = C.c_int()
+        self._check(self.lib.bdb_get_factor_tuning(self.h, C.byref(a)))
+        return a.value
+
+    def set_factor_tuning(self, chain_sms: int):
+        self._check(self.lib.bdb_set_factor_tuning(self.h, int(chain_sms)))
 
     def factor_error(self) -> float:
         out = C.c_double()

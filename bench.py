@@ -36,13 +36,14 @@ sys.path.insert(0, ROOT)
 
 N_BEADS = 4096
 REFRESH = 10
+REFRESH_TIMED = 10   # refreshes timed by themselves for the roofline
 SEED = 2
 METRIC = "BD steps/s at N=4096, mixed vs FP64 GPU at stated error; Cholesky TFLOP/s"
 
 
-def make_deck(tmp: str):
+def make_deck(tmp: str, beads: int = N_BEADS):
     from bd_box_b200 import decks
-    p = decks.write_chain_deck(tmp, "chain4096", N_BEADS, seed=SEED, hydro="cholesky", steps=1000)
+    p = decks.write_chain_deck(tmp, f"chain{beads}", beads, seed=SEED, hydro="cholesky", steps=1000)
     return p, decks.read_deck(p)
 
 
@@ -103,7 +104,7 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------- CPU baseline
-def reference_cpu(prm_path: str, deck, steps: int):
+def reference_cpu(prm_path: str, deck, steps: int, single_thread: bool = True):
     """The reference's own CPU build (oracle/_ref/ref_harness: BD_BOX sources,
     -O3, OpenMP, LAPACK via OpenBLAS) on this host's cores, `steps` steps
     with D and its Cholesky factor rebuilt every REFRESH steps. Falls back to
@@ -118,20 +119,29 @@ def reference_cpu(prm_path: str, deck, steps: int):
     env = dict(os.environ, BDB_GAUSS_FILE=gpath, OMP_NUM_THREADS=str(cores),
                OPENBLAS_NUM_THREADS=str(cores))
     if os.path.exists(harness):
-        def run(k):
+        def run(mode, threads, *extra):
+            e = dict(env, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS=str(threads))
             t0 = time.perf_counter()
-            subprocess.run([harness, os.path.basename(prm_path), "steps", "out.bin", str(k), str(REFRESH)],
-                           cwd=d, env=env, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            subprocess.run([harness, os.path.basename(prm_path), mode, "out.bin", *extra], cwd=d, env=e, check=True,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
             return time.perf_counter() - t0
-        t = run(steps)
-        # start-up (reading the deck, first forces) is timed separately and removed
-        t0 = time.perf_counter()
-        subprocess.run([harness, os.path.basename(prm_path), "forces", "f.bin"], cwd=d, env=env, check=True,
-                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-        t_init = time.perf_counter() - t0
-        return {"value": steps / max(t - t_init, 1e-9), "unit": "steps/s", "cores": cores, "kind": "reference",
+
+        def rate(threads, reps):
+            # start-up (reading the deck, first forces) is timed in its own
+            # run of the same process and removed
+            out = []
+            for _ in range(reps):
+                t = run("steps", threads, str(steps), str(REFRESH))
+                t_init = run("forces", threads)
+                out.append(steps / max(t - t_init, 1e-9))
+            return out
+
+        runs = rate(cores, 3)
+        single = rate(1, 1)[0] if single_thread else None
+        return {"value": float(np.median(runs)), "unit": "steps/s", "cores": cores, "kind": "reference",
+                "runs": runs, "statistic": "median of 3 runs", "single_thread_value": single,
                 "sample": f"{steps} steps of the N={deck.n} chain with one D build + LAPACK dpotrf per {REFRESH} "
-                          f"steps (BD_BOX CPU sources, OpenMP + OpenBLAS, {cores} threads)"}
+                          f"steps (BD_BOX CPU sources, OpenMP + OpenBLAS, {cores} threads; start-up removed)"}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     o = pyoracle.Oracle(deck)
@@ -161,6 +171,21 @@ def time_steps(torch, sysm, K, per_call=None):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1)
+
+
+def time_refresh(torch, sysm, K):
+    """K refreshes of the stored tensor and its factor (bdb_refresh: the
+    refresh graph that the timed steps replay every REFRESH steps), CUDA
+    events on the engine's stream; ms per refresh."""
+    stream = torch.cuda.ExternalStream(sysm.lib.bdb_stream(sysm.h))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sysm.refresh(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / K
 
 
 def phase(sysm, name):
@@ -209,7 +234,7 @@ def run_ours(args):
     dist, rank, world, local = ranks.init("nccl")
     tmp = tempfile.mkdtemp(prefix="bdb_bench_")
     try:
-        prm, deck = make_deck(tmp)
+        prm, deck = make_deck(tmp, args.beads)
         n3 = 3 * deck.n
         sysm = engine.System(deck, precision=engine.PREC_MIXED, refresh=REFRESH,
                              noise=engine.NOISE_PHILOX, seed=ranks.replica_seed(SEED, rank))
@@ -227,6 +252,9 @@ def run_ours(args):
             ms = time_steps(torch, sysm, args.steps)
         launches = C.c_longlong()
         sysm.lib.bdb_launches(sysm.h, C.byref(launches))
+        # the refresh (tensor build + factorisation) alone, replayed from the
+        # same graph as inside the timed steps: the roofline's launch
+        refresh_ms = time_refresh(torch, sysm, REFRESH_TIMED)
         # the same steps as K one-step calls (a host round trip per step)
         ms_single = time_steps(torch, sysm, args.steps, per_call=1)
         # phase breakdown: a separate profiled pass of the same length (CUDA
@@ -270,45 +298,49 @@ def run_ours(args):
         # plain FP64 GPU path (full Cholesky every step, the reference schedule)
         fp64 = None
         if rank == 0 and world == 1 and not args.skip_fp64:
-            s64 = engine.System(deck, precision=engine.PREC_FP64, refresh=1, noise=engine.NOISE_PHILOX, seed=5)
-            s64.step(1)
-            k64 = 3
-            ms64 = time_steps(torch, s64, k64)
-            fp64 = {"value": k64 / (ms64 / 1e3), "unit": "steps/s",
-                    "note": "FP64 everywhere, D and Cholesky rebuilt every step"}
-            s64.close()
+            fp64 = fp64_case(torch, engine, deck, value)
 
         errors = None
         if rank == 0 and world == 1 and not args.skip_errors:
             errors = accuracy(torch, engine, deck)
 
         hbm, bf16, bf16s, src = peaks()
-        # dominant phase: the Cholesky factorisation (amortised over REFRESH steps)
+        # dominant phase: the refresh (tensor build + Cholesky factorisation,
+        # one graph launch every REFRESH steps), timed by itself above
         n = 3 * deck.n
         flops = n ** 3 / 3.0
         fac_avg = fac_ms / max(fac_calls, 1)
         mv_avg = mv_ms / max(mv_calls, 1)
-        share_fac = fac_ms / ms_prof if ms_prof else 0
-        share_mv = mv_ms / ms_prof if ms_prof else 0
-        if share_fac >= share_mv:
-            ach = flops / (fac_avg / 1e3) / 1e12
-            roof = {"kernel": "cholesky factorisation (k_potrf128 + k_trsm128 + k_syrk_tc; one launch = one "
-                              "factorisation of the 12288^2 tensor)", "bound": "tensor",
-                    "achieved": ach, "peak": bf16s, "unit": "TFLOP/s", "frac": ach / bf16s,
-                    "traffic": profile_traffic("cholesky_n12288"),
-                    "peak_source": f"{src} bf16 sustained", "ms_per_launch": fac_avg, "share_of_step_time": share_fac}
-        else:
-            bytes_ = 4.0 * n * n
-            ach = bytes_ / (mv_avg / 1e3) / 1e9
-            roof = {"kernel": "k_strip_mv_tma (D.F + L.X)", "bound": "hbm", "achieved": ach, "peak": hbm,
-                    "unit": "GB/s", "frac": ach / hbm, "traffic": profile_traffic("k_strip_mv_tma_n12288"),
-                    "peak_source": f"{src} hbm", "ms_per_launch": mv_avg, "share_of_step_time": share_mv}
-        roof["phases_ms_per_call"] = {"factor": fac_avg, "build": bld_ms / max(bld_calls, 1),
-                                      "matvec": mv_avg, "forces": frc_ms / max(frc_calls, 1)}
-        # live per-launch time of the factorisation's kernels (profiled pass)
-        roof["factor_kernels_us_per_launch"] = {
-            k: 1e3 * t / max(c, 1) for k, (t, c) in
-            ((k, phase(sysm, k)) for k in ("potrf", "trsm", "syrk_col", "syrk_rest"))}
+        refreshes_timed = -(-args.steps // REFRESH)
+        ach = flops / (refresh_ms / 1e3) / 1e12
+        tf32x3 = bf16s / 6.0
+        roof = {"kernel": "refresh graph: k_build (tensor) + Cholesky factorisation (k_potrf128, k_trsm128, "
+                          "k_syrk_tc); one launch = one refresh of the 12288^2 stored tensor and its factor",
+                "bound": "tensor", "achieved": ach, "peak": bf16s, "unit": "TFLOP/s", "frac": ach / bf16s,
+                "frac_of_3xtf32_ceiling": ach / tf32x3,
+                "ceiling_3xtf32": {"value": tf32x3, "note": "measured bf16 sustained / 2 (TF32 rate) / 3 (three "
+                                                            "MMAs per split product)"},
+                "algorithmic_flops_per_launch": flops,
+                "traffic": profile_traffic("cholesky_n12288"),
+                "peak_source": f"{src} bf16 sustained", "ms_per_launch": refresh_ms,
+                "launches_in_timed_region": refreshes_timed,
+                "timed_region_consistency": {"refresh_ms_x_refreshes": refresh_ms * refreshes_timed,
+                                             "timed_ms": ms,
+                                             "ok": refresh_ms * refreshes_timed <= ms},
+                "share_of_step_time": refresh_ms * refreshes_timed / ms,
+                "autotuned_chain_sms": sysm.factor_tuning()}
+        # diagnostic split from the profiled pass (events around every phase
+        # and kernel, eager launches): not the timed configuration
+        roof["profiled_pass"] = {
+            "phases_ms_per_call": {"factor": fac_avg, "build": bld_ms / max(bld_calls, 1),
+                                   "matvec": mv_avg, "forces": frc_ms / max(frc_calls, 1)},
+            "factor_kernels_us_per_launch": {
+                k: 1e3 * t / max(c, 1) for k, (t, c) in
+                ((k, phase(sysm, k)) for k in ("potrf", "trsm", "syrk_col", "syrk_rest"))}}
+        roof["matvec"] = {"kernel": "k_strip_mv_tma (D.F + L.X, one pass over the stored matrix)", "bound": "hbm",
+                          "achieved": 4.0 * n * n / (mv_avg / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                          "frac": 4.0 * n * n / (mv_avg / 1e3) / 1e9 / hbm, "ms_per_launch": mv_avg,
+                          "traffic": profile_traffic("k_strip_mv_tma_n12288"), "peak_source": f"{src} hbm"}
         reps = None
         if not args.skip_replicas:
             # every rank takes part: with N processes the 256 chains are
@@ -353,6 +385,37 @@ def run_ours(args):
         ranks.finish(dist)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+def fp64_case(torch, engine, deck, mixed_value):
+    """This library's plain FP64 path: FP64 tensor, FP64 Cholesky (DMMA
+    panels and trailing updates), FP64 products. Steps/s with D and its
+    factor rebuilt every step (BD_BOX's schedule) and every REFRESH steps
+    (the mixed path's schedule, so that mixed/FP64 at the same schedule is
+    the gain of the precision alone); Cholesky TFLOP/s of the FP64 refresh."""
+    out = {}
+    s64 = engine.System(deck, precision=engine.PREC_FP64, refresh=1, noise=engine.NOISE_PHILOX, seed=5)
+    s64.step(2)
+    k64 = 3
+    ms = time_steps(torch, s64, k64)
+    out["refresh_1"] = {"value": k64 / (ms / 1e3), "unit": "steps/s"}
+    rms = time_refresh(torch, s64, 3)
+    n = 3 * deck.n
+    out["refresh_ms"] = rms
+    out["cholesky_tflops"] = n ** 3 / 3.0 / (rms / 1e3) / 1e12
+    s64.close()
+    s10 = engine.System(deck, precision=engine.PREC_FP64, refresh=REFRESH, noise=engine.NOISE_PHILOX, seed=5)
+    s10.step(REFRESH + 2)
+    k10 = 2 * REFRESH
+    ms = time_steps(torch, s10, k10)
+    out[f"refresh_{REFRESH}"] = {"value": k10 / (ms / 1e3), "unit": "steps/s"}
+    s10.close()
+    out["value"] = out["refresh_1"]["value"]
+    out["unit"] = "steps/s"
+    out["mixed_over_fp64"] = {"same_schedule": mixed_value / out[f"refresh_{REFRESH}"]["value"],
+                              "fp64_every_step": mixed_value / out["refresh_1"]["value"]}
+    out["note"] = "FP64 everywhere; value = D and Cholesky rebuilt every step (BD_BOX's schedule)"
+    return out
 
 
 def accuracy(torch, engine, deck):
@@ -502,15 +565,18 @@ def adjoint_case(torch, engine):
             "grad_scale_factors": {"lj_epsilon": gp[0], "lj_sigma": gp[1], "bond_H": gp[2], "debye_length": gp[3]}}
 
 
+EWALD_R = 4   # lattice radius of the Ewald sums: D.F within 1e-6 of R = 5 (R = 3: 7e-6)
+
+
 def ewald_case(torch, engine, steps=3, method="beenakker"):
     """Periodic suspension: N=4096 spheres of radius 1 A at volume fraction
-    0.10, Ewald-summed RPY (Beenakker or Smith, lattice radius 3) with TEA
-    noise computed on the fly, WCA repulsion via cell lists; steps/s of the
-    mixed path and one step's displacement error against the FP64 path with
-    the same noise."""
+    0.10, Ewald-summed RPY (Beenakker or Smith) over the lattice sphere of
+    radius EWALD_R, with TEA noise computed on the fly, WCA repulsion via
+    cell lists; steps/s of the mixed path and one step's displacement error
+    against the FP64 path with the same noise."""
     from bd_box_b200 import decks
     with tempfile.TemporaryDirectory() as d:
-        deck = decks.read_deck(decks.write_suspension_deck(d, "susp4096", 4096, seed=8, ewald_r=3,
+        deck = decks.read_deck(decks.write_suspension_deck(d, "susp4096", 4096, seed=8, ewald_r=EWALD_R,
                                                            extra={"ewald_method": method}))
     s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_PHILOX, seed=SEED)
     s.autotune(True)
@@ -534,7 +600,7 @@ def ewald_case(torch, engine, steps=3, method="beenakker"):
     dm -= box * np.round(dm / box)
     sm.close()
     s64.close()
-    return {"workload": f"periodic suspension N=4096, phi=0.10, {method.capitalize()} Ewald R=3, TEA on the fly, "
+    return {"workload": f"periodic suspension N=4096, phi=0.10, {method.capitalize()} Ewald R={EWALD_R}, TEA on the fly, "
                         "mixed precision",
             "metric": "steps/s", "value": steps / (ms / 1e3), "ms_per_step": ms / steps,
             "fp64_steps_per_s": 1.0 / t64, "autotuned_tea_tile": tea_tile,
@@ -584,7 +650,7 @@ def run_reference(args):
     try:
         prm, deck = make_deck(tmp)
         steps = max(1, min(args.steps, args.cpu_steps))
-        cpu = reference_cpu(prm, deck, steps)
+        cpu = reference_cpu(prm, deck, steps, single_thread=False)
         out = {"metric": METRIC, "value": cpu["value"], "unit": "steps/s", "n_gpus": world, "steps": steps,
                "warmup": 0, "ms_per_step": 1e3 / cpu["value"], "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded self-avoiding chain)",
@@ -595,6 +661,44 @@ def run_reference(args):
         print(json.dumps(out), flush=True)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+def relaunch_as_ranks(n: int):
+    """--gpus N > 1 outside a torchrun launch: run this script again as N
+    ranks on this node (one process per GPU) under torch.distributed.run, so
+    that --gpus N always means N processes."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    sys.stdout.flush()
+    os.execv(sys.executable, cmd)
+
+
+def run_stub(args):
+    """The launcher and the timing protocol without a GPU (gloo ranks on
+    CPU): each rank sleeps a rank-dependent time per step in place of the
+    step, the time is bracketed by barriers and reduced as the max over
+    ranks, and rank 0 prints the JSON line. For tests of the multi-process
+    path only."""
+    from bd_box_b200 import ranks
+    dist, rank, world, _ = ranks.init("gloo", timeout_s=60)
+    for _ in range(args.warmup):
+        time.sleep(0.001)
+    ranks.barrier(dist)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        time.sleep(0.01 * (1 + rank))
+    ranks.barrier(dist)
+    ms = 1e3 * (time.perf_counter() - t0)
+    ms = ranks.max_over_ranks(dist, ms, "cpu")
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": world * args.steps / (ms / 1e3), "unit": "steps/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms / args.steps, "scaling": "weak", "stub": True}), flush=True)
+    ranks.finish(dist)
 
 
 def main():
@@ -611,10 +715,17 @@ def main():
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-ewald", action="store_true")
     ap.add_argument("--skip-igt", action="store_true")
+    ap.add_argument("--stub", action="store_true", help="CPU-only stand-in step (tests of the launcher)")
+    ap.add_argument("--beads", type=int, default=N_BEADS,
+                    help="chain length of the main workload (smaller sizes for profiler captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        relaunch_as_ranks(args.gpus)
+    if args.stub:
+        run_stub(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

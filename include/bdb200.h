@@ -255,6 +255,15 @@ int bdb_compute_r(bdb_system* s, const double* gauss, double* Rs);
  * caller's, as in comp_step_ermak) or a negative error. */
 int bdb_step(bdb_system* s, int K, const double* gauss);
 
+/* The refresh of the stored-tensor path that bdb_step runs every `refresh`
+ * steps -- compute_D (diff_tensor.c:472-544) then the Cholesky factor of
+ * compute_r (diff_rand.c:64-85) -- `count` times at the current positions,
+ * replayed from its CUDA graph after the first (mixed precision), on the
+ * system's stream; the next bdb_step reuses the last factor for `refresh`
+ * steps. For timing the refresh by itself. BDB_ERR_UNSUPPORTED unless
+ * hydro is cholesky. */
+int bdb_refresh(bdb_system* s, int count);
+
 /* IGT predictor-corrector steps (comp_step_IGT_const, diff_comp.c:76-107;
  * compute_hydro_IGT + compute_hydro_IGT_second_phase,
  * diff_equation.c:288-374) for hydro none or cholesky (one system): a
@@ -295,6 +304,15 @@ int bdb_step_igt_corrector(bdb_system* s, const double* gauss);
 int bdb_autotune(bdb_system* s, int enable);
 int bdb_get_tuning(bdb_system* s, int* tea_tile, int* mv_warps_per_sm);
 int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm);
+
+/* The third tunable site (no reference counterpart): how the mixed-precision
+ * Cholesky splits the GPU. Its panel chain (panel solve, next block-column
+ * update, next diagonal block) runs beside the bulk trailing updates, which
+ * leave chain_sms SMs to it (8, 16, 32 or 48 tried at the first refresh when
+ * autotuning is on; 16 otherwise). bdb_set_factor_tuning pins it (0 keeps
+ * the value). */
+int bdb_get_factor_tuning(bdb_system* s, int* chain_sms);
+int bdb_set_factor_tuning(bdb_system* s, int chain_sms);
 
 /* CUDA graphs (no reference counterpart). Mode bit 1: steps (profiling
  * off) replay the steady part of a step -- noise, D.F and the random

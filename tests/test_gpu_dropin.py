@@ -44,6 +44,9 @@ def rel(a, b):
 def run(d, mode, *args, env=None):
     out = os.path.join(d, "out.bin")
     e = dict(os.environ, BDB_GAUSS_FILE=os.path.join(d, "g.bin"), OMP_NUM_THREADS="1", **(env or {}))
+    extra = os.path.join(d, "cos_dihe.txt")
+    if os.path.exists(extra):   # cosine dihedrals, added through add_dihe by the harness
+        e["BDB_EXTRA_DIHE"] = extra
     r = subprocess.run([HARNESS, "c.prm", mode, out, *args], cwd=d, env=e, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
@@ -58,6 +61,10 @@ def write_case(name, d):
     with open(os.path.join(d, "c.str"), "w") as f:
         f.write(str(z["str"]))
     z["gauss"].tofile(os.path.join(d, "g.bin"))
+    if "cos_dihe" in z.files:
+        with open(os.path.join(d, "cos_dihe.txt"), "w") as f:
+            for r in z["cos_dihe"]:
+                f.write("%d %d %d %d %.17g %.17g %.17g\n" % tuple(r))
     return {k: z[k] for k in z.files if k not in ("prm", "str")}
 
 

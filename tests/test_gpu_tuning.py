@@ -64,3 +64,33 @@ def test_autotuned_batch_steps_like_untuned(tmp_path):
     x0 = np.concatenate([d.coord for d in ds])
     disp = np.abs(ref.get_coord()[:, :3] - x0[:, :3]).max()
     assert np.abs(tuned.get_coord() - ref.get_coord()).max() <= 1e-12 * disp
+
+
+def test_factor_split_candidates_give_identical_bits(deck_dir):
+    """The mixed Cholesky's GPU split (SMs left to its panel chain) changes
+    where the trailing updates run, not their order: every candidate gives
+    the same factor and the same step, bit for bit; the autotuner picks one
+    of them."""
+    deck = decks.read_deck(decks.write_chain_deck(deck_dir, "fsplit", 700, seed=52, hydro="cholesky"))
+    g = np.random.default_rng(8).standard_normal(3 * deck.n)
+    ref = None
+    for c in (8, 16, 32, 48):
+        s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
+        s.set_factor_tuning(c)
+        assert s.factor_tuning() == c
+        s.step(1, g)
+        out = (s.factor_error(), s.get_coord())
+        s.close()
+        if ref is None:
+            ref = out
+        else:
+            # the error metric sums over blocks in arbitrary order; the
+            # positions after the step are the bit-exact check
+            assert abs(out[0] - ref[0]) <= 1e-12 * ref[0]
+            assert np.array_equal(out[1], ref[1])
+    s = engine.System(deck, precision=engine.PREC_MIXED, noise=engine.NOISE_HOST)
+    s.autotune(True)
+    s.step(1, g)
+    assert s.factor_tuning() in (8, 16, 32, 48)
+    assert np.array_equal(s.get_coord(), ref[1])
+    s.close()

@@ -90,3 +90,24 @@ def test_shard_replicas_small_cases():
     for bad in (([5, 1], 2), ([5, 6], 0)):
         with pytest.raises(engine.BDBError):
             engine.shard_replicas(*bad)
+
+
+def test_bench_gpus_flag_launches_that_many_ranks():
+    """`bench.py --gpus 2` started without torchrun starts two ranks itself
+    (torch.distributed.run on this node) and reports n_gpus 2 with the
+    slowest rank's time; the stub step keeps the GPU out of it."""
+    import json
+    import subprocess
+    import sys
+    pytest.importorskip("torch")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--stub", "--steps", "5",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=240, env=env, cwd=root)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    out = json.loads(lines[0])
+    assert out["n_gpus"] == 2 and out["steps"] == 5
+    # rank 1 sleeps 20 ms per step: the job's time is its time
+    assert out["ms_per_step"] >= 19.0
