@@ -146,6 +146,7 @@ struct bdb_system {
     bool factor_valid = false;
     alignas(64) unsigned char tc_map[1024];    // CUtensorMaps: TF32 hi / lo panel buffers (x3), FP32 matrix
     bool tc_map_ok = false;
+    bool tc64_ok = false;                      // FP64 tensor-core Cholesky set up
     alignas(64) unsigned char mv_map[384];     // CUtensorMaps for the stored matvec: FP32 matrix, X, F
     const void* mv_map_src[3] = {};            // buffers the maps were encoded for
     int mv_ctas_per_sm = 0;                    // resident CTAs of the TMA matvec kernel per SM

@@ -148,11 +148,15 @@ __global__ void __launch_bounds__(256) k_syrk(T* __restrict__ M, int npad, int k
 }
 
 int factor_mixed_tc(bdb_system* s);   // chol_tc.cu
+int factor_fp64_tc(bdb_system* s);    // chol_tc.cu
 
 int factor_run(bdb_system* s)
 {
-    const bool no_tc = getenv("BDB_NO_TC") != nullptr;   // diagnostics: SIMT FP32 trailing update
-    if (s->p.precision == BDB_PREC_MIXED && !no_tc && s->npad % 128 == 0) return factor_mixed_tc(s);
+    // BDB_NO_TC (diagnostics): the SIMT kernels below instead of the
+    // tensor-core factorisations of chol_tc.cu
+    const bool no_tc = getenv("BDB_NO_TC") != nullptr;
+    if (!no_tc && s->npad % 128 == 0)
+        return s->p.precision == BDB_PREC_MIXED ? factor_mixed_tc(s) : factor_fp64_tc(s);
     const int nb = s->npad / NB;
     for (int k = 0; k < nb; ++k) {
         const int rows_below = s->npad - (k + 1) * NB;

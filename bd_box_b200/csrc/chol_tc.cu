@@ -209,6 +209,9 @@ __device__ __forceinline__ double rcp_nr(double x)
 // computed, so one reciprocal and one FMA separate two pivots), then the
 // other entries as a_ic -= a_ij (a_cj q_j), one FMA each after the 7-j
 // scaled column entries. The columns are scaled by 1/sqrt(a_jj) at the end.
+// With kFull (the plain FP64 path) every reciprocal and reciprocal square
+// root takes a second Newton step, which brings it to FP64 rounding.
+template <bool kFull>
 __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
 {
     double a[8][8];
@@ -220,7 +223,8 @@ __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         if (!(a[j][j] > 0.0)) ok = false;
-        const double q = rcp_nr(a[j][j]);
+        double q = rcp_nr(a[j][j]);
+        if (kFull) q = fma(q, fma(-a[j][j], q, 1.0), q);
         if (j + 1 < 8) a[j + 1][j + 1] = fma(-(a[j + 1][j] * a[j + 1][j]), q, a[j + 1][j + 1]);
         double t[8];
 #pragma unroll
@@ -233,13 +237,30 @@ __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
     }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        const double r = rsqrt_nr(a[j][j]);
+        double r = rsqrt_nr(a[j][j]);
+        if (kFull) r = r * (1.5 - 0.5 * a[j][j] * r * r);
         rd[j] = r;
         Dg[j * 9 + j] = a[j][j] * r;
 #pragma unroll
         for (int i = j + 1; i < 8; ++i) Dg[i * 9 + j] = a[i][j] * r;
     }
     return ok;
+}
+
+// two consecutive elements of an FP32 or FP64 matrix as doubles, and back
+__device__ __forceinline__ double2 ld_pair(const float* p)
+{
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    return make_double2(v.x, v.y);
+}
+__device__ __forceinline__ double2 ld_pair(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ void st_pair(float* p, double a, double b)
+{
+    *reinterpret_cast<float2*>(p) = make_float2((float)a, (float)b);
+}
+__device__ __forceinline__ void st_pair(double* p, double a, double b)
+{
+    *reinterpret_cast<double2*>(p) = make_double2(a, b);
 }
 
 static constexpr int POTRF_THREADS = 512;
@@ -274,8 +295,9 @@ __device__ __forceinline__ bool bar_wait0(uint64_t* b, volatile int* abort_flag)
 
 // A solved off-diagonal tile X (C fragments x0, x1 of lane (fr, fq)) of
 // L_PP, tile index t = tix(g, n): to the shared tiles (A order), to the FP64
-// hand-off for the panel solve (the same order) and, as FP32, to M
-__device__ __forceinline__ void put_tile(double* Lt, double* Wt, float* M, size_t row0, size_t col0, int npad, int t,
+// hand-off for the panel solve (the same order) and, in M's precision, to M
+template <typename T>
+__device__ __forceinline__ void put_tile(double* Lt, double* Wt, T* M, size_t row0, size_t col0, int npad, int t,
                                          int fr, int fq, double x0, double x1)
 {
     const int p0 = t * 64 + apos(fr, 2 * fq), p1 = t * 64 + apos(fr, 2 * fq + 1);
@@ -283,7 +305,7 @@ __device__ __forceinline__ void put_tile(double* Lt, double* Wt, float* M, size_
     Lt[p1] = x1;
     Wt[p0] = x0;
     Wt[p1] = x1;
-    *reinterpret_cast<float2*>(M + (row0 + fr) * npad + col0 + 2 * fq) = make_float2((float)x0, (float)x1);
+    st_pair(M + (row0 + fr) * npad + col0 + 2 * fq, x0, x1);
 }
 
 // X = C W^T for an 8x8 tile C held as C fragments (c0, c1) and W in A order
@@ -326,7 +348,8 @@ __device__ __forceinline__ void solve_tile(double c0, double c1, const double* W
 // then the 16 W_kk; PANEL_FAC doubles) as soon as it is final, so nothing
 // is left to store at the end. Every wait is bounded: a time-out sets
 // ST_TIMEOUT and every warp runs out to the final barrier.
-__global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict__ M, int npad, int P,
+template <typename T>
+__global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M, int npad, int P,
                                                             double* __restrict__ Wt, unsigned* __restrict__ status)
 {
     extern __shared__ double sh[];
@@ -379,8 +402,8 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         }
         double t1[2], t2[2];
         {
-            const float2 a = *reinterpret_cast<const float2*>(M + (base + 8 + fr) * npad + base + 2 * fq);
-            const float2 b = *reinterpret_cast<const float2*>(M + (base + 8 + fr) * npad + base + 8 + 2 * fq);
+            const double2 a = ld_pair(M + (base + 8 + fr) * npad + base + 2 * fq);
+            const double2 b = ld_pair(M + (base + 8 + fr) * npad + base + 8 + 2 * fq);
             t1[0] = a.x;
             t1[1] = a.y;
             t2[0] = 2 * fq <= fr ? (double)b.x : 0.0;
@@ -388,7 +411,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         }
         for (int k = 0; k < NT; ++k) {
             __syncwarp();
-            if (lane == 0 && !pivot8(Dg, rd)) bad = 1;
+            if (lane == 0 && !pivot8<sizeof(T) == 8>(Dg, rd)) bad = 1;
             __syncwarp();
             if (lane < 8) {
                 // column c of W_kk = L_kk^-1 by right-looking forward
@@ -471,7 +494,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                 const double l = Lt[tix(k, k) * 64 + p];
                 Wt[tix(k, k) * 64 + p] = l;
                 Wt[(NTILE + k) * 64 + p] = Wa[k * 64 + p];
-                if (c <= r) M[(base + 8 * k + r) * npad + base + 8 * k + c] = (float)l;
+                if (c <= r) M[(base + 8 * k + r) * npad + base + 8 * k + c] = (T)l;
             }
             if (k + 1 == NT) break;
             if (!bar_wait0(&bars.lcol[k], &abort_flag)) break;
@@ -480,7 +503,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
                 const int p = 2 * lane + h, r = p >> 3, c = ((p & 1) << 2) | ((p & 7) >> 1);
                 const double l = Lt[tix(k + 1, k) * 64 + p];
                 Wt[tix(k + 1, k) * 64 + p] = l;
-                M[(base + 8 * (k + 1) + r) * npad + base + 8 * k + c] = (float)l;
+                M[(base + 8 * (k + 1) + r) * npad + base + 8 * k + c] = (T)l;
             }
         }
     } else {
@@ -490,10 +513,9 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
         for (int n = 0; n < NT; ++n) {
             cacc[n][0] = cacc[n][1] = 0.0;
             if (n <= g) {
-                const float2 v =
-                    *reinterpret_cast<const float2*>(M + (base + 8 * g + fr) * npad + base + 8 * n + 2 * fq);
-                cacc[n][0] = (n < g || 2 * fq <= fr) ? (double)v.x : 0.0;
-                cacc[n][1] = (n < g || 2 * fq + 1 <= fr) ? (double)v.y : 0.0;
+                const double2 v = ld_pair(M + (base + 8 * g + fr) * npad + base + 8 * n + 2 * fq);
+                cacc[n][0] = (n < g || 2 * fq <= fr) ? v.x : 0.0;
+                cacc[n][1] = (n < g || 2 * fq + 1 <= fr) ? v.y : 0.0;
             }
         }
         for (int k = 0; k + 1 < g; ++k) {
@@ -574,9 +596,10 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(float* __restrict
 // factor (76 KB) into shared memory once. The grid is persistent: unit u goes
 // to warp slot u mod (8 grid), slots ordered so that the first 4 grid slots
 // put one warp on every SM sub-partition, the next 4 grid a second one.
-// Writes the rows to M and their TF32 split L = L_hi + L_lo (L_hi: low 13
-// mantissa bits cleared, exactly TF32; L_lo = L - L_hi) to the panel
-// buffers.
+// Writes the rows to M and, for the mixed path (T = float), their TF32
+// split L = L_hi + L_lo (L_hi: low 13 mantissa bits cleared, exactly TF32;
+// L_lo = L - L_hi) to the panel buffers; for the FP64 path (T = double) the
+// rows in FP64 to one panel buffer (Lhi, as doubles; Llo unused).
 static constexpr int TRSM_THREADS = 256;
 static constexpr int TRSM_SMEM = PANEL_FAC * 8;
 
@@ -590,7 +613,8 @@ __device__ __forceinline__ double c2a(double c0, double c1, int h, int fr, int f
     return (fq & 1) ? v1 : v0;
 }
 
-__global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__ M, int npad, int P,
+template <typename T>
+__global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, int npad, int P,
                                                           const double* __restrict__ Lf, float* __restrict__ Lhi,
                                                           float* __restrict__ Llo, unsigned* __restrict__ status)
 {
@@ -636,7 +660,7 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__
         double c[16][2];
 #pragma unroll
         for (int n = 0; n < 16; ++n) {
-            const float2 v = *reinterpret_cast<const float2*>(M + row * npad + base + 8 * n + 2 * fq);
+            const double2 v = ld_pair(M + row * npad + base + 8 * n + 2 * fq);
             c[n][0] = v.x;
             c[n][1] = v.y;
         }
@@ -647,11 +671,16 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(float* __restrict__
             dmma884(x0, x1, c2a(c[n][0], c[n][1], 0, fr, fq), w.x);
             dmma884(x0, x1, c2a(c[n][0], c[n][1], 1, fr, fq), w.y);
             const int col = 8 * n + 2 * fq;
-            const float o0 = (float)x0, o1 = (float)x1;
-            const float h0 = tf32_hi(o0), h1 = tf32_hi(o1);
-            *reinterpret_cast<float2*>(M + row * npad + base + col) = make_float2(o0, o1);
-            *reinterpret_cast<float2*>(Lhi + row * PW + col) = make_float2(h0, h1);
-            *reinterpret_cast<float2*>(Llo + row * PW + col) = make_float2(o0 - h0, o1 - h1);
+            if constexpr (sizeof(T) == 4) {
+                const float o0 = (float)x0, o1 = (float)x1;
+                const float h0 = tf32_hi(o0), h1 = tf32_hi(o1);
+                *reinterpret_cast<float2*>(M + row * npad + base + col) = make_float2(o0, o1);
+                *reinterpret_cast<float2*>(Lhi + row * PW + col) = make_float2(h0, h1);
+                *reinterpret_cast<float2*>(Llo + row * PW + col) = make_float2(o0 - h0, o1 - h1);
+            } else {
+                st_pair(M + row * npad + base + col, x0, x1);
+                st_pair(reinterpret_cast<double*>(Lhi) + row * PW + col, x0, x1);
+            }
             if (n < 15) {
                 const double xa0 = -c2a(x0, x1, 0, fr, fq), xa1 = -c2a(x0, x1, 1, fr, fq);
 #pragma unroll
@@ -855,6 +884,129 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
     }
 }
 
+// ------------------------------------------------- FP64 trailing update
+//
+// The plain FP64 path's C -= L_i L_j^T on the FP64 tensor instruction
+// (mma.sync m8n8k4 f64; tcgen05 has no FP64 kind): a persistent CTA of 8
+// warps per 128x128 tile, warp w owning rows 32 (w mod 4).. and columns
+// 64 (w / 4).. as 32 accumulator tiles in registers, initialised from C and
+// stored back (lower triangle only on diagonal tiles, whose upper triangle
+// holds D). The panel rows of tiles i and j stream through shared memory in
+// chunks of 16 columns (cp.async, two stages, rows padded to 20 doubles: at
+// most two-way bank conflicts on the 8-byte fragment loads, which take two
+// wavefronts anyway). Per chunk a warp issues 128 DMMAs from 48 fragment
+// loads.
+static constexpr int S64_THREADS = 256;
+static constexpr int S64_KC = 16;                        // panel columns per staged chunk
+static constexpr int S64_LD = 20;                        // padded row stride of a staged chunk (doubles)
+static constexpr int S64_CHUNK = PW * S64_LD;            // doubles of one operand chunk
+static constexpr int S64_SMEM = 2 * 2 * S64_CHUNK * 8;   // two stages of A and B chunks: 80 KB
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// columns [k0, k0 + 16) of the panel rows of tiles ra (A) and rb (B):
+// 2 x 1024 16-byte pieces, 8 per thread
+__device__ __forceinline__ void s64_stage(double* As, double* Bs, const double* __restrict__ Lp, int ra, int rb,
+                                          int k0, int tid)
+{
+#pragma unroll
+    for (int q = tid; q < PW * S64_KC / 2; q += S64_THREADS) {
+        const int r = q >> 3, c = (q & 7) * 2;
+        cp_async16(smem_u32(As + r * S64_LD + c), Lp + (size_t)(ra + r) * PW + k0 + c);
+        cp_async16(smem_u32(Bs + r * S64_LD + c), Lp + (size_t)(rb + r) * PW + k0 + c);
+    }
+}
+
+__global__ void __launch_bounds__(S64_THREADS, 1) k_syrk64(double* __restrict__ M, int npad,
+                                                         const double* __restrict__ Lp, int t0, int ntiles, int mode,
+                                                         unsigned* __restrict__ status)
+{
+    extern __shared__ __align__(16) double sm64[];
+    {
+        uint32_t dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (blockDim.x != S64_THREADS || dyn < (uint32_t)S64_SMEM) {
+            if (threadIdx.x == 0) atomicOr(status, ST_LAUNCH);
+            return;
+        }
+    }
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int fr = lane >> 2, fq = lane & 3;
+    const int wr = warp & 3, wc = warp >> 2;
+    // a programmatic dependent of the previous kernel on the stream: nothing
+    // it produces is read before this
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
+    constexpr int NCH = PW / S64_KC;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int ti, tj;
+        tile_of_mode(t, mode, ti, tj);
+        const int ra = (t0 + ti) * PW, rb = (t0 + tj) * PW;
+        const bool diag = ti == tj;
+        s64_stage(sm64, sm64 + S64_CHUNK, Lp, ra, rb, 0, tid);
+        cp_async_commit();
+        double acc[4][8][2];
+#pragma unroll
+        for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+            for (int ct = 0; ct < 8; ++ct) {
+                const size_t row = (size_t)ra + 32 * wr + 8 * rt + fr;
+                const double2 v = *reinterpret_cast<const double2*>(M + row * npad + rb + 64 * wc + 8 * ct + 2 * fq);
+                acc[rt][ct][0] = v.x;
+                acc[rt][ct][1] = v.y;
+            }
+#pragma unroll 1
+        for (int kc = 0; kc < NCH; ++kc) {
+            const double* As = sm64 + (kc & 1) * 2 * S64_CHUNK;
+            const double* Bs = As + S64_CHUNK;
+            if (kc + 1 < NCH) {
+                double* nA = sm64 + ((kc + 1) & 1) * 2 * S64_CHUNK;
+                s64_stage(nA, nA + S64_CHUNK, Lp, ra, rb, (kc + 1) * S64_KC, tid);
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < S64_KC; kk += 4) {
+                double a[4], b[8];
+#pragma unroll
+                for (int rt = 0; rt < 4; ++rt) a[rt] = -As[(32 * wr + 8 * rt + fr) * S64_LD + kk + fq];
+#pragma unroll
+                for (int ct = 0; ct < 8; ++ct) b[ct] = Bs[(64 * wc + 8 * ct + fr) * S64_LD + kk + fq];
+#pragma unroll
+                for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+                    for (int ct = 0; ct < 8; ++ct) dmma884(acc[rt][ct][0], acc[rt][ct][1], a[rt], b[ct]);
+            }
+            __syncthreads();   // this stage is read; it may be staged again
+        }
+#pragma unroll
+        for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+            for (int ct = 0; ct < 8; ++ct) {
+                const int r = 32 * wr + 8 * rt + fr, c = 64 * wc + 8 * ct + 2 * fq;
+                double* dst = M + ((size_t)ra + r) * npad + rb + c;
+                if (!diag) {
+                    *reinterpret_cast<double2*>(dst) = make_double2(acc[rt][ct][0], acc[rt][ct][1]);
+                } else {
+                    if (c <= r) dst[0] = acc[rt][ct][0];
+                    if (c + 1 <= r) dst[1] = acc[rt][ct][1];
+                }
+            }
+    }
+}
+
 // ---------------------------------------------------------------- host side
 
 // row-major FP32 [rows][cols] buffer, boxes of 128 rows x 32 columns
@@ -910,8 +1062,8 @@ static int tc_setup(bdb_system* s)
     int rc = make_panel_map(s->M32.p, s->npad, &maps[2 * PANEL_SETS], s->npad);
     if (rc) return rc;
     BDB_CUDA(cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
-    BDB_CUDA(cudaFuncSetAttribute(k_potrf128, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM));
-    BDB_CUDA(cudaFuncSetAttribute(k_trsm128, cudaFuncAttributeMaxDynamicSharedMemorySize, TRSM_SMEM));
+    BDB_CUDA(cudaFuncSetAttribute(k_potrf128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM));
+    BDB_CUDA(cudaFuncSetAttribute(k_trsm128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRSM_SMEM));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -939,7 +1091,8 @@ static cudaError_t launch_syrk(bdb_system* s, int grid, cudaStream_t st, const C
 }
 
 // k_potrf128 the same way, behind the update of its block column
-static cudaError_t launch_potrf(bdb_system* s, cudaStream_t st, int P, double* lkk)
+template <typename T>
+static cudaError_t launch_potrf(bdb_system* s, cudaStream_t st, T* M, int P, double* lkk)
 {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(1);
@@ -951,7 +1104,7 @@ static cudaError_t launch_potrf(bdb_system* s, cudaStream_t st, int P, double* l
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_potrf128, s->M32.p, s->npad, P, lkk, s->status.p);
+    return cudaLaunchKernelEx(&cfg, k_potrf128<T>, M, s->npad, P, lkk, s->status.p);
 }
 
 // Factorisation with two panels of look-ahead on two streams. Panel P's
@@ -980,7 +1133,7 @@ int factor_mixed_tc(bdb_system* s)
     double* lkk;
     panel_ptrs(s, 0, &hi, &lo, &lkk);
     phase_mark_on(s, P_POTRF, st);
-    BDB_CUDA(launch_potrf(s, st, 0, lkk));
+    BDB_CUDA(launch_potrf(s, st, s->M32.p, 0, lkk));
     phase_mark_on(s, P_POTRF, st);
     s->launches += 1;
     // the bulk stream starts after everything before the factorisation
@@ -994,7 +1147,7 @@ int factor_mixed_tc(bdb_system* s)
         const int units = (s->npad - (P + 1) * PW) / 8;
         const int per_cta = TRSM_THREADS / 32;
         phase_mark_on(s, P_TRSM, st);
-        k_trsm128<<<std::min(s->sm_count, (units + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st>>>(
+        k_trsm128<float><<<std::min(s->sm_count, (units + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st>>>(
             s->M32.p, s->npad, P, lkk, hi, lo, s->status.p);
         phase_mark_on(s, P_TRSM, st);
         BDB_CUDA(cudaGetLastError());
@@ -1023,11 +1176,111 @@ int factor_mixed_tc(bdb_system* s)
         float *hi1, *lo1;
         panel_ptrs(s, (P + 1) % PANEL_SETS, &hi1, &lo1, &lkk1);
         phase_mark_on(s, P_POTRF, st);
-        BDB_CUDA(launch_potrf(s, st, P + 1, lkk1));
+        BDB_CUDA(launch_potrf(s, st, s->M32.p, P + 1, lkk1));
         phase_mark_on(s, P_POTRF, st);
         s->launches += 3;
     }
     // join the bulk stream
+    BDB_CUDA(cudaEventRecord(ev_end, st2));
+    BDB_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
+    BDB_CUDA(cudaGetLastError());
+    return BDB_OK;
+}
+
+// ------------------------------------------------------ FP64 factorisation
+
+static int tc64_setup(bdb_system* s)
+{
+    if (s->tc64_ok) return BDB_OK;
+    const size_t pan = (size_t)s->npad * PW;
+    // one FP64 panel buffer per set (the room of a mixed-path hi/lo pair)
+    if (s->panel64.alloc((size_t)PANEL_SETS * pan + (size_t)PANEL_SETS * PANEL_FAC + 64)) return BDB_ERR_NOMEM;
+    BDB_CUDA(cudaMemset(s->panel64.p, 0, s->panel64.n * sizeof(double)));
+    BDB_CUDA(cudaFuncSetAttribute(k_potrf128<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM));
+    BDB_CUDA(cudaFuncSetAttribute(k_trsm128<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRSM_SMEM));
+    BDB_CUDA(cudaFuncSetAttribute(k_syrk64, cudaFuncAttributeMaxDynamicSharedMemorySize, S64_SMEM));
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    s->sm_count = sms;
+    s->tc64_ok = true;
+    return BDB_OK;
+}
+
+static cudaError_t launch_syrk64(bdb_system* s, int grid, cudaStream_t st, const double* Lp, int t0, int ntiles,
+                                 int mode)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(S64_THREADS);
+    cfg.dynamicSmemBytes = S64_SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_syrk64, s->M64.p, s->npad, Lp, t0, ntiles, mode, s->status.p);
+}
+
+// The plain FP64 path: the schedule of factor_mixed_tc (two panels of
+// look-ahead, A on the chain stream, B and C on the bulk stream) with FP64
+// panels and FP64 DMMA trailing updates.
+int factor_fp64_tc(bdb_system* s)
+{
+    int rc = tc64_setup(s);
+    if (rc) return rc;
+    const int nt = s->npad / PW;
+    cudaStream_t st = s->stream, st2 = s->stream2;
+    cudaEvent_t ev_solved = s->la_ev[0], ev_b = s->la_ev[1], ev_end = s->la_ev[2];
+    const int bulk_sms = std::max(1, s->sm_count - std::min(std::max(s->chain_sms, 0), s->sm_count - 1));
+    float *hi, *lo;
+    double* lkk;
+    panel_ptrs(s, 0, &hi, &lo, &lkk);
+    phase_mark_on(s, P_POTRF, st);
+    BDB_CUDA(launch_potrf(s, st, s->M64.p, 0, lkk));
+    phase_mark_on(s, P_POTRF, st);
+    s->launches += 1;
+    BDB_CUDA(cudaEventRecord(ev_solved, st));
+    BDB_CUDA(cudaStreamWaitEvent(st2, ev_solved, 0));
+    for (int P = 0; P + 1 < nt; ++P) {
+        const int set = P % PANEL_SETS;
+        panel_ptrs(s, set, &hi, &lo, &lkk);
+        const double* Lp = reinterpret_cast<const double*>(hi);
+        const int rem = nt - P - 1;
+        if (P > 0) BDB_CUDA(cudaStreamWaitEvent(st, ev_b, 0));   // B(P-1)
+        const int units = (s->npad - (P + 1) * PW) / 8;
+        const int per_cta = TRSM_THREADS / 32;
+        phase_mark_on(s, P_TRSM, st);
+        k_trsm128<double><<<std::min(s->sm_count, (units + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st>>>(
+            s->M64.p, s->npad, P, lkk, hi, lo, s->status.p);
+        phase_mark_on(s, P_TRSM, st);
+        BDB_CUDA(cudaGetLastError());
+        BDB_CUDA(cudaEventRecord(ev_solved, st));
+        BDB_CUDA(cudaStreamWaitEvent(st2, ev_solved, 0));
+        phase_mark_on(s, P_SYRK_REST, st2);
+        if (rem >= 2) {
+            BDB_CUDA(launch_syrk64(s, std::min(bulk_sms, rem - 1), st2, Lp, P + 1, rem - 1, 2));
+            s->launches += 1;
+        }
+        BDB_CUDA(cudaEventRecord(ev_b, st2));
+        if (rem >= 3) {
+            const int ntc = (rem - 2) * (rem - 1) / 2;
+            BDB_CUDA(launch_syrk64(s, std::min(bulk_sms, ntc), st2, Lp, P + 1, ntc, 3));
+            s->launches += 1;
+        }
+        phase_mark_on(s, P_SYRK_REST, st2);
+        phase_mark_on(s, P_SYRK_COL, st);
+        BDB_CUDA(launch_syrk64(s, std::min(s->sm_count, rem), st, Lp, P + 1, rem, 1));
+        phase_mark_on(s, P_SYRK_COL, st);
+        double* lkk1;
+        float *hi1, *lo1;
+        panel_ptrs(s, (P + 1) % PANEL_SETS, &hi1, &lo1, &lkk1);
+        phase_mark_on(s, P_POTRF, st);
+        BDB_CUDA(launch_potrf(s, st, s->M64.p, P + 1, lkk1));
+        phase_mark_on(s, P_POTRF, st);
+        s->launches += 3;
+    }
     BDB_CUDA(cudaEventRecord(ev_end, st2));
     BDB_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
     BDB_CUDA(cudaGetLastError());
