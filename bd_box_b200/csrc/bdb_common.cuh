@@ -151,6 +151,7 @@ struct bdb_system {
     const void* mv_map_src[3] = {};            // buffers the maps were encoded for
     int mv_ctas_per_sm = 0;                    // resident CTAs of the TMA matvec kernel per SM
     int sm_count = 148;
+    unsigned wait_limit = 1u << 22;            // tries of every bounded device wait (bdb_set_wait_limit)
     int steps_since_refresh = 0;
 
     // noise: Philox stream index and finished-block count (device)

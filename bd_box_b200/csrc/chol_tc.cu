@@ -288,9 +288,9 @@ struct PotrfBars {
 };
 
 // all 32 lanes wait; false on a time-out or an abort seen by this lane
-__device__ __forceinline__ bool bar_wait0(uint64_t* b, volatile int* abort_flag)
+__device__ __forceinline__ bool bar_wait0(uint64_t* b, volatile int* abort_flag, uint32_t limit)
 {
-    return mbar_wait(smem_u32(b), 0, abort_flag);
+    return mbar_wait(smem_u32(b), 0, abort_flag, limit);
 }
 
 // A solved off-diagonal tile X (C fragments x0, x1 of lane (fr, fq)) of
@@ -350,7 +350,8 @@ __device__ __forceinline__ void solve_tile(double c0, double c1, const double* W
 // ST_TIMEOUT and every warp runs out to the final barrier.
 template <typename T>
 __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M, int npad, int P,
-                                                            double* __restrict__ Wt, unsigned* __restrict__ status)
+                                                            double* __restrict__ Wt, unsigned* __restrict__ status,
+                                                            uint32_t wlim)
 {
     extern __shared__ double sh[];
     double* Lt = sh;                       // [NTILE][64] A order
@@ -451,7 +452,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
             if (k > 0) {
                 // tiles (k+1, k) and (k+1, k+1) through column k-2 and
                 // L[k+1][k-1] from their owner; column k-1 applied here
-                if (!bar_wait0(&bars.hand[k - 1], &abort_flag)) break;
+                if (!bar_wait0(&bars.hand[k - 1], &abort_flag, wlim)) break;
                 const double2 a = *reinterpret_cast<const double2*>(Hd + (size_t)(k - 1) * 128 + 2 * lane);
                 const double2 b = *reinterpret_cast<const double2*>(Hd + (size_t)(k - 1) * 128 + 64 + 2 * lane);
                 const double2 u = *reinterpret_cast<const double2*>(Lt + tix(k + 1, k - 1) * 64 + 2 * lane);
@@ -487,7 +488,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
         // chain: L_kk and W_kk once published, L[k+1][k] once block column k
         // is solved; FP64 in A order to Wt, L as FP32 to M
         for (int k = 0; k < NT; ++k) {
-            if (!bar_wait0(&bars.w[k], &abort_flag)) break;
+            if (!bar_wait0(&bars.w[k], &abort_flag, wlim)) break;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int p = 2 * lane + h, r = p >> 3, c = ((p & 1) << 2) | ((p & 7) >> 1);
@@ -497,7 +498,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
                 if (c <= r) M[(base + 8 * k + r) * npad + base + 8 * k + c] = (T)l;
             }
             if (k + 1 == NT) break;
-            if (!bar_wait0(&bars.lcol[k], &abort_flag)) break;
+            if (!bar_wait0(&bars.lcol[k], &abort_flag, wlim)) break;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int p = 2 * lane + h, r = p >> 3, c = ((p & 1) << 2) | ((p & 7) >> 1);
@@ -519,7 +520,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
             }
         }
         for (int k = 0; k + 1 < g; ++k) {
-            if (!bar_wait0(&bars.w[k], &abort_flag)) break;
+            if (!bar_wait0(&bars.w[k], &abort_flag, wlim)) break;
             // L[g][k] = C[g][k] W_kk^T
             double c0 = 0.0, c1 = 0.0;
 #pragma unroll
@@ -553,7 +554,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
             const double2 av = *reinterpret_cast<const double2*>(Lt + tix(g, k) * 64 + 2 * lane);
             // the bulk updates of step k wait for its hand-over, so that the
             // solve on the pivot chain does not queue behind them
-            if (!bar_wait0(&bars.hand[k], &abort_flag) || !bar_wait0(&bars.lcol[k], &abort_flag)) break;
+            if (!bar_wait0(&bars.hand[k], &abort_flag, wlim) || !bar_wait0(&bars.lcol[k], &abort_flag, wlim)) break;
             // C[g][n] -= L[g][k] L[n][k]^T for n = k+1..g, four tiles per
             // batch: their operand loads first (predicated, no branch), then
             // the MMAs
@@ -697,7 +698,7 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, 
 // ------------------------------------------------------- tensor-core update
 
 struct SyrkBars {
-    uint64_t full[STAGES], empty[STAGES], accfull[2], accempty[2];
+    uint64_t full[STAGES], empty[STAGES], accfull[2], accempty[2], drain;
 };
 
 // Staging slot cc of the C update in shared memory: one 128x32 box, 128
@@ -710,7 +711,8 @@ __device__ __forceinline__ float4* c_chunk(unsigned char* cbuf, int cc, int r, i
 
 __global__ void __launch_bounds__(192, 1)
 k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
-          const __grid_constant__ CUtensorMap map_c, int t0, int ntiles, int mode, unsigned* __restrict__ status)
+          const __grid_constant__ CUtensorMap map_c, int t0, int ntiles, int mode, unsigned* __restrict__ status,
+          uint32_t wlim)
 {
     {
         uint32_t dyn;
@@ -739,6 +741,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             mbar_init(smem_u32(&bars.accfull[b]), 1);
             mbar_init(smem_u32(&bars.accempty[b]), 4);
         }
+        mbar_init(smem_u32(&bars.drain), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -766,7 +769,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                 const int ra = (t0 + ti) * PW, rb = (t0 + tj) * PW;
                 for (int kc = 0; kc < NCHUNK; ++kc, ++g) {
                     const int s = g % STAGES;
-                    if (!mbar_wait(smem_u32(&bars.empty[s]), ((g / STAGES) & 1) ^ 1, &abort_flag)) break;
+                    if (!mbar_wait(smem_u32(&bars.empty[s]), ((g / STAGES) & 1) ^ 1, &abort_flag, wlim)) break;
                     const uint32_t st = sbase + s * STAGE_BYTES;
                     const uint32_t fb = smem_u32(&bars.full[s]);
                     mbar_expect_tx(fb, STAGE_BYTES);
@@ -776,6 +779,13 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                     tma_load_2d(st + 3 * BOX_BYTES, &map_lo, kc * KC, rb, fb);
                 }
             }
+            if (abort_flag) {
+                // the loads still in flight (the last fill of each stage)
+                // must land before the CTA exits
+                volatile int never = 0;
+                for (uint32_t j = g > (uint32_t)STAGES ? g - STAGES : 0; j < g; ++j)
+                    mbar_wait(smem_u32(&bars.full[j % STAGES]), (j / STAGES) & 1, &never);
+            }
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -784,13 +794,13 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             uint32_t g = 0, tl = 0;
             for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++tl) {
                 const uint32_t b = tl & 1;
-                if (!mbar_wait(smem_u32(&bars.accempty[b]), ((tl >> 1) & 1) ^ 1, &abort_flag)) break;
+                if (!mbar_wait(smem_u32(&bars.accempty[b]), ((tl >> 1) & 1) ^ 1, &abort_flag, wlim)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t acc = tmem + b * 128;
                 bool ok = true;
                 for (int kc = 0; kc < NCHUNK; ++kc, ++g) {
                     const int s = g % STAGES;
-                    if (!mbar_wait(smem_u32(&bars.full[s]), (g / STAGES) & 1, &abort_flag)) {
+                    if (!mbar_wait(smem_u32(&bars.full[s]), (g / STAGES) & 1, &abort_flag, wlim)) {
                         ok = false;
                         break;
                     }
@@ -810,6 +820,13 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                 if (!ok) break;
                 umma_commit(smem_u32(&bars.accfull[b]));
             }
+            if (abort_flag) {
+                // every MMA issued so far completes before the tensor
+                // memory is freed: commit once more and wait for it
+                volatile int never = 0;
+                umma_commit(smem_u32(&bars.drain));
+                mbar_wait(smem_u32(&bars.drain), 0, &never);
+            }
         }
     } else {
         // epilogue warps 2..5: TMEM lane quarter = warp % 4. C is never
@@ -828,7 +845,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             const uint32_t b = tl & 1;
             // a time-out or abort seen by any epilogue thread stops all of
             // them before the next barrier
-            if (epi_any(!mbar_wait(smem_u32(&bars.accfull[b]), (tl >> 1) & 1, &abort_flag))) break;
+            if (epi_any(!mbar_wait(smem_u32(&bars.accfull[b]), (tl >> 1) & 1, &abort_flag, wlim))) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
             for (int cc = 0; cc < PW / 32; ++cc) {
@@ -1087,7 +1104,7 @@ static cudaError_t launch_syrk(bdb_system* s, int grid, cudaStream_t st, const C
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_syrk_tc, hi, lo, c, t0, ntiles, mode, s->status.p);
+    return cudaLaunchKernelEx(&cfg, k_syrk_tc, hi, lo, c, t0, ntiles, mode, s->status.p, (uint32_t)s->wait_limit);
 }
 
 // k_potrf128 the same way, behind the update of its block column
@@ -1104,7 +1121,7 @@ static cudaError_t launch_potrf(bdb_system* s, cudaStream_t st, T* M, int P, dou
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_potrf128<T>, M, s->npad, P, lkk, s->status.p);
+    return cudaLaunchKernelEx(&cfg, k_potrf128<T>, M, s->npad, P, lkk, s->status.p, (uint32_t)s->wait_limit);
 }
 
 // Factorisation with two panels of look-ahead on two streams. Panel P's

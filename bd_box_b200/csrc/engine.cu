@@ -94,10 +94,16 @@ int check_status(bdb_system* s, bool* overlap)
     unsigned st = 0;
     BDB_CUDA(cudaMemcpyAsync(&st, s->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
     BDB_CUDA(cudaStreamSynchronize(s->stream));
+    // a factorisation that met a non-positive pivot, gave up waiting or was
+    // launched wrongly left no usable factor: the next step rebuilds it
+    if (st & (ST_NOT_SPD | ST_TIMEOUT | ST_LAUNCH)) s->factor_valid = false;
     if (st & ST_BOND) return fail(BDB_ERR_BOND, "Overstretched bond (bond.c:73-78)");
-    if (st & ST_NOT_SPD) return fail(BDB_ERR_NOT_SPD, "Cholesky decomposition error: non-positive pivot");
-    if (st & ST_TIMEOUT) return fail(BDB_ERR_TIMEOUT, "device wait timed out");
+    // a kernel that did nothing or gave up leaves the rest of the
+    // factorisation working on partial data, whose pivots may then fail:
+    // report the cause first
     if (st & ST_LAUNCH) return fail(BDB_ERR_CUDA, "a kernel was launched with the wrong shape");
+    if (st & ST_TIMEOUT) return fail(BDB_ERR_TIMEOUT, "device wait timed out");
+    if (st & ST_NOT_SPD) return fail(BDB_ERR_NOT_SPD, "Cholesky decomposition error: non-positive pivot");
     if (overlap) *overlap = (st & ST_OVERLAP) != 0;
     return BDB_OK;
 }
@@ -765,6 +771,15 @@ int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm)
         drop_graph(s);
     }
     s->tea_tuned = s->mv_tuned = true;   // pinned values are not re-tuned
+    return BDB_OK;
+}
+
+int bdb_set_wait_limit(bdb_system* s, long long tries)
+{
+    if (!s) return fail(BDB_ERR_ARG, "null system");
+    if (tries > 0xffffffffll) return fail(BDB_ERR_ARG, "wait limit too large");
+    s->wait_limit = tries < 0 ? (1u << 22) : (unsigned)tries;
+    drop_graph(s);   // the graphs hold the limit their launches were made with
     return BDB_OK;
 }
 

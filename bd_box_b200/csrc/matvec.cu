@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
 k_strip_mv_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap map_x,
                const __grid_constant__ CUtensorMap map_f, int n3, int ntc, long long T, int slots,
                const double* __restrict__ F, double* __restrict__ rowp, double* __restrict__ colp,
-               unsigned* __restrict__ status)
+               unsigned* __restrict__ status, uint32_t wlim)
 {
     {
         uint32_t dyn;
@@ -280,7 +280,7 @@ k_strip_mv_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
             long long i = 0;
             for (long long t = t_beg; t < t_end && !abort_flag; ++t, ++i) {
                 const int st = (int)(i % MT_STAGES);
-                if (!mbar_wait(smem_u32(&bars.empty[st]), (uint32_t)((i / MT_STAGES) & 1) ^ 1u, &abort_flag)) break;
+                if (!mbar_wait(smem_u32(&bars.empty[st]), (uint32_t)((i / MT_STAGES) & 1) ^ 1u, &abort_flag, wlim)) break;
                 const uint32_t fb = smem_u32(&bars.full[st]);
                 const uint32_t dst = sbase + st * MT_STAGE_BYTES;
                 const int c0 = (int)(t % ntc) * MT_COLS;
@@ -304,7 +304,7 @@ k_strip_mv_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
             const int s = (int)(t / ntc), c0 = (int)(t % ntc) * MT_COLS;
             if (mt_lower(s * MT_ROWS, c0)) continue;
             const int b = (int)(u % MT_NB);
-            if (!mbar_wait(smem_u32(&bars.cfull[b]), (uint32_t)((u / MT_NB) & 1), &abort_flag)) break;
+            if (!mbar_wait(smem_u32(&bars.cfull[b]), (uint32_t)((u / MT_NB) & 1), &abort_flag, wlim)) break;
             const double2* cp = reinterpret_cast<const double2*>(cpart + (size_t)b * MT_CPART_DOUBLES) + 2 * lane;
             double2 a0 = cp[0], a1 = cp[1];
 #pragma unroll
@@ -356,7 +356,7 @@ k_strip_mv_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
             const int c = c0 + 4 * lane;
             const bool lower = mt_lower(r0, c0), upper = mt_upper(r0, c0);
             const int st = (int)(i % MT_STAGES);
-            ok = mbar_wait(smem_u32(&bars.full[st]), (uint32_t)((i / MT_STAGES) & 1), &abort_flag);
+            ok = mbar_wait(smem_u32(&bars.full[st]), (uint32_t)((i / MT_STAGES) & 1), &abort_flag, wlim);
             if (!ok) break;
             const unsigned char* stage = sm + st * MT_STAGE_BYTES;
             const float4* tile = reinterpret_cast<const float4*>(stage) + 32 * MT_RW * warp + lane;
@@ -423,7 +423,7 @@ k_strip_mv_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
             if (lane == 0) mbar_arrive(smem_u32(&bars.empty[st]));
             if (!lower) {
                 const int b = (int)(u % MT_NB);
-                ok = mbar_wait(smem_u32(&bars.cempty[b]), (uint32_t)((u / MT_NB) & 1) ^ 1u, &abort_flag);
+                ok = mbar_wait(smem_u32(&bars.cempty[b]), (uint32_t)((u / MT_NB) & 1) ^ 1u, &abort_flag, wlim);
                 if (!ok) break;
                 double2* cp = reinterpret_cast<double2*>(cpart + (size_t)b * MT_CPART_DOUBLES + warp * MT_COLS) + 2 * lane;
                 cp[0] = make_double2(pc[0], pc[1]);
@@ -619,7 +619,8 @@ static int stored_matvec_tma(bdb_system* s, bool want_rs)
     const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(s->mv_map);
     // X: any valid vector when Rs is not wanted
     k_strip_mv_tma<<<G, MT_THREADS, MT_SMEM, s->stream>>>(maps[0], want_rs ? maps[1] : maps[2], maps[2], n3, ntc, T,
-                                                           slots, s->F.p, rowp, colp, s->status.p);
+                                                           slots, s->F.p, rowp, colp, s->status.p,
+                                                           (uint32_t)s->wait_limit);
     BDB_CUDA(cudaGetLastError());
     const double pre = s->p.dt / (BDB_KB * s->p.T);
     k_mv_finish_tma<<<(n3 + FIN_ROWS - 1) / FIN_ROWS, FIN_ROWS * FIN_GROUPS, 0, s->stream>>>(

@@ -33,10 +33,13 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// bounded wait for the phase of the given parity; false on time-out or abort
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort)
+// bounded wait for the phase of the given parity, at most `limit` tries
+// (WAIT_LIMIT by default; a system's kernels take bdb_set_wait_limit's);
+// false on time-out or abort
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
+                                          uint32_t limit = WAIT_LIMIT)
 {
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

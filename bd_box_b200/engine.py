@@ -46,7 +46,7 @@ EXPORTS = [
     "bdb_frames_start", "bdb_frames_take", "bdb_frames_pending", "bdb_frames_flush", "bdb_frames_stop",
     "bdb_set_time", "bdb_get_time", "bdb_newton_resolve",
     "bdb_checkpoint_size", "bdb_checkpoint_save", "bdb_checkpoint_load", "bdb_refresh",
-    "bdb_get_factor_tuning", "bdb_set_factor_tuning",
+    "bdb_get_factor_tuning", "bdb_set_factor_tuning", "bdb_set_wait_limit",
 ]
 
 
@@ -116,6 +116,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_get_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.bdb_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.bdb_get_factor_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    lib.bdb_set_wait_limit.argtypes = [C.c_void_p, C.c_longlong]
     lib.bdb_set_factor_tuning.argtypes = [C.c_void_p, C.c_int]
     lib.bdb_adjoint.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _ip, _dp, _dp, _dp, _dp]
     lib.bdb_factor_error.argtypes = [C.c_void_p, _dp]
@@ -366,6 +367,11 @@ class System:
 
     def set_tuning(self, tea_tile: int = 0, mv_warps_per_sm: int = 0):
         self._check(self.lib.bdb_set_tuning(self.h, tea_tile, mv_warps_per_sm))
+
+    def set_wait_limit(self, tries: int):
+        """Tries of every bounded device wait (bdb_set_wait_limit; < 0: the
+        default)."""
+        self._check(self.lib.bdb_set_wait_limit(self.h, int(tries)))
 
     def factor_tuning(self) -> int:
         """SMs the mixed Cholesky's bulk updates leave to its panel chain."""

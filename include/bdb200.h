@@ -305,6 +305,18 @@ int bdb_autotune(bdb_system* s, int enable);
 int bdb_get_tuning(bdb_system* s, int* tea_tile, int* mv_warps_per_sm);
 int bdb_set_tuning(bdb_system* s, int tea_tile, int mv_warps_per_sm);
 
+/* Bounded device waits (no reference counterpart). Every wait of this
+ * system's kernels on another warp's or the copy engine's progress (mbarrier
+ * try_wait loops in the tensor-core Cholesky, its diagonal-block kernel and
+ * the TMA-fed stored-matrix product) gives up after `tries` tries (default
+ * 2^22, restored by a negative value): the kernel then sets its time-out
+ * flag, lets the copies and tensor-core operations it has in flight finish,
+ * frees its tensor memory and returns, and the call reports
+ * BDB_ERR_TIMEOUT with the context still usable; the next step rebuilds the
+ * factor. 0 makes every such wait give up at once, which tests that path
+ * without a hung GPU. */
+int bdb_set_wait_limit(bdb_system* s, long long tries);
+
 /* The third tunable site (no reference counterpart): how the mixed-precision
  * Cholesky splits the GPU. Its panel chain (panel solve, next block-column
  * update, next diagonal block) runs beside the bulk trailing updates, which

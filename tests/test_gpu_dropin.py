@@ -134,6 +134,35 @@ def test_stock_main_program_matches_cpu_build(case, tmp_path):
     assert np.allclose(eb, ec, rtol=1e-5, atol=2e-6)
 
 
+def test_stock_main_ermak_var_retries_match_cpu_build(tmp_path):
+    """comp_step_ermak's retry loop with ermak_var (diff_comp.c:152-179): a
+    dense suspension with overlap checks, where almost every move overlaps
+    at first and dt is halved until it does not. BD_BOX's stock main() on
+    the drop-in and the CPU build take the same retries (the frame times
+    show the halvings) and write the same frames."""
+    need(STOCK_B200)
+    need(STOCK_CPU)
+    outs = {}
+    for tag, exe in (("cpu", STOCK_CPU), ("b200", STOCK_B200)):
+        d = tmp_path / tag
+        d.mkdir()
+        decks.write_suspension_deck(str(d), "c", 100, seed=5, ewald_r=2, phi=0.3, dt=0.05,
+                                    extra={"hydro": "none", "check_overlap": "yes", "algorithm": "ermak_var",
+                                           "bdsteps": 6, "xyz_filename": "out.xyz", "save_xyz_freq": 1,
+                                           "move_attempts": 200})
+        r = subprocess.run([exe, "c.prm"], cwd=d, capture_output=True, text=True, timeout=600,
+                           env=dict(os.environ, OMP_NUM_THREADS="1"))
+        assert r.returncode == 0, (tag, r.stdout[-1000:], r.stderr[-1000:])
+        text = (d / "out.xyz").read_text()
+        times = [float(ln.split()[-1]) for ln in text.splitlines() if "time" in ln]
+        outs[tag] = (times, _numbers(d / "out.xyz"))
+    (tc, xc), (tb, xb) = outs["cpu"], outs["b200"]
+    assert tc == tb and len(tc) >= 6
+    assert (np.diff(tc) < 0.05 - 1e-9).any()     # retries with a halved dt happened
+    assert xc.size == xb.size
+    assert np.abs(xc - xb).max() <= 2e-6
+
+
 @pytest.mark.parametrize("name", ["rf", "sphere"])
 def test_dropin_external_forces_match_cpu_build(name, tmp_path):
     """Electric field and bounding sphere through the drop-in: BD_BOX's own
