@@ -19,8 +19,13 @@
 //   triangle with half the diagonal, gives
 //     lambda'^T dB X = <Dbar, dD>,  Dbar = B^-T Phi(v X^T) B^-1,  v = B^T lambda',
 //   formed with two blocked triangular solves (k_gemm_tn, k_trinv64).
-// Everything is FP64; the forward pass is recomputed from checkpoints every
-// `checkpoint` steps.
+// The forward pass is recomputed from checkpoints every `checkpoint` steps.
+// Precision follows the system's: FP64 throughout for an FP64 system; for a
+// mixed-precision system (FP32 tensor, 3xTF32 Cholesky) the forward steps
+// are the mixed path's, and the backward's O(n^3) part -- Phi(v X^T), the
+// two blocked triangular solves and their transposes -- runs in FP32 on its
+// FP32 factor, while the O(N^2) tile gradients and force products keep FP64
+// arithmetic and FP64 sums.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -70,9 +75,10 @@ __device__ __forceinline__ void tile_grad(const double* r, double si, double sj,
 //   G_ij = c (lam_i F_j^T + lam_j F_i^T) + S_ij,
 // S the (symmetric) noise weight matrix Z + Z^T (3x3 tile ij, row-major, ld),
 // or none. One warp per bead, lanes over j, fixed-order reduction.
+template <typename T>
 __global__ void k_tile_grad(int n, const double4* __restrict__ pos, double preDii, double preDij, double c,
                             const double* __restrict__ lam, const double* __restrict__ F,
-                            const double* __restrict__ S, int ld, double* __restrict__ grad)
+                            const T* __restrict__ S, int ld, double* __restrict__ grad)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i >= n) return;
@@ -91,7 +97,7 @@ __global__ void k_tile_grad(int n, const double4* __restrict__ pos, double preDi
         for (int a = 0; a < 3; ++a)
             for (int b = 0; b < 3; ++b)
                 G[3 * a + b] = c * (li[a] * F[3 * j + b] + lam[3 * j + a] * fi[b]) +
-                               (S ? S[(size_t)(3 * i + a) * ld + 3 * j + b] : 0.0);
+                               (S ? (double)S[(size_t)(3 * i + a) * ld + 3 * j + b] : 0.0);
         double g[3];
         tile_grad(r, pj.w, pi.w, preDii, preDij, G, g);
         acc[0] += g[0];
@@ -225,7 +231,8 @@ __global__ void k_force_jvp(int n, AdjForce fp, const double4* __restrict__ pos,
 // in a fixed order.
 static constexpr int MV2_COLS = 64, MV2_ROWS = 256;
 
-__global__ void __launch_bounds__(256) k_mv2(const double* __restrict__ M, int n, int ld,
+template <typename TM>
+__global__ void __launch_bounds__(256) k_mv2(const TM* __restrict__ M, int n, int ld,
                                              const double* __restrict__ lam, double* __restrict__ colp,
                                              double* __restrict__ rowp)
 {
@@ -239,7 +246,7 @@ __global__ void __launch_bounds__(256) k_mv2(const double* __restrict__ M, int n
         const int row = rb * MV2_ROWS + g * 64 + k;
         double rsum = 0;
         if (row < n && col < n) {
-            const double m = M[(size_t)row * ld + col];
+            const double m = (double)M[(size_t)row * ld + col];
             const double lr = lam[row];
             if (col <= row) {
                 sl += m * lr;
@@ -283,18 +290,20 @@ __global__ void k_mv2_finish(int n, int nrb, int ncb, const double* __restrict__
 }
 
 // R = Phi(v X^T): lower triangle, half the diagonal
-__global__ void k_phi(int n, const double* __restrict__ v, const double* __restrict__ X, double* __restrict__ R)
+template <typename T>
+__global__ void k_phi(int n, const double* __restrict__ v, const double* __restrict__ X, T* __restrict__ R)
 {
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (size_t)n * n) return;
     const int a = (int)(idx / n), b = (int)(idx % n);
-    R[idx] = a > b ? v[a] * X[b] : (a == b ? 0.5 * v[a] * X[a] : 0.0);
+    R[idx] = (T)(a > b ? v[a] * X[b] : (a == b ? 0.5 * v[a] * X[a] : 0.0));
 }
 
 // out = in^T (n x n, row-major), or out = in + in^T when sym
-__global__ void k_transpose(int n, const double* __restrict__ in, double* __restrict__ out, int sym)
+template <typename T>
+__global__ void k_transpose(int n, const T* __restrict__ in, T* __restrict__ out, int sym)
 {
-    __shared__ double t[32][33];
+    __shared__ T t[32][33];
     const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
     for (int k = threadIdx.y; k < 32; k += 8) {
         const int r = by + k, c = bx + threadIdx.x;
@@ -304,56 +313,59 @@ __global__ void k_transpose(int n, const double* __restrict__ in, double* __rest
     for (int k = threadIdx.y; k < 32; k += 8) {
         const int r = bx + k, c = by + threadIdx.x;
         if (r < n && c < n) {
-            const double tv = t[threadIdx.x][k];
+            const T tv = t[threadIdx.x][k];
             out[(size_t)r * n + c] = sym ? in[(size_t)r * n + c] + tv : tv;
         }
     }
 }
 
 // inverses of the 64x64 diagonal blocks of the lower-triangular B (ld):
-// Winv[k] row-major 64x64, column c by forward substitution (thread c)
-__global__ void k_trinv64(const double* __restrict__ B, int ld, double* __restrict__ Winv)
+// Winv[k] row-major 64x64, column c by forward substitution (thread c),
+// accumulated in FP64 over the column's entries as stored (T)
+template <typename TM, typename T>
+__global__ void k_trinv64(const TM* __restrict__ B, int ld, T* __restrict__ Winv)
 {
     __shared__ double Bs[64][65];
     const int k = blockIdx.x, c = threadIdx.x;
     const size_t o = (size_t)k * 64;
-    for (int r = 0; r < 64; ++r) Bs[r][c] = c <= r ? B[(o + r) * ld + o + c] : 0.0;
+    for (int r = 0; r < 64; ++r) Bs[r][c] = c <= r ? (double)B[(o + r) * ld + o + c] : 0.0;
     __syncthreads();
-    double* W = Winv + (size_t)k * 64 * 64;
+    T* W = Winv + (size_t)k * 64 * 64;
     for (int i = 0; i < 64; ++i) {
         double w;
         if (i < c) {
             w = 0.0;
         } else {
             double s = i == c ? 1.0 : 0.0;
-            for (int m = c; m < i; ++m) s -= Bs[i][m] * W[m * 64 + c];
+            for (int m = c; m < i; ++m) s -= Bs[i][m] * (double)W[m * 64 + c];
             w = s / Bs[i][i];
         }
-        W[i * 64 + c] = w;
+        W[i * 64 + c] = (T)w;
     }
 }
 
-// C[M x N] = alpha A^T B + beta C, FP64; A is K x M (lda), B K x N (ldb), C
-// M x N (ldc), all row-major; M, N multiples of 64, K of 16. 64x64 tiles,
-// 256 threads with 4x4 outputs each (rows ty + 16 i, columns tx + 16 j).
-__global__ void __launch_bounds__(256) k_gemm_tn(int M, int N, int K, double alpha, const double* __restrict__ A,
-                                                 int lda, const double* __restrict__ B, int ldb, double beta,
-                                                 double* __restrict__ C, int ldc)
+// C[M x N] = alpha A^T B + beta C in T (FP64 or FP32) arithmetic; A is
+// K x M (lda, elements TA), B K x N (ldb), C M x N (ldc), all row-major; M,
+// N multiples of 64, K of 16. 64x64 tiles, 256 threads with 4x4 outputs
+// each (rows ty + 16 i, columns tx + 16 j).
+template <typename T, typename TA>
+__global__ void __launch_bounds__(256) k_gemm_tn(int M, int N, int K, T alpha, const TA* __restrict__ A, int lda,
+                                                 const T* __restrict__ B, int ldb, T beta, T* __restrict__ C, int ldc)
 {
-    __shared__ double As[16][64 + 2], Bs[16][64 + 2];
+    __shared__ T As[16][64 + 2], Bs[16][64 + 2];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    double acc[4][4] = {};
+    T acc[4][4] = {};
     for (int k0 = 0; k0 < K; k0 += 16) {
         for (int e = threadIdx.x; e < 16 * 64; e += 256) {
             const int kk = e >> 6, mm = e & 63;
-            As[kk][mm] = A[(size_t)(k0 + kk) * lda + m0 + mm];
+            As[kk][mm] = (T)A[(size_t)(k0 + kk) * lda + m0 + mm];
             Bs[kk][mm] = B[(size_t)(k0 + kk) * ldb + n0 + mm];
         }
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < 16; ++kk) {
-            double a[4], b[4];
+            T a[4], b[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 a[i] = As[kk][ty + 16 * i];
@@ -370,31 +382,33 @@ __global__ void __launch_bounds__(256) k_gemm_tn(int M, int N, int K, double alp
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            double* cp = C + (size_t)(m0 + ty + 16 * i) * ldc + n0 + tx + 16 * j;
-            *cp = beta == 0.0 ? alpha * acc[i][j] : alpha * acc[i][j] + beta * *cp;
+            T* cp = C + (size_t)(m0 + ty + 16 * i) * ldc + n0 + tx + 16 * j;
+            *cp = beta == (T)0 ? alpha * acc[i][j] : alpha * acc[i][j] + beta * *cp;
         }
 }
 
-static void gemm_tn(cudaStream_t st, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
-                    int ldb, double beta, double* C, int ldc)
+template <typename T, typename TA>
+static void gemm_tn(cudaStream_t st, int M, int N, int K, T alpha, const TA* A, int lda, const T* B, int ldb, T beta,
+                    T* C, int ldc)
 {
     dim3 grid(N / 64, M / 64);
-    k_gemm_tn<<<grid, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    k_gemm_tn<T, TA><<<grid, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
 // Y = B^-T R for the lower-triangular B (ld ldb, n x n, n a multiple of 64),
 // right-looking from the last 64-row block; R (n x n) is overwritten.
 // Winv: inverses of B's diagonal blocks (k_trinv64).
-static int trsm_lt(bdb_system* s, int n, const double* B, int ldb, const double* Winv, double* R, double* Y)
+template <typename T, typename TM>
+static int trsm_lt(bdb_system* s, int n, const TM* B, int ldb, const T* Winv, T* R, T* Y)
 {
     const int nb = n / 64;
     for (int k = nb - 1; k >= 0; --k) {
-        double* Yk = Y + (size_t)k * 64 * n;
+        T* Yk = Y + (size_t)k * 64 * n;
         // Y_k = Winv_k^T R_k
-        gemm_tn(s->stream, 64, n, 64, 1.0, Winv + (size_t)k * 64 * 64, 64, R + (size_t)k * 64 * n, n, 0.0, Yk, n);
+        gemm_tn<T, T>(s->stream, 64, n, 64, (T)1, Winv + (size_t)k * 64 * 64, 64, R + (size_t)k * 64 * n, n, (T)0, Yk, n);
         // R_0..k-1 -= B[k, 0:k]^T Y_k
         if (k > 0)
-            gemm_tn(s->stream, 64 * k, n, 64, -1.0, B + (size_t)k * 64 * ldb, ldb, Yk, n, 1.0, R, n);
+            gemm_tn<T, TM>(s->stream, 64 * k, n, 64, (T)-1, B + (size_t)k * 64 * ldb, ldb, Yk, n, (T)1, R, n);
         s->launches += 1 + (k > 0);
     }
     BDB_CUDA(cudaGetLastError());
@@ -415,6 +429,27 @@ struct Scratch {
         return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * std::max<size_t>(n, 1)) == cudaSuccess ? 0 : 1;
     }
 };
+
+// u = D lam and v = B^T lam from the stored matrix M (D upper, B lower),
+// then S = Z + Z^T with Z^T = Dbar = B^-T Phi(v X^T) B^-1 into R (T, np x
+// np); Y is scratch of the same size
+template <typename T, typename TM>
+static int adjoint_linalg(bdb_system* s, const TM* M, int np, int n3, int nrb, int ncb, const double* lam,
+                          double* colp, double* rowp, double* u, double* v, const double* Xp, T* R, T* Y, T* Winv)
+{
+    cudaStream_t st = s->stream;
+    k_mv2<TM><<<dim3(ncb, nrb), 256, 0, st>>>(M, n3, np, lam, colp, rowp);
+    k_mv2_finish<<<(n3 + 255) / 256, 256, 0, st>>>(n3, nrb, ncb, colp, rowp, s->dD.p, lam, u, v);
+    k_phi<T><<<(unsigned)(((size_t)np * np + 255) / 256), 256, 0, st>>>(np, v, Xp, R);
+    k_trinv64<TM, T><<<np / 64, 64, 0, st>>>(M, np, Winv);
+    int rc = trsm_lt<T, TM>(s, np, M, np, Winv, R, Y);
+    if (rc) return rc;
+    k_transpose<T><<<dim3(np / 32, np / 32), dim3(32, 8), 0, st>>>(np, Y, R, 0);
+    if ((rc = trsm_lt<T, TM>(s, np, M, np, Winv, R, Y))) return rc;
+    k_transpose<T><<<dim3(np / 32, np / 32), dim3(32, 8), 0, st>>>(np, Y, R, 1);
+    s->launches += 6;
+    return BDB_OK;
+}
 
 static int set_counter(bdb_system* s, unsigned long long v)
 {
@@ -441,10 +476,11 @@ extern "C" int bdb_adjoint(bdb_system* s, int K, int checkpoint, int npairs, con
 {
     if (!s || K < 1 || checkpoint < 1 || npairs < 1 || !pairs || !targets || !loss || !grad_coord || !grad_params)
         return fail(BDB_ERR_ARG, "bad arguments");
-    if (s->p.hydro != BDB_HYDRO_CHOLESKY || s->p.precision != BDB_PREC_FP64 || s->p.refresh != 1 ||
-        s->p.noise != BDB_NOISE_PHILOX || s->p.bc != 0 || s->segs.size() != 1)
+    if (s->p.hydro != BDB_HYDRO_CHOLESKY || s->p.refresh != 1 || s->p.noise != BDB_NOISE_PHILOX || s->p.bc != 0 ||
+        s->segs.size() != 1)
         return fail(BDB_ERR_UNSUPPORTED,
-                    "the adjoint needs one free-space system, hydro cholesky, FP64, refresh 1 and device noise");
+                    "the adjoint needs one free-space system, hydro cholesky, refresh 1 and device noise");
+    const bool mixed = s->p.precision == BDB_PREC_MIXED;
     if (s->p.e_ext && s->p.e_type != 0)
         return fail(BDB_ERR_UNSUPPORTED, "the adjoint takes a constant (DC) external field only");
     if (s->n_angle || s->n_angle_cos || s->n_dihe || s->n_dihe_angle)
@@ -555,25 +591,28 @@ extern "C" int bdb_adjoint(bdb_system* s, int K, int checkpoint, int npairs, con
                 (rc = noise_fill(s, nullptr)))
                 return rc;
             BDB_CUDA(cudaMemcpyAsync(Xp.p, s->X.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
-            // u = D lam, v = B^T lam
-            k_mv2<<<dim3(ncb, nrb), 256, 0, st>>>(s->M64.p, n3, np, lam.p, colp.p, rowp.p);
-            k_mv2_finish<<<(n3 + 255) / 256, 256, 0, st>>>(n3, nrb, ncb, colp.p, rowp.p, s->dD.p, lam.p, u.p, v.p);
-            // S = Z + Z^T with Z^T = Dbar = B^-T Phi(v X^T) B^-1
-            k_phi<<<(unsigned)(((size_t)np * np + 255) / 256), 256, 0, st>>>(np, v.p, Xp.p, R.p);
-            k_trinv64<<<np / 64, 64, 0, st>>>(s->M64.p, np, Winv.p);
-            if ((rc = trsm_lt(s, np, s->M64.p, np, Winv.p, R.p, Y.p))) return rc;
-            k_transpose<<<dim3(np / 32, np / 32), dim3(32, 8), 0, st>>>(np, Y.p, R.p, 0);
-            if ((rc = trsm_lt(s, np, s->M64.p, np, Winv.p, R.p, Y.p))) return rc;
-            k_transpose<<<dim3(np / 32, np / 32), dim3(32, 8), 0, st>>>(np, Y.p, R.p, 1);
+            // u = D lam, v = B^T lam; S = Z + Z^T with Z^T = Dbar = B^-T Phi(v X^T) B^-1
+            if (mixed)
+                rc = adjoint_linalg<float, float>(s, s->M32.p, np, n3, nrb, ncb, lam.p, colp.p, rowp.p, u.p, v.p, Xp.p,
+                                                  reinterpret_cast<float*>(R.p), reinterpret_cast<float*>(Y.p),
+                                                  reinterpret_cast<float*>(Winv.p));
+            else
+                rc = adjoint_linalg<double, double>(s, s->M64.p, np, n3, nrb, ncb, lam.p, colp.p, rowp.p, u.p, v.p,
+                                                    Xp.p, R.p, Y.p, Winv.p);
+            if (rc) return rc;
             // lam_k = lam + c (dD/dx : F)^T lam + (d(BX)/dx)^T lam + c (dF/dx) u
             BDB_CUDA(cudaMemcpyAsync(lam2.p, lam.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
-            k_tile_grad<<<warps_blocks, 256, 0, st>>>(n, s->pos.p, s->preDii, s->preDij, c, lam.p, s->F.p, R.p, np,
-                                                     lam2.p);
+            if (mixed)
+                k_tile_grad<float><<<warps_blocks, 256, 0, st>>>(n, s->pos.p, s->preDii, s->preDij, c, lam.p, s->F.p,
+                                                                reinterpret_cast<const float*>(R.p), np, lam2.p);
+            else
+                k_tile_grad<double><<<warps_blocks, 256, 0, st>>>(n, s->pos.p, s->preDii, s->preDij, c, lam.p, s->F.p,
+                                                                 R.p, np, lam2.p);
             k_force_jvp<<<warps_blocks, 256, 0, st>>>(n, fp, s->pos.p, s->Q.p, s->LJ.p, s->conn_ptr.p,
                                                      s->conn_list.p, d_bptr.p, d_blist.p, s->bond_pairs.p,
                                                      s->bond_parms.p, u.p, c, lam2.p, ppart.p);
             BDB_CUDA(cudaGetLastError());
-            s->launches += 9;
+            s->launches += 3;
             BDB_CUDA(cudaMemcpyAsync(pph.data(), ppart.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, st));
             BDB_CUDA(cudaStreamSynchronize(st));
             for (int i = 0; i < n; ++i)

@@ -505,64 +505,89 @@ def replicas(torch, engine, steps, warmup, dist=None, rank=0, world=1):
 
 def adjoint_case(torch, engine):
     """Adjoint workload: an N=1024 chain with the chain force field, free-space
-    RPY with Cholesky noise (a fixed Philox sequence), 200 steps, checkpoint
-    every 20; loss = mean squared deviation of 128 seeded pair distances from
-    seeded targets in [10, 60] A. One gradient (forward, recomputation and
-    backward) is timed; one random direction of the position gradient is
-    checked against a central difference of the FP64 forward."""
+    RPY with Cholesky noise at a fixed Philox sequence, 200 steps, checkpoint
+    every 20; loss = mean squared deviation of 128 seeded bead-pair distances
+    from seeded targets in [10, 60] A. The electrostatic and LJ cutoffs lie
+    beyond the chain's extent, so no pair crosses a cutoff under the finite
+    differences. The mixed-precision adjoint (FP32 forward and triangular
+    solves, FP64 sums) and the FP64 one are timed; both are checked against
+    central differences (h = 1e-4) of the FP64 forward along a random
+    direction of the initial positions and for the four scale factors (LJ
+    epsilon, LJ sigma, bond H, Debye length)."""
+    import copy
     from bd_box_b200 import decks
     with tempfile.TemporaryDirectory() as d:
-        deck = decks.read_deck(decks.write_chain_deck(d, "adj1024", 1024, seed=21, hydro="cholesky"))
+        deck = decks.read_deck(decks.write_chain_deck(d, "adj1024", 1024, seed=21, hydro="cholesky",
+                                                      extra={"cutoff_c": 1000, "cutoff_lj": 1000}))
     rng = np.random.default_rng(4)
     pairs = np.array([rng.choice(deck.n, 2, replace=False) for _ in range(128)], dtype=np.int32)
     targets = rng.uniform(10, 60, size=len(pairs))
-    K, ck = 200, 20
+    K, ck, h = 200, 20, 1e-4
 
-    def new_sys(coord=None):
-        s = engine.System(deck, precision=engine.PREC_FP64, refresh=1, noise=engine.NOISE_PHILOX, seed=99)
-        if coord is not None:
-            s.set_coord(coord)
-        return s
+    def scaled(x0=None, sc=(1.0, 1.0, 1.0, 1.0)):
+        dk = copy.deepcopy(deck)
+        if x0 is not None:
+            dk.coord = dk.coord.copy()
+            dk.coord[:, :3] = x0
+        dk.LJ = dk.LJ.copy()
+        dk.LJ[:, 1] *= sc[0]
+        dk.LJ[:, 0] *= sc[1]
+        dk.bond_parms = dk.bond_parms.copy()
+        dk.bond_parms[:, 2] *= sc[2]
+        dk.prm = dict(dk.prm)
+        dk.prm["kappa_c"] = dk.prm["kappa_c"] / sc[3]
+        return dk
 
-    s = new_sys()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    loss, gx, gp = s.adjoint(K, ck, pairs, targets)
-    torch.cuda.synchronize()
-    t_grad = time.perf_counter() - t0
-    s.close()
-    s = new_sys()
-    t0 = time.perf_counter()
-    s.step(K)
-    torch.cuda.synchronize()
-    t_fwd = time.perf_counter() - t0
-    s.close()
-
-    def loss_at(coord):
-        s = new_sys(coord)
+    def loss_at(dk):
+        s = engine.System(dk, precision=engine.PREC_FP64, refresh=1, noise=engine.NOISE_PHILOX, seed=99)
         s.step(K)
         x = s.get_coord()[:, :3]
         s.close()
         r = np.linalg.norm(x[pairs[:, 1]] - x[pairs[:, 0]], axis=1)
         return float(np.mean((r - targets) ** 2))
 
+    out = {"workload": "chain N=1024, Cholesky noise (fixed Philox sequence), 200 steps, checkpoint 20, 128 "
+                       "pair-distance loss; cutoffs beyond the chain's extent"}
+    grads = {}
+    for name, prec in (("mixed", engine.PREC_MIXED), ("fp64", engine.PREC_FP64)):
+        s = engine.System(deck, precision=prec, refresh=1, noise=engine.NOISE_PHILOX, seed=99)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss, gx, gp = s.adjoint(K, ck, pairs, targets)
+        torch.cuda.synchronize()
+        t_grad = time.perf_counter() - t0
+        s.close()
+        s = engine.System(deck, precision=prec, refresh=1, noise=engine.NOISE_PHILOX, seed=99)
+        t0 = time.perf_counter()
+        s.step(K)
+        torch.cuda.synchronize()
+        t_fwd = time.perf_counter() - t0
+        s.close()
+        grads[name] = (gx, gp)
+        out[name] = {"loss": loss, "seconds_per_gradient": t_grad, "seconds_forward_only": t_fwd,
+                     "gradient_over_forward": t_grad / t_fwd}
     v = rng.standard_normal((deck.n, 3))
     v /= np.linalg.norm(v)
-    # h = 1e-5 A: with the 12 A cutoffs a few of the ~5e5 pairs cross a
-    # cutoff between the two h = 1e-4 trajectories over 200 steps, and the
-    # force jump swamps that difference
-    h = 1e-5
-    c0 = deck.coord.copy()
-    cp, cm = c0.copy(), c0.copy()
-    cp[:, :3] += h * v
-    cm[:, :3] -= h * v
-    fd = (loss_at(cp) - loss_at(cm)) / (2 * h)
-    an = float(np.sum(gx * v))
-    return {"workload": "chain N=1024, Cholesky noise, 200 steps, checkpoint 20, 128 pair-distance loss, FP64",
-            "loss": loss, "seconds_per_gradient": t_grad, "seconds_forward_only": t_fwd,
-            "gradient_over_forward": t_grad / t_fwd,
-            "fd_check": {"direction": "random unit", "h": h, "fd": fd, "adjoint": an, "rel_err": abs(fd - an) / abs(fd)},
-            "grad_scale_factors": {"lj_epsilon": gp[0], "lj_sigma": gp[1], "bond_H": gp[2], "debye_length": gp[3]}}
+    c0 = deck.coord[:, :3]
+    fd_x = (loss_at(scaled(c0 + h * v)) - loss_at(scaled(c0 - h * v))) / (2 * h)
+    fd_p = []
+    for k in range(4):
+        sp, sm = [1.0] * 4, [1.0] * 4
+        sp[k] += h
+        sm[k] -= h
+        fd_p.append((loss_at(scaled(sc=sp)) - loss_at(scaled(sc=sm))) / (2 * h))
+    for name in ("mixed", "fp64"):
+        gx, gp = grads[name]
+        an = float(np.sum(gx * v))
+        out[name]["fd_check"] = {
+            "h": h, "position_direction": {"fd": fd_x, "adjoint": an, "rel_err": abs(fd_x - an) / abs(fd_x)},
+            "scale_factors": {nm: {"fd": fd_p[k], "adjoint": float(gp[k]), "rel_err": abs(fd_p[k] - gp[k]) / abs(fd_p[k])}
+                              for k, nm in enumerate(("lj_epsilon", "lj_sigma", "bond_H", "debye_length"))}}
+    gxm, gpm = grads["mixed"]
+    gxd, gpd = grads["fp64"]
+    out["mixed_vs_fp64_gradient_rel"] = {"positions": float(np.linalg.norm(gxm - gxd) / np.linalg.norm(gxd)),
+                                         "scale_factors": [float(abs(a - b) / abs(b)) for a, b in zip(gpm, gpd)]}
+    return out
 
 
 EWALD_R = 4   # lattice radius of the Ewald sums: D.F within 1e-6 of R = 5 (R = 3: 7e-6)
