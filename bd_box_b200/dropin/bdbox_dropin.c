@@ -31,11 +31,16 @@
  * BDB_REFRESH=K (rebuild D and its Cholesky factor every K steps; default 1,
  * the reference schedule).
  *
- * Not available in the engine, and reported through the host's
- * unexpected_error (err.c:48-90) like any other fatal input error: IGT
- * algorithms with hydro geyer, Newton overlap removal when an overlap
- * actually occurs, Chebyshev noise, sphere boundaries, external electric
- * fields and velocity-gradient flows.
+ * Supported beyond the plain Ermak-McCammon step: ermak_var (dt halving on
+ * overlaps), ermak_newton (elastic-collision overlap removal,
+ * bdb_newton_resolve), igt_const / igt_var with hydro none or cholesky,
+ * external electric fields (DC, AC, RF), the bounding sphere (bc sphere,
+ * sboundary) and flowing solvent (vel_grad_tensor). Reported through the
+ * host's unexpected_error (err.c:48-90) like any other fatal input error:
+ * the IGT algorithms with hydro geyer, comp_step_rev_IGT (unimplemented in
+ * BD_BOX itself), hydro methods other than none, cholesky and geyer (the
+ * Chebyshev noise), a tensor that is not positive definite, an
+ * over-stretched bond and CUDA errors.
  */
 #if HAVE_CONFIG_H
 #include <config.h>
