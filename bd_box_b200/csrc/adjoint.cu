@@ -495,7 +495,7 @@ extern "C" int bdb_adjoint(bdb_system* s, int K, int checkpoint, int npairs, con
     // bead -> bond list (host CSR, fixed order)
     std::vector<int> bp_h(2 * std::max(1, s->n_bond)), bptr(n + 1, 0), blist;
     if (s->n_bond)
-        BDB_CUDA(cudaMemcpy(bp_h.data(), s->bond_pairs.p, sizeof(int) * 2 * s->n_bond, cudaMemcpyDeviceToHost));
+        BDB_CUDA(d2h(s, bp_h.data(), s->bond_pairs.p, sizeof(int) * 2 * s->n_bond));
     for (int t = 0; t < s->n_bond; ++t) {
         bptr[bp_h[2 * t] + 1]++;
         bptr[bp_h[2 * t + 1] + 1]++;
@@ -519,8 +519,8 @@ extern "C" int bdb_adjoint(bdb_system* s, int K, int checkpoint, int npairs, con
         rowp.alloc((size_t)ncb * n3) || ppart.alloc(4 * (size_t)n) || ckpt.alloc((size_t)nck * n) ||
         seg.alloc((size_t)checkpoint * n) || xK.alloc(n) || d_bptr.alloc(n + 1) || d_blist.alloc(blist.size()))
         return fail(BDB_ERR_NOMEM, "adjoint scratch allocation failed");
-    BDB_CUDA(cudaMemcpy(d_bptr.p, bptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-    BDB_CUDA(cudaMemcpy(d_blist.p, blist.data(), sizeof(int) * blist.size(), cudaMemcpyHostToDevice));
+    BDB_CUDA(h2d(s, d_bptr.p, bptr.data(), sizeof(int) * (n + 1)));
+    BDB_CUDA(h2d(s, d_blist.p, blist.data(), sizeof(int) * blist.size()));
     BDB_CUDA(cudaMemsetAsync(u.p, 0, sizeof(double) * np, st));
     BDB_CUDA(cudaMemsetAsync(v.p, 0, sizeof(double) * np, st));
     BDB_CUDA(cudaMemsetAsync(Xp.p, 0, sizeof(double) * np, st));

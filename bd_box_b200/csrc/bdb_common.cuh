@@ -74,8 +74,9 @@ struct bdb_system {
     int n3 = 0;      // 3n
     int npad = 0;    // stored-matrix dimension (3n rounded up to the tile)
     cudaStream_t stream = nullptr;
-    cudaStream_t stream2 = nullptr;            // look-ahead panel factorisation
-    cudaEvent_t la_ev[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t stream2 = nullptr;            // Cholesky: bulk trailing updates
+    cudaStream_t stream3 = nullptr;            // Cholesky: the panel chain's side work
+    cudaEvent_t la_ev[6] = {};                 // their hand-offs (chol_tc.cu)
     double inv_L[3] = {0, 0, 0};
     double preDii = 0, preDij = 0;
 
@@ -260,4 +261,25 @@ int diag_noise(bdb_system* s);        // hydro none: Rs = X sqrt(2 dt D_ii)
 int factor_error(bdb_system* s, double* rel);
 int ensure_matrix(bdb_system* s);    // allocate the stored matrix (identity padding)
 int engine_step(bdb_system* s);      // one Ermak-McCammon step, device noise
+
+// Copies and fills ordered on the system's stream. The system's streams are
+// non-blocking: they do not wait for the legacy default stream, where a plain
+// cudaMemcpy / cudaMemset goes, so a fill queued there may land after (and
+// erase) what a kernel on the system's stream has written since, and a plain
+// device-to-host copy may read before that kernel has finished.
+inline cudaError_t h2d(const bdb_system* s, void* dst, const void* src, size_t bytes)
+{
+    // a pageable source is staged before the call returns
+    return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->stream) : cudaSuccess;
+}
+inline cudaError_t d2h(const bdb_system* s, void* dst, const void* src, size_t bytes)
+{
+    if (!bytes) return cudaSuccess;
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->stream);
+    return e != cudaSuccess ? e : cudaStreamSynchronize(s->stream);
+}
+inline cudaError_t dzero(const bdb_system* s, void* dst, size_t bytes)
+{
+    return bytes ? cudaMemsetAsync(dst, 0, bytes, s->stream) : cudaSuccess;
+}
 }  // namespace bdb

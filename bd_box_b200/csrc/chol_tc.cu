@@ -142,10 +142,14 @@ __device__ __forceinline__ void tri_index(int idx, int& ti, int& tj)
 
 // tile t of a launch -> (ti, tj) relative to the first trailing block:
 // mode 0 all tiles of the lower triangle, 1 only block column 0, 2 only
-// block column 1, 3 block columns 2 and beyond
+// block column 1, 3 block columns 2 and beyond, 4 block column 0 below its
+// diagonal tile
 __device__ __forceinline__ void tile_of_mode(int t, int mode, int& ti, int& tj)
 {
-    if (mode == 1 || mode == 2) {
+    if (mode == 4) {
+        ti = t + 1;
+        tj = 0;
+    } else if (mode == 1 || mode == 2) {
         tj = mode - 1;
         ti = t + tj;
     } else {
@@ -615,7 +619,7 @@ __device__ __forceinline__ double c2a(double c0, double c1, int h, int fr, int f
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, int npad, int P,
+__global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, int npad, int P, int unit0, int units,
                                                           const double* __restrict__ Lf, float* __restrict__ Lhi,
                                                           float* __restrict__ Llo, unsigned* __restrict__ status)
 {
@@ -634,8 +638,8 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int fr = lane >> 2, fq = lane & 3;
     const size_t base = (size_t)P * PW;
-    const size_t row0 = base + PW;
-    const int units = (int)(((size_t)npad - row0) / 8);
+    // units unit0 .. unit0 + units - 1 of 8 rows below the block
+    const size_t row0 = base + PW + (size_t)8 * unit0;
     {
         // the factor: a plain copy, loads batched ahead of stores
         const double2* src = reinterpret_cast<const double2*>(Lf);
@@ -1064,7 +1068,7 @@ static int tc_setup(bdb_system* s)
     const size_t pan = (size_t)s->npad * PW;
     // floats of the panel sets are counted as half a double each
     if (s->panel64.alloc((size_t)PANEL_SETS * pan + (size_t)PANEL_SETS * PANEL_FAC + 64)) return BDB_ERR_NOMEM;
-    BDB_CUDA(cudaMemset(s->panel64.p, 0, s->panel64.n * sizeof(double)));
+    BDB_CUDA(dzero(s, s->panel64.p, s->panel64.n * sizeof(double)));
     static_assert(sizeof(CUtensorMap) * (2 * PANEL_SETS + 1) <= sizeof(bdb_system::tc_map), "tensor-map storage");
     CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(s->tc_map);   // hi0, lo0, hi1, lo1, hi2, lo2, M
     for (int set = 0; set < PANEL_SETS; ++set) {
@@ -1124,84 +1128,125 @@ static cudaError_t launch_potrf(bdb_system* s, cudaStream_t st, T* M, int P, dou
     return cudaLaunchKernelEx(&cfg, k_potrf128<T>, M, s->npad, P, lkk, s->status.p, (uint32_t)s->wait_limit);
 }
 
-// Factorisation with two panels of look-ahead on two streams. Panel P's
-// trailing update is split three ways: A (block column P+1), B (block
-// column P+2) and C (block columns P+3 and beyond).
-//   chain stream:  panel solve P -> A(P) -> diagonal block P+1 -> ...
-//   bulk stream:   B(P) -> C(P) -> B(P+1) -> C(P+1) -> ...
-// The bulk stream starts B(P) once panel P is solved; the chain stream
-// waits for B(P-1) before the panel solve P, since A(P) updates block
-// column P+1 after B(P-1) did. So C(P) runs beside the next two steps of
-// the chain, and every tile still receives its updates in panel order
-// (the same sums, so the same bits, as with no look-ahead).
-int factor_mixed_tc(bdb_system* s)
+// The factorisation schedule, on three streams. Panel P's trailing update
+// is split four ways: the diagonal tile of block column P+1 (A0), the rest
+// of that column (A1), block column P+2 (B) and block columns P+3 on (C);
+// its panel solve two ways: block row P+1 (top) and the rows below (rest).
+//   chain stream: top(P) -> A0(P) -> diagonal block P+1 -> top(P+1) -> ...
+//   side stream:  rest(P) -> A1(P) -> rest(P+1) -> ...
+//   bulk stream:  B(P) -> C(P) -> B(P+1) -> C(P+1) -> ...
+// So the diagonal block P+1 waits only for one panel-solve block row and
+// one tile update, while the rest of panel P's solve and of its column
+// update run beside it; the bulk updates of panel P run beside the next two
+// steps of the chain. Hand-offs:
+//   rest(P) after the diagonal block P; top(P) after A1(P-1) and B(P-1)
+//   (both update block column P or P+1 before panel P's updates do);
+//   A1(P) after top(P) (its B operand rows) and B(P-1); B(P) once the whole
+//   panel is solved.
+// Every tile still receives its updates in panel order (the same sums, so
+// the same bits, as with no look-ahead). Three panel-buffer sets let C(P)
+// read panel P while panels P+1 and P+2 are solved. The persistent bulk
+// updates leave s->chain_sms SMs to the chain and side kernels (tuned).
+template <typename T, typename Update>
+static int factor_schedule(bdb_system* s, T* M, Update update)
 {
-    int rc = tc_setup(s);
-    if (rc) return rc;
-    const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(s->tc_map);
-    const CUtensorMap& mapc = maps[2 * PANEL_SETS];
     const int nt = s->npad / PW;
-    cudaStream_t st = s->stream, st2 = s->stream2;
-    cudaEvent_t ev_solved = s->la_ev[0], ev_b = s->la_ev[1], ev_end = s->la_ev[2];
-    // the persistent bulk updates leave s->chain_sms SMs to the chain
-    // kernels running beside them (tuned: engine.cu factor_tune)
-    const int bulk_sms = std::max(1, s->sm_count - std::min(std::max(s->chain_sms, 0), s->sm_count - 1));
+    cudaStream_t st = s->stream, st2 = s->stream2, st3 = s->stream3;
+    cudaEvent_t ev_potrf = s->la_ev[0], ev_top = s->la_ev[1], ev_rest = s->la_ev[2], ev_side = s->la_ev[3],
+                ev_b = s->la_ev[4], ev_end = s->la_ev[5];
+    const int chain = std::min(std::max(s->chain_sms, 1), s->sm_count - 1);
+    const int bulk_sms = std::max(1, s->sm_count - chain);
+    const int per_cta = TRSM_THREADS / 32, units_top = PW / 8;
+    // the side kernels take the chain's SMs but three (the diagonal block,
+    // the two CTAs of the top panel solve)
+    const int side = std::max(1, chain - 3);
     float *hi, *lo;
     double* lkk;
     panel_ptrs(s, 0, &hi, &lo, &lkk);
     phase_mark_on(s, P_POTRF, st);
-    BDB_CUDA(launch_potrf(s, st, s->M32.p, 0, lkk));
+    BDB_CUDA(launch_potrf(s, st, M, 0, lkk));
     phase_mark_on(s, P_POTRF, st);
     s->launches += 1;
-    // the bulk stream starts after everything before the factorisation
-    BDB_CUDA(cudaEventRecord(ev_solved, st));
-    BDB_CUDA(cudaStreamWaitEvent(st2, ev_solved, 0));
+    BDB_CUDA(cudaEventRecord(ev_potrf, st));
+    BDB_CUDA(cudaStreamWaitEvent(st2, ev_potrf, 0));   // the bulk stream starts after what came before
     for (int P = 0; P + 1 < nt; ++P) {
         const int set = P % PANEL_SETS;
         panel_ptrs(s, set, &hi, &lo, &lkk);
         const int rem = nt - P - 1;   // trailing block columns
-        if (P > 0) BDB_CUDA(cudaStreamWaitEvent(st, ev_b, 0));   // B(P-1)
-        const int units = (s->npad - (P + 1) * PW) / 8;
-        const int per_cta = TRSM_THREADS / 32;
+        const int units_rest = (rem - 1) * PW / 8;
+        // side: the panel solve below block row P+1
+        BDB_CUDA(cudaStreamWaitEvent(st3, ev_potrf, 0));
+        if (units_rest > 0) {
+            k_trsm128<T><<<std::min(side, (units_rest + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st3>>>(
+                M, s->npad, P, units_top, units_rest, lkk, hi, lo, s->status.p);
+            BDB_CUDA(cudaGetLastError());
+            s->launches += 1;
+        }
+        BDB_CUDA(cudaEventRecord(ev_rest, st3));
+        // chain: block row P+1 of the panel solve
+        if (P > 0) {
+            BDB_CUDA(cudaStreamWaitEvent(st, ev_side, 0));   // A1(P-1)
+            BDB_CUDA(cudaStreamWaitEvent(st, ev_b, 0));      // B(P-1)
+        }
         phase_mark_on(s, P_TRSM, st);
-        k_trsm128<float><<<std::min(s->sm_count, (units + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st>>>(
-            s->M32.p, s->npad, P, lkk, hi, lo, s->status.p);
+        k_trsm128<T><<<units_top / per_cta, TRSM_THREADS, TRSM_SMEM, st>>>(M, s->npad, P, 0, units_top, lkk, hi, lo,
+                                                                          s->status.p);
         phase_mark_on(s, P_TRSM, st);
         BDB_CUDA(cudaGetLastError());
-        BDB_CUDA(cudaEventRecord(ev_solved, st));
-        // bulk: B(P) and C(P)
-        BDB_CUDA(cudaStreamWaitEvent(st2, ev_solved, 0));
+        BDB_CUDA(cudaEventRecord(ev_top, st));
+        // side: block column P+1 below its diagonal tile
+        BDB_CUDA(cudaStreamWaitEvent(st3, ev_top, 0));
+        if (P > 0) BDB_CUDA(cudaStreamWaitEvent(st3, ev_b, 0));   // B(P-1)
+        if (rem > 1) {
+            BDB_CUDA(update(st3, std::min(rem - 1, side), set, P + 1, rem - 1, 4));
+            s->launches += 1;
+        }
+        BDB_CUDA(cudaEventRecord(ev_side, st3));
+        // bulk: block column P+2, then the rest
+        BDB_CUDA(cudaStreamWaitEvent(st2, ev_top, 0));
+        BDB_CUDA(cudaStreamWaitEvent(st2, ev_rest, 0));
         phase_mark_on(s, P_SYRK_REST, st2);
         if (rem >= 2) {
-            BDB_CUDA(launch_syrk(s, std::min(bulk_sms, rem - 1), st2, maps[2 * set], maps[2 * set + 1], mapc, P + 1,
-                                 rem - 1, 2));
+            BDB_CUDA(update(st2, std::min(bulk_sms, rem - 1), set, P + 1, rem - 1, 2));
             s->launches += 1;
         }
         BDB_CUDA(cudaEventRecord(ev_b, st2));
         if (rem >= 3) {
             const int ntc = (rem - 2) * (rem - 1) / 2;
-            BDB_CUDA(launch_syrk(s, std::min(bulk_sms, ntc), st2, maps[2 * set], maps[2 * set + 1], mapc, P + 1, ntc,
-                                 3));
+            BDB_CUDA(update(st2, std::min(bulk_sms, ntc), set, P + 1, ntc, 3));
             s->launches += 1;
         }
         phase_mark_on(s, P_SYRK_REST, st2);
-        // chain: A(P), then the diagonal block P+1
+        // chain: the diagonal tile of block column P+1, then its factorisation
         phase_mark_on(s, P_SYRK_COL, st);
-        BDB_CUDA(launch_syrk(s, std::min(s->sm_count, rem), st, maps[2 * set], maps[2 * set + 1], mapc, P + 1, rem, 1));
+        BDB_CUDA(update(st, 1, set, P + 1, 1, 1));
         phase_mark_on(s, P_SYRK_COL, st);
-        double *lkk1;
+        double* lkk1;
         float *hi1, *lo1;
         panel_ptrs(s, (P + 1) % PANEL_SETS, &hi1, &lo1, &lkk1);
         phase_mark_on(s, P_POTRF, st);
-        BDB_CUDA(launch_potrf(s, st, s->M32.p, P + 1, lkk1));
+        BDB_CUDA(launch_potrf(s, st, M, P + 1, lkk1));
         phase_mark_on(s, P_POTRF, st);
+        BDB_CUDA(cudaEventRecord(ev_potrf, st));
         s->launches += 3;
     }
-    // join the bulk stream
+    // join the side and bulk streams
+    BDB_CUDA(cudaEventRecord(ev_side, st3));
+    BDB_CUDA(cudaStreamWaitEvent(st, ev_side, 0));
     BDB_CUDA(cudaEventRecord(ev_end, st2));
     BDB_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
     BDB_CUDA(cudaGetLastError());
     return BDB_OK;
+}
+
+int factor_mixed_tc(bdb_system* s)
+{
+    int rc = tc_setup(s);
+    if (rc) return rc;
+    const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(s->tc_map);
+    return factor_schedule(s, s->M32.p, [&](cudaStream_t stream, int grid, int set, int t0, int ntiles, int mode) {
+        return launch_syrk(s, grid, stream, maps[2 * set], maps[2 * set + 1], maps[2 * PANEL_SETS], t0, ntiles, mode);
+    });
 }
 
 // ------------------------------------------------------ FP64 factorisation
@@ -1212,7 +1257,7 @@ static int tc64_setup(bdb_system* s)
     const size_t pan = (size_t)s->npad * PW;
     // one FP64 panel buffer per set (the room of a mixed-path hi/lo pair)
     if (s->panel64.alloc((size_t)PANEL_SETS * pan + (size_t)PANEL_SETS * PANEL_FAC + 64)) return BDB_ERR_NOMEM;
-    BDB_CUDA(cudaMemset(s->panel64.p, 0, s->panel64.n * sizeof(double)));
+    BDB_CUDA(dzero(s, s->panel64.p, s->panel64.n * sizeof(double)));
     BDB_CUDA(cudaFuncSetAttribute(k_potrf128<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_trsm128<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRSM_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_syrk64, cudaFuncAttributeMaxDynamicSharedMemorySize, S64_SMEM));
@@ -1240,68 +1285,18 @@ static cudaError_t launch_syrk64(bdb_system* s, int grid, cudaStream_t st, const
     return cudaLaunchKernelEx(&cfg, k_syrk64, s->M64.p, s->npad, Lp, t0, ntiles, mode, s->status.p);
 }
 
-// The plain FP64 path: the schedule of factor_mixed_tc (two panels of
-// look-ahead, A on the chain stream, B and C on the bulk stream) with FP64
-// panels and FP64 DMMA trailing updates.
+// The plain FP64 path: the same schedule with FP64 panels and FP64 DMMA
+// trailing updates
 int factor_fp64_tc(bdb_system* s)
 {
     int rc = tc64_setup(s);
     if (rc) return rc;
-    const int nt = s->npad / PW;
-    cudaStream_t st = s->stream, st2 = s->stream2;
-    cudaEvent_t ev_solved = s->la_ev[0], ev_b = s->la_ev[1], ev_end = s->la_ev[2];
-    const int bulk_sms = std::max(1, s->sm_count - std::min(std::max(s->chain_sms, 0), s->sm_count - 1));
-    float *hi, *lo;
-    double* lkk;
-    panel_ptrs(s, 0, &hi, &lo, &lkk);
-    phase_mark_on(s, P_POTRF, st);
-    BDB_CUDA(launch_potrf(s, st, s->M64.p, 0, lkk));
-    phase_mark_on(s, P_POTRF, st);
-    s->launches += 1;
-    BDB_CUDA(cudaEventRecord(ev_solved, st));
-    BDB_CUDA(cudaStreamWaitEvent(st2, ev_solved, 0));
-    for (int P = 0; P + 1 < nt; ++P) {
-        const int set = P % PANEL_SETS;
+    return factor_schedule(s, s->M64.p, [&](cudaStream_t stream, int grid, int set, int t0, int ntiles, int mode) {
+        float *hi, *lo;
+        double* lkk;
         panel_ptrs(s, set, &hi, &lo, &lkk);
-        const double* Lp = reinterpret_cast<const double*>(hi);
-        const int rem = nt - P - 1;
-        if (P > 0) BDB_CUDA(cudaStreamWaitEvent(st, ev_b, 0));   // B(P-1)
-        const int units = (s->npad - (P + 1) * PW) / 8;
-        const int per_cta = TRSM_THREADS / 32;
-        phase_mark_on(s, P_TRSM, st);
-        k_trsm128<double><<<std::min(s->sm_count, (units + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st>>>(
-            s->M64.p, s->npad, P, lkk, hi, lo, s->status.p);
-        phase_mark_on(s, P_TRSM, st);
-        BDB_CUDA(cudaGetLastError());
-        BDB_CUDA(cudaEventRecord(ev_solved, st));
-        BDB_CUDA(cudaStreamWaitEvent(st2, ev_solved, 0));
-        phase_mark_on(s, P_SYRK_REST, st2);
-        if (rem >= 2) {
-            BDB_CUDA(launch_syrk64(s, std::min(bulk_sms, rem - 1), st2, Lp, P + 1, rem - 1, 2));
-            s->launches += 1;
-        }
-        BDB_CUDA(cudaEventRecord(ev_b, st2));
-        if (rem >= 3) {
-            const int ntc = (rem - 2) * (rem - 1) / 2;
-            BDB_CUDA(launch_syrk64(s, std::min(bulk_sms, ntc), st2, Lp, P + 1, ntc, 3));
-            s->launches += 1;
-        }
-        phase_mark_on(s, P_SYRK_REST, st2);
-        phase_mark_on(s, P_SYRK_COL, st);
-        BDB_CUDA(launch_syrk64(s, std::min(s->sm_count, rem), st, Lp, P + 1, rem, 1));
-        phase_mark_on(s, P_SYRK_COL, st);
-        double* lkk1;
-        float *hi1, *lo1;
-        panel_ptrs(s, (P + 1) % PANEL_SETS, &hi1, &lo1, &lkk1);
-        phase_mark_on(s, P_POTRF, st);
-        BDB_CUDA(launch_potrf(s, st, s->M64.p, P + 1, lkk1));
-        phase_mark_on(s, P_POTRF, st);
-        s->launches += 3;
-    }
-    BDB_CUDA(cudaEventRecord(ev_end, st2));
-    BDB_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
-    BDB_CUDA(cudaGetLastError());
-    return BDB_OK;
+        return launch_syrk64(s, grid, stream, reinterpret_cast<const double*>(hi), t0, ntiles, mode);
+    });
 }
 
 }  // namespace bdb

@@ -114,17 +114,17 @@ int ensure_matrix(bdb_system* s)
     if (s->p.precision == BDB_PREC_FP64) {
         if (s->M64.p) return BDB_OK;
         if (s->M64.alloc(nn)) return BDB_ERR_NOMEM;
-        BDB_CUDA(cudaMemset(s->M64.p, 0, nn * sizeof(double)));
+        BDB_CUDA(dzero(s, s->M64.p, nn * sizeof(double)));
         std::vector<double> one(1, 1.0);
         for (int r = s->n3; r < s->npad; ++r)
-            BDB_CUDA(cudaMemcpy(s->M64.p + (size_t)r * s->npad + r, one.data(), sizeof(double), cudaMemcpyHostToDevice));
+            BDB_CUDA(h2d(s, s->M64.p + (size_t)r * s->npad + r, one.data(), sizeof(double)));
     } else {
         if (s->M32.p) return BDB_OK;
         if (s->M32.alloc(nn)) return BDB_ERR_NOMEM;
-        BDB_CUDA(cudaMemset(s->M32.p, 0, nn * sizeof(float)));
+        BDB_CUDA(dzero(s, s->M32.p, nn * sizeof(float)));
         float one = 1.0f;
         for (int r = s->n3; r < s->npad; ++r)
-            BDB_CUDA(cudaMemcpy(s->M32.p + (size_t)r * s->npad + r, &one, sizeof(float), cudaMemcpyHostToDevice));
+            BDB_CUDA(h2d(s, s->M32.p + (size_t)r * s->npad + r, &one, sizeof(float)));
     }
     return BDB_OK;
 }
@@ -148,7 +148,7 @@ int build_and_factor(bdb_system* s)
 // the current positions in place.
 static int factor_tune(bdb_system* s)
 {
-    const int cands[4] = {8, 16, 32, 48};
+    const int cands[5] = {16, 24, 32, 48, 64};
     float best_ms = 1e30f;
     int best = s->chain_sms;
     cudaEvent_t e0, e1;
@@ -407,14 +407,22 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
             return BDB_ERR_NOMEM;                \
         }                                        \
     } while (0)
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->la_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->la_ev[1], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->la_ev[2], cudaEventDisableTiming) != cudaSuccess) {
+    // stream priorities: the main stream (which runs the Cholesky's panel
+    // chain) first, then the chain's side work, then its bulk updates, so
+    // that a chain kernel's CTAs are dispatched ahead of queued bulk CTAs
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    if (cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&s->stream2, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&s->stream3, cudaStreamNonBlocking, (prio_low + prio_high) / 2) != cudaSuccess) {
         bdb_destroy(s);
-        return fail(BDB_ERR_CUDA, "stream/event creation failed");
+        return fail(BDB_ERR_CUDA, "stream creation failed");
     }
+    for (auto& e : s->la_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            bdb_destroy(s);
+            return fail(BDB_ERR_CUDA, "event creation failed");
+        }
     {
         int b = 0;
         for (int g = 0; g < nseg; ++g) {
@@ -434,28 +442,28 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     TRYA(s->dD, s->npad);
     TRYA(s->scal, 64 + 4 * (size_t)nseg + 64);
     TRYA(s->ctr, 2);
-    BDB_CUDA(cudaMemcpy(s->d_segs.p, s->segs.data(), sizeof(Segment) * nseg, cudaMemcpyHostToDevice));
+    BDB_CUDA(h2d(s, s->d_segs.p, s->segs.data(), sizeof(Segment) * nseg));
     {
         std::vector<int> bs(s->n);
         for (int g = 0; g < nseg; ++g)
             for (int i = 0; i < counts[g]; ++i) bs[s->segs[g].begin + i] = g;
-        BDB_CUDA(cudaMemcpy(s->d_bead_seg.p, bs.data(), sizeof(int) * s->n, cudaMemcpyHostToDevice));
+        BDB_CUDA(h2d(s, s->d_bead_seg.p, bs.data(), sizeof(int) * s->n));
     }
-    BDB_CUDA(cudaMemcpy(s->pos.p, coord, sizeof(double) * 4 * s->n, cudaMemcpyHostToDevice));
-    BDB_CUDA(cudaMemcpy(s->Q.p, Q, sizeof(double) * s->n, cudaMemcpyHostToDevice));
-    BDB_CUDA(cudaMemcpy(s->LJ.p, LJ, sizeof(double) * 2 * s->n, cudaMemcpyHostToDevice));
-    BDB_CUDA(cudaMemset(s->scal.p, 0, sizeof(double) * s->scal.n));
-    BDB_CUDA(cudaMemset(s->ctr.p, 0, sizeof(unsigned long long) * 2));
-    BDB_CUDA(cudaMemset(s->Rf.p, 0, sizeof(double) * s->n3));
-    BDB_CUDA(cudaMemset(s->Rs.p, 0, sizeof(double) * s->n3));
-    BDB_CUDA(cudaMemset(s->X.p, 0, sizeof(double) * s->n3));
+    BDB_CUDA(h2d(s, s->pos.p, coord, sizeof(double) * 4 * s->n));
+    BDB_CUDA(h2d(s, s->Q.p, Q, sizeof(double) * s->n));
+    BDB_CUDA(h2d(s, s->LJ.p, LJ, sizeof(double) * 2 * s->n));
+    BDB_CUDA(dzero(s, s->scal.p, sizeof(double) * s->scal.n));
+    BDB_CUDA(dzero(s, s->ctr.p, sizeof(unsigned long long) * 2));
+    BDB_CUDA(dzero(s, s->Rf.p, sizeof(double) * s->n3));
+    BDB_CUDA(dzero(s, s->Rs.p, sizeof(double) * s->n3));
+    BDB_CUDA(dzero(s, s->X.p, sizeof(double) * s->n3));
     {
         std::vector<double> dd(s->npad, 1.0);
-        BDB_CUDA(cudaMemcpy(s->dD.p, dd.data(), sizeof(double) * s->npad, cudaMemcpyHostToDevice));
+        BDB_CUDA(h2d(s, s->dD.p, dd.data(), sizeof(double) * s->npad));
     }
     TRY(forces_setup(s));
     TRY(bonded_setup(s));
-    BDB_CUDA(cudaMemset(s->status.p, 0, sizeof(unsigned) * 4));
+    BDB_CUDA(dzero(s, s->status.p, sizeof(unsigned) * 4));
 #undef TRY
 #undef TRYA
     *out = s;
@@ -483,10 +491,12 @@ int bdb_destroy(bdb_system* s)
     for (auto& r : s->phases)
         for (auto e : r.ev) cudaEventDestroy(e);
     if (s->stream2) cudaStreamSynchronize(s->stream2);
+    if (s->stream3) cudaStreamSynchronize(s->stream3);
     for (auto e : s->la_ev)
         if (e) cudaEventDestroy(e);
     drop_graph(s);
     frames_release(s);
+    if (s->stream3) cudaStreamDestroy(s->stream3);
     if (s->stream2) cudaStreamDestroy(s->stream2);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -531,8 +541,8 @@ int bdb_set_bonded(bdb_system* s, int n_bond, const int* bond_pairs, const doubl
         if (t.di->alloc(std::max(1, t.cnt * t.members)) || t.dp->alloc(std::max(1, t.cnt * t.npar)))
             return BDB_ERR_NOMEM;
         if (t.cnt) {
-            BDB_CUDA(cudaMemcpy(t.di->p, t.idx, sizeof(int) * t.cnt * t.members, cudaMemcpyHostToDevice));
-            BDB_CUDA(cudaMemcpy(t.dp->p, t.par, sizeof(double) * t.cnt * t.npar, cudaMemcpyHostToDevice));
+            BDB_CUDA(h2d(s, t.di->p, t.idx, sizeof(int) * t.cnt * t.members));
+            BDB_CUDA(h2d(s, t.dp->p, t.par, sizeof(double) * t.cnt * t.npar));
         }
     }
     s->have_forces = false;
@@ -614,7 +624,7 @@ int bdb_compute_D(bdb_system* s, double* D)
         // compute_D does nothing without hydrodynamics; the tensor is diag_D
         // (diff_tensor.c:477, main_loop.c:161-175)
         std::vector<double4> pos(s->n);
-        BDB_CUDA(cudaMemcpy(pos.data(), s->pos.p, sizeof(double4) * s->n, cudaMemcpyDeviceToHost));
+        BDB_CUDA(d2h(s, pos.data(), s->pos.p, sizeof(double4) * s->n));
         memset(D, 0, sizeof(double) * (size_t)n3 * n3);
         for (int r = 0; r < n3; ++r) D[(size_t)r * n3 + r] = s->preDii / pos[r / 3].w;
         return BDB_OK;
@@ -637,7 +647,7 @@ int bdb_compute_D(bdb_system* s, double* D)
     }
     // the diagonal of D lives in dD (the matrix diagonal is shared with L)
     std::vector<double> dd(n3);
-    BDB_CUDA(cudaMemcpy(dd.data(), s->dD.p, sizeof(double) * n3, cudaMemcpyDeviceToHost));
+    BDB_CUDA(d2h(s, dd.data(), s->dD.p, sizeof(double) * n3));
     for (int r = 0; r < n3; ++r) D[(size_t)r * n3 + r] = dd[r];
     return BDB_OK;
 }
@@ -883,6 +893,7 @@ int bdb_phase_stats(bdb_system* s, const char* phase, double* total_ms, long lon
     if (ph < 0) return fail(BDB_ERR_ARG, "unknown phase");
     BDB_CUDA(cudaStreamSynchronize(s->stream));
     if (s->stream2) BDB_CUDA(cudaStreamSynchronize(s->stream2));
+    if (s->stream3) BDB_CUDA(cudaStreamSynchronize(s->stream3));
     auto& r = s->phases[ph];
     double tot = 0;
     for (size_t k = 0; k + 1 < r.used; k += 2) {

@@ -821,7 +821,7 @@ int bonded_setup(bdb_system* s)
     };
     auto fetch = [&](DevBuf<int>& b, int count) {
         std::vector<int> v(count);
-        if (count) cudaMemcpy(v.data(), b.p, sizeof(int) * count, cudaMemcpyDeviceToHost);
+        if (count) d2h(s, v.data(), b.p, sizeof(int) * count);
         return v;
     };
     add_terms(s->n_bond, 2, fetch(s->bond_pairs, 2 * s->n_bond));
@@ -840,9 +840,9 @@ int bonded_setup(bdb_system* s)
     if (s->slot_list.alloc(std::max<size_t>(1, list.size()))) return BDB_ERR_NOMEM;
     if (s->contrib.alloc(3 * std::max(1, s->n_slots))) return BDB_ERR_NOMEM;
     if (s->term_energy.alloc(std::max(1, s->n_terms))) return BDB_ERR_NOMEM;
-    BDB_CUDA(cudaMemcpy(s->slot_ptr.p, ptr.data(), sizeof(int) * (s->n + 1), cudaMemcpyHostToDevice));
+    BDB_CUDA(h2d(s, s->slot_ptr.p, ptr.data(), sizeof(int) * (s->n + 1)));
     if (!list.empty())
-        BDB_CUDA(cudaMemcpy(s->slot_list.p, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice));
+        BDB_CUDA(h2d(s, s->slot_list.p, list.data(), sizeof(int) * list.size()));
 
     // are_conn (bond.c:87-92, alloc_connections :113-130): live only when a
     // 1-2 scale factor differs from 1
@@ -862,9 +862,9 @@ int bonded_setup(bdb_system* s)
     }
     if (s->conn_ptr.alloc(s->n + 1)) return BDB_ERR_NOMEM;
     if (s->conn_list.alloc(std::max<size_t>(1, clist.size()))) return BDB_ERR_NOMEM;
-    BDB_CUDA(cudaMemcpy(s->conn_ptr.p, cptr.data(), sizeof(int) * (s->n + 1), cudaMemcpyHostToDevice));
+    BDB_CUDA(h2d(s, s->conn_ptr.p, cptr.data(), sizeof(int) * (s->n + 1)));
     if (!clist.empty())
-        BDB_CUDA(cudaMemcpy(s->conn_list.p, clist.data(), sizeof(int) * clist.size(), cudaMemcpyHostToDevice));
+        BDB_CUDA(h2d(s, s->conn_list.p, clist.data(), sizeof(int) * clist.size()));
     return BDB_OK;
 }
 
@@ -876,7 +876,7 @@ int forces_setup(bdb_system* s)
     if (s->grid.alloc(nseg)) return BDB_ERR_NOMEM;
     if (s->grid_dims.alloc(nseg)) return BDB_ERR_NOMEM;
     if (s->pos_build.alloc(s->n) || s->cells_built.alloc(nseg)) return BDB_ERR_NOMEM;
-    BDB_CUDA(cudaMemset(s->cells_built.p, 0, sizeof(int) * nseg));
+    BDB_CUDA(dzero(s, s->cells_built.p, sizeof(int) * nseg));
     // dense cell tables: 32 cells per bead (at least 4096) per segment
     std::vector<long long> off(2 * nseg);
     long long tot = 0;
@@ -887,7 +887,7 @@ int forces_setup(bdb_system* s)
         tot += cap;
     }
     if (s->cell_range.alloc(tot) || s->cell_off.alloc(2 * nseg)) return BDB_ERR_NOMEM;
-    BDB_CUDA(cudaMemcpy(s->cell_off.p, off.data(), sizeof(long long) * 2 * nseg, cudaMemcpyHostToDevice));
+    BDB_CUDA(h2d(s, s->cell_off.p, off.data(), sizeof(long long) * 2 * nseg));
     if (s->e_part.alloc(2 * s->n + 16)) return BDB_ERR_NOMEM;
     if (s->status.alloc(4)) return BDB_ERR_NOMEM;
     if (s->counts.alloc(2)) return BDB_ERR_NOMEM;
@@ -897,7 +897,7 @@ int forces_setup(bdb_system* s)
     // cell size: the widest interaction range of force_single plus the
     // LJ_force_check distance (init_cutoff, pre_func.c:197-232)
     std::vector<double2> lj(s->n);
-    BDB_CUDA(cudaMemcpy(lj.data(), s->LJ.p, sizeof(double2) * s->n, cudaMemcpyDeviceToHost));
+    BDB_CUDA(d2h(s, lj.data(), s->LJ.p, sizeof(double2) * s->n));
     double maxsig = 0;
     for (int i = 0; i < s->n; ++i) maxsig = std::max(maxsig, lj[i].x);
     double c = 2 * maxsig;

@@ -89,17 +89,17 @@ static int ensure_matrix_b(bdb_system* s)
     if (s->p.precision == BDB_PREC_FP64) {
         if (s->M64b.p) return BDB_OK;
         if (s->M64b.alloc(nn)) return BDB_ERR_NOMEM;
-        BDB_CUDA(cudaMemset(s->M64b.p, 0, nn * sizeof(double)));
+        BDB_CUDA(dzero(s, s->M64b.p, nn * sizeof(double)));
         const double one = 1.0;
         for (int r = s->n3; r < s->npad; ++r)
-            BDB_CUDA(cudaMemcpy(s->M64b.p + (size_t)r * s->npad + r, &one, sizeof(double), cudaMemcpyHostToDevice));
+            BDB_CUDA(h2d(s, s->M64b.p + (size_t)r * s->npad + r, &one, sizeof(double)));
     } else {
         if (s->M32b.p) return BDB_OK;
         if (s->M32b.alloc(nn)) return BDB_ERR_NOMEM;
-        BDB_CUDA(cudaMemset(s->M32b.p, 0, nn * sizeof(float)));
+        BDB_CUDA(dzero(s, s->M32b.p, nn * sizeof(float)));
         const float one = 1.0f;
         for (int r = s->n3; r < s->npad; ++r)
-            BDB_CUDA(cudaMemcpy(s->M32b.p + (size_t)r * s->npad + r, &one, sizeof(float), cudaMemcpyHostToDevice));
+            BDB_CUDA(h2d(s, s->M32b.p + (size_t)r * s->npad + r, &one, sizeof(float)));
     }
     return BDB_OK;
 }

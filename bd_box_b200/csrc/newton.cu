@@ -218,7 +218,7 @@ extern "C" int bdb_newton_resolve(bdb_system* s, double e_collision, const doubl
         np = std::min(np, n);
         hp.resize(np);
         if (np) {
-            BDB_CUDA(cudaMemcpy(hp.data(), s->nw_pairs.p, sizeof(int2) * np, cudaMemcpyDeviceToHost));
+            BDB_CUDA(d2h(s, hp.data(), s->nw_pairs.p, sizeof(int2) * np));
             std::sort(hp.begin(), hp.end(), [](const int2& a, const int2& b) {
                 return a.x != b.x ? a.x < b.x : a.y < b.y;
             });

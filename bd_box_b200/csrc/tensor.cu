@@ -99,8 +99,8 @@ static int ewald_tables(bdb_system* s)
     s->ewald_nimg = (int)(img.size() / 4);
     if (s->ewald_tab.alloc(rk.size() + img.size())) return BDB_ERR_NOMEM;
     if (!rk.empty())
-        BDB_CUDA(cudaMemcpy(s->ewald_tab.p, rk.data(), sizeof(double) * rk.size(), cudaMemcpyHostToDevice));
-    BDB_CUDA(cudaMemcpy(s->ewald_tab.p + rk.size(), img.data(), sizeof(double) * img.size(), cudaMemcpyHostToDevice));
+        BDB_CUDA(h2d(s, s->ewald_tab.p, rk.data(), sizeof(double) * rk.size()));
+    BDB_CUDA(h2d(s, s->ewald_tab.p + rk.size(), img.data(), sizeof(double) * img.size()));
     return BDB_OK;
 }
 
@@ -563,10 +563,9 @@ int tea_setup(bdb_system* s)
     if (s->part.alloc(std::max<size_t>(9, 9 * part_records))) return BDB_ERR_NOMEM;
     const size_t head = sizeof(TeaSeg) * ts.size() + sizeof(int) * job_begin.size();
     if (s->tea_meta.alloc(head)) return BDB_ERR_NOMEM;
-    BDB_CUDA(cudaMemcpy(s->jobs.p, jobs.data(), sizeof(TileJob) * jobs.size(), cudaMemcpyHostToDevice));
-    BDB_CUDA(cudaMemcpy(s->tea_meta.p, ts.data(), sizeof(TeaSeg) * ts.size(), cudaMemcpyHostToDevice));
-    BDB_CUDA(cudaMemcpy(s->tea_meta.p + sizeof(TeaSeg) * ts.size(), job_begin.data(),
-                        sizeof(int) * job_begin.size(), cudaMemcpyHostToDevice));
+    BDB_CUDA(h2d(s, s->jobs.p, jobs.data(), sizeof(TileJob) * jobs.size()));
+    BDB_CUDA(h2d(s, s->tea_meta.p, ts.data(), sizeof(TeaSeg) * ts.size()));
+    BDB_CUDA(h2d(s, s->tea_meta.p + sizeof(TeaSeg) * ts.size(), job_begin.data(), sizeof(int) * job_begin.size()));
     return BDB_OK;
 }
 
