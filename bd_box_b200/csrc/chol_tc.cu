@@ -143,10 +143,13 @@ __device__ __forceinline__ void tri_index(int idx, int& ti, int& tj)
 // tile t of a launch -> (ti, tj) relative to the first trailing block:
 // mode 0 all tiles of the lower triangle, 1 only block column 0, 2 only
 // block column 1, 3 block columns 2 and beyond, 4 block column 0 below its
-// diagonal tile
+// diagonal tile, 5 only block column 2
 __device__ __forceinline__ void tile_of_mode(int t, int mode, int& ti, int& tj)
 {
-    if (mode == 4) {
+    if (mode == 5) {
+        ti = t + 2;
+        tj = 2;
+    } else if (mode == 4) {
         ti = t + 1;
         tj = 0;
     } else if (mode == 1 || mode == 2) {
@@ -905,6 +908,331 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
     }
 }
 
+// ------------------------------------------- 2-SM tensor-core bulk update
+//
+// Block columns 2 and beyond of the trailing update (mode 3, most of the
+// factorisation's work) on CTA pairs: a cluster of two CTAs computes a
+// 256x256 block (2x2 tiles) of -L_i L_j^T with tcgen05.mma.cta_group::2,
+// M = N = 256. CTA r of the pair stages the 128 rows of tile row 2I+r (its
+// half of A) and of tile column 2J+r (its half of B) in the same ring as the
+// 1-SM kernel, so each SM pulls the same 64 KB per K chunk from L2 for twice
+// the MMA work: the operand feed that bounds the 1-SM kernel is halved.
+// CTA r's tensor memory holds its 128 rows x 256 columns of the block, two
+// buffers (all 512 columns). Protocol: the leader (rank 0) owns the full
+// barriers (it expects both CTAs' bytes; each CTA's loads complete on the
+// leader's barrier) and the accumulator-empty barriers (both CTAs' epilogue
+// warps arrive there); its single MMA thread commits stage release and
+// accumulator-full to both CTAs at once. Every wait is bounded; a time-out in
+// either CTA stops both. With npan = 2 the block takes the updates of two
+// panels at once (K = 256: the second panel's maps continue the K loop), so
+// C is read and written once for both.
+__host__ __device__ constexpr uint32_t idesc_tf32_256x256()
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32_pair(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                               uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// arrive once on the barrier at offset `bar` of both CTAs of the pair when
+// this thread's MMAs so far have completed
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar)
+{
+    asm volatile(
+        "{\n\t.reg .b16 m;\n\tmov.b16 m, 3;\n\t"
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], m;\n\t}" ::"r"(
+            bar)
+        : "memory");
+}
+
+// shared::cluster address of `addr` (a shared::cta address of this CTA) in
+// CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t addr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// 2-D load into this CTA's shared memory whose completion is counted on the
+// pair leader's barrier (cluster address `bar`); no multicast
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+struct PairBars {
+    uint64_t full[STAGES], empty[STAGES], accfull[2], accempty[2], drain;
+};
+
+// block t of the lower triangle of 256-wide blocks over the trailing tile
+// columns c0 .. cols-1 -> tile row and column of its top-left tile
+__device__ __forceinline__ void pair_block(int t, int c0, int& ti, int& tj)
+{
+    int bi, bj;
+    tri_index(t, bi, bj);
+    ti = c0 + 2 * bi;
+    tj = c0 + 2 * bj;
+}
+
+__global__ void __launch_bounds__(192, 1)
+k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+           const __grid_constant__ CUtensorMap map_hi2, const __grid_constant__ CUtensorMap map_lo2,
+           const __grid_constant__ CUtensorMap map_c, int t0, int c0, int cols, int npan, unsigned* __restrict__ status,
+           uint32_t wlim)
+{
+    {
+        uint32_t dyn, ncta;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
+        if (blockDim.x != 192 || dyn < (uint32_t)SYRK_SMEM || ncta != 2 || npan < 1 || npan > 2) {
+            if (threadIdx.x == 0) atomicOr(status, ST_LAUNCH);
+            return;
+        }
+    }
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ PairBars bars;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ volatile int abort_flag;
+    uint32_t rank, cid, ncl;
+    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    asm("mov.u32 %0, %%clusterid.x;" : "=r"(cid));
+    asm("mov.u32 %0, %%nclusterid.x;" : "=r"(ncl));
+    const bool leader = rank == 0;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_u32(sm);
+    unsigned char* cbuf = sm + STAGES * STAGE_BYTES;
+    const uint32_t cbase = sbase + STAGES * STAGE_BYTES;
+    // the other CTA's abort flag: a time-out here stops the pair
+    const uint32_t peer_abort = cluster_addr(smem_u32((const void*)&abort_flag), rank ^ 1u);
+    auto stop_pair = [&]() {
+        abort_flag = 1;
+        asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(peer_abort), "r"(1) : "memory");
+    };
+    if (tid == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&bars.full[s]), 1);
+            mbar_init(smem_u32(&bars.empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&bars.accfull[b]), 1);
+            mbar_init(smem_u32(&bars.accempty[b]), 8);   // 4 epilogue warps x 2 CTAs
+        }
+        mbar_init(smem_u32(&bars.drain), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    // both CTAs' barriers are initialised (and their flags cleared) before
+    // either signals the other's
+    cluster_sync_all();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
+
+    const int nb = (cols - c0 + 1) / 2;   // 256-wide block columns
+    const int nblocks = nb * (nb + 1) / 2;
+    const int nchunk = NCHUNK * npan;     // K chunks of a block
+    if (warp == 0) {
+        if (lane == 0) {
+            // TMA producer: this CTA's half of A (tile row ti + rank) and of B
+            // (tile column tj + rank); rows past the matrix read as zeros
+            uint32_t g = 0;
+            const uint32_t full0 = cluster_addr(smem_u32(&bars.full[0]), 0);
+            for (int t = cid; t < nblocks && !abort_flag; t += ncl) {
+                int ti, tj;
+                pair_block(t, c0, ti, tj);
+                const int ra = (t0 + ti + (int)rank) * PW, rb = (t0 + tj + (int)rank) * PW;
+                bool ok = true;
+                for (int kc = 0; kc < nchunk; ++kc, ++g) {
+                    const int s = g % STAGES;
+                    if (!mbar_wait(smem_u32(&bars.empty[s]), ((g / STAGES) & 1) ^ 1, &abort_flag, wlim)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t st = sbase + s * STAGE_BYTES;
+                    const uint32_t fb = full0 + s * sizeof(uint64_t);
+                    const CUtensorMap* mh = kc < NCHUNK ? &map_hi : &map_hi2;
+                    const CUtensorMap* ml = kc < NCHUNK ? &map_lo : &map_lo2;
+                    const int x = (kc % NCHUNK) * KC;
+                    if (leader) mbar_expect_tx(smem_u32(&bars.full[s]), 2 * STAGE_BYTES);
+                    tma_load_2d_pair(st, mh, x, ra, fb);
+                    tma_load_2d_pair(st + BOX_BYTES, ml, x, ra, fb);
+                    tma_load_2d_pair(st + 2 * BOX_BYTES, mh, x, rb, fb);
+                    tma_load_2d_pair(st + 3 * BOX_BYTES, ml, x, rb, fb);
+                }
+                if (!ok) {
+                    stop_pair();
+                    break;
+                }
+            }
+            if (abort_flag && leader) {
+                // the loads still in flight (the last fill of each stage, both
+                // CTAs' bytes) land before the pair exits
+                volatile int never = 0;
+                for (uint32_t j = g > (uint32_t)STAGES ? g - STAGES : 0; j < g; ++j)
+                    mbar_wait(smem_u32(&bars.full[j % STAGES]), (j / STAGES) & 1, &never);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // the pair's MMA issuer
+            const uint32_t idesc = idesc_tf32_256x256();
+            uint32_t g = 0, tl = 0;
+            for (int t = cid; t < nblocks && !abort_flag; t += ncl, ++tl) {
+                const uint32_t b = tl & 1;
+                if (!mbar_wait(smem_u32(&bars.accempty[b]), ((tl >> 1) & 1) ^ 1, &abort_flag, wlim)) {
+                    stop_pair();
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc = tmem + b * 256;
+                bool ok = true;
+                for (int kc = 0; kc < nchunk; ++kc, ++g) {
+                    const int s = g % STAGES;
+                    if (!mbar_wait(smem_u32(&bars.full[s]), (g / STAGES) & 1, &abort_flag, wlim)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t ah = sbase + s * STAGE_BYTES, al = ah + BOX_BYTES;
+                    const uint32_t bh = ah + 2 * BOX_BYTES, bl = ah + 3 * BOX_BYTES;
+#pragma unroll
+                    for (int ks = 0; ks < KC / 8; ++ks) {
+                        const uint32_t off = ks * 32;
+                        umma_tf32_pair(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc,
+                                       (kc | ks) ? 1u : 0u);
+                        umma_tf32_pair(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
+                        umma_tf32_pair(acc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
+                    }
+                    umma_commit_pair(smem_u32(&bars.empty[s]));
+                }
+                if (!ok) {
+                    stop_pair();
+                    break;
+                }
+                umma_commit_pair(smem_u32(&bars.accfull[b]));
+            }
+            if (abort_flag) {
+                volatile int never = 0;
+                asm volatile(
+                    "{\n\t.reg .b16 m;\n\tmov.b16 m, 1;\n\t"
+                    "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], "
+                    "m;\n\t}" ::"r"(smem_u32(&bars.drain))
+                    : "memory");
+                mbar_wait(smem_u32(&bars.drain), 0, &never);
+            }
+        }
+    } else {
+        // epilogue warps 2..5: this CTA's 128 rows (tile row ti + rank) of
+        // the block, its two 128-column tiles in turn; tiles above the
+        // diagonal or past the matrix are read from tensor memory (so that
+        // the buffer's release is counted alike) but not written
+        const int quarter = warp & 3;
+        const int rl = 32 * quarter + lane;
+        const uint32_t accempty0 = cluster_addr(smem_u32(&bars.accempty[0]), 0);
+        uint32_t tl = 0;
+        for (int t = cid; t < nblocks; t += ncl, ++tl) {
+            int ti, tj;
+            pair_block(t, c0, ti, tj);
+            ti += (int)rank;
+            const uint32_t b = tl & 1;
+            if (epi_any(!mbar_wait(smem_u32(&bars.accfull[b]), (tl >> 1) & 1, &abort_flag, wlim))) {
+                if (tid == 64) stop_pair();
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {
+                const int tjh = tj + h;
+                const bool live = ti < cols && tjh <= ti;
+                const bool diag = ti == tjh;
+                const int ra = (t0 + ti) * PW, rb = (t0 + tjh) * PW;
+#pragma unroll 1
+                for (int cc = 0; cc < PW / 32; ++cc) {
+                    uint32_t v[32];
+                    const uint32_t taddr =
+                        tmem + b * 256 + h * 128 + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(32 * cc);
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                        "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+                        "%30, %31}, [%32];"
+                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                          "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                          "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                        : "r"(taddr));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    if (h == 1 && cc == PW / 32 - 1) {
+                        // the buffer is free once both CTAs have read it all
+                        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0)
+                            asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(
+                                             accempty0 + b * (uint32_t)sizeof(uint64_t))
+                                         : "memory");
+                    }
+                    if (!live) continue;
+                    if (tid == 64) bulk_wait_read_ring();
+                    epi_sync();
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int c = 32 * cc + 4 * j;
+                        float4 d;
+                        d.x = (!diag || c <= rl) ? -__uint_as_float(v[4 * j]) : -0.0f;
+                        d.y = (!diag || c + 1 <= rl) ? -__uint_as_float(v[4 * j + 1]) : -0.0f;
+                        d.z = (!diag || c + 2 <= rl) ? -__uint_as_float(v[4 * j + 2]) : -0.0f;
+                        d.w = (!diag || c + 3 <= rl) ? -__uint_as_float(v[4 * j + 3]) : -0.0f;
+                        *c_chunk(cbuf, cc % C_BOXES, rl, j) = d;
+                    }
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    epi_sync();
+                    if (tid == 64) {
+                        tma_reduce_add_2d(&map_c, cbase + (cc % C_BOXES) * BOX_BYTES, rb + cc * KC, ra);
+                        bulk_commit();
+                    }
+                }
+            }
+        }
+        if (tid == 64) bulk_wait0();
+    }
+    if (abort_flag && tid == 0) atomicOr(status, ST_TIMEOUT);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    // neither CTA frees its tensor memory or exits while the other may still
+    // signal its barriers or (the leader's MMAs) write its tensor memory
+    cluster_sync_all();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+    }
+}
+
 // ------------------------------------------------- FP64 trailing update
 //
 // The plain FP64 path's C -= L_i L_j^T on the FP64 tensor instruction
@@ -1051,7 +1379,7 @@ static int make_panel_map(float* buf, int rows, CUtensorMap* map, int cols = PW)
 // [npad][128] each), then three FP64 128x128 hand-offs of L_PP / W_kk; panel
 // P uses set P mod 3, so a panel's update may still read its set while the
 // next two panels are solved
-static constexpr int PANEL_SETS = 3;
+static constexpr int PANEL_SETS = 4;
 
 static void panel_ptrs(bdb_system* s, int set, float** hi, float** lo, double** lkk)
 {
@@ -1070,7 +1398,7 @@ static int tc_setup(bdb_system* s)
     if (s->panel64.alloc((size_t)PANEL_SETS * pan + (size_t)PANEL_SETS * PANEL_FAC + 64)) return BDB_ERR_NOMEM;
     BDB_CUDA(dzero(s, s->panel64.p, s->panel64.n * sizeof(double)));
     static_assert(sizeof(CUtensorMap) * (2 * PANEL_SETS + 1) <= sizeof(bdb_system::tc_map), "tensor-map storage");
-    CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(s->tc_map);   // hi0, lo0, hi1, lo1, hi2, lo2, M
+    CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(s->tc_map);   // hi0, lo0, ..., hi3, lo3, M
     for (int set = 0; set < PANEL_SETS; ++set) {
         float *hi, *lo;
         double* lkk;
@@ -1083,6 +1411,7 @@ static int tc_setup(bdb_system* s)
     int rc = make_panel_map(s->M32.p, s->npad, &maps[2 * PANEL_SETS], s->npad);
     if (rc) return rc;
     BDB_CUDA(cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
+    BDB_CUDA(cudaFuncSetAttribute(k_syrk_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_potrf128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_trsm128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRSM_SMEM));
     int dev = 0, sms = 148;
@@ -1109,6 +1438,32 @@ static cudaError_t launch_syrk(bdb_system* s, int grid, cudaStream_t st, const C
     cfg.attrs = at;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, k_syrk_tc, hi, lo, c, t0, ntiles, mode, s->status.p, (uint32_t)s->wait_limit);
+}
+
+// k_syrk_tc2 on `clusters` CTA pairs over block columns c0 .. cols-1 of
+// the trailing matrix at block t0 with the updates of npan panels (the
+// first in hi / lo, the second in hi2 / lo2), behind the previous kernel on
+// the stream like launch_syrk
+static cudaError_t launch_syrk_pair(bdb_system* s, int clusters, cudaStream_t st, const CUtensorMap& hi,
+                                    const CUtensorMap& lo, const CUtensorMap& hi2, const CUtensorMap& lo2,
+                                    const CUtensorMap& c, int t0, int c0, int cols, int npan)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * clusters);
+    cfg.blockDim = dim3(192);
+    cfg.dynamicSmemBytes = SYRK_SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    at[1].id = cudaLaunchAttributeClusterDimension;
+    at[1].val.clusterDim.x = 2;
+    at[1].val.clusterDim.y = 1;
+    at[1].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    return cudaLaunchKernelEx(&cfg, k_syrk_tc2, hi, lo, hi2, lo2, c, t0, c0, cols, npan, s->status.p,
+                              (uint32_t)s->wait_limit);
 }
 
 // k_potrf128 the same way, behind the update of its block column
@@ -1143,9 +1498,13 @@ static cudaError_t launch_potrf(bdb_system* s, cudaStream_t st, T* M, int P, dou
 //   (both update block column P or P+1 before panel P's updates do);
 //   A1(P) after top(P) (its B operand rows) and B(P-1); B(P) once the whole
 //   panel is solved.
-// Every tile still receives its updates in panel order (the same sums, so
-// the same bits, as with no look-ahead). Three panel-buffer sets let C(P)
-// read panel P while panels P+1 and P+2 are solved. The persistent bulk
+// The mixed path (T = float) pairs the panels for C: an even panel P
+// updates block column P+3 alone, and the odd panel P+1 applies both
+// panels' updates to block columns P+4 on in one K = 256 pass on CTA pairs,
+// which halves the reads and writes of C, the bulk's largest cost. Every tile
+// receives the same updates in the same order whatever the GPU split (the
+// same bits for every chain_sms). Four panel-buffer sets let C(P) read
+// panels P-1 and P while panels P+1 and P+2 are solved. The persistent bulk
 // updates leave s->chain_sms SMs to the chain and side kernels (tuned).
 template <typename T, typename Update>
 static int factor_schedule(bdb_system* s, T* M, Update update)
@@ -1160,6 +1519,7 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
     // the side kernels take the chain's SMs but three (the diagonal block,
     // the two CTAs of the top panel solve)
     const int side = std::max(1, chain - 3);
+    constexpr bool kPairs = sizeof(T) == 4;   // two panels per pass over C (mixed path)
     float *hi, *lo;
     double* lkk;
     panel_ptrs(s, 0, &hi, &lo, &lkk);
@@ -1198,7 +1558,7 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
         BDB_CUDA(cudaStreamWaitEvent(st3, ev_top, 0));
         if (P > 0) BDB_CUDA(cudaStreamWaitEvent(st3, ev_b, 0));   // B(P-1)
         if (rem > 1) {
-            BDB_CUDA(update(st3, std::min(rem - 1, side), set, P + 1, rem - 1, 4));
+            BDB_CUDA(update(st3, std::min(rem - 1, side), set, -1, P + 1, rem - 1, 4));
             s->launches += 1;
         }
         BDB_CUDA(cudaEventRecord(ev_side, st3));
@@ -1207,19 +1567,28 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
         BDB_CUDA(cudaStreamWaitEvent(st2, ev_rest, 0));
         phase_mark_on(s, P_SYRK_REST, st2);
         if (rem >= 2) {
-            BDB_CUDA(update(st2, std::min(bulk_sms, rem - 1), set, P + 1, rem - 1, 2));
+            BDB_CUDA(update(st2, std::min(bulk_sms, rem - 1), set, -1, P + 1, rem - 1, 2));
             s->launches += 1;
         }
         BDB_CUDA(cudaEventRecord(ev_b, st2));
         if (rem >= 3) {
-            const int ntc = (rem - 2) * (rem - 1) / 2;
-            BDB_CUDA(update(st2, std::min(bulk_sms, ntc), set, P + 1, ntc, 3));
+            if (kPairs && P % 2 == 0) {
+                // block column P+3 alone; the columns beyond take this
+                // panel's update together with panel P+1's
+                BDB_CUDA(update(st2, std::min(bulk_sms, rem - 2), set, -1, P + 1, rem - 2, 5));
+            } else {
+                // block columns P+3 on: panel P, and on the mixed path panel
+                // P-1 (deferred there) in the same pass
+                const int ntc = (rem - 2) * (rem - 1) / 2;
+                const int set_prev = kPairs ? (P - 1) % PANEL_SETS : -1;
+                BDB_CUDA(update(st2, std::min(bulk_sms, ntc), set, set_prev, P + 1, ntc, 3));
+            }
             s->launches += 1;
         }
         phase_mark_on(s, P_SYRK_REST, st2);
         // chain: the diagonal tile of block column P+1, then its factorisation
         phase_mark_on(s, P_SYRK_COL, st);
-        BDB_CUDA(update(st, 1, set, P + 1, 1, 1));
+        BDB_CUDA(update(st, 1, set, -1, P + 1, 1, 1));
         phase_mark_on(s, P_SYRK_COL, st);
         double* lkk1;
         float *hi1, *lo1;
@@ -1244,7 +1613,18 @@ int factor_mixed_tc(bdb_system* s)
     int rc = tc_setup(s);
     if (rc) return rc;
     const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(s->tc_map);
-    return factor_schedule(s, s->M32.p, [&](cudaStream_t stream, int grid, int set, int t0, int ntiles, int mode) {
+    const int nt = s->npad / PW;
+    return factor_schedule(s, s->M32.p, [&](cudaStream_t stream, int grid, int set, int set_prev, int t0, int ntiles,
+                                            int mode) {
+        if (mode == 3) {
+            // block columns 2.. of the trailing matrix: 256-wide blocks on
+            // CTA pairs, with the previous panel's update too if it is given
+            const int cols = nt - t0, nb = (cols - 1) / 2;
+            const int clusters = std::max(1, std::min(grid / 2, nb * (nb + 1) / 2));
+            const int first = set_prev >= 0 ? set_prev : set;
+            return launch_syrk_pair(s, clusters, stream, maps[2 * first], maps[2 * first + 1], maps[2 * set],
+                                    maps[2 * set + 1], maps[2 * PANEL_SETS], t0, 2, cols, set_prev >= 0 ? 2 : 1);
+        }
         return launch_syrk(s, grid, stream, maps[2 * set], maps[2 * set + 1], maps[2 * PANEL_SETS], t0, ntiles, mode);
     });
 }
@@ -1291,7 +1671,8 @@ int factor_fp64_tc(bdb_system* s)
 {
     int rc = tc64_setup(s);
     if (rc) return rc;
-    return factor_schedule(s, s->M64.p, [&](cudaStream_t stream, int grid, int set, int t0, int ntiles, int mode) {
+    return factor_schedule(s, s->M64.p, [&](cudaStream_t stream, int grid, int set, int, int t0, int ntiles,
+                                            int mode) {
         float *hi, *lo;
         double* lkk;
         panel_ptrs(s, set, &hi, &lo, &lkk);
