@@ -110,6 +110,9 @@ struct bdb_system {
     bdb::DevBuf<int2> cell_range;              // dense per-segment table: [first, end) of each cell
     bdb::DevBuf<long long> cell_off;           // per segment: offset of its table, capacity
     bdb::DevBuf<int> cells_built;              // per segment: 1 once sorted
+    bdb::DevBuf<int> cells_resort;             // per segment above the shared-memory sort: re-sort now
+    bdb::DevBuf<unsigned long long> big_keys;  // two key buffers of the multi-CTA sort (forces.cu)
+    size_t big_npow = 0;                       // their length each: the largest such segment, to a power of 2
     double cell_size = 0;
     double skin = 0;
 

@@ -73,11 +73,26 @@ static ForceParams make_fp(const bdb_system* s)
 
 // ---------------------------------------------------------------- cell list
 
+// cell index along one axis. A periodic grid wraps, so that a coordinate
+// outside the box (set by a caller; steps wrap positions) lies in its image's
+// cell, which the neighbour search's minimum-image distances expect; a
+// free-space grid clamps to its table. The wrap is taken in double, so a
+// far-flung or non-finite coordinate cannot overflow the conversion (NaN
+// converts to 0).
+__device__ __forceinline__ int cell_axis(double x, double o, double w, int n, bool periodic)
+{
+    double t = floor((x - o) / w);
+    if (periodic) t -= n * floor(t / n);
+    const int ci = (int)t;
+    return ci < 0 ? 0 : (ci >= n ? n - 1 : ci);
+}
+
 __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restrict__ segs,
                         double cell, double skin, int periodic, double3 box,
                         unsigned long long* __restrict__ keys_out, int* __restrict__ idx_out,
                         double4* __restrict__ grid, int4* __restrict__ dims, double4* __restrict__ pos_build,
-                        int* __restrict__ built, int2* __restrict__ cell_range, const long long* __restrict__ cell_off)
+                        int* __restrict__ built, int2* __restrict__ cell_range, const long long* __restrict__ cell_off,
+                        int* __restrict__ resort)
 {
     extern __shared__ unsigned long long sk[];
     __shared__ double red[6][32];
@@ -86,6 +101,8 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
     __shared__ int moved;
     const Segment sg = segs[blockIdx.x];
     const int tid = threadIdx.x, nt = blockDim.x;
+    const bool big = sg.count > SORT_MAX;   // sorted by the multi-CTA kernels below
+    if (big && tid == 0) resort[blockIdx.x] = 0;
     if (built[blockIdx.x]) {
         // re-sort only when a bead has moved more than skin/2 since the last sort
         if (tid == 0) moved = 0;
@@ -105,10 +122,6 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
         if (far) moved = 1;
         __syncthreads();
         if (!moved) return;
-    }
-    if (sg.count > SORT_MAX) {
-        if (tid == 0) dims[blockIdx.x] = make_int4(0, 0, 0, 1);   // brute force
-        return;
     }
     if (!periodic) {
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -186,6 +199,11 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
     const double4 gr = grid[blockIdx.x];
     const int4 gd = dims[blockIdx.x];
     if (gd.w) return;
+    if (big) {
+        // the grid is set; k_big_keys .. k_big_fill sort and tabulate
+        if (tid == 0) resort[blockIdx.x] = 1;
+        return;
+    }
     // keys
     int npow = 1;
     while (npow < sg.count) npow <<= 1;
@@ -195,12 +213,8 @@ __global__ void k_cells(const double4* __restrict__ pos, const Segment* __restri
             double4 p = pos[sg.begin + i];
             double x[3] = {p.x, p.y, p.z};
             int c[3];
-            for (int k = 0; k < 3; ++k) {
-                double w = periodic ? (&gr.x)[k] : gr.w;
-                int ci = (int)floor((x[k] - g_origin[k]) / w);
-                ci = ci < 0 ? 0 : (ci >= g_n[k] ? g_n[k] - 1 : ci);   // NaN coordinates stay in the table
-                c[k] = ci;
-            }
+            for (int k = 0; k < 3; ++k)
+                c[k] = cell_axis(x[k], g_origin[k], periodic ? (&gr.x)[k] : gr.w, g_n[k], periodic);
             unsigned long long cl = ((unsigned long long)c[2] * g_n[1] + c[1]) * g_n[0] + c[0];
             key = (cl << 24) | (unsigned long long)i;
         }
@@ -248,6 +262,127 @@ __device__ __forceinline__ int lower_bound_key(const unsigned long long* keys, i
         if (keys[mid] < key) lo = mid + 1; else hi = mid;
     }
     return lo;
+}
+
+// --------------------------------------- cell list of a large segment
+//
+// A segment of more than SORT_MAX beads is sorted by several CTAs: the keys
+// (cell << 24 | bead, the shared-memory path's keys, all distinct, so every
+// correct sort gives the same order and the forces the same bits) are
+// bitonic-sorted in chunks of SORT_MAX in shared memory, the chunks merged
+// pairwise in global memory (each key's place found by a binary search in
+// the other run), and the dense cell table rebuilt from the sorted keys.
+// Each kernel does nothing unless k_cells flagged the segment for a re-sort
+// (a bead moved more than skin/2, or the first build). npow is the
+// segment's bead count rounded up to a power of two (at least SORT_MAX);
+// the keys past the segment are ~0.
+
+// cell of a position in the segment's grid, as k_cells computes it
+__device__ __forceinline__ unsigned long long cell_of(const double4 p, const double4 gr, const int4 gd, int periodic,
+                                                      double3 box)
+{
+    const double x[3] = {p.x, p.y, p.z};
+    const double org[3] = {periodic ? -0.5 * box.x : gr.x, periodic ? -0.5 * box.y : gr.y,
+                           periodic ? -0.5 * box.z : gr.z};
+    const int n[3] = {gd.x, gd.y, gd.z};
+    int c[3];
+    for (int k = 0; k < 3; ++k) c[k] = cell_axis(x[k], org[k], periodic ? (&gr.x)[k] : gr.w, n[k], periodic);
+    return ((unsigned long long)c[2] * n[1] + c[1]) * n[0] + c[0];
+}
+
+__global__ void k_big_keys(int g, const double4* __restrict__ pos, const Segment* __restrict__ segs,
+                           const double4* __restrict__ grid, const int4* __restrict__ dims, int periodic, double3 box,
+                           const int* __restrict__ resort, unsigned long long* __restrict__ keys, int npow)
+{
+    if (!resort[g]) return;
+    const Segment sg = segs[g];
+    const double4 gr = grid[g];
+    const int4 gd = dims[g];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npow; i += gridDim.x * blockDim.x)
+        keys[i] = i < sg.count ? (cell_of(pos[sg.begin + i], gr, gd, periodic, box) << 24) | (unsigned long long)i
+                               : ~0ull;
+}
+
+// one chunk of SORT_MAX keys per CTA, ascending
+__global__ void __launch_bounds__(1024) k_big_chunks(int g, const int* __restrict__ resort,
+                                                     unsigned long long* __restrict__ keys)
+{
+    if (!resort[g]) return;
+    extern __shared__ unsigned long long sk[];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    unsigned long long* src = keys + (size_t)blockIdx.x * SORT_MAX;
+    for (int i = tid; i < SORT_MAX; i += nt) sk[i] = src[i];
+    __syncthreads();
+    for (int k = 2; k <= SORT_MAX; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < SORT_MAX; i += nt) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long a = sk[i], b = sk[ixj];
+                    if ((a > b) == ((i & k) == 0)) {
+                        sk[i] = b;
+                        sk[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = tid; i < SORT_MAX; i += nt) src[i] = sk[i];
+}
+
+// sorted runs of w keys -> runs of 2w: a key of the left run lands after the
+// keys of the right run that are smaller, a key of the right run after
+// those of the left run that are smaller or equal (the pad keys repeat)
+__global__ void k_big_merge(int g, const int* __restrict__ resort, const unsigned long long* __restrict__ src,
+                            unsigned long long* __restrict__ dst, int npow, int w)
+{
+    if (!resort[g]) return;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npow; p += gridDim.x * blockDim.x) {
+        const unsigned long long key = src[p];
+        const int base = (p / (2 * w)) * (2 * w);
+        const bool left = p - base < w;
+        const unsigned long long* other = src + (left ? base + w : base);
+        int lo = 0, hi = w;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (left ? other[mid] < key : other[mid] <= key) lo = mid + 1; else hi = mid;
+        }
+        dst[base + (p - base - (left ? 0 : w)) + lo] = key;
+    }
+}
+
+__global__ void k_big_clear(int g, const int* __restrict__ resort, const int4* __restrict__ dims,
+                            int2* __restrict__ cell_range, const long long* __restrict__ cell_off)
+{
+    if (!resort[g]) return;
+    const int4 gd = dims[g];
+    const long long ncell = (long long)gd.x * gd.y * gd.z;
+    int2* tab = cell_range + cell_off[2 * g];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ncell; k += (long long)gridDim.x * blockDim.x)
+        tab[k] = make_int2(0, 0);
+}
+
+// the sorted keys -> the segment's sorted bead order, its cell table and
+// the positions the next skin test compares against
+__global__ void k_big_fill(int g, const int* __restrict__ resort, const Segment* __restrict__ segs,
+                           const unsigned long long* __restrict__ sorted, const double4* __restrict__ pos,
+                           unsigned long long* __restrict__ keys_out, int* __restrict__ idx_out,
+                           double4* __restrict__ pos_build, int2* __restrict__ cell_range,
+                           const long long* __restrict__ cell_off, int* __restrict__ built)
+{
+    if (!resort[g]) return;
+    const Segment sg = segs[g];
+    int2* tab = cell_range + cell_off[2 * g];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < sg.count; i += gridDim.x * blockDim.x) {
+        const unsigned long long key = sorted[i] >> 24;
+        keys_out[sg.begin + i] = key;
+        idx_out[sg.begin + i] = sg.begin + (int)(sorted[i] & 0xffffffull);
+        pos_build[sg.begin + i] = pos[sg.begin + i];
+        if (i == 0 || (sorted[i - 1] >> 24) != key) tab[key].x = sg.begin + i;
+        if (i == sg.count - 1 || (sorted[i + 1] >> 24) != key) tab[key].y = sg.begin + i + 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) built[g] = 1;
 }
 
 // ------------------------------------------------------------- non-bonded
@@ -370,12 +505,9 @@ k_nonbonded(ForceParams fp, int n, const double4* __restrict__ pos, const double
             const double x[3] = {p.x, p.y, p.z};
             int c[3];
             const int nn[3] = {gd.x, gd.y, gd.z};
-            for (int k = 0; k < 3; ++k) {
-                const double w = fp.periodic ? (&gr.x)[k] : gr.w;
-                const double o = fp.periodic ? -0.5 * fp.box[k] : (&gr.x)[k];
-                const int ci = (int)floor((x[k] - o) / w);
-                c[k] = ci < 0 ? 0 : (ci >= nn[k] ? nn[k] - 1 : ci);
-            }
+            for (int k = 0; k < 3; ++k)
+                c[k] = cell_axis(x[k], fp.periodic ? -0.5 * fp.box[k] : (&gr.x)[k], fp.periodic ? (&gr.x)[k] : gr.w,
+                                 nn[k], fp.periodic);
             const int2* tab = cell_range + cell_off[2 * sgi];
             // lanes 0..26 fetch the [first, end) range of one neighbour cell each
             int2 rg = make_int2(0, 0);
@@ -868,6 +1000,25 @@ int bonded_setup(bdb_system* s)
     return BDB_OK;
 }
 
+}  // namespace bdb
+
+extern "C" int bdb_cell_grid(bdb_system* s, int segment, int* dims)
+{
+    using namespace bdb;
+    if (!s || !dims) return fail(BDB_ERR_ARG, "null argument");
+    if (segment < 0 || segment >= (int)s->segs.size()) return fail(BDB_ERR_ARG, "segment out of range");
+    if (!s->grid_dims.p) return fail(BDB_ERR_ARG, "no force evaluation yet");
+    int4 d;
+    BDB_CUDA(d2h(s, &d, s->grid_dims.p + segment, sizeof(int4)));
+    dims[0] = d.x;
+    dims[1] = d.y;
+    dims[2] = d.z;
+    dims[3] = d.w;
+    return BDB_OK;
+}
+
+namespace bdb {
+
 int forces_setup(bdb_system* s)
 {
     const int nseg = (int)s->segs.size();
@@ -887,6 +1038,20 @@ int forces_setup(bdb_system* s)
         tot += cap;
     }
     if (s->cell_range.alloc(tot) || s->cell_off.alloc(2 * nseg)) return BDB_ERR_NOMEM;
+    if (s->cells_resort.alloc(nseg)) return BDB_ERR_NOMEM;
+    BDB_CUDA(dzero(s, s->cells_resort.p, sizeof(int) * nseg));
+    int big = 0;
+    for (auto& g : s->segs) big = std::max(big, g.count > SORT_MAX ? g.count : 0);
+    if (big) {
+        // bead index in the low 24 bits of a key
+        if (big > (1 << 24)) return fail(BDB_ERR_ARG, "segment of more than 2^24 beads");
+        size_t np = SORT_MAX;
+        while (np < (size_t)big) np <<= 1;
+        s->big_npow = np;
+        if (s->big_keys.alloc(2 * np)) return BDB_ERR_NOMEM;
+        BDB_CUDA(cudaFuncSetAttribute(k_big_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      SORT_MAX * (int)sizeof(unsigned long long)));
+    }
     BDB_CUDA(h2d(s, s->cell_off.p, off.data(), sizeof(long long) * 2 * nseg));
     if (s->e_part.alloc(2 * s->n + 16)) return BDB_ERR_NOMEM;
     if (s->status.alloc(4)) return BDB_ERR_NOMEM;
@@ -951,8 +1116,32 @@ int forces_run(bdb_system* s, bool want_energy, bool want_counts)
     size_t shm = sizeof(unsigned long long) * (size_t)std::min(np, SORT_MAX);
     k_cells<<<nseg, 1024, shm, st>>>(s->pos.p, s->d_segs.p, s->cell_size, s->skin, s->p.bc == 1, box,
                                       s->sorted_keys.p, s->sorted_idx.p, s->grid.p, s->grid_dims.p,
-                                      s->pos_build.p, s->cells_built.p, s->cell_range.p, s->cell_off.p);
+                                      s->pos_build.p, s->cells_built.p, s->cell_range.p, s->cell_off.p,
+                                      s->cells_resort.p);
     BDB_CUDA(cudaGetLastError());
+    for (int g = 0; g < nseg; ++g) {
+        const int cnt = s->segs[g].count;
+        if (cnt <= SORT_MAX) continue;
+        int np = SORT_MAX;
+        while (np < cnt) np <<= 1;
+        unsigned long long *a = s->big_keys.p, *b = a + s->big_npow;
+        const int blocks = std::min(4 * s->sm_count, (np + 255) / 256);
+        k_big_keys<<<blocks, 256, 0, st>>>(g, s->pos.p, s->d_segs.p, s->grid.p, s->grid_dims.p, s->p.bc == 1, box,
+                                           s->cells_resort.p, a, np);
+        k_big_chunks<<<np / SORT_MAX, 1024, SORT_MAX * sizeof(unsigned long long), st>>>(g, s->cells_resort.p, a);
+        s->launches += 2;
+        for (int w = SORT_MAX; w < np; w <<= 1) {
+            k_big_merge<<<blocks, 256, 0, st>>>(g, s->cells_resort.p, a, b, np, w);
+            std::swap(a, b);
+            s->launches += 1;
+        }
+        k_big_clear<<<blocks, 256, 0, st>>>(g, s->cells_resort.p, s->grid_dims.p, s->cell_range.p, s->cell_off.p);
+        k_big_fill<<<blocks, 256, 0, st>>>(g, s->cells_resort.p, s->d_segs.p, a, s->pos.p, s->sorted_keys.p,
+                                           s->sorted_idx.p, s->pos_build.p, s->cell_range.p, s->cell_off.p,
+                                           s->cells_built.p);
+        s->launches += 2;
+        BDB_CUDA(cudaGetLastError());
+    }
     double* Fb = s->work.p;
     if (s->n_terms) {
         BondedArgs A = bonded_args(s);

@@ -46,7 +46,7 @@ EXPORTS = [
     "bdb_frames_start", "bdb_frames_take", "bdb_frames_pending", "bdb_frames_flush", "bdb_frames_stop",
     "bdb_set_time", "bdb_get_time", "bdb_newton_resolve",
     "bdb_checkpoint_size", "bdb_checkpoint_save", "bdb_checkpoint_load", "bdb_refresh",
-    "bdb_get_factor_tuning", "bdb_set_factor_tuning", "bdb_set_wait_limit",
+    "bdb_get_factor_tuning", "bdb_set_factor_tuning", "bdb_set_wait_limit", "bdb_cell_grid",
 ]
 
 
@@ -124,6 +124,7 @@ def load_library(path: str = LIB_PATH):
     lib.bdb_phase_stats.argtypes = [C.c_void_p, C.c_char_p, _dp, C.POINTER(C.c_longlong)]
     lib.bdb_reset_stats.argtypes = [C.c_void_p]
     lib.bdb_launches.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+    lib.bdb_cell_grid.argtypes = [C.c_void_p, C.c_int, _ip]
     lib.bdb_stream.argtypes = [C.c_void_p]
     lib.bdb_stream.restype = C.c_void_p
     lib.bdb_stored_matvec_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -489,6 +490,13 @@ class System:
         out = C.c_longlong()
         self._check(self.lib.bdb_launches(self.h, C.byref(out)))
         return out.value
+
+    def cell_grid(self, segment: int = 0):
+        """(nx, ny, nz, all_pairs) of a segment's neighbour-cell grid after
+        the last force evaluation (bdb_cell_grid)."""
+        d = np.zeros(4, np.int32)
+        self._check(self.lib.bdb_cell_grid(self.h, segment, d.ctypes.data_as(C.POINTER(C.c_int))))
+        return tuple(int(x) for x in d)
 
 
 def shard_replicas(beads, nshards: int) -> np.ndarray:

@@ -232,6 +232,14 @@ int bdb_load_state(bdb_system* s);     /* load_coord + load_forces */
  * flag (0 or 1) or a negative error. */
 int bdb_compute_forces(bdb_system* s, double* F, double* E, long long* counts);
 
+/* The neighbour-cell grid of a segment (system or replica) as the last force
+ * evaluation built it: dims[0..2] cells along x, y, z, dims[3] 1 where the
+ * segment takes all pairs instead (a grid of fewer than 3 periodic cells
+ * along an axis, or a non-finite coordinate). BD_BOX keeps its bucket grid
+ * internal (bucket.c:173-379, bucket_space); this query is for checking that
+ * a large system uses cells. Synchronises the system's stream. */
+int bdb_cell_grid(bdb_system* s, int segment, int* dims);
+
 /* compute_D / compute_single_D (diff_tensor.c:472-544): the full symmetric
  * 3N x 3N tensor at the current coordinates, row-major, into host D. */
 int bdb_compute_D(bdb_system* s, double* D);

@@ -652,10 +652,13 @@ static double lj_range(const orc_system* s, int i, int j)
 static int force_single(const orc_system* s, int i, int j, double* F, double* E, long long* counts)
 {
     double r_norm, r_sq, e[3];
-    int rep = 0, conn;
+    int rep = 0, conn = -1;
     const double* LJ = s->LJ;
     v2_norms(s, i, j, e, &r_norm, &r_sq);
-    conn = bonded_pair(s, i, j);
+    /* the 1-2 connection only matters inside a cut-off: looked up there (a
+     * scan of the bond list, so not for every pair) */
+    if ((s->elec && r_norm <= s->cutoff_c) || (s->alpha_lj != 0.0 && r_norm <= lj_range(s, i, j)))
+        conn = bonded_pair(s, i, j);
     if (s->elec && r_norm <= s->cutoff_c) {
         if (counts) counts[0]++;
         if (!conn)
