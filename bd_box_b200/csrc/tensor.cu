@@ -124,11 +124,11 @@ static TensorArgs targs(const bdb_system* s)
     return a;
 }
 
-template <typename T>
-__device__ __forceinline__ void tile_of(const TensorArgs& A, const double4* pos, int i, int j, T* t)
+template <typename T, bool kEwald>
+__device__ __forceinline__ void tile_of_k(const TensorArgs& A, const double4* pos, int i, int j, T* t)
 {
     const double4 pi = pos[i], pj = pos[j];
-    if (A.ewald) {
+    if constexpr (kEwald) {
         double d[6];
         if (A.ec.smith)
             rpy_smith_tab<sizeof(T) == 4>(pi, pj, i == j, A.preDii, A.preDij, A.ec, d);
@@ -147,6 +147,21 @@ __device__ __forceinline__ void tile_of(const TensorArgs& A, const double4* pos,
 }
 
 template <typename T>
+__device__ __forceinline__ void tile_of(const TensorArgs& A, const double4* pos, int i, int j, T* t)
+{
+    if (A.ewald)
+        tile_of_k<T, true>(A, pos, i, j, t);
+    else
+        tile_of_k<T, false>(A, pos, i, j, t);
+}
+
+// One CTA per pair of 32-bead blocks (I >= J): the 96x96 tile of D in
+// shared memory, then stored straight and (off the diagonal) transposed,
+// both triangles, one warp per matrix row so that every store of a warp is
+// one contiguous run of the row. The free-space variant (kEwald false)
+// carries none of the Ewald code, so it keeps few registers and several
+// CTAs per SM.
+template <typename T, bool kEwald>
 __global__ void __launch_bounds__(256) k_build(TensorArgs A, const double4* __restrict__ pos, T* __restrict__ M,
                                                double* __restrict__ dD)
 {
@@ -160,7 +175,7 @@ __global__ void __launch_bounds__(256) k_build(TensorArgs A, const double4* __re
         const int li = p / TB, lj = p % TB;
         const int i = I * TB + li, j = J * TB + lj;
         T t[6] = {0, 0, 0, 0, 0, 0};
-        if (i < A.n && j < A.n) tile_of<T>(A, pos, i, j, t);
+        if (i < A.n && j < A.n) tile_of_k<T, kEwald>(A, pos, i, j, t);
         const int r = 3 * li, c = 3 * lj;
         tile[r][c] = t[0];
         tile[r + 1][c + 1] = t[1];
@@ -171,14 +186,24 @@ __global__ void __launch_bounds__(256) k_build(TensorArgs A, const double4* __re
     }
     __syncthreads();
     const int r0 = 3 * TB * I, c0 = 3 * TB * J;
-    for (int idx = tid; idx < 9 * TB * TB; idx += blockDim.x) {
-        const int r = idx / (3 * TB), c = idx % (3 * TB);
-        if (r0 + r < n3 && c0 + c < n3) M[(size_t)(r0 + r) * A.npad + c0 + c] = tile[r][c];
+    const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    const int rows = min(3 * TB, n3 - r0), cols = min(3 * TB, n3 - c0);
+    for (int r = warp; r < rows; r += nw) {
+        T* dst = M + (size_t)(r0 + r) * A.npad + c0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int c = lane + 32 * k;
+            if (c < cols) dst[c] = tile[r][c];
+        }
     }
     if (I != J) {
-        for (int idx = tid; idx < 9 * TB * TB; idx += blockDim.x) {
-            const int c = idx / (3 * TB), r = idx % (3 * TB);
-            if (r0 + r < n3 && c0 + c < n3) M[(size_t)(c0 + c) * A.npad + r0 + r] = tile[r][c];
+        for (int c = warp; c < cols; c += nw) {
+            T* dst = M + (size_t)(c0 + c) * A.npad + r0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int r = lane + 32 * k;
+                if (r < rows) dst[r] = tile[r][c];
+            }
         }
     } else {
         for (int r = tid; r < 3 * TB; r += blockDim.x)
@@ -209,9 +234,16 @@ int tensor_build(bdb_system* s)
     const int nt = (s->n + TB - 1) / TB;
     dim3 grid(nt, nt);
     if (s->p.precision == BDB_PREC_FP64) {
-        k_build<double><<<grid, 256, build_smem_bytes<double>(), s->stream>>>(A, s->pos.p, s->M64.p, s->dD.p);
+        if (A.ewald)
+            k_build<double, true><<<grid, 256, build_smem_bytes<double>(), s->stream>>>(A, s->pos.p, s->M64.p, s->dD.p);
+        else
+            k_build<double, false><<<grid, 256, build_smem_bytes<double>(), s->stream>>>(A, s->pos.p, s->M64.p,
+                                                                                        s->dD.p);
     } else {
-        k_build<float><<<grid, 256, build_smem_bytes<float>(), s->stream>>>(A, s->pos.p, s->M32.p, s->dD.p);
+        if (A.ewald)
+            k_build<float, true><<<grid, 256, build_smem_bytes<float>(), s->stream>>>(A, s->pos.p, s->M32.p, s->dD.p);
+        else
+            k_build<float, false><<<grid, 256, build_smem_bytes<float>(), s->stream>>>(A, s->pos.p, s->M32.p, s->dD.p);
     }
     s->launches += 1;
     BDB_CUDA(cudaGetLastError());
@@ -573,9 +605,13 @@ static int tensor_attrs()
 {
     static bool done = false;
     if (done) return BDB_OK;
-    BDB_CUDA(cudaFuncSetAttribute(k_build<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    BDB_CUDA(cudaFuncSetAttribute(k_build<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)build_smem_bytes<double>()));
-    BDB_CUDA(cudaFuncSetAttribute(k_build<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    BDB_CUDA(cudaFuncSetAttribute(k_build<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)build_smem_bytes<double>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_build<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)build_smem_bytes<float>()));
+    BDB_CUDA(cudaFuncSetAttribute(k_build<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)build_smem_bytes<float>()));
     BDB_CUDA(cudaFuncSetAttribute(k_tea<double, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)tea_smem_bytes<double, 32>()));
