@@ -175,6 +175,7 @@ struct bdb_system {
     cudaGraphExec_t refresh_graph = nullptr;   // tensor build + factorisation (mixed path)
     long long refresh_launches = 0, eager_refreshes = 0;
     bool graphs = true, graph_refresh = true;
+    bool fuse_step = true;                     // Cholesky steps: noise drawn ahead, update in the product's finisher
 
     // steps taken (bdb_step, bdb_step_igt), simulated time, and the frame
     // ring of bdb_frames_start
@@ -257,6 +258,7 @@ int tensor_build(bdb_system* s);       // stored D into M64/M32 + dD
 int tensor_tile_host(bdb_system* s, int i, int j, double* tD);
 int factor_run(bdb_system* s);         // Cholesky of the stored D in place
 int stored_matvec(bdb_system* s, bool want_rs);   // Rf = D.F (upper), Rs = L.X (lower)
+int stored_matvec_step(bdb_system* s);   // mixed path: noise drawn in the product, update in its finisher
 int tea_run(bdb_system* s, bool want_rs);         // matrix-free D.F (+ TEA noise)
 int noise_fill(bdb_system* s, const double* host_gauss);   // X = unit Gaussians
 int update_positions(bdb_system* s, double* fs = nullptr);  // pos += Rf + Rs, periodic wrap

@@ -238,6 +238,16 @@ int forces_phase(bdb_system* s)
 static int step_body(bdb_system* s, const double* dev_gauss)
 {
     int rc;
+    // the mixed Cholesky step with device noise and no flow: the product
+    // draws the noise and its finisher moves the beads (two launches fewer,
+    // no noise vector in HBM; the same bits as the separate kernels)
+    if (s->fuse_step && !dev_gauss && s->p.hydro == BDB_HYDRO_CHOLESKY && s->p.precision != BDB_PREC_FP64 &&
+        !(s->p.flow && s->p.bc != 2)) {
+        phase_mark(s, P_MATVEC);
+        if ((rc = stored_matvec_step(s))) return rc;
+        phase_mark(s, P_MATVEC);
+        return forces_phase(s);
+    }
     phase_mark(s, P_NOISE);
     if ((rc = noise_fill(s, dev_gauss))) return rc;
     phase_mark(s, P_NOISE);
@@ -392,6 +402,9 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     for (int k = 0; k < 3; ++k) s->inv_L[k] = p->bc == 1 ? 1 / p->box[k] : 0.0;
     s->preDii = BDB_KB_1_6PI * p->T / (p->visc * p->vfactor);
     s->preDij = BDB_KB_1_8PI * p->T / (p->visc * p->vfactor);
+    // BDB_NO_FUSE (diagnostics): separate noise and update kernels on the
+    // Cholesky path, to compare against the fused step
+    s->fuse_step = getenv("BDB_NO_FUSE") == nullptr;
     int rc = BDB_OK;
 #define TRY(x)                       \
     do {                             \
@@ -441,7 +454,7 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     TRYA(s->X, s->n3);
     TRYA(s->dD, s->npad);
     TRYA(s->scal, 64 + 4 * (size_t)nseg + 64);
-    TRYA(s->ctr, 2);
+    TRYA(s->ctr, 3);
     BDB_CUDA(h2d(s, s->d_segs.p, s->segs.data(), sizeof(Segment) * nseg));
     {
         std::vector<int> bs(s->n);
@@ -453,7 +466,7 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     BDB_CUDA(h2d(s, s->Q.p, Q, sizeof(double) * s->n));
     BDB_CUDA(h2d(s, s->LJ.p, LJ, sizeof(double) * 2 * s->n));
     BDB_CUDA(dzero(s, s->scal.p, sizeof(double) * s->scal.n));
-    BDB_CUDA(dzero(s, s->ctr.p, sizeof(unsigned long long) * 2));
+    BDB_CUDA(dzero(s, s->ctr.p, sizeof(unsigned long long) * 3));
     BDB_CUDA(dzero(s, s->Rf.p, sizeof(double) * s->n3));
     BDB_CUDA(dzero(s, s->Rs.p, sizeof(double) * s->n3));
     BDB_CUDA(dzero(s, s->X.p, sizeof(double) * s->n3));
@@ -861,7 +874,11 @@ int bdb_set_graphs(bdb_system* s, int mode)
 int bdb_set_dt(bdb_system* s, double dt)
 {
     if (!s || !(dt > 0.0)) return fail(BDB_ERR_ARG, "time step must be positive");
-    if (s->p.dt != dt) drop_graph(s);
+    if (s->p.dt != dt) {
+        drop_graph(s);
+        // the noise drawn ahead for the next step was scaled with the old dt
+        BDB_CUDA(cudaMemsetAsync(s->ctr.p + 2, 0, sizeof(unsigned long long), s->stream));
+    }
     s->p.dt = dt;
     return BDB_OK;
 }

@@ -289,7 +289,8 @@ int bdb_checkpoint_load(bdb_system* s, const void* buf, size_t bytes)
     if (h.n != s->n || bytes < bdb_checkpoint_size(s)) return fail(BDB_ERR_ARG, "checkpoint of another bead count");
     const unsigned char* in = static_cast<const unsigned char*>(buf);
     BDB_CUDA(cudaMemcpyAsync(s->pos.p, in + sizeof h, sizeof(double4) * s->n, cudaMemcpyHostToDevice, s->stream));
-    const unsigned long long ctr[2] = {h.philox_stream, 0ull};
+    // the stream index, the block count, no noise drawn ahead
+    const unsigned long long ctr[3] = {h.philox_stream, 0ull, 0ull};
     BDB_CUDA(cudaMemcpyAsync(s->ctr.p, ctr, sizeof ctr, cudaMemcpyHostToDevice, s->stream));
     BDB_CUDA(cudaMemsetAsync(s->cells_built.p, 0, sizeof(int) * s->segs.size(), s->stream));
     BDB_CUDA(cudaStreamSynchronize(s->stream));   // ctr is a stack array

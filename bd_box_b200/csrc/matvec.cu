@@ -23,6 +23,7 @@
 #include <string>
 
 #include "bdb_common.cuh"
+#include "philox.cuh"
 #include "sm100.cuh"
 
 namespace bdb {
@@ -241,7 +242,8 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
 k_strip_mv_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap map_x,
                const __grid_constant__ CUtensorMap map_f, int n3, int ntc, long long T, int slots,
                const double* __restrict__ F, double* __restrict__ rowp, double* __restrict__ colp,
-               unsigned* __restrict__ status, uint32_t wlim)
+               unsigned* __restrict__ status, uint32_t wlim, int gen_x, uint64_t seed,
+               const unsigned long long* __restrict__ ctr, double xscale)
 {
     {
         uint32_t dyn;
@@ -275,7 +277,63 @@ k_strip_mv_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
     }
     __syncthreads();
 
-    if (warp == MT_CW) {
+    // gen_x (the fused Cholesky step): the noise of this step is normally
+    // drawn ahead into X by the previous step's finisher, tagged ctr[2] =
+    // stream + 1. Without that tag (the first fused step, or after another
+    // writer of X or of the stream index) the producer warp draws it itself.
+    bool draw = false;
+    uint64_t stream = 0;
+    if (gen_x) {
+        stream = *reinterpret_cast<const volatile unsigned long long*>(ctr);
+        draw = *reinterpret_cast<const volatile unsigned long long*>(ctr + 2) != stream + 1;
+    }
+    if (warp == MT_CW && draw) {
+        // the whole warp computes each tile's 128 entries of X -- the
+        // Philox Gaussians k_noise would write, scaled the same way -- into
+        // the stage (tiles with an L part only), then lane 0 loads the
+        // matrix box and F. Waits and stops are decided by lane 0 and
+        // shared, so the lanes never part.
+        long long i = 0;
+        for (long long t = t_beg; t < t_end; ++t, ++i) {
+            if (__shfl_sync(0xffffffffu, lane == 0 ? (int)abort_flag : 0, 0)) break;
+            const int st = (int)(i % MT_STAGES);
+            bool ok = true;
+            if (lane == 0)
+                ok = mbar_wait(smem_u32(&bars.empty[st]), (uint32_t)((i / MT_STAGES) & 1) ^ 1u, &abort_flag, wlim);
+            if (!__shfl_sync(0xffffffffu, (int)ok, 0)) break;
+            __syncwarp();
+            const int r0 = (int)(t / ntc) * MT_ROWS, c0 = (int)(t % ntc) * MT_COLS;
+            if (!mt_upper(r0, c0)) {
+                double2* xs = reinterpret_cast<double2*>(sm + st * MT_STAGE_BYTES + MT_BOX_BYTES);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int m = lane + 32 * h;   // entries c0 + 2m and c0 + 2m + 1
+                    const int i0 = c0 + 2 * m;
+                    double2 v = make_double2(0.0, 0.0);
+                    if (i0 < n3) {
+                        double g0, g1;
+                        gauss2(seed, stream, (uint32_t)(i0 / 2), g0, g1);
+                        v.x = g0 * xscale;
+                        v.y = i0 + 1 < n3 ? g1 * xscale : 0.0;
+                    }
+                    xs[m] = v;
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                const uint32_t fb = smem_u32(&bars.full[st]);
+                const uint32_t dst = sbase + st * MT_STAGE_BYTES;
+                mbar_expect_tx(fb, MT_BOX_BYTES + MT_VEC_BYTES);
+                tma_load_2d_stream(dst, &map, c0, r0, fb);
+                tma_load_1d(dst + MT_BOX_BYTES + MT_VEC_BYTES, &map_f, c0, fb);
+            }
+        }
+        if (lane == 0 && abort_flag) {
+            volatile int never = 0;
+            for (long long j = i > MT_STAGES ? i - MT_STAGES : 0; j < i; ++j)
+                mbar_wait(smem_u32(&bars.full[j % MT_STAGES]), (uint32_t)((j / MT_STAGES) & 1), &never);
+        }
+    } else if (warp == MT_CW) {
         if (lane == 0) {
             long long i = 0;
             for (long long t = t_beg; t < t_end && !abort_flag; ++t, ++i) {
@@ -454,7 +512,9 @@ k_strip_mv_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
 __global__ void __launch_bounds__(FIN_ROWS * FIN_GROUPS)
 k_mv_finish_tma(int n3, int ntc, long long T, int G, int slots, const double* __restrict__ rowp, const double* __restrict__ colp,
                 const double* __restrict__ dD, const double* __restrict__ F, double pre, double* __restrict__ Rf,
-                double* __restrict__ Rs, int want_rs)
+                double* __restrict__ Rs, int want_rs, double* __restrict__ pos_d, int periodic, double3 box,
+                double3 inv_L, unsigned long long* __restrict__ ctr, uint64_t seed, double xscale,
+                double* __restrict__ X)
 {
     __shared__ double part[FIN_GROUPS][FIN_ROWS + 1];
     const int tx = threadIdx.x % FIN_ROWS, ty = threadIdx.x / FIN_ROWS;
@@ -489,6 +549,43 @@ k_mv_finish_tma(int n3, int ntc, long long T, int G, int slots, const double* __
         for (int g = 0; g < FIN_GROUPS; ++g) f += part[g][tx];
         Rf[r] = f * pre;
         if (want_rs) Rs[r] = sr;
+        if (pos_d) {
+            // the position update of k_update (no flow) for this coordinate:
+            // the same operations in the same order, so the same bits
+            double* pc = pos_d + 4 * (r / 3) + r % 3;
+            double v = add(add(f * pre, sr), *pc);
+            if (periodic) {
+                const double L = (&box.x)[r % 3], iL = (&inv_L.x)[r % 3];
+                v = sub(v, mul(L, floor(add(mul(v, iL), 0.5))));
+            }
+            *pc = v;
+        }
+    }
+    if (ctr) {
+        // the next step's noise, drawn ahead (the product of this step is
+        // done with X): the Gaussians of stream index + 1, as k_noise would
+        // draw them
+        const uint64_t next = *reinterpret_cast<volatile unsigned long long*>(ctr) + 1;
+        if (ty == 0 && r < n3 && (r & 1) == 0) {
+            double g0, g1;
+            gauss2(seed, next, (uint32_t)(r / 2), g0, g1);
+            X[r] = g0 * xscale;
+            if (r + 1 < n3) X[r + 1] = g1 * xscale;
+        }
+        // the last block advances the Philox stream index, as k_noise does,
+        // and tags X as holding its noise
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            const unsigned done = atomicAdd(reinterpret_cast<unsigned*>(ctr + 1), 1u);
+            if (done == gridDim.x - 1) {
+                const unsigned long long stream = *reinterpret_cast<volatile unsigned long long*>(ctr);
+                ctr[1] = 0;
+                ctr[0] = stream + 1;
+                ctr[2] = stream + 2;
+                __threadfence();
+            }
+        }
     }
 }
 
@@ -601,7 +698,11 @@ static int mv_tma_slots(long long T, int G, int ntc)
     return (int)((len + ntc - 1) / ntc) + 1;
 }
 
-static int stored_matvec_tma(bdb_system* s, bool want_rs)
+// fused: the position update inside the finisher, which also draws the
+// next step's Philox noise into X (Cholesky scaling sqrt(2 dt)); the
+// product uses that X, or draws its own when X does not hold this step's
+// noise. The caller has checked that no flow is on.
+static int stored_matvec_tma(bdb_system* s, bool want_rs, bool fused = false)
 {
     int rc = mv_tma_setup(s);
     if (rc) return rc;
@@ -620,15 +721,21 @@ static int stored_matvec_tma(bdb_system* s, bool want_rs)
     // X: any valid vector when Rs is not wanted
     k_strip_mv_tma<<<G, MT_THREADS, MT_SMEM, s->stream>>>(maps[0], want_rs ? maps[1] : maps[2], maps[2], n3, ntc, T,
                                                            slots, s->F.p, rowp, colp, s->status.p,
-                                                           (uint32_t)s->wait_limit);
+                                                           (uint32_t)s->wait_limit, fused ? 1 : 0, s->p.seed,
+                                                           s->ctr.p, sqrt(2 * s->p.dt));
     BDB_CUDA(cudaGetLastError());
     const double pre = s->p.dt / (BDB_KB * s->p.T);
     k_mv_finish_tma<<<(n3 + FIN_ROWS - 1) / FIN_ROWS, FIN_ROWS * FIN_GROUPS, 0, s->stream>>>(
-        n3, ntc, T, G, slots, rowp, colp, s->dD.p, s->F.p, pre, s->Rf.p, s->Rs.p, want_rs);
+        n3, ntc, T, G, slots, rowp, colp, s->dD.p, s->F.p, pre, s->Rf.p, s->Rs.p, want_rs,
+        fused ? reinterpret_cast<double*>(s->pos.p) : nullptr, s->p.bc == 1,
+        make_double3(s->p.box[0], s->p.box[1], s->p.box[2]), make_double3(s->inv_L[0], s->inv_L[1], s->inv_L[2]),
+        fused ? s->ctr.p : nullptr, s->p.seed, sqrt(2 * s->p.dt), s->X.p);
     BDB_CUDA(cudaGetLastError());
     s->launches += 2;
     return BDB_OK;
 }
+
+int stored_matvec_step(bdb_system* s) { return stored_matvec_tma(s, true, true); }
 
 int stored_matvec(bdb_system* s, bool want_rs)
 {
