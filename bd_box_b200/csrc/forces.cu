@@ -522,14 +522,36 @@ k_nonbonded(ForceParams fp, int n, const double4* __restrict__ pos, const double
                 }
                 if (!skip) rg = tab[((long long)cc[2] * nn[1] + cc[1]) * nn[0] + cc[0]];
             }
-            for (int nc = 0; nc < 27; ++nc) {
-                const int lo = __shfl_sync(0xffffffffu, rg.x, nc);
-                const int hi = __shfl_sync(0xffffffffu, rg.y, nc);
-                for (int q = lo + lane; q < hi; q += 32) {
-                    const int j = sidx[q];
-                    if (j == i) continue;
-                    const int a = i < j ? i : j, b = i < j ? j : i;
-                    pair_term(fp, pos, Q, LJ, conn_ptr, conn_list, a, b, i, f, e_lj, e_c, cnt_c, cnt_lj, rep);
+            // the 27 cells' beads as one list: lane k's candidates are
+            // entries k, k + 32, ... of it (a scan of the cell counts and a
+            // search over it), so a warp does a few full rounds instead of
+            // one sparse round per cell; the rounds are warp-uniform
+            const int cnt = rg.y - rg.x;
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int base = 0; base < total; base += 32) {
+                const int q = base + lane;
+                // the cell holding entry q: the first lane whose inclusive
+                // count exceeds q (cells 27..31 add nothing)
+                int c = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int probe = __shfl_sync(0xffffffffu, incl, c + step - 1);
+                    if (probe <= q) c += step;
+                }
+                const int first = __shfl_sync(0xffffffffu, rg.x, c);
+                const int excl = __shfl_sync(0xffffffffu, incl, c) - __shfl_sync(0xffffffffu, cnt, c);
+                if (q < total) {
+                    const int j = sidx[first + (q - excl)];
+                    if (j != i) {
+                        const int a = i < j ? i : j, b = i < j ? j : i;
+                        pair_term(fp, pos, Q, LJ, conn_ptr, conn_list, a, b, i, f, e_lj, e_c, cnt_c, cnt_lj, rep);
+                    }
                 }
             }
         }
