@@ -287,8 +287,9 @@ struct TeaSeg {
 // walks both read consecutive words), then (phase 2) the row sums into the
 // beads of I and (phase 3) the column sums into the beads of J. Within a job
 // the sums run in T (FP32 on the mixed path); the records they produce and
-// every sum across jobs are FP64.
-template <typename T, int TT>
+// every sum across jobs are FP64. The free-space variant (kEwald false)
+// carries none of the lattice-sum code: fewer registers, more CTAs per SM.
+template <typename T, int TT, bool kEwald>
 __global__ void __launch_bounds__(256)
 k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__ segs,
       const double4* __restrict__ pos, const double* __restrict__ F, const double* __restrict__ X,
@@ -321,7 +322,7 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
     for (int p = tid; p < TT * TT; p += blockDim.x) {
         const int li = p / TT, lj = p % TT;
         T t[6] = {0, 0, 0, 0, 0, 0};
-        if (li < ni && lj < nj && (!diag || lj < li)) tile_of<T>(A, pos, bi0 + li, bj0 + lj, t);
+        if (li < ni && lj < nj && (!diag || lj < li)) tile_of_k<T, kEwald>(A, pos, bi0 + li, bj0 + lj, t);
         for (int k = 0; k < 6; ++k) tD[k][li][lj] = t[k];
     }
     __syncthreads();
@@ -480,12 +481,21 @@ int tea_setup(bdb_system* s);
 template <int TT>
 static void tea_launch(bdb_system* s, const TensorArgs& A, const TeaSeg* tsegs, bool want_rs)
 {
-    if (s->p.precision == BDB_PREC_FP64)
-        k_tea<double, TT><<<s->n_jobs, 256, tea_smem_bytes<double, TT>(), s->stream>>>(
-            A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
-    else
-        k_tea<float, TT><<<s->n_jobs, 256, tea_smem_bytes<float, TT>(), s->stream>>>(
-            A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+    if (s->p.precision == BDB_PREC_FP64) {
+        if (A.ewald)
+            k_tea<double, TT, true><<<s->n_jobs, 256, tea_smem_bytes<double, TT>(), s->stream>>>(
+                A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+        else
+            k_tea<double, TT, false><<<s->n_jobs, 256, tea_smem_bytes<double, TT>(), s->stream>>>(
+                A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+    } else {
+        if (A.ewald)
+            k_tea<float, TT, true><<<s->n_jobs, 256, tea_smem_bytes<float, TT>(), s->stream>>>(
+                A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+        else
+            k_tea<float, TT, false><<<s->n_jobs, 256, tea_smem_bytes<float, TT>(), s->stream>>>(
+                A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+    }
 }
 
 static void tea_dispatch(bdb_system* s, const TensorArgs& A, const TeaSeg* tsegs, bool want_rs)
@@ -613,14 +623,18 @@ static int tensor_attrs()
                                   (int)build_smem_bytes<float>()));
     BDB_CUDA(cudaFuncSetAttribute(k_build<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)build_smem_bytes<float>()));
-    BDB_CUDA(cudaFuncSetAttribute(k_tea<double, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)tea_smem_bytes<double, 32>()));
-    BDB_CUDA(cudaFuncSetAttribute(k_tea<float, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)tea_smem_bytes<float, 32>()));
-    BDB_CUDA(cudaFuncSetAttribute(k_tea<double, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)tea_smem_bytes<double, 16>()));
-    BDB_CUDA(cudaFuncSetAttribute(k_tea<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)tea_smem_bytes<float, 16>()));
+#define BDB_TEA_ATTR(T, TT, E)                                                                                \
+    BDB_CUDA(cudaFuncSetAttribute(k_tea<T, TT, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)tea_smem_bytes<T, TT>()))
+    BDB_TEA_ATTR(double, 32, true);
+    BDB_TEA_ATTR(double, 32, false);
+    BDB_TEA_ATTR(float, 32, true);
+    BDB_TEA_ATTR(float, 32, false);
+    BDB_TEA_ATTR(double, 16, true);
+    BDB_TEA_ATTR(double, 16, false);
+    BDB_TEA_ATTR(float, 16, true);
+    BDB_TEA_ATTR(float, 16, false);
+#undef BDB_TEA_ATTR
     done = true;
     return BDB_OK;
 }
