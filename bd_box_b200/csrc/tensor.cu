@@ -220,7 +220,7 @@ static size_t build_smem_bytes()
 template <typename T, int TT>
 static size_t tea_smem_bytes()
 {
-    return sizeof(T) * TT * (TT + 1) * 6;
+    return 0;   // k_tea's shared memory is static
 }
 
 static int tensor_attrs();
@@ -282,28 +282,32 @@ struct TeaSeg {
     int begin, count, ntile, part_begin;
 };
 
-// One job = the tile pair (I, J) of a segment: 32 x 32 bead tiles D_ij
-// computed once into shared memory (six planes, so that row and column
-// walks both read consecutive words), then (phase 2) the row sums into the
-// beads of I and (phase 3) the column sums into the beads of J. Within a job
-// the sums run in T (FP32 on the mixed path); the records they produce and
-// every sum across jobs are FP64. The free-space variant (kEwald false)
-// carries none of the lattice-sum code: fewer registers, more CTAs per SM.
+// One job = the tile pair (I, J) of a segment (TT x TT beads). Warp w holds
+// rows li of the pair (32 / TT rows at a time, one lane per column lj); each
+// lane evaluates its tile D_ij in registers and uses it twice: in the row
+// sums of bead i (a shuffle tree over the row's lanes) and in the column
+// sums of bead j (accumulated by the lane over the rows it visits, then the
+// warps' partials added in warp order through shared memory). The tiles never
+// go through shared memory. Within a job the sums run in T (FP32 on the mixed
+// path); the records they produce and every sum across jobs are FP64. The
+// free-space variant (kEwald false) carries none of the lattice-sum code.
 template <typename T, int TT, bool kEwald>
 __global__ void __launch_bounds__(256)
 k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__ segs,
       const double4* __restrict__ pos, const double* __restrict__ F, const double* __restrict__ X,
       double* __restrict__ part, double* __restrict__ eps_part, int want_rs)
 {
-    extern __shared__ __align__(16) unsigned char tea_smem[];
-    constexpr int LPR = 256 / TT;   // lanes per row (phase 2) or column (phase 3)
-    T(*tD)[TT][TT + 1] = reinterpret_cast<T(*)[TT][TT + 1]>(tea_smem);   // [6][TT][TT+1]
+    constexpr int NW = 8;              // warps
+    constexpr int RPW = 32 / TT;       // rows a warp holds at once
+    constexpr int RSTEP = NW * RPW;    // rows of one pass of the block
+    static_assert(TT == 16 || TT == 32, "tile edge");
     __shared__ T sF[2][TT][3], sX[2][TT][3], sInv[2][TT];
-    __shared__ double sAcc[TT][9];
-    __shared__ double sEps[8];
+    __shared__ T sCol[NW][TT][9];      // the warps' column partials
+    __shared__ T sRowDiag[TT][9];      // diagonal job: row sums, added to the column records
+    __shared__ double sEps[NW];
     const TileJob jb = jobs[blockIdx.x];
     const TeaSeg g = segs[jb.seg];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int bi0 = g.begin + jb.I * TT, bj0 = g.begin + jb.J * TT;
     const int ni = min(TT, g.count - jb.I * TT), nj = min(TT, g.count - jb.J * TT);
     const bool diag = jb.I == jb.J;
@@ -318,88 +322,85 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
             sInv[side][tid] = ok ? (T)(pos[b].w / A.preDii) : (T)0;   // 1/diag_D (diff_decl.c:94-99)
         }
     }
-    // phase 1: tiles
-    for (int p = tid; p < TT * TT; p += blockDim.x) {
-        const int li = p / TT, lj = p % TT;
+    __syncthreads();
+    const int lj = lane % TT, sub = lane / TT;
+    const T* fc = sF[1][lj];
+    const T* xc = sX[1][lj];
+    const T invc = sInv[1][lj];
+    T col[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    T eps = 0;
+#pragma unroll 1
+    for (int r0 = 0; r0 < TT; r0 += RSTEP) {
+        const int li = r0 + warp * RPW + sub;
         T t[6] = {0, 0, 0, 0, 0, 0};
         if (li < ni && lj < nj && (!diag || lj < li)) tile_of_k<T, kEwald>(A, pos, bi0 + li, bj0 + lj, t);
-        for (int k = 0; k < 6; ++k) tD[k][li][lj] = t[k];
-    }
-    __syncthreads();
-    // phase 2: rows (into bead i of tile I), 8 lanes per row
-    const int row = tid / LPR, lane = tid % LPR;
-    T acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    T eps = 0;
-    for (int lj = lane; lj < TT; lj += LPR) {
-        const T xx = tD[0][row][lj], yy = tD[1][row][lj], zz = tD[2][row][lj];
-        const T xy = tD[3][row][lj], xz = tD[4][row][lj], yz = tD[5][row][lj];
-        const T* f = sF[1][lj];
-        const T* x = sX[1][lj];
-        const T inv = sInv[1][lj];
-        acc[0] += xx * f[0] + xy * f[1] + xz * f[2];
-        acc[1] += xy * f[0] + yy * f[1] + yz * f[2];
-        acc[2] += xz * f[0] + yz * f[1] + zz * f[2];
-        acc[3] += (xx * xx + xy * xy + xz * xz) * inv;
-        acc[4] += (xy * xy + yy * yy + yz * yz) * inv;
-        acc[5] += (xz * xz + yz * yz + zz * zz) * inv;
-        acc[6] += xx * x[0] + xy * x[1] + xz * x[2];
-        acc[7] += xy * x[0] + yy * x[1] + yz * x[2];
-        acc[8] += xz * x[0] + yz * x[1] + zz * x[2];
+        const T xx = t[0], yy = t[1], zz = t[2], xy = t[3], xz = t[4], yz = t[5];
+        // bead li: products with bead lj's F, X and 1/D_jj
+        T row[9];
+        row[0] = xx * fc[0] + xy * fc[1] + xz * fc[2];
+        row[1] = xy * fc[0] + yy * fc[1] + yz * fc[2];
+        row[2] = xz * fc[0] + yz * fc[1] + zz * fc[2];
+        row[3] = (xx * xx + xy * xy + xz * xz) * invc;
+        row[4] = (xy * xy + yy * yy + yz * yz) * invc;
+        row[5] = (xz * xz + yz * yz + zz * zz) * invc;
+        row[6] = xx * xc[0] + xy * xc[1] + xz * xc[2];
+        row[7] = xy * xc[0] + yy * xc[1] + yz * xc[2];
+        row[8] = xz * xc[0] + yz * xc[1] + zz * xc[2];
         eps += xx + yy + zz + 2 * (xy + xz + yz);
+        // bead lj: products with bead li's
+        const T* fr = sF[0][li];
+        const T* xr = sX[0][li];
+        const T invr = sInv[0][li];
+        col[0] += xx * fr[0] + xy * fr[1] + xz * fr[2];
+        col[1] += xy * fr[0] + yy * fr[1] + yz * fr[2];
+        col[2] += xz * fr[0] + yz * fr[1] + zz * fr[2];
+        col[3] += (xx * xx + xy * xy + xz * xz) * invr;
+        col[4] += (xy * xy + yy * yy + yz * yz) * invr;
+        col[5] += (xz * xz + yz * yz + zz * zz) * invr;
+        col[6] += xx * xr[0] + xy * xr[1] + xz * xr[2];
+        col[7] += xy * xr[0] + yy * xr[1] + yz * xr[2];
+        col[8] += xz * xr[0] + yz * xr[1] + zz * xr[2];
+#pragma unroll
+        for (int o = 1; o < TT; o <<= 1)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) row[k] += __shfl_xor_sync(0xffffffffu, row[k], o);
+        if (lj == 0 && li < ni) {
+            if (diag) {
+                for (int k = 0; k < 9; ++k) sRowDiag[li][k] = row[k];
+            } else {
+                // record (T = J, bead in I)
+                double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.J * g.count + jb.I * TT + li);
+                for (int k = 0; k < 9; ++k) dst[k] = (double)row[k];
+            }
+        }
     }
-    for (int o = 1; o < LPR; o <<= 1) {
-        for (int k = 0; k < 9; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-        eps += __shfl_xor_sync(0xffffffffu, eps, o);
+    if constexpr (RPW == 2) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) col[k] += __shfl_xor_sync(0xffffffffu, col[k], 16);
     }
-    if (lane == 0)
-        for (int k = 0; k < 9; ++k) sAcc[row][k] = (double)acc[k];
-    // eps: one value per warp (its 32 / LPR rows), then fixed-order sum
+    if (sub == 0)
+        for (int k = 0; k < 9; ++k) sCol[warp][lj][k] = col[k];
     {
-        double e = lane == 0 ? (double)eps : 0.0;
-        for (int o = LPR; o < 32; o <<= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
-        if ((tid & 31) == 0) sEps[tid >> 5] = e;
+        double e = (double)eps;
+        for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        if (lane == 0) sEps[warp] = e;
     }
     __syncthreads();
     if (tid == 0) {
         double e = 0;
-        for (int w = 0; w < 8; ++w) e += sEps[w];
+        for (int w = 0; w < NW; ++w) e += sEps[w];
         eps_part[blockIdx.x] = e;
     }
-    // write rows: record (T = J, bead in I); on the diagonal tile add the
-    // column sums below first
-    if (!diag) {
-        if (lane == 0 && row < ni) {
-            double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.J * g.count + jb.I * TT + row);
-            for (int k = 0; k < 9; ++k) dst[k] = sAcc[row][k];
-        }
-    }
-    // phase 3: columns (into bead j of tile J)
-    const int col = tid / LPR;
-    for (int k = 0; k < 9; ++k) acc[k] = 0;
-    for (int li = lane; li < TT; li += LPR) {
-        const T xx = tD[0][li][col], yy = tD[1][li][col], zz = tD[2][li][col];
-        const T xy = tD[3][li][col], xz = tD[4][li][col], yz = tD[5][li][col];
-        const T* f = sF[0][li];
-        const T* x = sX[0][li];
-        const T inv = sInv[0][li];
-        acc[0] += xx * f[0] + xy * f[1] + xz * f[2];
-        acc[1] += xy * f[0] + yy * f[1] + yz * f[2];
-        acc[2] += xz * f[0] + yz * f[1] + zz * f[2];
-        acc[3] += (xx * xx + xy * xy + xz * xz) * inv;
-        acc[4] += (xy * xy + yy * yy + yz * yz) * inv;
-        acc[5] += (xz * xz + yz * yz + zz * zz) * inv;
-        acc[6] += xx * x[0] + xy * x[1] + xz * x[2];
-        acc[7] += xy * x[0] + yy * x[1] + yz * x[2];
-        acc[8] += xz * x[0] + yz * x[1] + zz * x[2];
-    }
-    for (int o = 1; o < LPR; o <<= 1)
-        for (int k = 0; k < 9; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-    if (lane == 0 && col < nj) {
-        double* dst = part + 9 * ((size_t)g.part_begin + (size_t)jb.I * g.count + jb.J * TT + col);
-        if (diag) {
-            for (int k = 0; k < 9; ++k) dst[k] = (double)acc[k] + sAcc[col][k];
-        } else {
-            for (int k = 0; k < 9; ++k) dst[k] = (double)acc[k];
+    // column records (T = I, bead in J), the warps' partials in order; on a
+    // diagonal job the row sums of the same bead join them
+    for (int q = tid; q < TT * 9; q += blockDim.x) {
+        const int c = q / 9, k = q % 9;
+        if (c < nj) {
+            T a = 0;
+            for (int w = 0; w < NW; ++w) a += sCol[w][c][k];
+            double v = (double)a;
+            if (diag) v += (double)sRowDiag[c][k];
+            part[9 * ((size_t)g.part_begin + (size_t)jb.I * g.count + jb.J * TT + c) + k] = v;
         }
     }
 }
