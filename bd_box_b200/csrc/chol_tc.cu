@@ -687,7 +687,11 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, 
                 *reinterpret_cast<float2*>(Llo + row * PW + col) = make_float2(o0 - h0, o1 - h1);
             } else {
                 st_pair(M + row * npad + base + col, x0, x1);
-                st_pair(reinterpret_cast<double*>(Lhi) + row * PW + col, x0, x1);
+                // the FP64 panel in k_syrk64's fragment order: within each
+                // group of 8 columns, column c at 2 (c mod 4) + (c / 4 mod 2)
+                double* pr = reinterpret_cast<double*>(Lhi) + row * PW + 8 * n;
+                pr[(((2 * fq) & 3) << 1) | (fq >> 1)] = x0;
+                pr[(((2 * fq + 1) & 3) << 1) | (fq >> 1)] = x1;
             }
             if (n < 15) {
                 const double xa0 = -c2a(x0, x1, 0, fr, fq), xa1 = -c2a(x0, x1, 1, fr, fq);
@@ -1241,15 +1245,18 @@ k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ C
 // 64 (w / 4).. as 32 accumulator tiles in registers, initialised from C and
 // stored back (lower triangle only on diagonal tiles, whose upper triangle
 // holds D). The panel rows of tiles i and j stream through shared memory in
-// chunks of 16 columns (cp.async, two stages, rows padded to 20 doubles: at
-// most two-way bank conflicts on the 8-byte fragment loads, which take two
-// wavefronts anyway). Per chunk a warp issues 128 DMMAs from 48 fragment
-// loads.
+// chunks of 32 columns (cp.async, two stages). The panel solve stores the
+// FP64 panel with each group of 8 columns permuted (column c at 2 (c mod 4)
+// + (c / 4 mod 2)), so a lane's operands of k-steps kk and kk + 4 are
+// adjacent: one 16-byte shared load feeds two k-steps. Rows padded to 40
+// doubles (an 8-row quarter-warp's 16-byte loads then hit distinct banks).
+// Per chunk a warp issues 256 DMMAs from 48 fragment loads; every
+// accumulator takes its k-steps in order, as with natural column order.
 static constexpr int S64_THREADS = 256;
-static constexpr int S64_KC = 16;                        // panel columns per staged chunk
-static constexpr int S64_LD = 20;                        // padded row stride of a staged chunk (doubles)
+static constexpr int S64_KC = 32;                        // panel columns per staged chunk
+static constexpr int S64_LD = 40;                        // padded row stride of a staged chunk (doubles)
 static constexpr int S64_CHUNK = PW * S64_LD;            // doubles of one operand chunk
-static constexpr int S64_SMEM = 2 * 2 * S64_CHUNK * 8;   // two stages of A and B chunks: 80 KB
+static constexpr int S64_SMEM = 2 * 2 * S64_CHUNK * 8;   // two stages of A and B chunks: 160 KB
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src)
 {
@@ -1262,14 +1269,15 @@ __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// columns [k0, k0 + 16) of the panel rows of tiles ra (A) and rb (B):
-// 2 x 1024 16-byte pieces, 8 per thread
+// columns [k0, k0 + 32) of the panel rows of tiles ra (A) and rb (B), as
+// stored (fragment order): 2 x 2048 16-byte pieces, 8 + 8 per thread
 __device__ __forceinline__ void s64_stage(double* As, double* Bs, const double* __restrict__ Lp, int ra, int rb,
                                           int k0, int tid)
 {
+    constexpr int PIECES = S64_KC / 2;   // 16-byte pieces per row
 #pragma unroll
-    for (int q = tid; q < PW * S64_KC / 2; q += S64_THREADS) {
-        const int r = q >> 3, c = (q & 7) * 2;
+    for (int q = tid; q < PW * PIECES; q += S64_THREADS) {
+        const int r = q / PIECES, c = (q % PIECES) * 2;
         cp_async16(smem_u32(As + r * S64_LD + c), Lp + (size_t)(ra + r) * PW + k0 + c);
         cp_async16(smem_u32(Bs + r * S64_LD + c), Lp + (size_t)(rb + r) * PW + k0 + c);
     }
@@ -1327,16 +1335,26 @@ __global__ void __launch_bounds__(S64_THREADS, 1) k_syrk64(double* __restrict__ 
             }
             __syncthreads();
 #pragma unroll
-            for (int kk = 0; kk < S64_KC; kk += 4) {
-                double a[4], b[8];
+            for (int kk = 0; kk < S64_KC; kk += 8) {
+                // k-steps kk (.x) and kk + 4 (.y) of this lane's fragments
+                double2 a[4], b[8];
 #pragma unroll
-                for (int rt = 0; rt < 4; ++rt) a[rt] = -As[(32 * wr + 8 * rt + fr) * S64_LD + kk + fq];
+                for (int rt = 0; rt < 4; ++rt) {
+                    const double2 v =
+                        *reinterpret_cast<const double2*>(As + (32 * wr + 8 * rt + fr) * S64_LD + kk + 2 * fq);
+                    a[rt] = make_double2(-v.x, -v.y);
+                }
 #pragma unroll
-                for (int ct = 0; ct < 8; ++ct) b[ct] = Bs[(64 * wc + 8 * ct + fr) * S64_LD + kk + fq];
+                for (int ct = 0; ct < 8; ++ct)
+                    b[ct] = *reinterpret_cast<const double2*>(Bs + (64 * wc + 8 * ct + fr) * S64_LD + kk + 2 * fq);
 #pragma unroll
                 for (int rt = 0; rt < 4; ++rt)
 #pragma unroll
-                    for (int ct = 0; ct < 8; ++ct) dmma884(acc[rt][ct][0], acc[rt][ct][1], a[rt], b[ct]);
+                    for (int ct = 0; ct < 8; ++ct) dmma884(acc[rt][ct][0], acc[rt][ct][1], a[rt].x, b[ct].x);
+#pragma unroll
+                for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+                    for (int ct = 0; ct < 8; ++ct) dmma884(acc[rt][ct][0], acc[rt][ct][1], a[rt].y, b[ct].y);
             }
             __syncthreads();   // this stage is read; it may be staged again
         }
@@ -1375,10 +1393,11 @@ static int make_panel_map(float* buf, int rows, CUtensorMap* map, int cols = PW)
     return BDB_OK;
 }
 
-// scratch layout in panel64: three panel buffer sets (hi, lo: FP32
-// [npad][128] each), then three FP64 128x128 hand-offs of L_PP / W_kk; panel
-// P uses set P mod 3, so a panel's update may still read its set while the
-// next two panels are solved
+// scratch layout in panel64: four panel buffer sets (hi, lo: FP32
+// [npad][128] each; on the FP64 path one FP64 [npad][128] panel in their
+// room), then four FP64 128x128 hand-offs of L_PP / W_kk; panel P uses set
+// P mod 4, so a panel's updates may still read its set (and the previous
+// panel's) while the next two panels are solved
 static constexpr int PANEL_SETS = 4;
 
 static void panel_ptrs(bdb_system* s, int set, float** hi, float** lo, double** lkk)
