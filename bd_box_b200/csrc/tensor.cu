@@ -291,11 +291,17 @@ struct TeaSeg {
 // go through shared memory. Within a job the sums run in T (FP32 on the mixed
 // path); the records they produce and every sum across jobs are FP64. The
 // free-space variant (kEwald false) carries none of the lattice-sum code.
+// The grid is persistent, as many CTAs as the SMs hold: each CTA takes the
+// next job of the whole batch (every replica's tile pairs in one list) from
+// a counter until none is left -- fetching its next job while it works on
+// the current one -- so replicas of uneven size share the GPU in one launch
+// and a CTA that drew short jobs draws more. A job writes only its own
+// records, so which CTA runs it does not change a bit.
 template <typename T, int TT, bool kEwald>
 __global__ void __launch_bounds__(256)
-k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__ segs,
-      const double4* __restrict__ pos, const double* __restrict__ F, const double* __restrict__ X,
-      double* __restrict__ part, double* __restrict__ eps_part, int want_rs)
+k_tea(TensorArgs A, const TileJob* __restrict__ jobs, int n_jobs, int* __restrict__ next,
+      const TeaSeg* __restrict__ segs, const double4* __restrict__ pos, const double* __restrict__ F,
+      const double* __restrict__ X, double* __restrict__ part, double* __restrict__ eps_part, int want_rs)
 {
     constexpr int NW = 8;              // warps
     constexpr int RPW = 32 / TT;       // rows a warp holds at once
@@ -305,7 +311,14 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
     __shared__ T sCol[NW][TT][9];      // the warps' column partials
     __shared__ T sRowDiag[TT][9];      // diagonal job: row sums, added to the column records
     __shared__ double sEps[NW];
-    const TileJob jb = jobs[blockIdx.x];
+    __shared__ int sJob[2];
+    if (threadIdx.x == 0) sJob[0] = atomicAdd(next, 1);
+    __syncthreads();
+    int slot = 0;
+    for (int job = sJob[0]; job < n_jobs; job = sJob[slot]) {
+    // the next job, read after this one's last barrier
+    if (threadIdx.x == 0) sJob[slot ^ 1] = atomicAdd(next, 1);
+    const TileJob jb = jobs[job];
     const TeaSeg g = segs[jb.seg];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int bi0 = g.begin + jb.I * TT, bj0 = g.begin + jb.J * TT;
@@ -389,7 +402,7 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
     if (tid == 0) {
         double e = 0;
         for (int w = 0; w < NW; ++w) e += sEps[w];
-        eps_part[blockIdx.x] = e;
+        eps_part[job] = e;
     }
     // column records (T = I, bead in J), the warps' partials in order; on a
     // diagonal job the row sums of the same bead join them
@@ -402,6 +415,9 @@ k_tea(TensorArgs A, const TileJob* __restrict__ jobs, const TeaSeg* __restrict__
             if (diag) v += (double)sRowDiag[c][k];
             part[9 * ((size_t)g.part_begin + (size_t)jb.I * g.count + jb.J * TT + c) + k] = v;
         }
+    }
+    __syncthreads();   // the job's shared arrays are read; the next job may write them
+    slot ^= 1;
     }
 }
 
@@ -482,20 +498,21 @@ int tea_setup(bdb_system* s);
 template <int TT>
 static void tea_launch(bdb_system* s, const TensorArgs& A, const TeaSeg* tsegs, bool want_rs)
 {
+    // persistent grid: the SMs' capacity for this variant, at most one CTA per job
+    auto go = [&](auto kern) {
+        int occ = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, 0);
+        const int grid = std::max(1, std::min(s->n_jobs, std::max(1, occ) * s->sm_count));
+        cudaMemsetAsync(s->tea_next.p, 0, sizeof(int), s->stream);
+        kern<<<grid, 256, 0, s->stream>>>(A, s->jobs.p, s->n_jobs, s->tea_next.p, tsegs, s->pos.p, s->F.p, s->X.p,
+                                          s->part.p, s->eps_part.p, want_rs);
+    };
     if (s->p.precision == BDB_PREC_FP64) {
-        if (A.ewald)
-            k_tea<double, TT, true><<<s->n_jobs, 256, tea_smem_bytes<double, TT>(), s->stream>>>(
-                A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
-        else
-            k_tea<double, TT, false><<<s->n_jobs, 256, tea_smem_bytes<double, TT>(), s->stream>>>(
-                A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+        if (A.ewald) go(k_tea<double, TT, true>);
+        else go(k_tea<double, TT, false>);
     } else {
-        if (A.ewald)
-            k_tea<float, TT, true><<<s->n_jobs, 256, tea_smem_bytes<float, TT>(), s->stream>>>(
-                A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
-        else
-            k_tea<float, TT, false><<<s->n_jobs, 256, tea_smem_bytes<float, TT>(), s->stream>>>(
-                A, s->jobs.p, tsegs, s->pos.p, s->F.p, s->X.p, s->part.p, s->eps_part.p, want_rs);
+        if (A.ewald) go(k_tea<float, TT, true>);
+        else go(k_tea<float, TT, false>);
     }
 }
 
@@ -602,6 +619,7 @@ int tea_setup(bdb_system* s)
     job_begin.push_back((int)jobs.size());
     s->n_jobs = (int)jobs.size();
     if (s->jobs.alloc(std::max<size_t>(1, jobs.size()))) return BDB_ERR_NOMEM;
+    if (!s->tea_next.p && s->tea_next.alloc(1)) return BDB_ERR_NOMEM;
     if (s->eps_part.alloc(std::max<size_t>(1, jobs.size()))) return BDB_ERR_NOMEM;
     if (s->part.alloc(std::max<size_t>(9, 9 * part_records))) return BDB_ERR_NOMEM;
     const size_t head = sizeof(TeaSeg) * ts.size() + sizeof(int) * job_begin.size();
