@@ -1536,7 +1536,9 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
     const int bulk_sms = std::max(1, s->sm_count - chain);
     const int per_cta = TRSM_THREADS / 32, units_top = PW / 8;
     // the side kernels take the chain's SMs but three (the diagonal block,
-    // the two CTAs of the top panel solve)
+    // the two CTAs of the top panel solve); the panel solve two CTAs per SM
+    // (its registers and shared memory allow it), for more warps on the FP64
+    // pipes
     const int side = std::max(1, chain - 3);
     constexpr bool kPairs = sizeof(T) == 4;   // two panels per pass over C (mixed path)
     float *hi, *lo;
@@ -1556,7 +1558,7 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
         // side: the panel solve below block row P+1
         BDB_CUDA(cudaStreamWaitEvent(st3, ev_potrf, 0));
         if (units_rest > 0) {
-            k_trsm128<T><<<std::min(side, (units_rest + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st3>>>(
+            k_trsm128<T><<<std::min(2 * side, (units_rest + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st3>>>(
                 M, s->npad, P, units_top, units_rest, lkk, hi, lo, s->status.p);
             BDB_CUDA(cudaGetLastError());
             s->launches += 1;
