@@ -1535,11 +1535,11 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
     const int chain = std::min(std::max(s->chain_sms, 1), s->sm_count - 1);
     const int bulk_sms = std::max(1, s->sm_count - chain);
     const int per_cta = TRSM_THREADS / 32, units_top = PW / 8;
-    // the side kernels take the chain's SMs but three (the diagonal block,
-    // the two CTAs of the top panel solve); the panel solve two CTAs per SM
+    // the side kernels take the chain's SMs but five (the diagonal block,
+    // the four CTAs of the top panel solve); the panel solve two CTAs per SM
     // (its registers and shared memory allow it), for more warps on the FP64
     // pipes
-    const int side = std::max(1, chain - 3);
+    const int side = std::max(1, chain - 5);
     constexpr bool kPairs = sizeof(T) == 4;   // two panels per pass over C (mixed path)
     float *hi, *lo;
     double* lkk;
@@ -1570,8 +1570,10 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
             BDB_CUDA(cudaStreamWaitEvent(st, ev_b, 0));      // B(P-1)
         }
         phase_mark_on(s, P_TRSM, st);
-        k_trsm128<T><<<units_top / per_cta, TRSM_THREADS, TRSM_SMEM, st>>>(M, s->npad, P, 0, units_top, lkk, hi, lo,
-                                                                          s->status.p);
+        // block row P+1: its 16 units on 4 CTAs, so that each unit's warp
+        // has an SM sub-partition (and its FP64 pipe) to itself
+        k_trsm128<T><<<units_top / 4, TRSM_THREADS, TRSM_SMEM, st>>>(M, s->npad, P, 0, units_top, lkk, hi, lo,
+                                                                   s->status.p);
         phase_mark_on(s, P_TRSM, st);
         BDB_CUDA(cudaGetLastError());
         BDB_CUDA(cudaEventRecord(ev_top, st));
