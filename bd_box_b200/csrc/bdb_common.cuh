@@ -132,7 +132,8 @@ struct bdb_system {
     int n_jobs = 0;
     int tea_tile = 32;                         // TEA tile edge (16 or 32 beads)
     int mv_warps = 16;                         // stored matvec: target warps per SM
-    int chain_sms = 16;                        // mixed Cholesky: SMs the bulk updates leave to the panel chain
+    int chain_sms = 32;                        // Cholesky: SMs the bulk updates leave to the panel chain
+                                               // (set per precision at creation)
     bool autotune = false, tea_tuned = false, mv_tuned = false, factor_tuned = false;
     bdb::DevBuf<double> ewald_tab;             // Ewald lattice tables (rpy_tile.cuh EwaldConst)
     int ewald_nk = 0, ewald_nimg = 0;

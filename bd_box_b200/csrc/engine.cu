@@ -405,6 +405,10 @@ static int create_system(bdb_system** out, const bdb_params* p, int nseg, const 
     // BDB_NO_FUSE (diagnostics): separate noise and update kernels on the
     // Cholesky path, to compare against the fused step
     s->fuse_step = getenv("BDB_NO_FUSE") == nullptr;
+    // the Cholesky's chain reserve, measured at 3N = 12288 on B200: the
+    // mixed path's bulk update is fast enough to spare 32 SMs; the FP64
+    // path's DMMA update is the slower side and keeps all but 16
+    s->chain_sms = p->precision == BDB_PREC_FP64 ? 16 : 32;
     int rc = BDB_OK;
 #define TRY(x)                       \
     do {                             \

@@ -277,6 +277,7 @@ def run_ours(args):
         ch = torch.empty(4 * deck.n, dtype=torch.float64).pin_memory()
         hsys = engine.System(deck, precision=engine.PREC_MIXED, refresh=REFRESH,
                              noise=engine.NOISE_HOST, seed=ranks.replica_seed(SEED, rank))
+        hsys.autotune(True)   # the same configuration as the device-resident arm
         gp = C.cast(gh.data_ptr(), C.POINTER(C.c_double))
         cp = C.cast(ch.data_ptr(), C.POINTER(C.c_double))
         for k in range(warm):

@@ -329,8 +329,8 @@ int bdb_set_wait_limit(bdb_system* s, long long tries);
  * Cholesky splits the GPU. Its panel chain (panel solve, next block-column
  * update, next diagonal block) runs beside the bulk trailing updates, which
  * leave chain_sms SMs to it (16, 24, 32, 48 or 64 tried at the first refresh when
- * autotuning is on; 16 otherwise). bdb_set_factor_tuning pins it (0 keeps
- * the value). */
+ * autotuning is on; 32 otherwise; 16 on the FP64 path, which is not tuned).
+ * bdb_set_factor_tuning pins it (0 keeps the value). */
 int bdb_get_factor_tuning(bdb_system* s, int* chain_sms);
 int bdb_set_factor_tuning(bdb_system* s, int chain_sms);
 
