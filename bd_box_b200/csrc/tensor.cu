@@ -217,11 +217,6 @@ static size_t build_smem_bytes()
     return sizeof(T) * 3 * TB * (3 * TB + 1);
 }
 
-template <typename T, int TT>
-static size_t tea_smem_bytes()
-{
-    return 0;   // k_tea's shared memory is static
-}
 
 static int tensor_attrs();
 
@@ -642,18 +637,6 @@ static int tensor_attrs()
                                   (int)build_smem_bytes<float>()));
     BDB_CUDA(cudaFuncSetAttribute(k_build<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)build_smem_bytes<float>()));
-#define BDB_TEA_ATTR(T, TT, E)                                                                                \
-    BDB_CUDA(cudaFuncSetAttribute(k_tea<T, TT, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                  (int)tea_smem_bytes<T, TT>()))
-    BDB_TEA_ATTR(double, 32, true);
-    BDB_TEA_ATTR(double, 32, false);
-    BDB_TEA_ATTR(float, 32, true);
-    BDB_TEA_ATTR(float, 32, false);
-    BDB_TEA_ATTR(double, 16, true);
-    BDB_TEA_ATTR(double, 16, false);
-    BDB_TEA_ATTR(float, 16, true);
-    BDB_TEA_ATTR(float, 16, false);
-#undef BDB_TEA_ATTR
     done = true;
     return BDB_OK;
 }

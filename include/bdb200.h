@@ -339,7 +339,7 @@ int bdb_set_factor_tuning(bdb_system* s, int chain_sms);
  * displacement, the update, the forces -- from a graph captured on the
  * second step; steps with caller Gaussians use a second graph that reads
  * them from a fixed device staging slot. Bit 2: on the mixed path, refreshes of
- * D and its factor (tensor build and the two-stream factorisation) replay a
+ * D and its factor (tensor build and the three-stream factorisation) replay a
  * graph captured on the second refresh. Default 3 (both); 0 runs
  * everything eagerly. */
 int bdb_set_graphs(bdb_system* s, int mode);
