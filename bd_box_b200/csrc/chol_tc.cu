@@ -972,7 +972,8 @@ __device__ __forceinline__ void cluster_sync_all()
 }
 
 // 2-D load into this CTA's shared memory whose completion is counted on the
-// pair leader's barrier (cluster address `bar`); no multicast
+// pair leader's barrier (cluster address `bar`); the data lands in this
+// CTA's shared memory only
 __device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
 {
     asm volatile(
