@@ -205,6 +205,22 @@ def peaks():
     return 6650.0, 1590.0, 1400.0, "fallback"
 
 
+def profile_value(name: str, key: str):
+    """A figure recorded in a committed ncu summary (profiles/<name>.md,
+    line '<key>: X'), or None."""
+    p = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for ln in f:
+            if ln.startswith(key + ":"):
+                try:
+                    return float(ln.split(":", 1)[1])
+                except ValueError:
+                    return None
+    return None
+
+
 def profile_traffic(name: str):
     """dram bytes per launch of the dominant kernel from the committed ncu
     summary (profiles/<name>.md, line 'traffic_bytes_per_launch: X')."""
@@ -339,7 +355,14 @@ def run_ours(args):
                                              "timed_ms": ms,
                                              "ok": refresh_ms * refreshes_timed <= ms},
                 "share_of_step_time": refresh_ms * refreshes_timed / ms,
-                "autotuned_chain_sms": sysm.factor_tuning()}
+                "autotuned_chain_sms": sysm.factor_tuning(),
+                # tensor-pipe utilisation of the bulk update (ncu, not live)
+                "tensor_pipe": {"kernel": "k_syrk_tc2",
+                                "active_pct_of_active_cycles": profile_value("k_syrk_tc2_n12288",
+                                                                             "tensor_pipe_active_pct"),
+                                "active_pct_of_elapsed": profile_value("k_syrk_tc2_n12288",
+                                                                       "tensor_pipe_elapsed_pct"),
+                                "source": "profiles/k_syrk_tc2_n12288.md (one ncu capture)"}}
         # diagnostic split from the profiled pass (events around every phase
         # and kernel, eager launches): not the timed configuration
         roof["profiled_pass"] = {
