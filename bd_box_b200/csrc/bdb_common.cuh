@@ -128,6 +128,7 @@ struct bdb_system {
     bdb::DevBuf<double> scal;                  // device scalars (eps, beta, ...)
     bdb::DevBuf<bdb::TileJob> jobs;
     bdb::DevBuf<int> tea_next;                 // job counter of the persistent TEA pair kernel
+    bdb::DevBuf<float> pscale;                 // mixed Cholesky: FP16 panel scale and 1/scale^2
     bdb::DevBuf<unsigned char> tea_meta;       // TEA segment table + job offsets
     int n_jobs = 0;
     int tea_tile = 32;                         // TEA tile edge (16 or 32 beads)

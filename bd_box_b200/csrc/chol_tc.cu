@@ -38,6 +38,8 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 
 #include "bdb_common.cuh"
@@ -46,10 +48,13 @@
 namespace bdb {
 
 static constexpr int PW = 128;                    // super-panel width = tile size
-static constexpr int KC = 32;                     // K columns per TMA box (128 B of FP32)
-static constexpr int NCHUNK = PW / KC;            // 4
+static constexpr int KC = 32;                     // FP32 columns of a box of the C update (128 B)
+static constexpr int KCP = 64;                    // panel K columns per TMA box (128 B of FP16)
+static constexpr int NCHUNK = PW / KCP;           // 2 boxes per panel
+static constexpr int KSTEPS = KCP / 16;           // MMA k-steps per box (K = 16 for kind::f16)
 static constexpr int STAGES = 3;
-static constexpr int BOX_BYTES = PW * KC * 4;     // 16 KB
+static constexpr int BOX_BYTES = PW * KC * 4;     // 16 KB: a C box, and a panel box (PW x KCP x 2 B)
+static_assert(PW * KCP * 2 == BOX_BYTES, "panel and C boxes have the same size");
 static constexpr int STAGE_BYTES = 4 * BOX_BYTES; // A_hi, A_lo, B_hi, B_lo
 static constexpr int C_BOXES = 2;                 // staging ring of 128x32 boxes for the C update
 static constexpr int SYRK_SMEM = STAGES * STAGE_BYTES + C_BOXES * BOX_BYTES + 1024;
@@ -108,19 +113,19 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
     return d;
 }
 
-// instruction descriptor: D=F32, A=B=TF32, both K-major, N=128, M=128
-__host__ __device__ constexpr uint32_t idesc_tf32_128x128()
+// instruction descriptor: D=F32, A=B=F16, both K-major, N=128, M=128
+__host__ __device__ constexpr uint32_t idesc_f16_128x128()
 {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+    return (1u << 4) | (0u << 7) | (0u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate)
+__device__ __forceinline__ void umma_f16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
@@ -164,7 +169,18 @@ __device__ __forceinline__ void tile_of_mode(int t, int mode, int& ti, int& tj)
     }
 }
 
-__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+// the mixed path's panel operands: x = (hi + lo) / scale with hi and lo in
+// FP16 (11 significant bits each, 22 together: the accuracy class of a
+// TF32 hi/lo split, at twice the tensor rate and half the bytes). scale is
+// a power of two chosen per factorisation from D's largest diagonal entry
+// (|L_ij| <= sqrt(D_ii)), so that every entry stays in FP16's normal range
+// where it matters; the products are unscaled exactly in the epilogue.
+__device__ __forceinline__ void f16_split(float x, float scale, __half& hi, __half& lo)
+{
+    const float xs = x * scale;
+    hi = __float2half_rn(xs);
+    lo = __float2half_rn(xs - __half2float(hi));
+}
 
 // ------------------------------------------------------------ FP64 panel
 
@@ -624,7 +640,8 @@ __device__ __forceinline__ double c2a(double c0, double c1, int h, int fr, int f
 template <typename T>
 __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, int npad, int P, int unit0, int units,
                                                           const double* __restrict__ Lf, float* __restrict__ Lhi,
-                                                          float* __restrict__ Llo, unsigned* __restrict__ status)
+                                                          float* __restrict__ Llo, unsigned* __restrict__ status,
+                                                          const float* __restrict__ pscale)
 {
     {
         uint32_t dyn;
@@ -681,10 +698,12 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, 
             const int col = 8 * n + 2 * fq;
             if constexpr (sizeof(T) == 4) {
                 const float o0 = (float)x0, o1 = (float)x1;
-                const float h0 = tf32_hi(o0), h1 = tf32_hi(o1);
                 *reinterpret_cast<float2*>(M + row * npad + base + col) = make_float2(o0, o1);
-                *reinterpret_cast<float2*>(Lhi + row * PW + col) = make_float2(h0, h1);
-                *reinterpret_cast<float2*>(Llo + row * PW + col) = make_float2(o0 - h0, o1 - h1);
+                __half2 h, l;
+                f16_split(o0, pscale[0], h.x, l.x);
+                f16_split(o1, pscale[0], h.y, l.y);
+                *reinterpret_cast<__half2*>(reinterpret_cast<__half*>(Lhi) + row * PW + col) = h;
+                *reinterpret_cast<__half2*>(reinterpret_cast<__half*>(Llo) + row * PW + col) = l;
             } else {
                 st_pair(M + row * npad + base + col, x0, x1);
                 // the FP64 panel in k_syrk64's fragment order: within each
@@ -723,7 +742,7 @@ __device__ __forceinline__ float4* c_chunk(unsigned char* cbuf, int cc, int r, i
 __global__ void __launch_bounds__(192, 1)
 k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
           const __grid_constant__ CUtensorMap map_c, int t0, int ntiles, int mode, unsigned* __restrict__ status,
-          uint32_t wlim)
+          uint32_t wlim, const float* __restrict__ pscale)
 {
     {
         uint32_t dyn;
@@ -784,10 +803,10 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                     const uint32_t st = sbase + s * STAGE_BYTES;
                     const uint32_t fb = smem_u32(&bars.full[s]);
                     mbar_expect_tx(fb, STAGE_BYTES);
-                    tma_load_2d(st, &map_hi, kc * KC, ra, fb);
-                    tma_load_2d(st + BOX_BYTES, &map_lo, kc * KC, ra, fb);
-                    tma_load_2d(st + 2 * BOX_BYTES, &map_hi, kc * KC, rb, fb);
-                    tma_load_2d(st + 3 * BOX_BYTES, &map_lo, kc * KC, rb, fb);
+                    tma_load_2d(st, &map_hi, kc * KCP, ra, fb);
+                    tma_load_2d(st + BOX_BYTES, &map_lo, kc * KCP, ra, fb);
+                    tma_load_2d(st + 2 * BOX_BYTES, &map_hi, kc * KCP, rb, fb);
+                    tma_load_2d(st + 3 * BOX_BYTES, &map_lo, kc * KCP, rb, fb);
                 }
             }
             if (abort_flag) {
@@ -801,7 +820,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
     } else if (warp == 1) {
         if (lane == 0) {
             // MMA issuer
-            const uint32_t idesc = idesc_tf32_128x128();
+            const uint32_t idesc = idesc_f16_128x128();
             uint32_t g = 0, tl = 0;
             for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++tl) {
                 const uint32_t b = tl & 1;
@@ -819,12 +838,12 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                     const uint32_t ah = sbase + s * STAGE_BYTES, al = ah + BOX_BYTES;
                     const uint32_t bh = ah + 2 * BOX_BYTES, bl = ah + 3 * BOX_BYTES;
 #pragma unroll
-                    for (int ks = 0; ks < KC / 8; ++ks) {
-                        const uint32_t off = ks * 32;
-                        umma_tf32(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc,
-                                  (kc | ks) ? 1u : 0u);
-                        umma_tf32(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
-                        umma_tf32(acc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
+                    for (int ks = 0; ks < KSTEPS; ++ks) {
+                        const uint32_t off = ks * 32;   // 16 FP16 of K
+                        umma_f16(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc,
+                                 (kc | ks) ? 1u : 0u);
+                        umma_f16(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
+                        umma_f16(acc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
                     }
                     umma_commit(smem_u32(&bars.empty[s]));
                 }
@@ -847,6 +866,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
         // receives -0.0, which leaves every value as it is.
         const int quarter = warp & 3;
         const int rl = 32 * quarter + lane;   // row inside the tile
+        const float is2 = pscale[1];         // 1 / scale^2: the panels' FP16 scaling undone, exactly
         uint32_t tl = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
             int ti, tj;
@@ -886,10 +906,10 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                 for (int j = 0; j < 8; ++j) {
                     const int c = 32 * cc + 4 * j;   // column inside the tile
                     float4 d;
-                    d.x = (!diag || c <= rl) ? -__uint_as_float(v[4 * j]) : -0.0f;
-                    d.y = (!diag || c + 1 <= rl) ? -__uint_as_float(v[4 * j + 1]) : -0.0f;
-                    d.z = (!diag || c + 2 <= rl) ? -__uint_as_float(v[4 * j + 2]) : -0.0f;
-                    d.w = (!diag || c + 3 <= rl) ? -__uint_as_float(v[4 * j + 3]) : -0.0f;
+                    d.x = (!diag || c <= rl) ? -is2 * __uint_as_float(v[4 * j]) : -0.0f;
+                    d.y = (!diag || c + 1 <= rl) ? -is2 * __uint_as_float(v[4 * j + 1]) : -0.0f;
+                    d.z = (!diag || c + 2 <= rl) ? -is2 * __uint_as_float(v[4 * j + 2]) : -0.0f;
+                    d.w = (!diag || c + 3 <= rl) ? -is2 * __uint_as_float(v[4 * j + 3]) : -0.0f;
                     *c_chunk(cbuf, cc % C_BOXES, rl, j) = d;
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -930,18 +950,18 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
 // either CTA stops both. With npan = 2 the block takes the updates of two
 // panels at once (K = 256: the second panel's maps continue the K loop), so
 // C is read and written once for both.
-__host__ __device__ constexpr uint32_t idesc_tf32_256x256()
+__host__ __device__ constexpr uint32_t idesc_f16_256x256()
 {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
+    return (1u << 4) | (0u << 7) | (0u << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_tf32_pair(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                               uint32_t accumulate)
+__device__ __forceinline__ void umma_f16_pair(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                              uint32_t accumulate)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
@@ -1001,7 +1021,7 @@ __global__ void __launch_bounds__(192, 1)
 k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
            const __grid_constant__ CUtensorMap map_hi2, const __grid_constant__ CUtensorMap map_lo2,
            const __grid_constant__ CUtensorMap map_c, int t0, int c0, int cols, int npan, unsigned* __restrict__ status,
-           uint32_t wlim)
+           uint32_t wlim, const float* __restrict__ pscale)
 {
     {
         uint32_t dyn, ncta;
@@ -1083,7 +1103,7 @@ k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ C
                     const uint32_t fb = full0 + s * sizeof(uint64_t);
                     const CUtensorMap* mh = kc < NCHUNK ? &map_hi : &map_hi2;
                     const CUtensorMap* ml = kc < NCHUNK ? &map_lo : &map_lo2;
-                    const int x = (kc % NCHUNK) * KC;
+                    const int x = (kc % NCHUNK) * KCP;
                     if (leader) mbar_expect_tx(smem_u32(&bars.full[s]), 2 * STAGE_BYTES);
                     tma_load_2d_pair(st, mh, x, ra, fb);
                     tma_load_2d_pair(st + BOX_BYTES, ml, x, ra, fb);
@@ -1106,7 +1126,7 @@ k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ C
     } else if (warp == 1) {
         if (lane == 0 && leader) {
             // the pair's MMA issuer
-            const uint32_t idesc = idesc_tf32_256x256();
+            const uint32_t idesc = idesc_f16_256x256();
             uint32_t g = 0, tl = 0;
             for (int t = cid; t < nblocks && !abort_flag; t += ncl, ++tl) {
                 const uint32_t b = tl & 1;
@@ -1127,12 +1147,12 @@ k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ C
                     const uint32_t ah = sbase + s * STAGE_BYTES, al = ah + BOX_BYTES;
                     const uint32_t bh = ah + 2 * BOX_BYTES, bl = ah + 3 * BOX_BYTES;
 #pragma unroll
-                    for (int ks = 0; ks < KC / 8; ++ks) {
-                        const uint32_t off = ks * 32;
-                        umma_tf32_pair(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc,
-                                       (kc | ks) ? 1u : 0u);
-                        umma_tf32_pair(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
-                        umma_tf32_pair(acc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
+                    for (int ks = 0; ks < KSTEPS; ++ks) {
+                        const uint32_t off = ks * 32;   // 16 FP16 of K
+                        umma_f16_pair(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc,
+                                      (kc | ks) ? 1u : 0u);
+                        umma_f16_pair(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
+                        umma_f16_pair(acc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
                     }
                     umma_commit_pair(smem_u32(&bars.empty[s]));
                 }
@@ -1159,6 +1179,7 @@ k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ C
         // the buffer's release is counted alike) but not written
         const int quarter = warp & 3;
         const int rl = 32 * quarter + lane;
+        const float is2 = pscale[1];   // 1 / scale^2: the panels' FP16 scaling undone, exactly
         const uint32_t accempty0 = cluster_addr(smem_u32(&bars.accempty[0]), 0);
         uint32_t tl = 0;
         for (int t = cid; t < nblocks; t += ncl, ++tl) {
@@ -1209,10 +1230,10 @@ k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ C
                     for (int j = 0; j < 8; ++j) {
                         const int c = 32 * cc + 4 * j;
                         float4 d;
-                        d.x = (!diag || c <= rl) ? -__uint_as_float(v[4 * j]) : -0.0f;
-                        d.y = (!diag || c + 1 <= rl) ? -__uint_as_float(v[4 * j + 1]) : -0.0f;
-                        d.z = (!diag || c + 2 <= rl) ? -__uint_as_float(v[4 * j + 2]) : -0.0f;
-                        d.w = (!diag || c + 3 <= rl) ? -__uint_as_float(v[4 * j + 3]) : -0.0f;
+                        d.x = (!diag || c <= rl) ? -is2 * __uint_as_float(v[4 * j]) : -0.0f;
+                        d.y = (!diag || c + 1 <= rl) ? -is2 * __uint_as_float(v[4 * j + 1]) : -0.0f;
+                        d.z = (!diag || c + 2 <= rl) ? -is2 * __uint_as_float(v[4 * j + 2]) : -0.0f;
+                        d.w = (!diag || c + 3 <= rl) ? -is2 * __uint_as_float(v[4 * j + 3]) : -0.0f;
                         *c_chunk(cbuf, cc % C_BOXES, rl, j) = d;
                     }
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1378,16 +1399,20 @@ __global__ void __launch_bounds__(S64_THREADS, 1) k_syrk64(double* __restrict__ 
 // ---------------------------------------------------------------- host side
 
 // row-major FP32 [rows][cols] buffer, boxes of 128 rows x 32 columns
-static int make_panel_map(float* buf, int rows, CUtensorMap* map, int cols = PW)
+// (f16: an FP16 panel buffer [rows][128], boxes of 128 rows x 64 columns;
+// otherwise FP32, boxes of 128 rows x 32 columns; 128 bytes a box row)
+static int make_panel_map(void* buf, int rows, CUtensorMap* map, int cols = PW, bool f16 = false)
 {
     auto enc = get_encode();
     if (!enc) return fail(BDB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     if (reinterpret_cast<uintptr_t>(buf) % 16) return fail(BDB_ERR_ARG, "panel buffer not 16-byte aligned");
+    const size_t es = f16 ? 2 : 4;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)cols * sizeof(float)};
-    cuuint32_t box[2] = {KC, PW};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * es};
+    cuuint32_t box[2] = {(cuuint32_t)(f16 ? KCP : KC), PW};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, buf, dims, strides, box, estr,
+    CUresult r = enc(map, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, buf, dims,
+                     strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(BDB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
@@ -1423,15 +1448,16 @@ static int tc_setup(bdb_system* s)
         float *hi, *lo;
         double* lkk;
         panel_ptrs(s, set, &hi, &lo, &lkk);
-        int rc = make_panel_map(hi, s->npad, &maps[2 * set]);
+        int rc = make_panel_map(hi, s->npad, &maps[2 * set], PW, true);
         if (rc) return rc;
-        rc = make_panel_map(lo, s->npad, &maps[2 * set + 1]);
+        rc = make_panel_map(lo, s->npad, &maps[2 * set + 1], PW, true);
         if (rc) return rc;
     }
     int rc = make_panel_map(s->M32.p, s->npad, &maps[2 * PANEL_SETS], s->npad);
     if (rc) return rc;
     BDB_CUDA(cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_syrk_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
+    if (s->pscale.alloc(2)) return BDB_ERR_NOMEM;
     BDB_CUDA(cudaFuncSetAttribute(k_potrf128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, POTRF_SMEM));
     BDB_CUDA(cudaFuncSetAttribute(k_trsm128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRSM_SMEM));
     int dev = 0, sms = 148;
@@ -1457,7 +1483,8 @@ static cudaError_t launch_syrk(bdb_system* s, int grid, cudaStream_t st, const C
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_syrk_tc, hi, lo, c, t0, ntiles, mode, s->status.p, (uint32_t)s->wait_limit);
+    return cudaLaunchKernelEx(&cfg, k_syrk_tc, hi, lo, c, t0, ntiles, mode, s->status.p, (uint32_t)s->wait_limit,
+                              (const float*)s->pscale.p);
 }
 
 // k_syrk_tc2 on `clusters` CTA pairs over block columns c0 .. cols-1 of
@@ -1483,7 +1510,7 @@ static cudaError_t launch_syrk_pair(bdb_system* s, int clusters, cudaStream_t st
     cfg.attrs = at;
     cfg.numAttrs = 2;
     return cudaLaunchKernelEx(&cfg, k_syrk_tc2, hi, lo, hi2, lo2, c, t0, c0, cols, npan, s->status.p,
-                              (uint32_t)s->wait_limit);
+                              (uint32_t)s->wait_limit, (const float*)s->pscale.p);
 }
 
 // k_potrf128 the same way, behind the update of its block column
@@ -1542,6 +1569,7 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
     // pipes
     const int side = std::max(1, chain - 5);
     constexpr bool kPairs = sizeof(T) == 4;   // two panels per pass over C (mixed path)
+    const float* pscale = sizeof(T) == 4 ? s->pscale.p : nullptr;   // FP16 panel scale (mixed path)
     float *hi, *lo;
     double* lkk;
     panel_ptrs(s, 0, &hi, &lo, &lkk);
@@ -1560,7 +1588,7 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
         BDB_CUDA(cudaStreamWaitEvent(st3, ev_potrf, 0));
         if (units_rest > 0) {
             k_trsm128<T><<<std::min(2 * side, (units_rest + per_cta - 1) / per_cta), TRSM_THREADS, TRSM_SMEM, st3>>>(
-                M, s->npad, P, units_top, units_rest, lkk, hi, lo, s->status.p);
+                M, s->npad, P, units_top, units_rest, lkk, hi, lo, s->status.p, pscale);
             BDB_CUDA(cudaGetLastError());
             s->launches += 1;
         }
@@ -1574,7 +1602,7 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
         // block row P+1: its 16 units on 4 CTAs, so that each unit's warp
         // has an SM sub-partition (and its FP64 pipe) to itself
         k_trsm128<T><<<units_top / 4, TRSM_THREADS, TRSM_SMEM, st>>>(M, s->npad, P, 0, units_top, lkk, hi, lo,
-                                                                   s->status.p);
+                                                                   s->status.p, pscale);
         phase_mark_on(s, P_TRSM, st);
         BDB_CUDA(cudaGetLastError());
         BDB_CUDA(cudaEventRecord(ev_top, st));
@@ -1632,10 +1660,37 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
     return BDB_OK;
 }
 
+// The FP16 panel scale of a factorisation, from D's diagonal (dD): 2^e with
+// the largest sqrt(D_ii) -- a bound of every |L_ij| -- just below 2^14;
+// pscale[0] = 2^e, pscale[1] = 2^-2e. One CTA.
+__global__ void k_panel_scale(const double* __restrict__ dD, int n3, float* __restrict__ pscale)
+{
+    __shared__ double red[32];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) m = fmax(m, dD[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+        int e = 0, sh = 0;
+        if (m > 0.0 && isfinite(m)) {
+            frexp(sqrt(m), &e);   // sqrt(m) < 2^e
+            sh = 14 - e;
+        }
+        sh = max(-60, min(60, sh));
+        pscale[0] = ldexpf(1.0f, sh);
+        pscale[1] = ldexpf(1.0f, -2 * sh);
+    }
+}
+
 int factor_mixed_tc(bdb_system* s)
 {
     int rc = tc_setup(s);
     if (rc) return rc;
+    k_panel_scale<<<1, 1024, 0, s->stream>>>(s->dD.p, s->n3, s->pscale.p);
+    BDB_CUDA(cudaGetLastError());
+    s->launches += 1;
     const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(s->tc_map);
     const int nt = s->npad / PW;
     return factor_schedule(s, s->M32.p, [&](cudaStream_t stream, int grid, int set, int set_prev, int t0, int ntiles,
