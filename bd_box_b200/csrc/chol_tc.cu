@@ -1,35 +1,39 @@
-// Mixed-precision blocked Cholesky for sm_100a: FP64 panels, 3xTF32
-// trailing updates on the 5th-generation tensor cores (tcgen05).
+// Mixed-precision blocked Cholesky for sm_100a: FP64 panels, FP16-split
+// trailing updates on the 5th-generation tensor cores (tcgen05), and the
+// plain FP64 path's updates on the FP64 tensor instruction (DMMA).
 //
-// M is FP32 (lower triangle: the factor, upper: D, never written here).
-// Super-panel P covers columns p0 = 128P .. p0+127:
+// M is FP32 (lower triangle: the factor, upper: D, never written here) or
+// FP64 on the FP64 path. Super-panel P covers columns p0 = 128P .. p0+127:
 //   k_potrf128  one CTA factors the 128x128 diagonal block in FP64,
-//               right-looking by 8 columns with the 8x8 pivot blocks factored
-//               in registers by one thread while the others update; L_PP goes
-//               to M (FP32), and its inverse W = L_PP^-1 (FP64, blocked
-//               forward substitution) transposed to a scratch block;
-//   k_trsm128   slabs of 64 rows below the block solve X L_PP^T = A in FP64
-//               as the product X = A W^T (no sequential dependency); each row
-//               goes to M and its TF32 split L = L_hi + L_lo (L_hi: low 13
-//               mantissa bits cleared, exactly TF32; L_lo = L - L_hi) to two
-//               panel buffers;
-//   k_syrk_tc   C -= L_i L_j^T over all 128x128 tiles ti >= tj > P of the
-//               trailing lower triangle, with
-//               L_i L_j^T ~= Lhi_i Lhi_j^T + Lhi_i Llo_j^T + Llo_i Lhi_j^T
-//               (the dropped lo*lo term is ~2^-22 relative: FP32 accuracy).
+//               right-looking by 8 columns (each 8x8 pivot block factored by
+//               one thread while the other warps solve and update), and
+//               hands L_PP and the inverses W_kk of its 8x8 diagonal tiles on
+//               to the panel solve;
+//   k_trsm128   the rows below, X L_PP^T = A, by blocked forward substitution
+//               in FP64 (one warp per 8 rows, DMMA); each row goes to M and,
+//               on the mixed path, as an FP16 hi/lo pair of the row scaled
+//               by a power of two (k_panel_scale) to two panel buffers;
+//   k_syrk_tc   C -= L_i L_j^T for single 128x128 tiles and block columns
+//               (the diagonal tile, the next two block columns), and
+//   k_syrk_tc2  for 256x256 blocks on CTA pairs (the columns beyond), two
+//               panels per pass over C, with
+//               L_i L_j^T ~= (Lhi_i Lhi_j^T + Lhi_i Llo_j^T + Llo_i Lhi_j^T)
+//                            / scale^2
+//               (the dropped lo*lo term is ~2^-22 relative: FP32 accuracy);
+//   k_syrk64    the FP64 path's updates on mma.sync.m8n8k4.f64.
 //
-// k_syrk_tc is persistent (one CTA per SM, static round-robin over tiles)
-// and warp-specialised:
-//   warp 0    TMA producer: per K chunk of 32 columns, four 128x32 FP32 boxes
-//             (A_hi, A_lo, B_hi, B_lo, 128-byte swizzle) into a 3-stage ring;
-//   warp 1    MMA issuer: tcgen05.mma.kind::tf32 M=128 N=128 K=8, three per
-//             K step, into one of two TMEM accumulators (128 columns each);
-//             tcgen05.commit frees a ring stage / publishes an accumulator;
+// The update kernels are persistent and warp-specialised:
+//   warp 0    TMA producer: per K chunk of 64 columns, four 128x64 FP16
+//             boxes (A_hi, A_lo, B_hi, B_lo, 128-byte swizzle) into a
+//             3-stage ring;
+//   warp 1    MMA issuer: tcgen05.mma.kind::f16 (K=16), three per K step,
+//             into one of two TMEM accumulators; tcgen05.commit frees a ring
+//             stage / publishes an accumulator;
 //   warps 2-5 epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
-//             lanes 32(w%4)..), hand the accumulator back, then -acc per
-//             128x32 box into a 2-box shared-memory ring and a TMA
-//             reduce-add into C (lower triangle only on diagonal tiles);
-//             C is never loaded.
+//             lanes 32(w%4)..), hand the accumulator back, then
+//             -acc / scale^2 per 128x32 box into a 2-box shared-memory ring
+//             and a TMA reduce-add into C (lower triangle only on diagonal
+//             tiles); C is never loaded.
 // The epilogue of tile t overlaps the MMAs of tile t+1 and the loads of the
 // tiles after it. Every mbarrier wait is bounded; a time-out sets
 // ST_TIMEOUT and a shared abort flag that stops all roles, and the CTA frees

@@ -208,14 +208,14 @@ def test_philox_moments(chain_none):
 
 
 def test_tensor_core_factor_large(deck_dir):
-    """3xTF32 tcgen05 trailing updates over many tiles (3N = 2100, 17 super
-    panels): ||L L^T - D||/||D|| within the stated 1e-5, and of the order of
-    the SIMT FP32 factor of the same matrix. The tensor-core factor carries
-    more rounding than the SIMT one (1.5e-6 against 9e-8 here): its FP32
-    accumulators in tensor memory sum 3 x 256 products per pass over C (two
-    panels at once) before one IEEE add into C, where the SIMT update rounds
-    every FMA to nearest. A wrong or missing update gives errors of order 1,
-    far above the factor of 30 allowed here."""
+    """tcgen05 trailing updates on FP16 hi/lo panels over many tiles (3N =
+    2100, 17 super panels): ||L L^T - D||/||D|| within the stated 1e-5, and
+    of the order of the SIMT FP32 factor of the same matrix. The tensor-core
+    factor carries more rounding than the SIMT one (5.1e-7 against 9.0e-8
+    measured here): its FP32 accumulators in tensor memory sum 3 x 256
+    products per pass over C (two panels at once) before one IEEE add into
+    C, where the SIMT update rounds every FMA to nearest. A wrong or missing
+    update gives errors of order 1, far above the factor of 10 allowed."""
     deck = decks.read_deck(decks.write_chain_deck(deck_dir, "big_chol", 700, seed=31, hydro="cholesky"))
     s = engine.System(deck, precision=engine.PREC_MIXED)
     err_tc = s.factor_error()
@@ -225,7 +225,7 @@ def test_tensor_core_factor_large(deck_dir):
     finally:
         del os.environ["BDB_NO_TC"]
     assert err_tc <= 1e-5, err_tc
-    assert err_tc <= 30 * err_simt + 1e-7, (err_tc, err_simt)
+    assert err_tc <= 10 * err_simt + 1e-7, (err_tc, err_simt)
 
 
 @pytest.mark.parametrize("name", ["chain_tea", "susp"])
