@@ -55,7 +55,7 @@ enum { BDB_EWALD_BEENAKKER = 0, BDB_EWALD_SMITH = 1 };
 /* arithmetic of the diffusion part of the step */
 enum {
     BDB_PREC_FP64 = 0,   /* everything in FP64 (the plain GPU path) */
-    BDB_PREC_MIXED = 1   /* FP32 tensor and stored D/L, 3xTF32 tcgen05 Cholesky
+    BDB_PREC_MIXED = 1   /* FP32 tensor and stored D/L, FP16-split tcgen05 Cholesky
                             updates with FP64 diagonal tiles, FP64 sums */
 };
 
