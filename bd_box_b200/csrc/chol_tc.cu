@@ -229,24 +229,30 @@ __device__ __forceinline__ double rcp_nr(double x)
     return fma(q, fma(-x, q, 1.0), q);
 }
 
-// Factor the 8x8 block in Dg ([8][9], lower triangle) in registers by one
-// thread: L_kk to the lower triangle of Dg, 1/L_jj to rd. The elimination
-// runs on the unscaled Schur complements with q_j = 1/a_jj: the next pivot
+// Factor the 8x8 block in Dg ([8][9], lower triangle) in registers and
+// invert the factor; every lane of the pivot warp runs the whole
+// factorisation (nothing passes between lanes), lane c (c < 8) returns
+// column c of L_kk and of W_kk = L_kk^-1. The elimination runs on the
+// unscaled Schur complements with q_j = 1/a_jj: the next pivot
 // a_{j+1,j+1} -= a_{j+1,j}^2 q_j first (the square is formed while q_j is
 // computed, so one reciprocal and one FMA separate two pivots), then the
 // other entries as a_ic -= a_ij (a_cj q_j), one FMA each after the 7-j
-// scaled column entries. The columns are scaled by 1/sqrt(a_jj) at the end.
-// With kFull (the plain FP64 path) every reciprocal and reciprocal square
-// root takes a second Newton step, which brings it to FP64 rounding.
+// scaled column entries. The columns are scaled by r_j = 1/sqrt(a_jj) at
+// the end, and column c of W follows by right-looking forward
+// substitution: w_m = acc_m r_m, then acc_i -= L_im w_m for i > m. It is
+// one straight-line block, so the substitution fills the latency of the
+// reciprocal chain. With kFull (the plain FP64 path) every reciprocal and
+// reciprocal square root takes a second Newton step, which brings it to
+// FP64 rounding.
 template <bool kFull>
-__device__ __forceinline__ bool pivot8(double* Dg, double* rd)
+__device__ __forceinline__ bool pivot8_inv(const double* Dg, int c, double (&lcol)[8], double (&wcol)[8])
 {
     double a[8][8];
     bool ok = true;
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-        for (int c = 0; c <= r; ++c) a[r][c] = Dg[r * 9 + c];
+        for (int k = 0; k <= r; ++k) a[r][k] = Dg[r * 9 + k];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         if (!(a[j][j] > 0.0)) ok = false;
@@ -255,21 +261,38 @@ __device__ __forceinline__ bool pivot8(double* Dg, double* rd)
         if (j + 1 < 8) a[j + 1][j + 1] = fma(-(a[j + 1][j] * a[j + 1][j]), q, a[j + 1][j + 1]);
         double t[8];
 #pragma unroll
-        for (int c = j + 1; c < 8; ++c) t[c] = a[c][j] * q;
+        for (int k = j + 1; k < 8; ++k) t[k] = a[k][j] * q;
 #pragma unroll
         for (int r = j + 1; r < 8; ++r)
 #pragma unroll
-            for (int c = j + 1; c <= r; ++c)
-                if (r != j + 1) a[r][c] = fma(-a[r][j], t[c], a[r][c]);
+            for (int k = j + 1; k <= r; ++k)
+                if (r != j + 1) a[r][k] = fma(-a[r][j], t[k], a[r][k]);
     }
+    double rj[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         double r = rsqrt_nr(a[j][j]);
         if (kFull) r = r * (1.5 - 0.5 * a[j][j] * r * r);
-        rd[j] = r;
-        Dg[j * 9 + j] = a[j][j] * r;
+        rj[j] = r;
 #pragma unroll
-        for (int i = j + 1; i < 8; ++i) Dg[i * 9 + j] = a[i][j] * r;
+        for (int i = j; i < 8; ++i) a[i][j] *= r;
+    }
+    double acc[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i] = i == c ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        wcol[m] = m >= c ? acc[m] * rj[m] : 0.0;
+#pragma unroll
+        for (int i = m + 1; i < 8; ++i) acc[i] = fma(-a[i][m], wcol[m], acc[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        double l = 0.0;
+#pragma unroll
+        for (int k = 0; k <= i; ++k)
+            if (k == c) l = a[i][k];
+        lcol[i] = l;
     }
     return ok;
 }
@@ -295,7 +318,7 @@ static constexpr int NT = PW / 8;                  // 16 row groups of 8 rows
 static constexpr int NTILE = NT * (NT + 1) / 2;    // 136 tiles in the lower triangle
 // Lt tiles, W_kk, the 8x8 block being factored [8][9], 1/L_jj, and one
 // hand-over slot of two tiles per step
-static constexpr int POTRF_SMEM = (NTILE * 64 + NT * 64 + 80 + 8 + NT * 128) * 8;
+static constexpr int POTRF_SMEM = (NTILE * 64 + NT * 64 + 80 + NT * 128) * 8;
 // factor hand-off to the panel solve: L_PP tiles then the W_kk, A order
 static constexpr int PANEL_FAC = (NTILE + NT) * 64;
 
@@ -357,8 +380,8 @@ __device__ __forceinline__ void solve_tile(double c0, double c1, const double* W
 // columns with the trailing matrix in registers: the warp owning row group g
 // keeps its tiles (g, n), n <= g, as DMMA accumulators. No CTA-wide barrier
 // orders the steps; per-step mbarriers carry exactly what each warp needs:
-//   pivot warp, step k: factor tile (k, k) (pivot8, one thread) and invert
-//     it (lanes 0-7) -> publish W_kk; take row group k+1's last two tiles
+//   pivot warp, step k: factor tile (k, k) and invert it (pivot8_inv, every
+//     lane the whole factorisation) -> publish W_kk; take row group k+1's last two tiles
 //     (k+1, k) and (k+1, k+1), handed over through column k-2 together with
 //     L[k+1][k-1], and apply column k-1 to them; solve L[k+1][k] = C[k+1][k]
 //     W_kk^T -> publish; update tile (k+1, k+1) with it and go on to pivot
@@ -384,8 +407,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
     double* Lt = sh;                       // [NTILE][64] A order
     double* Wa = Lt + NTILE * 64;          // [NT][64] W_kk in A order
     double* Dg = Wa + NT * 64;             // [8][9] diagonal block being factored
-    double* rd = Dg + 80;                  // [8] 1/L_jj of that block
-    double* Hd = rd + 8;                   // [NT][2][64] hand-over slots (C layout)
+    double* Hd = Dg + 80;                  // [NT][2][64] hand-over slots (C layout)
     __shared__ PotrfBars bars;
     __shared__ int bad;
     __shared__ volatile int abort_flag;
@@ -439,38 +461,16 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
         }
         for (int k = 0; k < NT; ++k) {
             __syncwarp();
-            if (lane == 0 && !pivot8<sizeof(T) == 8>(Dg, rd)) bad = 1;
-            __syncwarp();
-            if (lane < 8) {
-                // column c of W_kk = L_kk^-1 by right-looking forward
-                // substitution: w_m = acc_m / L_mm, then acc_i -= L_im w_m for
-                // i > m, so only w_m -> acc_m+1 -> w_m+1 is sequential; L_kk
-                // and 1/L_jj are read first
-                const int c = lane;
-                double lk[8][8], r8[8], acc[8], w[8];
+            {
+                double lc[8], wc[8];
+                if (!pivot8_inv<sizeof(T) == 8>(Dg, lane & 7, lc, wc) && lane == 0) bad = 1;
+                if (lane < 8) {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    r8[i] = rd[i];
-#pragma unroll
-                    for (int m = 0; m <= i; ++m) lk[i][m] = Dg[i * 9 + m];
-                }
-#pragma unroll
-                for (int i = 0; i < 8; ++i) acc[i] = i == c ? 1.0 : 0.0;
-#pragma unroll
-                for (int m = 0; m < 8; ++m) {
-                    w[m] = m >= c ? acc[m] * r8[m] : 0.0;
-#pragma unroll
-                    for (int i = m + 1; i < 8; ++i) acc[i] = fma(-lk[i][m], w[m], acc[i]);
-                }
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    double l = 0.0;
-#pragma unroll
-                    for (int cc = 0; cc <= i; ++cc)
-                        if (cc == c) l = lk[i][cc];
-                    const int pa = apos(i, c);
-                    Wa[k * 64 + pa] = w[i];
-                    Lt[tix(k, k) * 64 + pa] = l;
+                    for (int i = 0; i < 8; ++i) {
+                        const int pa = apos(i, lane);
+                        Wa[k * 64 + pa] = wc[i];
+                        Lt[tix(k, k) * 64 + pa] = lc[i];
+                    }
                 }
             }
             mbar_arrive(smem_u32(&bars.w[k]));   // release: this lane's writes
@@ -655,7 +655,11 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, 
             return;
         }
     }
-    asm volatile("griddepcontrol.launch_dependents;");
+    // block row P+1 (unit0 = 0) releases its dependent, the chain's one-CTA
+    // update, at once; the rows below only as their warps finish, because
+    // theirs is the side stream's column update, a grid that would
+    // otherwise wait on the free SMs the chain needs while this runs
+    if (unit0 == 0) asm volatile("griddepcontrol.launch_dependents;");
     extern __shared__ double sh[];
     const double2* Ls = reinterpret_cast<const double2*>(sh);               // [NTILE][32] pairs
     const double2* Ws = reinterpret_cast<const double2*>(sh + NTILE * 64);  // [NT][32] pairs
@@ -727,6 +731,7 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, 
             }
         }
     }
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 // ------------------------------------------------------- tensor-core update
@@ -791,7 +796,14 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
     // stream: the set-up above overlaps its tail; nothing below may read or
     // write what it produces before this wait (a no-op for a plain launch)
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;");
+    // The chain's and the side stream's updates (modes 1 and 4) let their
+    // dependents launch at once (a one-CTA factorisation; a plain launch).
+    // A bulk update's dependent is the next bulk update, a full grid of CTAs
+    // that, launched early, would sit on every free SM in its
+    // griddepcontrol.wait for as long as this launch runs, SMs the chain
+    // needs meanwhile: bulk updates release it only once their last loads
+    // are issued (below).
+    if (mode == 1 || mode == 4) asm volatile("griddepcontrol.launch_dependents;");
 
     if (warp == 0) {
         if (lane == 0) {
@@ -813,6 +825,7 @@ k_syrk_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                     tma_load_2d(st + 3 * BOX_BYTES, &map_lo, kc * KCP, rb, fb);
                 }
             }
+            if (mode != 1 && mode != 4) asm volatile("griddepcontrol.launch_dependents;");
             if (abort_flag) {
                 // the loads still in flight (the last fill of each stage)
                 // must land before the CTA exits
@@ -1080,8 +1093,10 @@ k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ C
     cluster_sync_all();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_sh;
+    // a bulk update: its dependent (the next bulk update) is released only
+    // once this CTA's last loads are issued, so that its CTAs do not wait on
+    // SMs the chain needs for as long as this launch runs
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;");
 
     const int nb = (cols - c0 + 1) / 2;   // 256-wide block columns
     const int nblocks = nb * (nb + 1) / 2;
@@ -1119,6 +1134,7 @@ k_syrk_tc2(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ C
                     break;
                 }
             }
+            asm volatile("griddepcontrol.launch_dependents;");
             if (abort_flag && leader) {
                 // the loads still in flight (the last fill of each stage, both
                 // CTAs' bytes) land before the pair exits
@@ -1326,11 +1342,15 @@ __global__ void __launch_bounds__(S64_THREADS, 1) k_syrk64(double* __restrict__ 
     const int fr = lane >> 2, fq = lane & 3;
     const int wr = warp & 3, wc = warp >> 2;
     // a programmatic dependent of the previous kernel on the stream: nothing
-    // it produces is read before this
+    // it produces is read before this. Dependents launch at once after the
+    // chain's and the side stream's updates (modes 1, 4), after a bulk
+    // update only when each CTA starts its last tile (a bulk dependent
+    // launched early would hold free SMs in its wait)
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;");
+    if (mode == 1 || mode == 4) asm volatile("griddepcontrol.launch_dependents;");
     constexpr int NCH = PW / S64_KC;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (t + (int)gridDim.x >= ntiles) asm volatile("griddepcontrol.launch_dependents;");
         int ti, tj;
         tile_of_mode(t, mode, ti, tj);
         const int ra = (t0 + ti) * PW, rb = (t0 + tj) * PW;

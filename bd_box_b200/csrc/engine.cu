@@ -199,7 +199,11 @@ static int refresh_factor(bdb_system* s)
                 if (g) cudaGraphDestroy(g);
                 return rc ? rc : cuda_fail(e, "cudaStreamEndCapture");
             }
-            const cudaError_t ei = cudaGraphInstantiate(&s->refresh_graph, g, 0);
+            // the nodes keep the priorities of the streams they were captured
+            // from (chain high, side middle, bulk low); without this flag a
+            // replay runs every node at the priority of the launching stream
+            const cudaError_t ei =
+                cudaGraphInstantiate(&s->refresh_graph, g, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(g);
             if (ei != cudaSuccess) {
                 s->refresh_graph = nullptr;
@@ -300,7 +304,7 @@ static int step_body_graph(bdb_system* s, const double* dev_gauss)
             if (g) cudaGraphDestroy(g);
             return rc ? rc : cuda_fail(e, "cudaStreamEndCapture");
         }
-        const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
+        const cudaError_t ei = cudaGraphInstantiate(exec, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (ei != cudaSuccess) {
             *exec = nullptr;
