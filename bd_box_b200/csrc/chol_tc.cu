@@ -668,23 +668,18 @@ __global__ void __launch_bounds__(TRSM_THREADS, 1) k_trsm128(T* __restrict__ M, 
     const size_t base = (size_t)P * PW;
     // units unit0 .. unit0 + units - 1 of 8 rows below the block
     const size_t row0 = base + PW + (size_t)8 * unit0;
+    // block row P+1 is launched as a programmatic dependent of the diagonal
+    // block's factorisation (a no-op wait for the rows below, a plain
+    // launch): nothing is read before this
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     {
-        // the factor: a plain copy, loads batched ahead of stores
-        const double2* src = reinterpret_cast<const double2*>(Lf);
-        double2* dst = reinterpret_cast<double2*>(sh);
-        constexpr int NC = PANEL_FAC / 2;
-        constexpr int PER = (NC + TRSM_THREADS - 1) / TRSM_THREADS;   // 19
-        double2 w[PER];
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const int f = tid + TRSM_THREADS * k;
-            if (f < NC) w[k] = __ldg(src + f);
-        }
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const int f = tid + TRSM_THREADS * k;
-            if (f < NC) dst[f] = w[k];
-        }
+        // the factor, by asynchronous 16-byte copies (no register staging)
+        const char* src = reinterpret_cast<const char*>(Lf);
+        const uint32_t dst = smem_u32(sh);
+        for (int f = tid; f < PANEL_FAC / 2; f += TRSM_THREADS)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16 * f), "l"(src + 16 * (size_t)f)
+                         : "memory");
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
     const int slot = (warp >> 2) * 4 * gridDim.x + blockIdx.x * 4 + (warp & 3);
@@ -1554,6 +1549,26 @@ static cudaError_t launch_potrf(bdb_system* s, cudaStream_t st, T* M, int P, dou
     return cudaLaunchKernelEx(&cfg, k_potrf128<T>, M, s->npad, P, lkk, s->status.p, (uint32_t)s->wait_limit);
 }
 
+// block row P+1 of panel P's solve (k_trsm128, units 0..15 on 4 CTAs) as a
+// programmatic dependent of the diagonal block's factorisation, so that its
+// launch overlaps that kernel's tail
+template <typename T>
+static cudaError_t launch_trsm_top(bdb_system* s, cudaStream_t st, T* M, int P, int units, const double* lkk,
+                                   float* hi, float* lo, const float* pscale)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(units / 4);
+    cfg.blockDim = dim3(TRSM_THREADS);
+    cfg.dynamicSmemBytes = TRSM_SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_trsm128<T>, M, s->npad, P, 0, units, lkk, hi, lo, s->status.p, pscale);
+}
+
 // The factorisation schedule, on three streams. Panel P's trailing update
 // is split four ways: the diagonal tile of block column P+1 (A0), the rest
 // of that column (A1), block column P+2 (B) and block columns P+3 on (C);
@@ -1625,10 +1640,8 @@ static int factor_schedule(bdb_system* s, T* M, Update update)
         phase_mark_on(s, P_TRSM, st);
         // block row P+1: its 16 units on 4 CTAs, so that each unit's warp
         // has an SM sub-partition (and its FP64 pipe) to itself
-        k_trsm128<T><<<units_top / 4, TRSM_THREADS, TRSM_SMEM, st>>>(M, s->npad, P, 0, units_top, lkk, hi, lo,
-                                                                   s->status.p, pscale);
+        BDB_CUDA(launch_trsm_top(s, st, M, P, units_top, lkk, hi, lo, pscale));
         phase_mark_on(s, P_TRSM, st);
-        BDB_CUDA(cudaGetLastError());
         BDB_CUDA(cudaEventRecord(ev_top, st));
         // side: block column P+1 below its diagonal tile
         BDB_CUDA(cudaStreamWaitEvent(st3, ev_top, 0));

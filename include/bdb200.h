@@ -328,8 +328,9 @@ int bdb_set_wait_limit(bdb_system* s, long long tries);
 /* The third tunable site (no reference counterpart): how the mixed-precision
  * Cholesky splits the GPU. Its panel chain (panel solve, next block-column
  * update, next diagonal block) runs beside the bulk trailing updates, which
- * leave chain_sms SMs to it (16, 24, 32, 48 or 64 tried at the first refresh when
- * autotuning is on; 32 otherwise; 16 on the FP64 path, which is not tuned).
+ * leave chain_sms SMs to it (16, 24, 32, 40, 48, 56 or 64 tried at the first
+ * refresh when autotuning is on, each as a replayed refresh graph; 32
+ * otherwise; 16 on the FP64 path, which is not tuned).
  * bdb_set_factor_tuning pins it (0 keeps the value). */
 int bdb_get_factor_tuning(bdb_system* s, int* chain_sms);
 int bdb_set_factor_tuning(bdb_system* s, int chain_sms);
