@@ -624,10 +624,10 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
 // factor (76 KB) into shared memory once. The grid is persistent: unit u goes
 // to warp slot u mod (8 grid), slots ordered so that the first 4 grid slots
 // put one warp on every SM sub-partition, the next 4 grid a second one.
-// Writes the rows to M and, for the mixed path (T = float), their TF32
-// split L = L_hi + L_lo (L_hi: low 13 mantissa bits cleared, exactly TF32;
-// L_lo = L - L_hi) to the panel buffers; for the FP64 path (T = double) the
-// rows in FP64 to one panel buffer (Lhi, as doubles; Llo unused).
+// Writes the rows to M and, for the mixed path (T = float), their FP16
+// split L s = hi + lo (f16_split, s = pscale[0]) to the panel buffers; for
+// the FP64 path (T = double) the rows in FP64 to one panel buffer (Lhi, as
+// doubles; Llo unused).
 static constexpr int TRSM_THREADS = 256;
 static constexpr int TRSM_SMEM = PANEL_FAC * 8;
 
