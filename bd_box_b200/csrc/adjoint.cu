@@ -21,7 +21,7 @@
 //   formed with two blocked triangular solves (k_gemm_tn, k_trinv64).
 // The forward pass is recomputed from checkpoints every `checkpoint` steps.
 // Precision follows the system's: FP64 throughout for an FP64 system; for a
-// mixed-precision system (FP32 tensor, 3xTF32 Cholesky) the forward steps
+// mixed-precision system (FP32 tensor, FP16-split Cholesky) the forward steps
 // are the mixed path's, and the backward's O(n^3) part -- Phi(v X^T), the
 // two blocked triangular solves and their transposes -- runs in FP32 on its
 // FP32 factor, while the O(N^2) tile gradients and force products keep FP64

@@ -151,7 +151,7 @@ struct bdb_system {
     bool igt_ready = false;                    // a predictor awaits its corrector
     bdb::DevBuf<double> panel64;               // Cholesky workspace
     bool factor_valid = false;
-    alignas(64) unsigned char tc_map[2048];    // CUtensorMaps: TF32 hi / lo panel buffers (x4), FP32 matrix
+    alignas(64) unsigned char tc_map[2048];    // CUtensorMaps: FP16 hi / lo panel buffers (x4), FP32 matrix
     bool tc_map_ok = false;
     bool tc64_ok = false;                      // FP64 tensor-core Cholesky set up
     alignas(64) unsigned char mv_map[384];     // CUtensorMaps for the stored matvec: FP32 matrix, X, F
