@@ -145,12 +145,13 @@ int build_and_factor(bdb_system* s)
 // One refresh (tensor build + factorisation) with the chain reserve c, timed
 // the way every refresh after the first runs: captured into a CUDA graph
 // (node priorities kept) and replayed, the faster of two replays after a
-// warm one. Eagerly, one run, while phases are being profiled (no graphs).
+// warm one. Eagerly, one run, where refreshes run eagerly (refresh graphs
+// switched off, or phases being profiled).
 static int tune_time(bdb_system* s, int c, cudaEvent_t e0, cudaEvent_t e1, float* ms_out)
 {
     s->chain_sms = c;
     *ms_out = 1e30f;
-    if (s->profiling) {
+    if (s->profiling || !s->graph_refresh) {
         BDB_CUDA(cudaEventRecord(e0, s->stream));
         const int rc = build_and_factor(s);
         if (rc) return rc;
