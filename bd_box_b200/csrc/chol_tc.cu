@@ -440,7 +440,6 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
     // launched as a programmatic dependent of the update of this block
     // column: the set-up above overlaps its tail, M is read only after it
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;");
     if (warp == 0) {
         // ---------------------------------------------------- pivot warp
         // tile (0, 0) to Dg; tiles (1, 0) and (1, 1) (nothing updates them
@@ -460,6 +459,10 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1) k_potrf128(T* __restrict__ M
             t2[1] = 2 * fq + 1 <= fr ? (double)b.y : 0.0;
         }
         for (int k = 0; k < NT; ++k) {
+            // the dependent (block row P+1's solve, 4 CTAs) launches for the
+            // last four steps only: launched at the start, its CTAs held 4
+            // SMs in their wait for the whole factorisation
+            if (k == NT - 4) asm volatile("griddepcontrol.launch_dependents;");
             __syncwarp();
             {
                 double lc[8], wc[8];
