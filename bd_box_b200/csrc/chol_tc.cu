@@ -5,8 +5,9 @@
 // M is FP32 (lower triangle: the factor, upper: D, never written here) or
 // FP64 on the FP64 path. Super-panel P covers columns p0 = 128P .. p0+127:
 //   k_potrf128  one CTA factors the 128x128 diagonal block in FP64,
-//               right-looking by 8 columns (each 8x8 pivot block factored by
-//               one thread while the other warps solve and update), and
+//               right-looking by 8 columns (each 8x8 pivot block factored and
+//               inverted by the pivot warp while the other warps solve and
+//               update), and
 //               hands L_PP and the inverses W_kk of its 8x8 diagonal tiles on
 //               to the panel solve;
 //   k_trsm128   the rows below, X L_PP^T = A, by blocked forward substitution
@@ -38,6 +39,13 @@
 // tiles after it. Every mbarrier wait is bounded; a time-out sets
 // ST_TIMEOUT and a shared abort flag that stops all roles, and the CTA frees
 // its tensor memory before returning.
+//
+// Kernels are chained as programmatic dependents (griddepcontrol): each
+// reads its inputs only after griddepcontrol.wait. Where the dependent is a
+// small kernel of the panel chain, it is released early so that its launch
+// overlaps; where it is a full grid (the next bulk update, the side
+// stream's column update), only near the end, since its CTAs would hold the
+// free SMs in their wait for as long as the releasing kernel runs.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
